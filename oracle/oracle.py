@@ -1,0 +1,192 @@
+"""ctypes front-end of the CPU oracles -- TEST INFRASTRUCTURE ONLY.
+
+Two libraries, both built by ``oracle/Makefile``:
+
+* ``_build/libseisoracle.so`` -- the plain-C restatement of the reference FD path
+  (``seis_oracle_body.h``) in float (``prec="f32"``) and double (``prec="f64"``).
+* ``_ref/libseisref.so`` -- the reference's own ``src/util/fd.cpp`` and helpers,
+  compiled in place (present only where the reference sources were available at
+  build time; the built file travels with the repository snapshot).
+
+Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
+import this module.  The product library never calls it.
+
+Array conventions follow the reference (``src/util/memory.h:29-44``): models and
+images ``[nx][nz]`` (z fastest), gathers ``[nx][nt]`` (t fastest), all C-ordered
+numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libseisoracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libseisref.so")
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_P)
+
+
+def _dtype(prec: str):
+    return {"f32": np.float32, "f64": np.float64}[prec]
+
+
+class _Lib:
+    def __init__(self, path: str):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (run make -C oracle)")
+        self.lib = ctypes.CDLL(path)
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        _oracle = _Lib(ORACLE_SO).lib
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        _ref = _Lib(REF_SO).lib
+    return _ref
+
+
+# --------------------------------------------------------------------------
+# restatement (orc_*)
+# --------------------------------------------------------------------------
+def _real(prec):
+    return ctypes.c_float if prec == "f32" else ctypes.c_double
+
+
+def ricker(dt, fr, delay, n, prec="f32", impl="oracle"):
+    if impl == "ref":
+        out = np.zeros(n, np.float32)
+        F = ctypes.c_float
+        ref_lib().ref_ricker(F(dt), F(fr), _I(delay), _I(n), _ptr(out))
+        return out
+    R = _real(prec)
+    out = np.zeros(n, _dtype(prec))
+    getattr(oracle_lib(), f"orc_ricker_{prec}")(R(dt), R(fr), _I(delay), _I(n), _ptr(out))
+    return out
+
+
+def set_abs(nz, nx, pml, prec="f32", impl="oracle"):
+    out = np.zeros((nx + 2 * pml, nz + 2 * pml), _dtype(prec) if impl == "oracle" else np.float32)
+    if impl == "ref":
+        ref_lib().ref_set_abs(_I(nz), _I(nx), _I(pml), _ptr(out))
+    else:
+        getattr(oracle_lib(), f"orc_set_abs_{prec}")(_I(nz), _I(nx), _I(pml), _ptr(out))
+    return out
+
+
+def set_vel(v, pml, prec="f32", impl="oracle"):
+    nx, nz = v.shape
+    dt = _dtype(prec) if impl == "oracle" else np.float32
+    v = np.ascontiguousarray(v, dt)
+    out = np.zeros((nx + 2 * pml, nz + 2 * pml), dt)
+    if impl == "ref":
+        ref_lib().ref_set_vel(_ptr(v), _I(nz), _I(nx), _I(pml), _ptr(out))
+    else:
+        getattr(oracle_lib(), f"orc_set_vel_{prec}")(_ptr(v), _I(nz), _I(nx), _I(pml), _ptr(out))
+    return out
+
+
+def hilbert(x, half=30, prec="f32", impl="oracle"):
+    dt = _dtype(prec) if impl == "oracle" else np.float32
+    x = np.ascontiguousarray(x, dt)
+    out = np.zeros_like(x)
+    if impl == "ref":
+        ref_lib().ref_hilbert(_ptr(x), _ptr(out), _I(x.size), _I(half))
+    else:
+        getattr(oracle_lib(), f"orc_hilbert_{prec}")(_ptr(x), _ptr(out), _I(x.size), _I(half))
+    return out
+
+
+def _common_args(shot, prec):
+    R = _real(prec) if prec else ctypes.c_float
+    s = shot
+    return [R(s.dt), R(s.dx), R(s.dz), _I(s.nt), _I(s.ndel), _I(s.nx), _I(s.nz), _I(s.pml),
+            _I(s.sx), _I(s.sz)]
+
+
+def _prep(shot, prec, impl, *arrays):
+    dt = np.float32 if impl == "ref" else _dtype(prec)
+    gz = np.ascontiguousarray(shot.gz, np.int32)
+    out = [gz] + [np.ascontiguousarray(a, dt) for a in arrays]
+    return dt, out
+
+
+def modeling(shot, wav, vel, prec="f32", impl="oracle"):
+    """Shot gather [nx][nt] of ``modeling`` (src/util/fd.cpp:15-80)."""
+    dt, (gz, wav, vel) = _prep(shot, prec, impl, wav, vel)
+    rec = np.zeros((shot.nx, shot.nt), dt)
+    if impl == "ref":
+        rc = ref_lib().ref_modeling(*_common_args(shot, None), _ptr(gz), _ptr(wav), _ptr(vel), _ptr(rec))
+    else:
+        rc = getattr(oracle_lib(), f"orc_modeling_{prec}")(*_common_args(shot, prec), _ptr(gz),
+                                                           _ptr(wav), _ptr(vel), _ptr(rec))
+    if rc != 0:
+        raise RuntimeError(f"oracle modeling failed ({rc})")
+    return rec
+
+
+def born(shot, wav, vel, dv, prec="f32", impl="oracle"):
+    """Scattered gather [nx][nt] of ``forward`` (src/util/fd.cpp:81-177)."""
+    dt, (gz, wav, vel, dv) = _prep(shot, prec, impl, wav, vel, dv)
+    rec = np.zeros((shot.nx, shot.nt), dt)
+    if impl == "ref":
+        rc = ref_lib().ref_born(*_common_args(shot, None), _ptr(gz), _ptr(wav), _ptr(vel), _ptr(dv),
+                                _ptr(rec))
+    else:
+        rc = getattr(oracle_lib(), f"orc_born_{prec}")(*_common_args(shot, prec), _ptr(gz), _ptr(wav),
+                                                       _ptr(vel), _ptr(dv), _ptr(rec))
+    if rc != 0:
+        raise RuntimeError(f"oracle born failed ({rc})")
+    return rec
+
+
+def rtm(shot, wav, vel, rec, prec="f32", impl="oracle"):
+    """Image [nx][nz] of the reference ``adjoint`` (src/util/fd.cpp:592-719)."""
+    dt, (gz, wav, vel, rec) = _prep(shot, prec, impl, wav, vel, rec)
+    img = np.zeros((shot.nx, shot.nz), dt)
+    if impl == "ref":
+        rc = ref_lib().ref_rtm(*_common_args(shot, None), _ptr(gz), _ptr(wav), _ptr(vel), _ptr(rec),
+                               _ptr(img))
+    else:
+        rc = getattr(oracle_lib(), f"orc_rtm_{prec}")(*_common_args(shot, prec), _ptr(gz), _ptr(wav),
+                                                      _ptr(vel), _ptr(rec), _ptr(img))
+    if rc != 0:
+        raise RuntimeError(f"oracle rtm failed ({rc})")
+    return img
+
+
+def born_adjoint(shot, wav, vel, rec, prec="f64"):
+    """Image [nx][nz] of the exact transpose of ``born`` (the library's own
+    adjoint; the reference has no exact adjoint to compare with)."""
+    dt, (gz, wav, vel, rec) = _prep(shot, prec, "oracle", wav, vel, rec)
+    img = np.zeros((shot.nx, shot.nz), dt)
+    rc = getattr(oracle_lib(), f"orc_born_adjoint_{prec}")(*_common_args(shot, prec), _ptr(gz),
+                                                           _ptr(wav), _ptr(vel), _ptr(rec), _ptr(img))
+    if rc != 0:
+        raise RuntimeError(f"oracle born_adjoint failed ({rc})")
+    return img
+
+
+def ref_set_threads(n: int):
+    ref_lib().ref_set_threads(_I(n))

@@ -1,0 +1,494 @@
+/*
+ * Body of the CPU oracle (TEST INFRASTRUCTURE ONLY), included twice by
+ * seis_oracle.c with REAL = float / double.  See seis_oracle.h.
+ *
+ * Every arithmetic expression keeps the evaluation order of the reference
+ * statement it restates (cited per function); the file is compiled with
+ * -ffp-contract=off so that each + - * / is rounded on its own, as the
+ * reference's x86-64 build does.
+ */
+#define CAT_(a, b) a##_##b
+#define CAT(a, b) CAT_(a, b)
+#define F(name) CAT(name, SFX)
+#define KR(x) ((REAL)(x))
+#define AT(a, ix, iz) (a)[(size_t)(ix) * (size_t)g->NZ + (size_t)(iz)]
+
+typedef struct {
+  int nx, nz, pml, NX, NZ;
+  REAL dt, dx, dz;
+} F(grid_t);
+
+static F(grid_t) F(mkgrid)(REAL dt, REAL dx, REAL dz, int nx, int nz, int pml)
+{
+  F(grid_t) g;
+  g.nx = nx; g.nz = nz; g.pml = pml;
+  g.NX = nx + 2 * pml; g.NZ = nz + 2 * pml;
+  g.dt = dt; g.dx = dx; g.dz = dz;
+  return g;
+}
+
+static REAL *F(zalloc)(size_t n) { return (REAL *)calloc(n ? n : 1, sizeof(REAL)); }
+
+/* rickerWavelet, src/util/wavelet.cpp:7-18.  tmp is formed in double from the
+ * 3.1415926 literal and rounded once; exp is the single-precision overload in
+ * the float build. */
+void F(orc_ricker)(REAL dt, REAL fr, int delay, int n, REAL *out)
+{
+  REAL tmp = (REAL)(3.1415926 * 3.1415926 * (double)fr * (double)fr);
+  for (int i = 0; i < n; i++) {
+    REAL t = (REAL)(i - delay) * KR(1.0) * dt;
+    REAL t2 = t * t;
+    out[i] = (KR(1.0) - KR(2.0) * tmp * t2) * EXPR(-tmp * t2);
+  }
+}
+
+/* setAbs, src/util/InitInversion.cpp:11-40: 1 inside, linear ramp to 0 at the
+ * outer edge; the x ramp covers the full height, the z ramp interior x only. */
+void F(orc_set_abs)(int nz, int nx, int pml, REAL *w)
+{
+  F(grid_t) gg = F(mkgrid)(KR(1), KR(1), KR(1), nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  REAL *ramp = F(zalloc)((size_t)pml);
+  for (int i = 0; i < pml; i++) ramp[i] = KR(1.0) - (REAL)(i + 1) * KR(1.0) / (REAL)pml;
+  for (size_t i = 0; i < (size_t)g->NX * g->NZ; i++) w[i] = KR(1.0);
+  for (int iz = 0; iz < g->NZ; iz++) {
+    for (int ix = 0; ix < pml; ix++) AT(w, ix, iz) = ramp[pml - ix - 1];
+    for (int ix = pml + nx; ix < g->NX; ix++) AT(w, ix, iz) = ramp[ix - pml - nx];
+  }
+  for (int ix = pml; ix < pml + nx; ix++) {
+    for (int iz = 0; iz < pml; iz++) AT(w, ix, iz) = ramp[pml - iz - 1];
+    for (int iz = pml + nz; iz < g->NZ; iz++) AT(w, ix, iz) = ramp[iz - pml - nz];
+  }
+  free(ramp);
+}
+
+/* setVel, src/util/InitInversion.cpp:92-113: the net effect of its two passes
+ * is clamp-to-edge replication of the model into the pad. */
+void F(orc_set_vel)(const REAL *v, int nz, int nx, int pml, REAL *out)
+{
+  F(grid_t) gg = F(mkgrid)(KR(1), KR(1), KR(1), nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  for (int ix = 0; ix < g->NX; ix++) {
+    int jx = ix - pml; jx = jx < 0 ? 0 : (jx >= nx ? nx - 1 : jx);
+    for (int iz = 0; iz < g->NZ; iz++) {
+      int jz = iz - pml; jz = jz < 0 ? 0 : (jz >= nz ? nz - 1 : jz);
+      AT(out, ix, iz) = v[(size_t)jx * nz + jz];
+    }
+  }
+}
+
+/* setDv, src/util/InitInversion.cpp:116-126: zero pad. */
+static void F(pad_zero)(const F(grid_t) *g, const REAL *dv, REAL *out)
+{
+  for (int ix = 0; ix < g->nx; ix++)
+    for (int iz = 0; iz < g->nz; iz++)
+      AT(out, ix + g->pml, iz + g->pml) = dv[(size_t)ix * g->nz + iz];
+}
+
+/* Hilbert<T>::designFilter, src/filter/hilbert.h:59-70.  The taper is formed
+ * in double and rounded to REAL; the tap value is formed in double from the
+ * REAL taper and rounded once. */
+static void F(hilbert_taps)(int half, REAL *h)
+{
+  h[half] = KR(0);
+  for (int i = 1; i <= half; i++) {
+    REAL taper = (REAL)(0.54 + 0.46 * cos(3.1415926 * i / half));
+    h[half + i] = (REAL)((double)(taper * (REAL)(i % 2)) * 2.0 / (3.1415926 * i));
+    h[half - i] = -h[half + i];
+  }
+}
+
+/* Hilbert<T>::apply, src/filter/hilbert.h:42-54: a full convolution cut to the
+ * input length, out[k] = sum_i in[i] h[k-i+half], summed in increasing i.  Taps
+ * that are exactly zero add a signed zero and are skipped. */
+static void F(hilbert_apply)(const REAL *h, int half, const REAL *in, REAL *out, int n)
+{
+  for (int k = 0; k < n; k++) {
+    int i0 = k - half < 0 ? 0 : k - half;
+    int i1 = k + half > n - 1 ? n - 1 : k + half;
+    REAL s = KR(0);
+    for (int i = i0; i <= i1; i++) {
+      REAL hk = h[k - i + half];
+      if (hk != KR(0)) s += in[i] * hk;
+    }
+    out[k] = s;
+  }
+}
+
+void F(orc_hilbert)(const REAL *in, REAL *out, int n, int half)
+{
+  REAL *h = F(zalloc)((size_t)(2 * half + 1));
+  F(hilbert_taps)(half, h);
+  F(hilbert_apply)(h, half, in, out, n);
+  free(h);
+}
+
+/* Per-shot coefficient fields, src/util/fd.cpp:34-40 and :115-116:
+ * vt2 = (v dt)^2, vvzz = vt2/dz^2, vvxx = vt2/dx^2, vel3 = 2/v^3. */
+typedef struct {
+  REAL *vel, *vt2, *vvzz, *vvxx, *vel3, *w, *u31;
+} F(coefs_t);
+
+static void F(coefs_init)(const F(grid_t) *g, const REAL *v, F(coefs_t) *c, int want_vel3)
+{
+  size_t n = (size_t)g->NX * g->NZ;
+  c->vel = F(zalloc)(n); c->vt2 = F(zalloc)(n); c->vvzz = F(zalloc)(n);
+  c->vvxx = F(zalloc)(n); c->w = F(zalloc)(n); c->u31 = F(zalloc)(n);
+  c->vel3 = want_vel3 ? F(zalloc)(n) : NULL;
+  F(orc_set_vel)(v, g->nz, g->nx, g->pml, c->vel);
+  F(orc_set_abs)(g->nz, g->nx, g->pml, c->w);
+  REAL invdx2 = KR(1.0) / (g->dx * g->dx);
+  REAL invdz2 = KR(1.0) / (g->dz * g->dz);
+  for (size_t i = 0; i < n; i++) {
+    REAL t = c->vel[i] * g->dt;
+    c->vt2[i] = t * t;
+    c->vvzz[i] = c->vt2[i] * invdz2;
+    c->vvxx[i] = c->vt2[i] * invdx2;
+    if (want_vel3) c->vel3[i] = KR(2.0) / (c->vel[i] * c->vel[i] * c->vel[i]);
+  }
+}
+
+static void F(coefs_free)(F(coefs_t) *c)
+{
+  free(c->vel); free(c->vt2); free(c->vvzz); free(c->vvxx); free(c->w); free(c->u31);
+  free(c->vel3);
+}
+
+/* Two-way update of the non-frame cells: modeling2D_low on [1,n-2]^2
+ * (src/util/fd.cpp:1226-1241), then modeling2D_high on [4,n-5]^2 (:1242-1271).
+ * nxt = vvzz*uzz + vvxx*uxx + 2 cur - prv. */
+static void F(twoway)(const F(grid_t) *g, const F(coefs_t) *c, const REAL *cur,
+                      const REAL *prv, REAL *nxt)
+{
+  static const REAL a[9] = {KR(-1.0) / KR(560.0), KR(8.0) / KR(315.0), KR(-1.0) / KR(5.0),
+                            KR(8.0) / KR(5.0),    KR(-205.0) / KR(72.0), KR(8.0) / KR(5.0),
+                            KR(-1.0) / KR(5.0),   KR(8.0) / KR(315.0), KR(-1.0) / KR(560.0)};
+  const int NX = g->NX, NZ = g->NZ;
+  for (int ix = 1; ix <= NX - 2; ix++)
+    for (int iz = 1; iz <= NZ - 2; iz++) {
+      REAL u = AT(cur, ix, iz);
+      REAL uzz, uxx;
+      int high = ix >= 4 && ix <= NX - 5 && iz >= 4 && iz <= NZ - 5;
+      if (high) {
+        uzz = AT(cur, ix, iz - 4) * a[0];
+        uxx = AT(cur, ix - 4, iz) * a[0];
+        for (int k = 1; k < 9; k++) {
+          uzz = uzz + AT(cur, ix, iz - 4 + k) * a[k];
+          uxx = uxx + AT(cur, ix - 4 + k, iz) * a[k];
+        }
+      } else {
+        uzz = AT(cur, ix, iz - 1) + AT(cur, ix, iz + 1) - KR(2) * u;
+        uxx = AT(cur, ix + 1, iz) + AT(cur, ix - 1, iz) - KR(2) * u;
+      }
+      AT(nxt, ix, iz) = AT(c->vvzz, ix, iz) * uzz + AT(c->vvxx, ix, iz) * uxx + KR(2) * u -
+                        AT(prv, ix, iz);
+    }
+}
+
+/* 1-D second difference along an edge: (v v k)((a+b) - 2c). */
+static REAL F(d2)(REAL v, REAL k, REAL a, REAL b, REAL c) { return v * v * k * (a + b - KR(2) * c); }
+
+/* Outer frame of the two-way field, processBoundary part (i),
+ * src/util/fd.cpp:1057-1091: a 1-D update along each edge (the right column
+ * uses the x coefficient, :1066), the four corners as 2 cur - prv, then a
+ * linearly extrapolated normal term, z first (:1072-1081) then x (:1082-1091). */
+static void F(frame)(const F(grid_t) *g, const F(coefs_t) *c, const REAL *cur,
+                     const REAL *prv, REAL *u3)
+{
+  const int NX = g->NX, NZ = g->NZ;
+  const REAL *vel = c->vel;
+  REAL dt2 = g->dt * g->dt;
+  REAL kx = (KR(1.0) / g->dx) * (KR(1.0) / g->dx) * dt2;
+  REAL kz = (KR(1.0) / g->dz) * (KR(1.0) / g->dz) * dt2;
+  for (int ix = 1; ix <= NX - 2; ix++) {
+    int e[2] = {0, NZ - 1};
+    for (int s = 0; s < 2; s++) {
+      int iz = e[s];
+      AT(u3, ix, iz) = F(d2)(AT(vel, ix, iz), kx, AT(cur, ix + 1, iz), AT(cur, ix - 1, iz),
+                             AT(cur, ix, iz)) + KR(2) * AT(cur, ix, iz) - AT(prv, ix, iz);
+    }
+  }
+  for (int iz = 1; iz <= NZ - 2; iz++) {
+    AT(u3, 0, iz) = F(d2)(AT(vel, 0, iz), kz, AT(cur, 0, iz + 1), AT(cur, 0, iz - 1),
+                          AT(cur, 0, iz)) + KR(2) * AT(cur, 0, iz) - AT(prv, 0, iz);
+    AT(u3, NX - 1, iz) = F(d2)(AT(vel, NX - 1, iz), kx, AT(cur, NX - 1, iz + 1),
+                               AT(cur, NX - 1, iz - 1), AT(cur, NX - 1, iz)) +
+                         KR(2) * AT(cur, NX - 1, iz) - AT(prv, NX - 1, iz);
+  }
+  {
+    int cx[4] = {0, 0, NX - 1, NX - 1}, cz[4] = {0, NZ - 1, 0, NZ - 1};
+    for (int k = 0; k < 4; k++)
+      AT(u3, cx[k], cz[k]) = KR(2) * AT(cur, cx[k], cz[k]) - AT(prv, cx[k], cz[k]);
+  }
+  for (int ix = 0; ix < NX; ix++) {
+    REAL y1 = F(d2)(AT(vel, ix, 1), kz, AT(cur, ix, 2), AT(cur, ix, 0), AT(cur, ix, 1));
+    REAL y2 = F(d2)(AT(vel, ix, 2), kz, AT(cur, ix, 3), AT(cur, ix, 1), AT(cur, ix, 2));
+    AT(u3, ix, 0) += y1 * KR(2) - y2;
+    y1 = F(d2)(AT(vel, ix, NZ - 2), kz, AT(cur, ix, NZ - 3), AT(cur, ix, NZ - 1), AT(cur, ix, NZ - 2));
+    y2 = F(d2)(AT(vel, ix, NZ - 3), kz, AT(cur, ix, NZ - 4), AT(cur, ix, NZ - 2), AT(cur, ix, NZ - 3));
+    AT(u3, ix, NZ - 1) += y1 * KR(2) - y2;
+  }
+  for (int iz = 0; iz < NZ; iz++) {
+    REAL y1 = F(d2)(AT(vel, 1, iz), kx, AT(cur, 2, iz), AT(cur, 0, iz), AT(cur, 1, iz));
+    REAL y2 = F(d2)(AT(vel, 2, iz), kx, AT(cur, 3, iz), AT(cur, 1, iz), AT(cur, 2, iz));
+    AT(u3, 0, iz) += y1 * KR(2) - y2;
+    y1 = F(d2)(AT(vel, NX - 2, iz), kx, AT(cur, NX - 3, iz), AT(cur, NX - 1, iz), AT(cur, NX - 2, iz));
+    y2 = F(d2)(AT(vel, NX - 3, iz), kx, AT(cur, NX - 4, iz), AT(cur, NX - 2, iz), AT(cur, NX - 3, iz));
+    AT(u3, NX - 1, iz) += y1 * KR(2) - y2;
+  }
+}
+
+/* One-way (paraxial) update of a strip cell, src/util/fd.cpp:1098-1104 and the
+ * three mirrored strips.  i = inner neighbour along the normal, t+/t- = the
+ * tangential neighbours of the inner cell (u3) and of the cell itself (prv);
+ * a1 = 1/(2 h_n dt), a2 = 1/(2 dt^2 v), a3 = v/(4 h_t^2). */
+static REAL F(oneway)(REAL a1, REAL a2, REAL a3, REAL u3i, REAL u3tp, REAL u3tm, REAL cK,
+                      REAL ci, REAL pK, REAL pi, REAL ptp, REAL ptm)
+{
+  REAL tmp = -a1 * u3i - a1 * (pK - pi) + a2 * (pK - KR(2) * cK + u3i + pi - KR(2) * ci) -
+             a3 * (u3tp + u3tm - KR(2) * u3i + ptp + ptm - KR(2) * pK);
+  return -tmp / (a1 + a2);
+}
+
+/* Diagonal corner cell, src/util/fd.cpp:1146-1178.  ax3 = sqrt(2)/v/dt is
+ * single precision except in the upper-left corner, where the reference writes
+ * sqrt(2) with an int argument and so forms ax3 in double (:1176). */
+static REAL F(corner)(REAL ax1, REAL ax2, REAL ax3, REAL u3z, REAL u3x, REAL cK)
+{
+  REAL tmp = -ax1 * u3z - ax2 * u3x + ax3 * (-cK);
+  return -tmp / (ax1 + ax2 + ax3);
+}
+
+/* processBoundary part (ii), src/util/fd.cpp:1092-1179: one-way field u31 on
+ * every ring IK = 1..pml; reads the two-way u3 (frame included), cur, prv. */
+static void F(rings)(const F(grid_t) *g, const F(coefs_t) *c, const REAL *u3,
+                     const REAL *cur, const REAL *prv, REAL *u31)
+{
+  const int nx = g->nx, nz = g->nz, pml = g->pml;
+  const REAL dt = g->dt, dx = g->dx, dz = g->dz;
+  const REAL *vel = c->vel;
+  for (int IK = 1; IK <= pml; IK++) {
+    int b1 = pml + 1 - IK, b2x = pml + nx + IK - 2, b2z = pml + nz + IK - 2;
+    /* up (inner +z) and down (inner -z) */
+    for (int s = 0; s < 2; s++) {
+      int K = s == 0 ? pml - IK : nz + IK + pml - 1;
+      int I = s == 0 ? K + 1 : K - 1;
+      for (int ix = b1; ix <= b2x; ix++) {
+        REAL v = AT(vel, ix, K);
+        REAL a1 = KR(1.0) / dz / KR(2.0) / dt;
+        REAL a2 = KR(1.0) / KR(2.0) / dt / dt / v;
+        REAL a3 = v / KR(4.0) / dx / dx;
+        AT(u31, ix, K) = F(oneway)(a1, a2, a3, AT(u3, ix, I), AT(u3, ix + 1, I), AT(u3, ix - 1, I),
+                                   AT(cur, ix, K), AT(cur, ix, I), AT(prv, ix, K), AT(prv, ix, I),
+                                   AT(prv, ix + 1, K), AT(prv, ix - 1, K));
+      }
+    }
+    /* right (inner -x) and left (inner +x) */
+    for (int s = 0; s < 2; s++) {
+      int K = s == 0 ? nx + IK + pml - 1 : pml - IK;
+      int I = s == 0 ? K - 1 : K + 1;
+      for (int iz = b1; iz <= b2z; iz++) {
+        REAL v = AT(vel, K, iz);
+        REAL a1 = KR(1.0) / dx / KR(2.0) / dt;
+        REAL a2 = KR(1.0) / KR(2.0) / dt / dt / v;
+        REAL a3 = v / KR(4.0) / dz / dz;
+        AT(u31, K, iz) = F(oneway)(a1, a2, a3, AT(u3, I, iz), AT(u3, I, iz + 1), AT(u3, I, iz - 1),
+                                   AT(cur, K, iz), AT(cur, I, iz), AT(prv, K, iz), AT(prv, I, iz),
+                                   AT(prv, K, iz + 1), AT(prv, K, iz - 1));
+      }
+    }
+    /* corners: (x, z, inner dx, inner dz) */
+    {
+      int xr = nx + pml + IK - 1, xl = pml - IK, zd = nz + pml + IK - 1, zu = pml - IK;
+      int cxs[4] = {xr, xl, xr, xl}, czs[4] = {zd, zd, zu, zu};
+      int dxs[4] = {-1, +1, -1, +1}, dzs[4] = {-1, -1, +1, +1};
+      REAL ax1 = KR(1.0) / dz, ax2 = KR(1.0) / dx;
+      for (int k = 0; k < 4; k++) {
+        int x = cxs[k], z = czs[k];
+        REAL v = AT(vel, x, z);
+        REAL ax3 = k == 3 ? (REAL)(sqrt(2.0) / (double)v / (double)dt)
+                          : SQRTR(KR(2.0)) / v / dt;
+        AT(u31, x, z) = F(corner)(ax1, ax2, ax3, AT(u3, x, z + dzs[k]), AT(u3, x + dxs[k], z),
+                                  AT(cur, x, z));
+      }
+    }
+  }
+}
+
+/* Hybrid absorbing boundary applied to a freshly stepped two-way field:
+ * processBoundary (src/util/fd.cpp:1053-1180) then the blend loop
+ * u = u w + u31 (1 - w) (:55-56). */
+static void F(absorb)(const F(grid_t) *g, const F(coefs_t) *c, REAL *u3, const REAL *cur,
+                      const REAL *prv)
+{
+  F(frame)(g, c, cur, prv, u3);
+  F(rings)(g, c, u3, cur, prv, c->u31);
+  size_t n = (size_t)g->NX * g->NZ;
+  for (size_t i = 0; i < n; i++) u3[i] = u3[i] * c->w[i] + c->u31[i] * (KR(1.0) - c->w[i]);
+}
+
+/* modeling, src/util/fd.cpp:15-80.  rec [nx][nt]. */
+int F(orc_modeling)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml,
+                    int sx, int sz, const int *gz, const REAL *wav, const REAL *vel, REAL *rec)
+{
+  F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  F(coefs_t) c;
+  F(coefs_init)(g, vel, &c, 0);
+  size_t n = (size_t)g->NX * g->NZ;
+  REAL *u0 = F(zalloc)(n), *u1 = F(zalloc)(n), *u2 = F(zalloc)(n);
+  int sxp = sx + pml, szp = sz + pml, NT = nt + ndel;
+  for (int it = 0; it < NT; it++) {
+    F(twoway)(g, &c, u1, u0, u2);
+    if (it >= 1) AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+    F(absorb)(g, &c, u2, u1, u0);
+    if (it >= ndel)
+      for (int ix = 0; ix < nx; ix++) rec[(size_t)ix * nt + (it - ndel)] = AT(u2, ix + pml, gz[ix] + pml);
+    REAL *t = u0; u0 = u1; u1 = u2; u2 = t;
+  }
+  free(u0); free(u1); free(u2);
+  F(coefs_free)(&c);
+  return 0;
+}
+
+/* forward (Born), src/util/fd.cpp:81-177.  Scattering source
+ * vt2 lap vel3 dv with lap = (u2 + u0 - 2 u1)/dt^2 of the blended background. */
+int F(orc_born)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml, int sx,
+                int sz, const int *gz, const REAL *wav, const REAL *vel, const REAL *dv, REAL *rec)
+{
+  F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  F(coefs_t) c;
+  F(coefs_init)(g, vel, &c, 1);
+  size_t n = (size_t)g->NX * g->NZ;
+  REAL *dvp = F(zalloc)(n);
+  F(pad_zero)(g, dv, dvp);
+  REAL *u0 = F(zalloc)(n), *u1 = F(zalloc)(n), *u2 = F(zalloc)(n);
+  REAL *b0 = F(zalloc)(n), *b1 = F(zalloc)(n), *b2 = F(zalloc)(n);
+  REAL idt2 = KR(1.0) / dt / dt;
+  int sxp = sx + pml, szp = sz + pml, NT = nt + ndel;
+  for (int it = 0; it < NT; it++) {
+    F(twoway)(g, &c, u1, u0, u2);
+    if (it >= 1) AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+    F(absorb)(g, &c, u2, u1, u0);
+    F(twoway)(g, &c, b1, b0, b2);
+    for (size_t i = 0; i < n; i++) {
+      REAL lap = (u2[i] + u0[i] - KR(2) * u1[i]) * idt2;
+      b2[i] += c.vt2[i] * lap * c.vel3[i] * dvp[i];
+    }
+    F(absorb)(g, &c, b2, b1, b0);
+    if (it >= ndel)
+      for (int ix = 0; ix < nx; ix++) rec[(size_t)ix * nt + (it - ndel)] = AT(b2, ix + pml, gz[ix] + pml);
+    REAL *t = u0; u0 = u1; u1 = u2; u2 = t;
+    t = b0; b0 = b1; b1 = b2; b2 = t;
+  }
+  free(u0); free(u1); free(u2); free(b0); free(b1); free(b2); free(dvp);
+  F(coefs_free)(&c);
+  return 0;
+}
+
+/* SaveAtBoundary, src/util/fd.cpp:1181-1225: the 4 outermost interior rows
+ * and columns of u, kept per time sample.  Storage here is time-major
+ * [it][strip] (the reference keeps time fastest; the values are the same). */
+#define ORC_LAYERS 4
+static size_t F(strip_len)(const F(grid_t) *g) { return (size_t)ORC_LAYERS * 2 * (g->nx + g->nz); }
+
+static void F(strips)(const F(grid_t) *g, REAL *u, REAL *store, int save)
+{
+  const int nx = g->nx, nz = g->nz, pml = g->pml;
+  size_t k = 0;
+#define ORC_MOVE(ix, iz)                                  \
+  do {                                                    \
+    if (save) store[k] = AT(u, (ix), (iz));               \
+    else AT(u, (ix), (iz)) = store[k];                    \
+    k++;                                                  \
+  } while (0)
+  for (int ix = pml; ix < nx + pml; ix++)
+    for (int il = 0; il < ORC_LAYERS; il++) {
+      ORC_MOVE(ix, pml + il);
+      ORC_MOVE(ix, nz + pml - 1 - il);
+    }
+  for (int il = 0; il < ORC_LAYERS; il++)
+    for (int iz = pml; iz < nz + pml; iz++) {
+      ORC_MOVE(pml + il, iz);
+      ORC_MOVE(nx + pml - 1 - il, iz);
+    }
+#undef ORC_MOVE
+}
+
+/* FaQi, src/util/fd.cpp:1272-1298: out += 0.5 (U R - H[U] H[R]) on interior
+ * columns, H = 61-tap Hilbert FIR along z applied to the whole padded column. */
+static void F(faqi)(const F(grid_t) *g, const REAL *h, const REAL *U, const REAL *R, REAL *out,
+                    REAL *uh, REAL *rh)
+{
+  const int pml = g->pml, NZ = g->NZ;
+  REAL scal = KR(2.0) / KR(4.0);
+  for (int ix = pml; ix < g->NX - pml; ix++) {
+    F(hilbert_apply)(h, 30, &AT(U, ix, 0), uh, NZ);
+    F(hilbert_apply)(h, 30, &AT(R, ix, 0), rh, NZ);
+    for (int iz = pml; iz < NZ - pml; iz++)
+      AT(out, ix, iz) += scal * (AT(U, ix, iz) * AT(R, ix, iz) - uh[iz] * rh[iz]);
+  }
+}
+
+/* adjoint (RTM), src/util/fd.cpp:592-719: forward source pass saving the
+ * boundary strips; reverse pass rebuilding the source field from the strips
+ * (starting from zero fields, subtracting the source), back-propagating the
+ * receiver data injected as rec*vt2, and imaging with lap*vel3*R plus FaQi.
+ * img [nx][nz]. */
+int F(orc_rtm)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml, int sx,
+               int sz, const int *gz, const REAL *wav, const REAL *vel, const REAL *rec, REAL *img)
+{
+  F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  F(coefs_t) c;
+  F(coefs_init)(g, vel, &c, 1);
+  size_t n = (size_t)g->NX * g->NZ, sl = F(strip_len)(g);
+  REAL *u0 = F(zalloc)(n), *u1 = F(zalloc)(n), *u2 = F(zalloc)(n);
+  REAL *b0 = F(zalloc)(n), *b1 = F(zalloc)(n), *b2 = F(zalloc)(n);
+  REAL *lap = F(zalloc)(n), *imgp = F(zalloc)(n);
+  REAL *store = F(zalloc)(sl * (size_t)nt);
+  REAL *h = F(zalloc)(61), *uh = F(zalloc)((size_t)g->NZ), *rh = F(zalloc)((size_t)g->NZ);
+  F(hilbert_taps)(30, h);
+  REAL idt2 = KR(1.0) / dt / dt;
+  int sxp = sx + pml, szp = sz + pml, NT = nt + ndel;
+  for (int it = 0; it < NT; it++) {
+    F(twoway)(g, &c, u1, u0, u2);
+    if (it >= 1) AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+    F(absorb)(g, &c, u2, u1, u0);
+    if (it >= ndel) F(strips)(g, u2, store + sl * (size_t)(it - ndel), 1);
+    REAL *t = u0; u0 = u1; u1 = u2; u2 = t;
+  }
+  memset(u0, 0, n * sizeof(REAL)); memset(u1, 0, n * sizeof(REAL)); memset(u2, 0, n * sizeof(REAL));
+  for (int it = NT - 1; it >= ndel; it--) {
+    if (it - 1 > 0) AT(u2, sxp, szp) -= AT(c.vt2, sxp, szp) * wav[it - 1];
+    int itp = it - ndel;
+    F(strips)(g, u1, store + sl * (size_t)itp, 0);
+    F(twoway)(g, &c, u1, u2, u0);
+    F(absorb)(g, &c, u0, u1, u2);
+    for (size_t i = 0; i < n; i++) lap[i] = (u2[i] + u0[i] - KR(2) * u1[i]) * idt2;
+    F(twoway)(g, &c, b1, b2, b0);
+    for (int ix = 0; ix < nx; ix++) {
+      int iz = gz[ix] + pml;
+      AT(b0, ix + pml, iz) += rec[(size_t)ix * nt + itp] * AT(c.vt2, ix + pml, iz);
+    }
+    F(absorb)(g, &c, b0, b1, b2);
+    for (size_t i = 0; i < n; i++) imgp[i] += lap[i] * c.vel3[i] * b0[i];
+    for (size_t i = 0; i < n; i++) lap[i] = lap[i] * c.vel3[i];
+    F(faqi)(g, h, lap, b0, imgp, uh, rh);
+    REAL *t = u2; u2 = u1; u1 = u0; u0 = t;
+    t = b2; b2 = b1; b1 = b0; b0 = t;
+  }
+  for (int ix = 0; ix < nx; ix++)
+    for (int iz = 0; iz < nz; iz++) img[(size_t)ix * nz + iz] = AT(imgp, ix + pml, iz + pml);
+  free(u0); free(u1); free(u2); free(b0); free(b1); free(b2); free(lap); free(imgp);
+  free(store); free(h); free(uh); free(rh);
+  F(coefs_free)(&c);
+  return 0;
+}
+
+#undef AT
+#undef KR
+#undef F
+#undef CAT
+#undef CAT_

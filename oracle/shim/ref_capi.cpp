@@ -1,0 +1,150 @@
+/*
+ * Flat-array C entry points around the reference's FD functions, so that
+ * Python tests and the CPU baseline can call the reference unmodified
+ * (test infrastructure only; compiled into oracle/_ref/libseisref.so).
+ *
+ * Arrays follow the reference layout: model/image [nx][nz] with z fastest
+ * (MyAlloc<float>::alc(nz,nx), src/util/memory.h:29-44), gathers [nx][nt] with
+ * t fastest.  Every call copies into MyAlloc arrays, calls the reference, and
+ * copies the result out.  Return value: 0 ok, -1 if the reference threw.
+ */
+#include "ref_shim.h"
+#include <cstring>
+#include <stdexcept>
+#include <streambuf>
+#include "memory.h"
+#include "fd.h"
+#include "wavelet.h"
+#include "InitInversion.h"
+#include <math.h> /* hilbert.h uses cos() without including it */
+#include "../filter/hilbert.h"
+
+extern int OMP_CORE;
+
+namespace {
+struct NullBuf : std::streambuf {
+  int overflow(int c) override { return c; }
+};
+NullBuf g_null;
+
+/* The reference prints progress lines to std::cout (fd.cpp:46); keep stdout
+ * clean for the JSON line of the benchmark unless the caller asks for them. */
+struct QuietCout {
+  std::streambuf *old;
+  explicit QuietCout(int verbose) : old(nullptr) {
+    if (!verbose) old = std::cout.rdbuf(&g_null);
+  }
+  ~QuietCout() { if (old) std::cout.rdbuf(old); }
+};
+
+float **to2d(const float *src, int n1, int n2) {
+  float **a = MyAlloc<float>::alc(n1, n2);
+  std::memcpy(a[0], src, sizeof(float) * (size_t)n1 * n2);
+  return a;
+}
+void from2d(float *dst, float **a, int n1, int n2) {
+  std::memcpy(dst, a[0], sizeof(float) * (size_t)n1 * n2);
+}
+int g_verbose = 0;
+}  // namespace
+
+extern "C" {
+
+void ref_set_threads(int n) { OMP_CORE = n > 0 ? n : 1; }
+void ref_set_verbose(int v) { g_verbose = v; }
+
+/* rickerWavelet (src/util/wavelet.cpp:7-18) */
+int ref_ricker(float dt, float fr, int delay, int NT, float *out) {
+  float *w = rickerWavelet(dt, fr, delay, NT);
+  std::memcpy(out, w, sizeof(float) * NT);
+  MyAlloc<float>::free(w);
+  return 0;
+}
+
+/* setAbs blend weights, padded [nxpml][nzpml] (src/util/InitInversion.cpp:11-40) */
+int ref_set_abs(int nz, int nx, int pml, float *out) {
+  float **w = setAbs(nz, nx, pml);
+  from2d(out, w, nz + 2 * pml, nx + 2 * pml);
+  MyAlloc<float>::free(w);
+  return 0;
+}
+
+/* setVel edge-replicating pad (src/util/InitInversion.cpp:92-113) */
+int ref_set_vel(const float *v, int nz, int nx, int pml, float *out) {
+  float **a = to2d(v, nz, nx);
+  float **p = setVel(a, nz, nx, pml);
+  from2d(out, p, nz + 2 * pml, nx + 2 * pml);
+  MyAlloc<float>::free(a);
+  MyAlloc<float>::free(p);
+  return 0;
+}
+
+/* Hilbert<float>::apply (src/filter/hilbert.h:42-54) */
+int ref_hilbert(const float *in, float *out, int n, int half) {
+  Hilbert<float> h(half);
+  h.apply(const_cast<float *>(in), out, n);
+  return 0;
+}
+
+/* modeling (src/util/fd.cpp:15-80): rec_out [nx][nt] */
+int ref_modeling(float dt, float dx, float dz, int nt, int ndel, int nx, int nz,
+                 int pml, int sx, int sz, const int *gz, const float *wav,
+                 const float *vel, float *rec_out) {
+  QuietCout q(g_verbose);
+  try {
+    float **v = to2d(vel, nz, nx);
+    float **rec = modeling(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz,
+                           const_cast<int *>(gz), const_cast<float *>(wav), v);
+    from2d(rec_out, rec, nt, nx);
+    MyAlloc<float>::free(rec);
+    MyAlloc<float>::free(v);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return -1;
+  }
+  return 0;
+}
+
+/* forward, Born modeling (src/util/fd.cpp:81-177): rec_out [nx][nt] */
+int ref_born(float dt, float dx, float dz, int nt, int ndel, int nx, int nz,
+             int pml, int sx, int sz, const int *gz, const float *wav,
+             const float *vel, const float *dv, float *rec_out) {
+  QuietCout q(g_verbose);
+  try {
+    float **v = to2d(vel, nz, nx);
+    float **d = to2d(dv, nz, nx);
+    float **rec = forward(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz,
+                          const_cast<int *>(gz), const_cast<float *>(wav), v, d);
+    from2d(rec_out, rec, nt, nx);
+    MyAlloc<float>::free(rec);
+    MyAlloc<float>::free(v);
+    MyAlloc<float>::free(d);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return -1;
+  }
+  return 0;
+}
+
+/* adjoint, RTM (src/util/fd.cpp:592-719): img_out [nx][nz] */
+int ref_rtm(float dt, float dx, float dz, int nt, int ndel, int nx, int nz,
+            int pml, int sx, int sz, const int *gz, const float *wav,
+            const float *vel, const float *rec, float *img_out) {
+  QuietCout q(g_verbose);
+  try {
+    float **v = to2d(vel, nz, nx);
+    float **r = to2d(rec, nt, nx);
+    float **img = adjoint(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz,
+                          const_cast<int *>(gz), const_cast<float *>(wav), v, r);
+    from2d(img_out, img, nz, nx);
+    MyAlloc<float>::free(img);
+    MyAlloc<float>::free(v);
+    MyAlloc<float>::free(r);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return -1;
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,70 @@
+"""Python mirror of the reference propagator call surface (src/util/fd.h:3-5).
+
+``modeling``, ``forward`` and ``adjoint`` take the reference's arguments in the
+reference's order and return numpy arrays in the reference's layout
+(gathers ``[nx][nt]``, images ``[nx][nz]``).  Each call runs on the GPU through
+the C ABI; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from ._lib import Context, Shot, ptr
+
+_default_ctx = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def _shot(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz) -> Shot:
+    return Shot(nx=nx, nz=nz, pml=pml, nt=nt, ndel=ndel, sx=sx, sz=sz, dt=dt, dx=dx, dz=dz, gz=gz)
+
+
+def _f32(a, shape):
+    a = np.ascontiguousarray(a, np.float32)
+    if a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+def modeling(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, ctx: Context = None):
+    """Shot gather ``rec[nx][nt]`` (reference ``modeling``, src/util/fd.cpp:15-80)."""
+    ctx = ctx or default_context()
+    s = _shot(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz)
+    wav = _f32(wav, (s.NT,))
+    vel = _f32(vel, (nx, nz))
+    rec = np.zeros((nx, nt), np.float32)
+    d = s.to_c()
+    ctx.check(ctx.L.seis_fd_modeling(ctx.h, d, ptr(wav), ptr(vel), ptr(rec)))
+    return rec
+
+
+def forward(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, dv, ctx: Context = None):
+    """Born gather ``rec[nx][nt]`` (reference ``forward``, src/util/fd.cpp:81-177)."""
+    ctx = ctx or default_context()
+    s = _shot(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz)
+    wav = _f32(wav, (s.NT,))
+    vel = _f32(vel, (nx, nz))
+    dv = _f32(dv, (nx, nz))
+    rec = np.zeros((nx, nt), np.float32)
+    d = s.to_c()
+    ctx.check(ctx.L.seis_fd_born(ctx.h, d, ptr(wav), ptr(vel), ptr(dv), ptr(rec)))
+    return rec
+
+
+def adjoint(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, rec, ctx: Context = None):
+    """RTM image ``img[nx][nz]`` (reference ``adjoint``, src/util/fd.cpp:592-719)."""
+    ctx = ctx or default_context()
+    s = _shot(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz)
+    wav = _f32(wav, (s.NT,))
+    vel = _f32(vel, (nx, nz))
+    rec = _f32(rec, (nx, nt))
+    img = np.zeros((nx, nz), np.float32)
+    d = s.to_c()
+    ctx.check(ctx.L.seis_fd_rtm(ctx.h, d, ptr(wav), ptr(vel), ptr(rec), ptr(img)))
+    return img
