@@ -69,6 +69,9 @@ const char *seis_fd_last_error(const seis_fd_ctx *ctx);
 /* Number of kernel launches this context has issued since creation
  * (graph-replayed launches included). */
 int64_t seis_fd_launch_count(const seis_fd_ctx *ctx);
+/* The cudaStream_t every call of this context is ordered on, so that callers
+ * can order (or time) their own work around it. */
+void *seis_fd_stream(const seis_fd_ctx *ctx);
 
 /* ------------------------------------------------------ host-only helpers */
 /* rickerWavelet (src/util/wavelet.cpp:7-18): out[n], (1-2 tmp t^2) exp(-tmp t^2)
@@ -94,6 +97,72 @@ int seis_fd_born(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wa
  * h_img[nx][nz] = image. */
 int seis_fd_rtm(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
                 const float *h_vel, const float *h_rec, float *h_img);
+
+/* ---------------------------------------------------------- shot batches */
+/* A plan is a batch of shots resident on the device.  It replaces the
+ * reference's MPI shot farm (masterRun + worker loops,
+ * src/lsrtm/inversion.cpp:141-551, :753-807): every shot of the batch
+ * advances in the same launches, one per time step.  All shots of a plan share
+ * nt, ndel and dt; nx, nz, pml, dx, dz, sources and receivers may differ.
+ * The first seis_fd_plan_run captures the time loop into a CUDA graph; later
+ * runs replay it.  Inputs persist across runs until overwritten. */
+#define SEIS_OP_MODELING 0 /* modeling (fd.cpp:15-80)                      */
+#define SEIS_OP_BORN 1     /* forward, Born (fd.cpp:81-177)                 */
+#define SEIS_OP_RTM 2      /* adjoint, reference RTM (fd.cpp:592-719)       */
+
+#define SEIS_IN_VEL 0      /* [nx][nz] velocity of the shot's model         */
+#define SEIS_IN_DV 1       /* [nx][nz] velocity perturbation (SEIS_OP_BORN) */
+#define SEIS_IN_WAVELET 2  /* [nt+ndel] source wavelet                      */
+#define SEIS_IN_GATHER 3   /* [nx][nt] receiver data (SEIS_OP_RTM)          */
+#define SEIS_OUT_GATHER 0  /* [nx][nt] recorded gather                      */
+#define SEIS_OUT_IMAGE 1   /* [nx][nz] image                                */
+
+int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *shots,
+                        seis_fd_plan **out);
+int seis_fd_plan_destroy(seis_fd_plan *plan);
+/* Copy one input of one shot from host memory (pinned memory makes it
+ * asynchronous on the context stream). */
+int seis_fd_plan_set(seis_fd_plan *plan, int shot, int what, const float *h_src);
+/* Same, from device memory of the context's device. */
+int seis_fd_plan_set_device(seis_fd_plan *plan, int shot, int what, const float *d_src);
+/* Enqueue the operator over every shot on the context stream. */
+int seis_fd_plan_run(seis_fd_plan *plan);
+/* Copy one output of one shot to host memory; synchronises the stream. */
+int seis_fd_plan_get(seis_fd_plan *plan, int shot, int what, float *h_dst);
+/* Wait for the plan's enqueued work. */
+int seis_fd_plan_sync(seis_fd_plan *plan);
+/* Padded cell-updates of one run (cells x steps x propagated fields). */
+int64_t seis_fd_plan_cell_updates(const seis_fd_plan *plan);
+/* Kernel launches of one run. */
+int64_t seis_fd_plan_launches_per_run(const seis_fd_plan *plan);
+
+/* Arithmetic flavour of a plan's propagation kernels.  exact = 1 (default):
+ * every operation rounds on its own in the reference's order, so results equal
+ * the reference's bit for bit.  exact = 0: multiply-add contraction and
+ * approximate division; results agree with the reference to FP32 rounding
+ * level (relative L2 well below 1e-5) and the kernels issue fewer
+ * instructions. */
+int seis_fd_plan_set_exact(seis_fd_plan *plan, int exact);
+/* Kernel timing: run `steps` time steps of the plan's propagation kernels
+ * eagerly (outside the graph) with CUDA events around each launch on its own
+ * stream, on the plan's current fields.  The interior-tile kernel and the
+ * pad-tile kernel of a step run concurrently.  ms[0] = mean interior-kernel
+ * duration, ms[1] = mean pad-kernel duration, ms[2] = mean step.  bytes[0] =
+ * algorithmic bytes one interior launch moves (16 per field-update: read prev,
+ * cur, velocity; write next), bytes[1] = same for the pad launch.  The plan's
+ * fields are clobbered; the next run starts from its cleared state. */
+int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double *bytes);
+
+/* Batched forms of the single-shot calls: h_*[i] are the arrays of shot i. */
+int seis_fd_modeling_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
+                           const float *const *h_wav, const float *const *h_vel,
+                           float *const *h_rec);
+int seis_fd_born_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
+                       const float *const *h_wav, const float *const *h_vel,
+                       const float *const *h_dv, float *const *h_rec);
+int seis_fd_rtm_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
+                      const float *const *h_wav, const float *const *h_vel,
+                      const float *const *h_rec, float *const *h_img);
 
 #ifdef __cplusplus
 }

@@ -84,9 +84,29 @@ def lib():
         L.seis_fd_last_error.restype = ctypes.c_char_p
         L.seis_fd_launch_count.argtypes = [P]
         L.seis_fd_launch_count.restype = ctypes.c_int64
+        L.seis_fd_stream.argtypes = [P]
+        L.seis_fd_stream.restype = P
         L.seis_fd_ricker.argtypes = [ctypes.c_float, ctypes.c_float, I, I, P]
         L.seis_fd_validate_shot.argtypes = [SD, ctypes.c_char_p, ctypes.c_size_t]
         L.seis_fd_modeling.argtypes = [P, SD, P, P, P]
+        L.seis_fd_plan_create.argtypes = [P, I, I, SD, ctypes.POINTER(P)]
+        L.seis_fd_plan_destroy.argtypes = [P]
+        L.seis_fd_plan_set.argtypes = [P, I, I, P]
+        L.seis_fd_plan_set_device.argtypes = [P, I, I, P]
+        L.seis_fd_plan_run.argtypes = [P]
+        L.seis_fd_plan_get.argtypes = [P, I, I, P]
+        L.seis_fd_plan_sync.argtypes = [P]
+        L.seis_fd_plan_cell_updates.argtypes = [P]
+        L.seis_fd_plan_cell_updates.restype = ctypes.c_int64
+        L.seis_fd_plan_launches_per_run.argtypes = [P]
+        L.seis_fd_plan_launches_per_run.restype = ctypes.c_int64
+        L.seis_fd_plan_set_exact.argtypes = [P, I]
+        L.seis_fd_plan_time_kernels.argtypes = [P, I, ctypes.POINTER(ctypes.c_double),
+                                                ctypes.POINTER(ctypes.c_double)]
+        PP = ctypes.POINTER(P)
+        L.seis_fd_modeling_batch.argtypes = [P, I, SD, PP, PP, PP]
+        L.seis_fd_born_batch.argtypes = [P, I, SD, PP, PP, PP, PP]
+        L.seis_fd_rtm_batch.argtypes = [P, I, SD, PP, PP, PP, PP]
         L.seis_fd_born.argtypes = [P, SD, P, P, P, P]
         L.seis_fd_rtm.argtypes = [P, SD, P, P, P, P]
         _lib = L
@@ -112,6 +132,11 @@ class Context:
         if rc != SEIS_OK:
             msg = self.L.seis_fd_last_error(self.h)
             raise SeisError(rc, msg.decode() if msg else "")
+
+    @property
+    def stream_ptr(self) -> int:
+        """cudaStream_t of this context (as an integer)."""
+        return int(self.L.seis_fd_stream(self.h) or 0)
 
     @property
     def launches(self) -> int:
@@ -150,3 +175,108 @@ def validate_shot(shot: "Shot") -> str:
     buf = ctypes.create_string_buffer(512)
     rc = lib().seis_fd_validate_shot(shot.to_c(), buf, 512)
     return "" if rc == SEIS_OK else (buf.value.decode() or f"error {rc}")
+
+
+OP_MODELING, OP_BORN, OP_RTM = 0, 1, 2
+IN_VEL, IN_DV, IN_WAVELET, IN_GATHER = 0, 1, 2, 3
+OUT_GATHER, OUT_IMAGE = 0, 1
+
+
+def shot_array(shots):
+    arr = (ShotDescC * len(shots))()
+    keep = []
+    for i, s in enumerate(shots):
+        c = s.to_c()
+        keep.append(c._keep)
+        arr[i] = c
+    arr._keep = keep
+    return arr
+
+
+class Plan:
+    """A batch of shots resident on the device (seis_fd_plan_*)."""
+
+    def __init__(self, ctx: Context, op: int, shots):
+        self.ctx, self.op, self.shots = ctx, op, list(shots)
+        self._descs = shot_array(self.shots)
+        h = ctypes.c_void_p()
+        ctx.check(ctx.L.seis_fd_plan_create(ctx.h, op, len(self.shots), self._descs, ctypes.byref(h)))
+        self.h = h
+
+    def set(self, shot: int, what: int, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, np.float32)
+        self.ctx.check(self.ctx.L.seis_fd_plan_set(self.h, shot, what, ptr(a)))
+        self.ctx.check(self.ctx.L.seis_fd_plan_sync(self.h))
+
+    def set_device(self, shot: int, what: int, dev_ptr: int):
+        self.ctx.check(self.ctx.L.seis_fd_plan_set_device(self.h, shot, what, ctypes.c_void_p(dev_ptr)))
+
+    def run(self):
+        self.ctx.check(self.ctx.L.seis_fd_plan_run(self.h))
+
+    def sync(self):
+        self.ctx.check(self.ctx.L.seis_fd_plan_sync(self.h))
+
+    def get(self, shot: int, what: int, out: np.ndarray = None) -> np.ndarray:
+        s = self.shots[shot]
+        shape = (s.nx, s.nt) if what == OUT_GATHER else (s.nx, s.nz)
+        if out is None:
+            out = np.zeros(shape, np.float32)
+        self.ctx.check(self.ctx.L.seis_fd_plan_get(self.h, shot, what, ptr(out)))
+        return out
+
+    def set_exact(self, exact: bool):
+        self.ctx.check(self.ctx.L.seis_fd_plan_set_exact(self.h, 1 if exact else 0))
+
+    def time_kernels(self, steps: int):
+        ms = (ctypes.c_double * 3)()
+        by = (ctypes.c_double * 2)()
+        self.ctx.check(self.ctx.L.seis_fd_plan_time_kernels(self.h, steps, ms, by))
+        return list(ms), list(by)
+
+    @property
+    def cell_updates(self) -> int:
+        return int(self.ctx.L.seis_fd_plan_cell_updates(self.h))
+
+    @property
+    def launches_per_run(self) -> int:
+        return int(self.ctx.L.seis_fd_plan_launches_per_run(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.seis_fd_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _ptr_list(arrays):
+    lst = (ctypes.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+    return lst
+
+
+def batch(ctx: Context, op: int, shots, wavs, vels, third=None):
+    """One-call batched operator (seis_fd_*_batch); returns per-shot outputs."""
+    shots = list(shots)
+    descs = shot_array(shots)
+    wavs = [np.ascontiguousarray(w, np.float32) for w in wavs]
+    vels = [np.ascontiguousarray(v, np.float32) for v in vels]
+    if op == OP_RTM:
+        outs = [np.zeros((s.nx, s.nz), np.float32) for s in shots]
+    else:
+        outs = [np.zeros((s.nx, s.nt), np.float32) for s in shots]
+    pw, pv, po = _ptr_list(wavs), _ptr_list(vels), _ptr_list(outs)
+    n = len(shots)
+    if op == OP_MODELING:
+        rc = ctx.L.seis_fd_modeling_batch(ctx.h, n, descs, pw, pv, po)
+    else:
+        thirds = [np.ascontiguousarray(t, np.float32) for t in third]
+        pt = _ptr_list(thirds)
+        fn = ctx.L.seis_fd_born_batch if op == OP_BORN else ctx.L.seis_fd_rtm_batch
+        rc = fn(ctx.h, n, descs, pw, pv, pt, po)
+    ctx.check(rc)
+    return outs

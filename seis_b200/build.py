@@ -22,8 +22,13 @@ LIB = os.path.join(OUT_DIR, "libseisfd.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
-              "-ftz=false", "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-warn-spills"]
+NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-ftz=false", "-Xcompiler", "-fPIC,-ffp-contract=off",
+               "-Xptxas", "-warn-spills"]
+# exact flavour: every operation rounds on its own, IEEE division and sqrt
+NVCC_EXACT = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"]
+# fast flavour (sources named *_fast.cu): contraction and approximate division,
+# denormals still kept (the decaying wavefield lives there)
+NVCC_FAST = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
 
 
@@ -70,7 +75,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if not force and not _stale(obj, [src] + headers + [__file__]):
             continue
         if src.endswith(".cu"):
-            cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-I", CSRC, "-I", INCLUDE, "-c", "-o", obj, src]
+            flav = NVCC_FAST if src.endswith("_fast.cu") else NVCC_EXACT
+            cmd = [nvcc, *ARCH, *NVCC_COMMON, *flav, "-I", CSRC, "-I", INCLUDE, "-c", "-o", obj, src]
         else:
             cmd = ["g++", *CXX_FLAGS, "-I", CSRC, "-I", INCLUDE, "-I", _cuda_include(), "-c", "-o", obj, src]
         out = _run(cmd)

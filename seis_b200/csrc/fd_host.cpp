@@ -11,6 +11,7 @@
 // formed here in single precision in the reference's operation order; this
 // file is compiled with -ffp-contract=off.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -28,7 +29,11 @@ using namespace seis;
 
 struct seis_fd_ctx {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;  // all work is ordered on this stream
+  cudaStream_t aux = nullptr;     // boundary tiles run here, joined every step
+  cudaEvent_t fork = nullptr, join = nullptr;
+  int *d_err = nullptr;  // set by kernels whose bounded waits ran out
+  int num_sms = 148;
   std::string err;
   int64_t launches = 0;
 };
@@ -92,8 +97,13 @@ struct Plan {
   std::vector<seis_shot_desc> desc;
   std::vector<std::vector<int>> gz;
   std::vector<ShotDev> sd;
-  std::vector<Tile> tiles;
+  std::vector<Tile> tiles;  // interior tiles first (n_int), then pad tiles
+  int n_int = 0, n_pad = 0;
   std::vector<int2> cols;
+  std::vector<float *> field_bases;  // allocation starts of margin-padded fields
+  std::vector<size_t> field_elems;
+  CUtensorMap *d_maps = nullptr;
+  bool exact = true;
   std::vector<void *> allocs;
   ShotDev *d_sd = nullptr;
   Tile *d_tiles = nullptr;
@@ -102,8 +112,14 @@ struct Plan {
   float *d_stage = nullptr;  // staging for unpadded uploads / transposes
   size_t stage_elems = 0;
   int NT = 0, nt = 0, ndel = 0, max_strip = 0, max_NZ = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int64_t launches_per_run = 0;
+  int64_t cell_updates = 0;
 
   ~Plan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
     for (void *p : allocs) cudaFree(p);
   }
   template <class T>
@@ -137,7 +153,7 @@ void hilbert_taps(float *h, int half) {
 void fill_scalars(ShotDev &g, const seis_shot_desc &s) {
   g.nx = s.nx; g.nz = s.nz; g.pml = s.pml;
   g.NX = s.nx + 2 * s.pml; g.NZ = s.nz + 2 * s.pml;
-  g.LDZ = round_up(g.NZ, 32);
+  g.LDZ = field_geom(g.NX, g.NZ).LDZ;
   g.sxp = s.sx + s.pml; g.szp = s.sz + s.pml;
   g.nt = s.nt; g.ndel = s.ndel; g.NT = s.nt + s.ndel;
   g.strip_len = LAYERS * 2 * (s.nx + s.nz);
@@ -158,9 +174,16 @@ void fill_scalars(ShotDev &g, const seis_shot_desc &s) {
   g.idt2 = 1.0f / dt / dt;
 }
 
+// Tiles of every shot's padded grid; interior tiles (every cell inside the
+// model and 8th order) take the kernel's fast path.  All interior tiles come
+// first, then all pad tiles, each group interleaved across shots: the
+// persistent CTAs then run one code path at a time (instruction-cache
+// locality) and shots are spread evenly over the SMs.
 void build_tiles(Plan &p) {
   p.tiles.clear();
   p.cols.clear();
+  std::vector<std::vector<Tile>> per(p.nshot);
+  size_t most = 0;
   for (int s = 0; s < p.nshot; s++) {
     const ShotDev &g = p.sd[s];
     int lox = std::max(g.pml, 4), hix = std::min(g.pml + g.nx, g.NX - 4);
@@ -168,10 +191,91 @@ void build_tiles(Plan &p) {
     for (int x0 = 0; x0 < g.NX; x0 += TX)
       for (int z0 = 0; z0 < g.NZ; z0 += TZ) {
         bool in = x0 >= lox && x0 + TX <= hix && z0 >= loz && z0 + TZ <= hiz;
-        p.tiles.push_back(Tile{s, x0, z0, in ? TILE_INTERIOR : TILE_BOUNDARY});
+        per[s].push_back(Tile{s, x0, z0, in ? TILE_INTERIOR : TILE_PAD});
       }
+    most = std::max(most, per[s].size());
     for (int x = 0; x < g.nx; x++) p.cols.push_back(make_int2(s, x));
   }
+  for (int kind : {TILE_INTERIOR, TILE_PAD})
+    for (size_t i = 0; i < most; i++)
+      for (int s = 0; s < p.nshot; s++)
+        if (i < per[s].size() && per[s][i].kind == kind) p.tiles.push_back(per[s][i]);
+  p.n_int = 0;
+  for (const Tile &t : p.tiles) p.n_int += t.kind == TILE_INTERIOR;
+  p.n_pad = (int)p.tiles.size() - p.n_int;
+}
+
+// One field of a shot in the margin-padded layout; returns the cell (0,0)
+// pointer.
+int alloc_field(Plan &p, const ShotDev &g, float **cell0) {
+  FieldGeom fg = field_geom(g.NX, g.NZ);
+  float *base = nullptr;
+  int rc = p.alloc(&base, fg.elems);
+  if (rc) return rc;
+  p.field_bases.push_back(base);
+  p.field_elems.push_back(fg.elems);
+  *cell0 = base + fg.origin;
+  return SEIS_OK;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// Tensor map of one field (cell (0,0) at `cell0`) with a box of the staged
+// rows by `width` columns.
+int encode_map(seis_fd_ctx *ctx, const ShotDev &g, const float *cell0, int width, CUtensorMap *m) {
+  auto fn = encode_fn();
+  if (!fn) return fail(ctx, SEIS_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  FieldGeom fg = field_geom(g.NX, g.NZ);
+  void *base = const_cast<float *>(cell0 - fg.origin);
+  cuuint64_t dims[2] = {(cuuint64_t)fg.LDZ, (cuuint64_t)fg.ncols};
+  cuuint64_t strides[1] = {(cuuint64_t)fg.LDZ * sizeof(float)};
+  cuuint32_t box[2] = {(cuuint32_t)(TZ + 2 * ZM), (cuuint32_t)width};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ctx, SEIS_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return SEIS_OK;
+}
+
+int encode_maps(Plan &p) {
+  std::vector<CUtensorMap> maps((size_t)p.nshot * NMAPS);
+  std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+  const int wide = TX + 2 * HXC, narrow = TX + 2;
+  for (int s = 0; s < p.nshot; s++) {
+    const ShotDev &g = p.sd[s];
+    CUtensorMap *m = maps.data() + (size_t)s * NMAPS;
+    int rc = SEIS_OK;
+    for (int k = 0; k < 3 && !rc; k++) {
+      rc = encode_map(p.ctx, g, g.fa[k], wide, &m[MAP_FA_WIDE + k]);
+      if (!rc) rc = encode_map(p.ctx, g, g.fa[k], narrow, &m[MAP_FA_NARROW + k]);
+      if (!rc && g.fb[k]) rc = encode_map(p.ctx, g, g.fb[k], wide, &m[MAP_FB_WIDE + k]);
+      if (!rc && g.fb[k]) rc = encode_map(p.ctx, g, g.fb[k], narrow, &m[MAP_FB_NARROW + k]);
+    }
+    if (!rc) rc = encode_map(p.ctx, g, g.vel, narrow, &m[MAP_VEL]);
+    if (!rc && g.dv) rc = encode_map(p.ctx, g, g.dv, narrow, &m[MAP_DV]);
+    if (rc) return rc;
+  }
+  int rc = p.alloc(&p.d_maps, maps.size());
+  if (rc) return rc;
+  seis_fd_ctx *ctx = p.ctx;
+  CK(cudaMemcpyAsync(p.d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  for (int s = 0; s < p.nshot; s++) p.sd[s].maps = p.d_maps + (size_t)s * NMAPS;
+  return SEIS_OK;
 }
 
 int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs, Plan **out) {
@@ -180,6 +284,10 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
   for (int i = 0; i < nshot; i++) {
     int rc = check_shot(ctx, &descs[i], i);
     if (rc) return rc;
+    // the reference keeps 4 boundary layers (fd.cpp:594, :1181-1203); they
+    // must stay inside the padded grid
+    if (op == OP_RTM && descs[i].pml + std::min(descs[i].nx, descs[i].nz) < LAYERS)
+      return fail(ctx, SEIS_ERR_ARG, "shot %d: RTM needs pml + min(nx, nz) >= %d", i, LAYERS);
     if (descs[i].nt != descs[0].nt || descs[i].ndel != descs[0].ndel || descs[i].dt != descs[0].dt)
       return fail(ctx, SEIS_ERR_ARG, "shot %d: nt, ndel and dt must match across a batch", i);
   }
@@ -202,17 +310,16 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     ShotDev &g = p->sd[s];
     std::memset(&g, 0, sizeof g);
     fill_scalars(g, d);
-    size_t cells = (size_t)g.NX * g.LDZ;
     p->max_strip = std::max(p->max_strip, g.strip_len);
     p->max_NZ = std::max(p->max_NZ, g.NZ);
     p->stage_elems = std::max(p->stage_elems, std::max((size_t)d.nx * d.nz, (size_t)d.nx * d.nt));
-    for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = p->alloc(&g.fa[k], cells);
+    for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fa[k]);
     if (op != OP_MODEL)
-      for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = p->alloc(&g.fb[k], cells);
+      for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fb[k]);
     float *vel = nullptr, *dv = nullptr, *wav = nullptr, *rec = nullptr;
     int *gzd = nullptr;
-    if (rc == SEIS_OK) rc = p->alloc(&vel, cells);
-    if (rc == SEIS_OK && op == OP_BORN) rc = p->alloc(&dv, cells);
+    if (rc == SEIS_OK) rc = alloc_field(*p, g, &vel);
+    if (rc == SEIS_OK && op == OP_BORN) rc = alloc_field(*p, g, &dv);
     if (rc == SEIS_OK) rc = p->alloc(&wav, (size_t)g.NT);
     if (rc == SEIS_OK) rc = p->alloc(&rec, (size_t)d.nt * d.nx);
     if (rc == SEIS_OK) rc = p->alloc(&gzd, (size_t)d.nx);
@@ -226,8 +333,15 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     }
   }
   if (rc == SEIS_OK) rc = p->alloc(&p->d_stage, p->stage_elems);
+  if (rc == SEIS_OK) rc = encode_maps(*p);
   if (rc == SEIS_OK) {
     build_tiles(*p);
+    int fields = op == OP_MODEL ? 1 : (op == OP_BORN ? 2 : 3);
+    for (const ShotDev &g : p->sd) {
+      int64_t steps = op == OP_RTM ? (int64_t)g.NT + g.nt : g.NT;
+      int64_t f = op == OP_RTM ? 1 : fields;  // RTM: NT source steps, nt x 2 reverse steps
+      p->cell_updates += (int64_t)g.NX * g.NZ * (op == OP_RTM ? (g.NT + 2LL * g.nt) : steps * f);
+    }
     rc = p->alloc(&p->d_sd, (size_t)nshot);
   }
   if (rc == SEIS_OK) rc = p->alloc(&p->d_tiles, p->tiles.size());
@@ -261,19 +375,36 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
 }
 
 // Upload an unpadded [nx][nz] model of shot s into a padded device field.
-int upload_model(Plan &p, int s, const float *h, float *d_padded, int clamp) {
+
+// One time step of every shot: the interior-tile kernel on the main stream and
+// the pad-tile kernel on the auxiliary stream, joined before the next step.
+int step(Plan &p, int mode, const StepArgs &a) {
   seis_fd_ctx *ctx = p.ctx;
-  const seis_shot_desc &d = p.desc[s];
-  const ShotDev &g = p.sd[s];
-  CK(cudaMemcpyAsync(p.d_stage, h, sizeof(float) * d.nx * d.nz, cudaMemcpyHostToDevice,
-                     ctx->stream));
-  CK(launch_pad(p.d_stage, d.nx, d.nz, d.pml, g.LDZ, clamp, d_padded, ctx->stream));
-  ctx->launches++;
+  CK(cudaEventRecord(ctx->fork, ctx->stream));
+  CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
+  CK(launch_step(mode, p.exact, p.d_sd, p.d_tiles, p.n_int, p.n_pad, ctx->num_sms, a, ctx->d_err,
+                 ctx->stream, ctx->aux));
+  CK(cudaEventRecord(ctx->join, ctx->aux));
+  CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
+  ctx->launches += (p.n_int > 0) + (p.n_pad > 0);
+  return SEIS_OK;
+}
+
+// Zero every wavefield buffer (margins included) and the images.
+int clear_fields(Plan &p) {
+  seis_fd_ctx *ctx = p.ctx;
+  for (const ShotDev &g : p.sd) {
+    FieldGeom fg = field_geom(g.NX, g.NZ);
+    for (int k = 0; k < 3; k++) {
+      CK(cudaMemsetAsync(g.fa[k] - fg.origin, 0, sizeof(float) * fg.elems, ctx->stream));
+      if (g.fb[k]) CK(cudaMemsetAsync(g.fb[k] - fg.origin, 0, sizeof(float) * fg.elems, ctx->stream));
+    }
+    if (g.img) CK(cudaMemsetAsync(g.img, 0, sizeof(float) * g.nx * g.nz, ctx->stream));
+  }
   return SEIS_OK;
 }
 
 int run_forward(Plan &p, int mode) {
-  seis_fd_ctx *ctx = p.ctx;
   StepArgs a{};
   a.nshots = p.nshot;
   for (int it = 0; it < p.NT; it++) {
@@ -283,8 +414,8 @@ int run_forward(Plan &p, int mode) {
     int itp = it - p.ndel;
     a.rec_k = (p.op != OP_RTM && itp >= 0) ? itp : -1;
     a.strip_k = (p.op == OP_RTM && itp >= 0) ? itp : -1;
-    CK(launch_step(mode, p.d_sd, p.d_tiles, (int)p.tiles.size(), a, ctx->stream));
-    ctx->launches++;
+    int rc = step(p, mode, a);
+    if (rc) return rc;
   }
   return SEIS_OK;
 }
@@ -293,9 +424,11 @@ int run_forward(Plan &p, int mode) {
 int run_rtm_reverse(Plan &p) {
   seis_fd_ctx *ctx = p.ctx;
   // the source fields restart from zero (fd.cpp:654-656)
-  for (int s = 0; s < p.nshot; s++)
+  for (int s = 0; s < p.nshot; s++) {
+    FieldGeom fg = field_geom(p.sd[s].NX, p.sd[s].NZ);
     for (int k = 0; k < 3; k++)
-      CK(cudaMemsetAsync(p.sd[s].fa[k], 0, sizeof(float) * p.sd[s].NX * p.sd[s].LDZ, ctx->stream));
+      CK(cudaMemsetAsync(p.sd[s].fa[k] - fg.origin, 0, sizeof(float) * fg.elems, ctx->stream));
+  }
   StepArgs a{};
   a.nshots = p.nshot;
   a.src_k = -1;
@@ -305,14 +438,55 @@ int run_rtm_reverse(Plan &p) {
     a.rot = k;
     a.rot_b = k;
     CK(launch_rtm_restore(p.d_sd, p.nshot, p.max_strip, a.rot, it, ctx->stream));
+    ctx->launches++;
     a.rec_k = -1;
-    CK(launch_step(MODE_MODEL, p.d_sd, p.d_tiles, (int)p.tiles.size(), a, ctx->stream));
+    int rc = step(p, MODE_MODEL, a);
+    if (rc) return rc;
     a.rec_k = it - p.ndel;
-    CK(launch_step(MODE_RCV, p.d_sd, p.d_tiles, (int)p.tiles.size(), a, ctx->stream));
+    rc = step(p, MODE_RCV, a);
+    if (rc) return rc;
     CK(launch_rtm_image(p.d_sd, p.d_cols, (int)p.cols.size(), a.rot, a.rot_b, p.max_NZ,
                         p.d_taps, ctx->stream));
-    ctx->launches += 4;
+    ctx->launches++;
   }
+  return SEIS_OK;
+}
+
+// The whole operator as a stream of launches (captured into a graph by
+// plan_run).
+int enqueue_operator(Plan &p) {
+  int rc = clear_fields(p);
+  if (rc) return rc;
+  switch (p.op) {
+    case OP_MODEL: return run_forward(p, MODE_MODEL);
+    case OP_BORN: return run_forward(p, MODE_BORN);
+    case OP_RTM:
+      rc = run_forward(p, MODE_MODEL);
+      return rc ? rc : run_rtm_reverse(p);
+  }
+  return fail(p.ctx, SEIS_ERR_NOTSUP, "unknown operator %d", p.op);
+}
+
+int plan_run(Plan &p) {
+  seis_fd_ctx *ctx = p.ctx;
+  if (!p.exec) {
+    int64_t before = ctx->launches;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_operator(p);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    CK(e);
+    p.graph = g;
+    CK(cudaGraphInstantiate(&p.exec, p.graph, 0));
+    p.launches_per_run = ctx->launches - before;
+    ctx->launches = before;
+  }
+  CK(cudaGraphLaunch(p.exec, ctx->stream));
+  ctx->launches += p.launches_per_run;
   return SEIS_OK;
 }
 
@@ -326,25 +500,16 @@ int download_gather(Plan &p, int s, float *h_rec) {
   return SEIS_OK;
 }
 
-int upload_gather(Plan &p, int s, const float *h_rec) {
-  seis_fd_ctx *ctx = p.ctx;
-  const seis_shot_desc &d = p.desc[s];
-  CK(cudaMemcpyAsync(p.d_stage, h_rec, sizeof(float) * d.nt * d.nx, cudaMemcpyHostToDevice,
-                     ctx->stream));
-  CK(launch_transpose(p.d_stage, d.nx, d.nt, p.sd[s].rec, ctx->stream));
-  ctx->launches++;
-  return SEIS_OK;
-}
 
-int upload_wavelet(Plan &p, int s, const float *h_wav) {
-  seis_fd_ctx *ctx = p.ctx;
-  CK(cudaMemcpyAsync(const_cast<float *>(p.sd[s].wav), h_wav, sizeof(float) * p.NT,
-                     cudaMemcpyHostToDevice, ctx->stream));
-  return SEIS_OK;
-}
 
 int sync(seis_fd_ctx *ctx) {
   CK(cudaStreamSynchronize(ctx->stream));
+  int flag = 0;
+  CK(cudaMemcpy(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
+    return fail(ctx, SEIS_ERR_CUDA, "a kernel gave up waiting for its staged input (code %d)", flag);
+  }
   return SEIS_OK;
 }
 
@@ -397,8 +562,16 @@ int seis_fd_create(seis_fd_ctx **out, int device) {
   ctx->device = device;
   e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = configure_kernels();
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, sizeof(int));
   if (e != cudaSuccess) {
-    delete ctx;
+    seis_fd_destroy(ctx);
     return SEIS_ERR_CUDA;
   }
   *out = ctx;
@@ -408,10 +581,13 @@ int seis_fd_create(seis_fd_ctx **out, int device) {
 int seis_fd_destroy(seis_fd_ctx *ctx) {
   if (!ctx) return SEIS_OK;
   cudaSetDevice(ctx->device);
-  if (ctx->stream) {
-    cudaStreamSynchronize(ctx->stream);
-    cudaStreamDestroy(ctx->stream);
-  }
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->aux) cudaStreamSynchronize(ctx->aux);
+  if (ctx->d_err) cudaFree(ctx->d_err);
+  if (ctx->fork) cudaEventDestroy(ctx->fork);
+  if (ctx->join) cudaEventDestroy(ctx->join);
+  if (ctx->aux) cudaStreamDestroy(ctx->aux);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return SEIS_OK;
 }
@@ -420,62 +596,257 @@ const char *seis_fd_last_error(const seis_fd_ctx *ctx) { return ctx ? ctx->err.c
 
 int64_t seis_fd_launch_count(const seis_fd_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
-int seis_fd_modeling(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
-                     const float *h_vel, float *h_rec) {
+void *seis_fd_stream(const seis_fd_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+// ---------------------------------------------------------------- plans
+struct seis_fd_plan {
+  Plan *p;
+};
+
+int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *shots,
+                        seis_fd_plan **out) {
   int rc = begin(ctx);
   if (rc) return rc;
-  if (!h_wav || !h_vel || !h_rec) return fail(ctx, SEIS_ERR_ARG, "null array");
+  if (!out) return fail(ctx, SEIS_ERR_ARG, "out is null");
+  *out = nullptr;
+  if (op < SEIS_OP_MODELING || op > SEIS_OP_RTM) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
   Plan *p = nullptr;
-  rc = plan_create(ctx, OP_MODEL, 1, shot, &p);
+  rc = plan_create(ctx, op, nshot, shots, &p);
   if (rc) return rc;
-  if (!rc) rc = upload_model(*p, 0, h_vel, const_cast<float *>(p->sd[0].vel), 1);
-  if (!rc) rc = upload_wavelet(*p, 0, h_wav);
-  if (!rc) rc = run_forward(*p, MODE_MODEL);
-  if (!rc) rc = download_gather(*p, 0, h_rec);
+  seis_fd_plan *h = new (std::nothrow) seis_fd_plan{p};
+  if (!h) {
+    delete p;
+    return fail(ctx, SEIS_ERR_NOMEM, "host allocation failed");
+  }
+  *out = h;
+  return SEIS_OK;
+}
+
+int seis_fd_plan_destroy(seis_fd_plan *plan) {
+  if (!plan) return SEIS_OK;
+  if (plan->p) {
+    seis_fd_ctx *ctx = plan->p->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    delete plan->p;
+  }
+  delete plan;
+  return SEIS_OK;
+}
+
+static int plan_input(seis_fd_plan *plan, int shot, int what, const float *src, bool device) {
+  if (!plan || !plan->p) return SEIS_ERR_ARG;
+  Plan &p = *plan->p;
+  seis_fd_ctx *ctx = p.ctx;
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (shot < 0 || shot >= p.nshot) return fail(ctx, SEIS_ERR_ARG, "shot=%d of %d", shot, p.nshot);
+  if (!src) return fail(ctx, SEIS_ERR_ARG, "null source");
+  const seis_shot_desc &d = p.desc[shot];
+  ShotDev &g = p.sd[shot];
+  cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  switch (what) {
+    case SEIS_IN_VEL:
+    case SEIS_IN_DV: {
+      if (what == SEIS_IN_DV && !g.dv) return fail(ctx, SEIS_ERR_NOTSUP, "plan has no dv input");
+      CK(cudaMemcpyAsync(p.d_stage, src, sizeof(float) * d.nx * d.nz, kind, ctx->stream));
+      float *dst = const_cast<float *>(what == SEIS_IN_VEL ? g.vel : g.dv);
+      CK(launch_pad(p.d_stage, d.nx, d.nz, d.pml, g.LDZ, what == SEIS_IN_VEL, dst, ctx->stream));
+      ctx->launches++;
+      return SEIS_OK;
+    }
+    case SEIS_IN_WAVELET:
+      CK(cudaMemcpyAsync(const_cast<float *>(g.wav), src, sizeof(float) * g.NT, kind, ctx->stream));
+      return SEIS_OK;
+    case SEIS_IN_GATHER:
+      if (p.op != OP_RTM) return fail(ctx, SEIS_ERR_NOTSUP, "plan takes no gather input");
+      CK(cudaMemcpyAsync(p.d_stage, src, sizeof(float) * d.nt * d.nx, kind, ctx->stream));
+      CK(launch_transpose(p.d_stage, d.nx, d.nt, g.rec, ctx->stream));
+      ctx->launches++;
+      return SEIS_OK;
+  }
+  return fail(ctx, SEIS_ERR_ARG, "unknown input %d", what);
+}
+
+int seis_fd_plan_set(seis_fd_plan *plan, int shot, int what, const float *h_src) {
+  return plan_input(plan, shot, what, h_src, false);
+}
+
+int seis_fd_plan_set_device(seis_fd_plan *plan, int shot, int what, const float *d_src) {
+  return plan_input(plan, shot, what, d_src, true);
+}
+
+int seis_fd_plan_run(seis_fd_plan *plan) {
+  if (!plan || !plan->p) return SEIS_ERR_ARG;
+  int rc = begin(plan->p->ctx);
+  return rc ? rc : plan_run(*plan->p);
+}
+
+int seis_fd_plan_get(seis_fd_plan *plan, int shot, int what, float *h_dst) {
+  if (!plan || !plan->p) return SEIS_ERR_ARG;
+  Plan &p = *plan->p;
+  seis_fd_ctx *ctx = p.ctx;
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (shot < 0 || shot >= p.nshot) return fail(ctx, SEIS_ERR_ARG, "shot=%d of %d", shot, p.nshot);
+  if (!h_dst) return fail(ctx, SEIS_ERR_ARG, "null destination");
+  if (what == SEIS_OUT_GATHER) {
+    if (p.op == OP_RTM) return fail(ctx, SEIS_ERR_NOTSUP, "RTM plans output images");
+    rc = download_gather(p, shot, h_dst);
+  } else if (what == SEIS_OUT_IMAGE) {
+    if (p.op != OP_RTM) return fail(ctx, SEIS_ERR_NOTSUP, "plan outputs gathers");
+    const seis_shot_desc &d = p.desc[shot];
+    CK(cudaMemcpyAsync(h_dst, p.sd[shot].img, sizeof(float) * d.nx * d.nz,
+                       cudaMemcpyDeviceToHost, ctx->stream));
+  } else {
+    return fail(ctx, SEIS_ERR_ARG, "unknown output %d", what);
+  }
+  return rc ? rc : sync(ctx);
+}
+
+int seis_fd_plan_sync(seis_fd_plan *plan) {
+  if (!plan || !plan->p) return SEIS_ERR_ARG;
+  int rc = begin(plan->p->ctx);
+  return rc ? rc : sync(plan->p->ctx);
+}
+
+int64_t seis_fd_plan_cell_updates(const seis_fd_plan *plan) {
+  return plan && plan->p ? plan->p->cell_updates : 0;
+}
+
+int64_t seis_fd_plan_launches_per_run(const seis_fd_plan *plan) {
+  return plan && plan->p ? plan->p->launches_per_run : 0;
+}
+
+int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double *bytes) {
+  if (!plan || !plan->p || !ms || !bytes || steps < 1) return SEIS_ERR_ARG;
+  Plan &p = *plan->p;
+  seis_fd_ctx *ctx = p.ctx;
+  int rc = begin(ctx);
+  if (rc) return rc;
+  int mode = p.op == OP_BORN ? MODE_BORN : MODE_MODEL;
+  int fields = p.op == OP_BORN ? 2 : 1;
+  cudaEvent_t ev[5];
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  int64_t cells_int = 0, cells_pad = 0;
+  for (size_t i = 0; i < p.tiles.size(); i++) {
+    const Tile &t = p.tiles[i];
+    const ShotDev &g = p.sd[t.shot];
+    int64_t c = (int64_t)std::min(TX, g.NX - t.x0) * std::min(TZ, g.NZ - t.z0);
+    ((int)i < p.n_int ? cells_int : cells_pad) += c;
+  }
+  StepArgs a{};
+  a.nshots = p.nshot;
+  a.strip_k = -1;
+  double t_int = 0, t_pad = 0, t_step = 0;
+  for (int k = 0; k < steps; k++) {
+    a.rot = k; a.rot_b = k;
+    int it = k % p.NT;
+    a.src_k = it >= 1 ? it - 1 : -1;
+    a.rec_k = it - p.ndel >= 0 && p.op != OP_RTM ? it - p.ndel : -1;
+    // interior kernel on the main stream, pad kernel on the auxiliary one,
+    // concurrently, each bracketed by events on its own stream
+    CK(cudaEventRecord(ev[0], ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->aux, ev[0], 0));
+    CK(cudaEventRecord(ev[2], ctx->aux));
+    CK(launch_step(mode, p.exact, p.d_sd, p.d_tiles, p.n_int, 0, ctx->num_sms, a, ctx->d_err,
+                   ctx->stream, ctx->aux));
+    CK(launch_step(mode, p.exact, p.d_sd, p.d_tiles + p.n_int, 0, p.n_pad, ctx->num_sms, a,
+                   ctx->d_err, ctx->stream, ctx->aux));
+    CK(cudaEventRecord(ev[1], ctx->stream));
+    CK(cudaEventRecord(ev[3], ctx->aux));
+    CK(cudaStreamWaitEvent(ctx->stream, ev[3], 0));
+    CK(cudaEventRecord(ev[4], ctx->stream));
+    CK(cudaEventSynchronize(ev[4]));
+    float a1 = 0, a2 = 0, a3 = 0;
+    CK(cudaEventElapsedTime(&a1, ev[0], ev[1]));
+    CK(cudaEventElapsedTime(&a2, ev[2], ev[3]));
+    CK(cudaEventElapsedTime(&a3, ev[0], ev[4]));
+    t_int += a1; t_pad += a2; t_step += a3;
+    ctx->launches += 2;
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  ms[0] = t_int / steps; ms[1] = t_pad / steps; ms[2] = t_step / steps;
+  bytes[0] = 16.0 * fields * (double)cells_int;
+  bytes[1] = 16.0 * fields * (double)cells_pad;
+  return clear_fields(p) ? SEIS_ERR_CUDA : sync(ctx);
+}
+
+int seis_fd_plan_set_exact(seis_fd_plan *plan, int exact) {
+  if (!plan || !plan->p) return SEIS_ERR_ARG;
+  Plan &p = *plan->p;
+  if (p.exact != (exact != 0)) {
+    p.exact = exact != 0;
+    if (p.exec) cudaGraphExecDestroy(p.exec);
+    if (p.graph) cudaGraphDestroy(p.graph);
+    p.exec = nullptr;
+    p.graph = nullptr;
+  }
+  return SEIS_OK;
+}
+
+// ------------------------------------------------------- one-call batches
+static int run_batch(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *shots,
+                     const float *const *in1, int what1, const float *const *in2, int what2,
+                     const float *const *in3, int what3, float *const *out, int what_out) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (!in1 || !in2 || (what3 >= 0 && !in3) || !out)
+    return fail(ctx, SEIS_ERR_ARG, "null array list");
+  Plan *p = nullptr;
+  rc = plan_create(ctx, op, nshot, shots, &p);
+  if (rc) return rc;
+  seis_fd_plan h{p};
+  for (int s = 0; s < nshot && !rc; s++) {
+    rc = plan_input(&h, s, what1, in1[s], false);
+    if (!rc) rc = plan_input(&h, s, what2, in2[s], false);
+    if (!rc && what3 >= 0) rc = plan_input(&h, s, what3, in3[s], false);
+  }
+  if (!rc) rc = enqueue_operator(*p);  // one run: no graph
+  for (int s = 0; s < nshot && !rc; s++) rc = seis_fd_plan_get(&h, s, what_out, out[s]);
   if (!rc) rc = sync(ctx);
+  cudaStreamSynchronize(ctx->stream);
   delete p;
   return rc;
+}
+
+int seis_fd_modeling(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
+                     const float *h_vel, float *h_rec) {
+  return run_batch(ctx, OP_MODEL, 1, shot, &h_wav, SEIS_IN_WAVELET, &h_vel, SEIS_IN_VEL, nullptr,
+                   -1, &h_rec, SEIS_OUT_GATHER);
 }
 
 int seis_fd_born(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
                  const float *h_vel, const float *h_dv, float *h_rec) {
-  int rc = begin(ctx);
-  if (rc) return rc;
-  if (!h_wav || !h_vel || !h_dv || !h_rec) return fail(ctx, SEIS_ERR_ARG, "null array");
-  Plan *p = nullptr;
-  rc = plan_create(ctx, OP_BORN, 1, shot, &p);
-  if (rc) return rc;
-  if (!rc) rc = upload_model(*p, 0, h_vel, const_cast<float *>(p->sd[0].vel), 1);
-  if (!rc) rc = upload_model(*p, 0, h_dv, const_cast<float *>(p->sd[0].dv), 0);
-  if (!rc) rc = upload_wavelet(*p, 0, h_wav);
-  if (!rc) rc = run_forward(*p, MODE_BORN);
-  if (!rc) rc = download_gather(*p, 0, h_rec);
-  if (!rc) rc = sync(ctx);
-  delete p;
-  return rc;
+  return run_batch(ctx, OP_BORN, 1, shot, &h_wav, SEIS_IN_WAVELET, &h_vel, SEIS_IN_VEL, &h_dv,
+                   SEIS_IN_DV, &h_rec, SEIS_OUT_GATHER);
 }
 
 int seis_fd_rtm(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
                 const float *h_vel, const float *h_rec, float *h_img) {
-  int rc = begin(ctx);
-  if (rc) return rc;
-  if (!h_wav || !h_vel || !h_rec || !h_img) return fail(ctx, SEIS_ERR_ARG, "null array");
-  Plan *p = nullptr;
-  rc = plan_create(ctx, OP_RTM, 1, shot, &p);
-  if (rc) return rc;
-  if (!rc) rc = upload_model(*p, 0, h_vel, const_cast<float *>(p->sd[0].vel), 1);
-  if (!rc) rc = upload_wavelet(*p, 0, h_wav);
-  if (!rc) rc = upload_gather(*p, 0, h_rec);
-  if (!rc) rc = run_forward(*p, MODE_MODEL);
-  if (!rc) rc = run_rtm_reverse(*p);
-  if (!rc) {
-    cudaError_t e = cudaMemcpyAsync(h_img, p->sd[0].img, sizeof(float) * shot->nx * shot->nz,
-                                    cudaMemcpyDeviceToHost, ctx->stream);
-    if (e != cudaSuccess) rc = fail(ctx, SEIS_ERR_CUDA, "image download: %s", cudaGetErrorString(e));
-  }
-  if (!rc) rc = sync(ctx);
-  delete p;
-  return rc;
+  return run_batch(ctx, OP_RTM, 1, shot, &h_wav, SEIS_IN_WAVELET, &h_vel, SEIS_IN_VEL, &h_rec,
+                   SEIS_IN_GATHER, &h_img, SEIS_OUT_IMAGE);
+}
+
+int seis_fd_modeling_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
+                           const float *const *h_wav, const float *const *h_vel,
+                           float *const *h_rec) {
+  return run_batch(ctx, OP_MODEL, nshot, shots, h_wav, SEIS_IN_WAVELET, h_vel, SEIS_IN_VEL,
+                   nullptr, -1, h_rec, SEIS_OUT_GATHER);
+}
+
+int seis_fd_born_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
+                       const float *const *h_wav, const float *const *h_vel,
+                       const float *const *h_dv, float *const *h_rec) {
+  return run_batch(ctx, OP_BORN, nshot, shots, h_wav, SEIS_IN_WAVELET, h_vel, SEIS_IN_VEL, h_dv,
+                   SEIS_IN_DV, h_rec, SEIS_OUT_GATHER);
+}
+
+int seis_fd_rtm_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
+                      const float *const *h_wav, const float *const *h_vel,
+                      const float *const *h_rec, float *const *h_img) {
+  return run_batch(ctx, OP_RTM, nshot, shots, h_wav, SEIS_IN_WAVELET, h_vel, SEIS_IN_VEL, h_rec,
+                   SEIS_IN_GATHER, h_img, SEIS_OUT_IMAGE);
 }
 
 }  // extern "C"

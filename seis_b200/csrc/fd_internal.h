@@ -1,30 +1,45 @@
 // Internal structures shared by the host runtime (fd_host.cpp) and the CUDA
 // kernels (fd_kernels.cu).  Not part of the public ABI.
 #pragma once
+#include <cuda.h>  // CUtensorMap (type only; maps are encoded through the runtime entry point)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace seis {
 
-// Tile of the padded grid handled by one CTA: TZ cells along z (contiguous)
-// by TX columns along x.  The shared-memory copy of the current field carries
-// a halo of HX columns and HZ rows (HZ rounded up to a float4 multiple).
-constexpr int TZ = 64;
+// Tiling.  The padded grid of every shot is cut into TX x TZ tiles (TZ rows
+// along the contiguous z axis).  Field arrays carry zero margins (ZM rows above
+// and below, XM columns on either side) so that every staged column segment
+// [z0 - ZM, z0 + TZ + ZM) of every tile, with an HXC-column halo, lies inside
+// the allocation.
 constexpr int TX = 32;
-constexpr int HX = 5;
-constexpr int HZ = 8;
-constexpr int SROWS = TZ + 2 * HZ;  // rows of the shared tile (z)
-constexpr int SCOLS = TX + 2 * HX;  // columns of the shared tile (x)
-constexpr int NTHREADS = 128;
-constexpr int LAYERS = 4;           // boundary layers kept for reconstruction
+constexpr int TZ = 64;
+constexpr int HXC = 5;      // column halo of the current field (stencil radius 4 + 1)
+constexpr int ZM = 8;
+constexpr int XM = 16;
+constexpr int LAYERS = 4;   // boundary layers kept for reconstruction
 
 enum TileKind : int {
-  TILE_INTERIOR = 0,  // every cell interior and 8th order: no absorbing terms
-  TILE_BOUNDARY = 1,  // touches the pad, the frame or the low-order rings
+  TILE_INTERIOR = 0,  // every cell inside the model and 8th order: no absorbing terms
+  TILE_PAD = 1,       // touches the pad, the frame or the low-order rings
 };
 
 struct Tile {
   int shot, x0, z0, kind;
+};
+
+// 2-D TMA tensor maps of one shot (each describes one margin-padded field
+// allocation, LDZ rows x ncols columns; box = staged rows x staged columns).
+// Wide boxes (TX + 2*HXC columns) stage a field read as "current"; narrow boxes
+// (TX + 2 columns) a field read as "previous", the velocity or dv.
+enum MapIndex : int {
+  MAP_FA_WIDE = 0,    // + rotating buffer index 0..2
+  MAP_FA_NARROW = 3,
+  MAP_FB_WIDE = 6,
+  MAP_FB_NARROW = 9,
+  MAP_VEL = 12,
+  MAP_DV = 13,
+  NMAPS = 14,
 };
 
 // Device descriptor of one shot in a batch.  Scalars derived from dt/dx/dz are
@@ -52,7 +67,10 @@ struct ShotDev {
   float *rec;            // gather, device layout [nt][nx]
   float *strips;         // boundary strips, [nt][strip_len]
   float *img;            // image [nx][nz]
+  const CUtensorMap *maps;  // NMAPS tensor maps of this shot (device memory)
 };
+static_assert(sizeof(ShotDev) % sizeof(int) == 0 && sizeof(ShotDev) <= 256 * sizeof(int),
+              "ShotDev is copied word by word into shared memory");
 
 // Per-launch step arguments.
 struct StepArgs {
@@ -64,15 +82,53 @@ struct StepArgs {
   int nshots;
 };
 
-// Kernel launchers (fd_kernels.cu).
+// Allocation geometry of one field of a shot: LDZ floats per column, and the
+// element offset of cell (0,0) from the allocation start.
+struct FieldGeom {
+  int LDZ;
+  int ncols;      // XM + NX + right margin
+  size_t elems;   // ncols * LDZ
+  size_t origin;  // XM * LDZ + ZM
+};
+inline FieldGeom field_geom(int NX, int NZ) {
+  FieldGeom f;
+  int nstrip = (NZ + TZ - 1) / TZ;
+  f.LDZ = ((ZM + nstrip * TZ + ZM) + 31) / 32 * 32;
+  int right = ((NX + TX - 1) / TX) * TX - NX + XM;
+  f.ncols = XM + NX + right;
+  f.elems = (size_t)f.ncols * f.LDZ;
+  f.origin = (size_t)XM * f.LDZ + ZM;
+  return f;
+}
+
+// Kernel launchers (fd_kernels.cu, fd_stream_*.cu).
 enum StepMode : int {
   MODE_MODEL = 0,    // field A; point source; record; optional strip save
   MODE_RCV = 1,      // field B; receiver injection rec*vt2 (reference RTM)
   MODE_BORN = 2,     // fields A (background) and B (scattered)
 };
 
-cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, int ntiles,
-                        const StepArgs &a, cudaStream_t s);
+// One time step over every tile of a batch: the first n_int tiles are
+// interior tiles (one CTA each, stream s_int), the next n_pad pad tiles
+// (persistent CTAs, stream s_pad).  `exact` selects the build that rounds like
+// the reference; otherwise the contracted build.
+cudaError_t launch_step(int mode, bool exact, const ShotDev *d_shots, const Tile *d_tiles,
+                        int n_int, int n_pad, int num_sms, const StepArgs &a, int *d_err,
+                        cudaStream_t s_int, cudaStream_t s_pad);
+namespace exact {
+cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, int n_int,
+                        int n_pad, int num_sms, const StepArgs &a, int *d_err, cudaStream_t s_int,
+                        cudaStream_t s_pad);
+cudaError_t configure();
+}  // namespace exact
+namespace fast {
+cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, int n_int,
+                        int n_pad, int num_sms, const StepArgs &a, int *d_err, cudaStream_t s_int,
+                        cudaStream_t s_pad);
+cudaError_t configure();
+}  // namespace fast
+// Set kernel attributes (shared-memory limits); call once per device.
+cudaError_t configure_kernels();
 cudaError_t launch_pad(const float *d_src, int nx, int nz, int pml, int LDZ, int clamp,
                        float *d_dst, cudaStream_t s);
 cudaError_t launch_transpose(const float *d_src, int rows, int cols, float *d_dst,
