@@ -64,6 +64,8 @@ typedef struct {
 /* ---------------------------------------------------------------- context */
 int seis_fd_abi_version(void);
 int seis_fd_create(seis_fd_ctx **out, int device);
+/* Destroys the context and the device state of every plan created on it; the
+ * plan handles stay valid for seis_fd_plan_destroy only. */
 int seis_fd_destroy(seis_fd_ctx *ctx);
 const char *seis_fd_last_error(const seis_fd_ctx *ctx);
 /* Number of kernel launches this context has issued since creation
@@ -109,6 +111,8 @@ int seis_fd_rtm(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav
 #define SEIS_OP_MODELING 0 /* modeling (fd.cpp:15-80)                      */
 #define SEIS_OP_BORN 1     /* forward, Born (fd.cpp:81-177)                 */
 #define SEIS_OP_RTM 2      /* adjoint, reference RTM (fd.cpp:592-719)       */
+#define SEIS_OP_BORN_ADJOINT 3 /* exact adjoint of SEIS_OP_BORN (no reference
+                                  counterpart): gather -> image             */
 
 #define SEIS_IN_VEL 0      /* [nx][nz] velocity of the shot's model         */
 #define SEIS_IN_DV 1       /* [nx][nz] velocity perturbation (SEIS_OP_BORN) */
@@ -116,6 +120,12 @@ int seis_fd_rtm(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav
 #define SEIS_IN_GATHER 3   /* [nx][nt] receiver data (SEIS_OP_RTM)          */
 #define SEIS_OUT_GATHER 0  /* [nx][nt] recorded gather                      */
 #define SEIS_OUT_IMAGE 1   /* [nx][nz] image                                */
+
+/* Storage of the source-term snapshots (background second time derivative)
+ * that SEIS_OP_BORN_ADJOINT images with. */
+#define SEIS_SNAP_F32 1
+#define SEIS_SNAP_BF16 2   /* one power-of-two scale per snapshot and 32x64 tile */
+#define SEIS_SNAP_F16 3    /* same */
 
 int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *shots,
                         seis_fd_plan **out);
@@ -136,6 +146,16 @@ int64_t seis_fd_plan_cell_updates(const seis_fd_plan *plan);
 /* Kernel launches of one run. */
 int64_t seis_fd_plan_launches_per_run(const seis_fd_plan *plan);
 
+/* Snapshots of SEIS_OP_BORN_ADJOINT plans: keep the source term every
+ * `every` steps (1 = every step) as `dtype` (SEIS_SNAP_*).  every = 1 with
+ * SEIS_SNAP_F32 makes the operator the exact transpose of SEIS_OP_BORN (up to
+ * FP32 rounding); larger intervals and 16-bit storage trade accuracy for
+ * memory (the imaging term of a stored step is weighted by `every`).  Default:
+ * every = 1, SEIS_SNAP_F32.  Call before the first run. */
+int seis_fd_plan_set_snapshots(seis_fd_plan *plan, int every, int dtype);
+/* Bytes of device memory the plan holds (fields, models, gathers, images,
+ * snapshots once allocated). */
+int64_t seis_fd_plan_device_bytes(const seis_fd_plan *plan);
 /* Arithmetic flavour of a plan's propagation kernels.  exact = 1 (default):
  * every operation rounds on its own in the reference's order, so results equal
  * the reference's bit for bit.  exact = 0: multiply-add contraction and
@@ -163,6 +183,12 @@ int seis_fd_born_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
 int seis_fd_rtm_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
                       const float *const *h_wav, const float *const *h_vel,
                       const float *const *h_rec, float *const *h_img);
+
+/* Exact adjoint of seis_fd_born (no reference counterpart): h_img[nx][nz] =
+ * L^T h_rec for the Born operator L of the same shot, snapshots every step in
+ * FP32.  <L m, d> = <m, L^T d> to FP32 rounding. */
+int seis_fd_born_adjoint(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
+                         const float *h_vel, const float *h_rec, float *h_img);
 
 #ifdef __cplusplus
 }

@@ -487,6 +487,249 @@ int F(orc_rtm)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int 
   return 0;
 }
 
+/* ---------------------------------------------------------------------------
+ * Exact adjoint of the Born operator above (no counterpart in the reference,
+ * whose adjoint() is a different imaging operator).  Every stage of one
+ * forward step is transposed in scatter form, in reverse order:
+ *   blend^T  (fd.cpp:55-56):       u3b = w y, u31b = (1-w) y
+ *   rings^T  (fd.cpp:1092-1179):   u31 = -tmp/D is linear in its 9 inputs
+ *   frame^T and stencil^T (fd.cpp:1057-1091, :1226-1271)
+ * The reverse time loop accumulates the adjoint fields; the gradient w.r.t.
+ * dv is sum_k vt2 lap_k vel3 * u3b_k over the interior (setDv^T = crop).
+ * ------------------------------------------------------------------------- */
+
+/* transposed one-way strip update: s = u31b * (-1/D) */
+static void F(oneway_T)(REAL s, REAL a1, REAL a2, REAL a3, REAL *u3i, REAL *u3tp, REAL *u3tm,
+                        REAL *cK, REAL *ci, REAL *pK, REAL *pi, REAL *ptp, REAL *ptm)
+{
+  *u3i += s * (-a1 + a2 + KR(2) * a3);
+  *u3tp += s * (-a3);
+  *u3tm += s * (-a3);
+  *cK += s * (KR(-2) * a2);
+  *ci += s * (KR(-2) * a2);
+  *pK += s * (-a1 + a2 + KR(2) * a3);
+  *pi += s * (a1 + a2);
+  *ptp += s * (-a3);
+  *ptm += s * (-a3);
+}
+
+static void F(rings_T)(const F(grid_t) *g, const F(coefs_t) *c, const REAL *u31b, REAL *u3b,
+                       REAL *cb, REAL *pb)
+{
+  const int nx = g->nx, nz = g->nz, pml = g->pml;
+  const REAL dt = g->dt, dx = g->dx, dz = g->dz;
+  const REAL *vel = c->vel;
+  for (int IK = 1; IK <= pml; IK++) {
+    int b1 = pml + 1 - IK, b2x = pml + nx + IK - 2, b2z = pml + nz + IK - 2;
+    for (int sd = 0; sd < 2; sd++) {
+      int K = sd == 0 ? pml - IK : nz + IK + pml - 1;
+      int I = sd == 0 ? K + 1 : K - 1;
+      for (int ix = b1; ix <= b2x; ix++) {
+        REAL v = AT(vel, ix, K);
+        REAL a1 = KR(1.0) / dz / KR(2.0) / dt, a2 = KR(1.0) / KR(2.0) / dt / dt / v;
+        REAL a3 = v / KR(4.0) / dx / dx;
+        REAL sc = AT(u31b, ix, K) * (KR(-1) / (a1 + a2));
+        F(oneway_T)(sc, a1, a2, a3, &AT(u3b, ix, I), &AT(u3b, ix + 1, I), &AT(u3b, ix - 1, I),
+                    &AT(cb, ix, K), &AT(cb, ix, I), &AT(pb, ix, K), &AT(pb, ix, I),
+                    &AT(pb, ix + 1, K), &AT(pb, ix - 1, K));
+      }
+    }
+    for (int sd = 0; sd < 2; sd++) {
+      int K = sd == 0 ? nx + IK + pml - 1 : pml - IK;
+      int I = sd == 0 ? K - 1 : K + 1;
+      for (int iz = b1; iz <= b2z; iz++) {
+        REAL v = AT(vel, K, iz);
+        REAL a1 = KR(1.0) / dx / KR(2.0) / dt, a2 = KR(1.0) / KR(2.0) / dt / dt / v;
+        REAL a3 = v / KR(4.0) / dz / dz;
+        REAL sc = AT(u31b, K, iz) * (KR(-1) / (a1 + a2));
+        F(oneway_T)(sc, a1, a2, a3, &AT(u3b, I, iz), &AT(u3b, I, iz + 1), &AT(u3b, I, iz - 1),
+                    &AT(cb, K, iz), &AT(cb, I, iz), &AT(pb, K, iz), &AT(pb, I, iz),
+                    &AT(pb, K, iz + 1), &AT(pb, K, iz - 1));
+      }
+    }
+    {
+      int xr = nx + pml + IK - 1, xl = pml - IK, zd = nz + pml + IK - 1, zu = pml - IK;
+      int cxs[4] = {xr, xl, xr, xl}, czs[4] = {zd, zd, zu, zu};
+      int dxs[4] = {-1, +1, -1, +1}, dzs[4] = {-1, -1, +1, +1};
+      REAL ax1 = KR(1.0) / dz, ax2 = KR(1.0) / dx;
+      for (int k = 0; k < 4; k++) {
+        int x = cxs[k], z = czs[k];
+        REAL v = AT(vel, x, z);
+        REAL ax3 = k == 3 ? (REAL)(sqrt(2.0) / (double)v / (double)dt) : SQRTR(KR(2.0)) / v / dt;
+        REAL sc = AT(u31b, x, z) * (KR(-1) / (ax1 + ax2 + ax3));
+        AT(u3b, x, z + dzs[k]) += sc * (-ax1);
+        AT(u3b, x + dxs[k], z) += sc * (-ax2);
+        AT(cb, x, z) += sc * (-ax3);
+      }
+    }
+  }
+}
+
+/* transposed 1-D second difference term (v v k)((a+b) - 2c) scaled by e */
+static void F(d2_T)(REAL e, REAL v, REAL k, REAL *a, REAL *b, REAL *cc)
+{
+  REAL t = v * v * k * e;
+  *a += t;
+  *b += t;
+  *cc += KR(-2) * t;
+}
+
+/* transpose of the frame (fd.cpp:1057-1091): scatter u3b of frame cells */
+static void F(frame_T)(const F(grid_t) *g, const F(coefs_t) *c, const REAL *u3b, REAL *cb,
+                       REAL *pb)
+{
+  const int NX = g->NX, NZ = g->NZ;
+  const REAL *vel = c->vel;
+  REAL dt2 = g->dt * g->dt;
+  REAL kx = (KR(1.0) / g->dx) * (KR(1.0) / g->dx) * dt2;
+  REAL kz = (KR(1.0) / g->dz) * (KR(1.0) / g->dz) * dt2;
+  /* base terms */
+  for (int ix = 1; ix <= NX - 2; ix++) {
+    int e[2] = {0, NZ - 1};
+    for (int sd = 0; sd < 2; sd++) {
+      int iz = e[sd];
+      REAL ub = AT(u3b, ix, iz);
+      F(d2_T)(ub, AT(vel, ix, iz), kx, &AT(cb, ix + 1, iz), &AT(cb, ix - 1, iz), &AT(cb, ix, iz));
+      AT(cb, ix, iz) += KR(2) * ub;
+      AT(pb, ix, iz) -= ub;
+    }
+  }
+  for (int iz = 1; iz <= NZ - 2; iz++) {
+    REAL ub = AT(u3b, 0, iz);
+    F(d2_T)(ub, AT(vel, 0, iz), kz, &AT(cb, 0, iz + 1), &AT(cb, 0, iz - 1), &AT(cb, 0, iz));
+    AT(cb, 0, iz) += KR(2) * ub;
+    AT(pb, 0, iz) -= ub;
+    ub = AT(u3b, NX - 1, iz);
+    F(d2_T)(ub, AT(vel, NX - 1, iz), kx, &AT(cb, NX - 1, iz + 1), &AT(cb, NX - 1, iz - 1),
+            &AT(cb, NX - 1, iz));
+    AT(cb, NX - 1, iz) += KR(2) * ub;
+    AT(pb, NX - 1, iz) -= ub;
+  }
+  {
+    int cxs[4] = {0, 0, NX - 1, NX - 1}, czs[4] = {0, NZ - 1, 0, NZ - 1};
+    for (int k = 0; k < 4; k++) {
+      REAL ub = AT(u3b, cxs[k], czs[k]);
+      AT(cb, cxs[k], czs[k]) += KR(2) * ub;
+      AT(pb, cxs[k], czs[k]) -= ub;
+    }
+  }
+  /* normal extrapolation terms: u3 += 2 y1 - y2 */
+  for (int ix = 0; ix < NX; ix++) {
+    REAL ub = AT(u3b, ix, 0);
+    F(d2_T)(KR(2) * ub, AT(vel, ix, 1), kz, &AT(cb, ix, 2), &AT(cb, ix, 0), &AT(cb, ix, 1));
+    F(d2_T)(-ub, AT(vel, ix, 2), kz, &AT(cb, ix, 3), &AT(cb, ix, 1), &AT(cb, ix, 2));
+    ub = AT(u3b, ix, NZ - 1);
+    F(d2_T)(KR(2) * ub, AT(vel, ix, NZ - 2), kz, &AT(cb, ix, NZ - 3), &AT(cb, ix, NZ - 1),
+            &AT(cb, ix, NZ - 2));
+    F(d2_T)(-ub, AT(vel, ix, NZ - 3), kz, &AT(cb, ix, NZ - 4), &AT(cb, ix, NZ - 2),
+            &AT(cb, ix, NZ - 3));
+  }
+  for (int iz = 0; iz < NZ; iz++) {
+    REAL ub = AT(u3b, 0, iz);
+    F(d2_T)(KR(2) * ub, AT(vel, 1, iz), kx, &AT(cb, 2, iz), &AT(cb, 0, iz), &AT(cb, 1, iz));
+    F(d2_T)(-ub, AT(vel, 2, iz), kx, &AT(cb, 3, iz), &AT(cb, 1, iz), &AT(cb, 2, iz));
+    ub = AT(u3b, NX - 1, iz);
+    F(d2_T)(KR(2) * ub, AT(vel, NX - 2, iz), kx, &AT(cb, NX - 3, iz), &AT(cb, NX - 1, iz),
+            &AT(cb, NX - 2, iz));
+    F(d2_T)(-ub, AT(vel, NX - 3, iz), kx, &AT(cb, NX - 4, iz), &AT(cb, NX - 2, iz),
+            &AT(cb, NX - 3, iz));
+  }
+}
+
+/* transpose of the two-way stencil on [1,n-2]^2 (fd.cpp:1226-1271) */
+static void F(twoway_T)(const F(grid_t) *g, const F(coefs_t) *c, const REAL *u3b, REAL *cb,
+                        REAL *pb)
+{
+  static const REAL a[9] = {KR(-1.0) / KR(560.0), KR(8.0) / KR(315.0), KR(-1.0) / KR(5.0),
+                            KR(8.0) / KR(5.0),    KR(-205.0) / KR(72.0), KR(8.0) / KR(5.0),
+                            KR(-1.0) / KR(5.0),   KR(8.0) / KR(315.0), KR(-1.0) / KR(560.0)};
+  const int NX = g->NX, NZ = g->NZ;
+  for (int ix = 1; ix <= NX - 2; ix++)
+    for (int iz = 1; iz <= NZ - 2; iz++) {
+      REAL ub = AT(u3b, ix, iz);
+      REAL vz = AT(c->vvzz, ix, iz) * ub, vx = AT(c->vvxx, ix, iz) * ub;
+      int high = ix >= 4 && ix <= NX - 5 && iz >= 4 && iz <= NZ - 5;
+      if (high) {
+        for (int k = 0; k < 9; k++) {
+          AT(cb, ix, iz - 4 + k) += a[k] * vz;
+          AT(cb, ix - 4 + k, iz) += a[k] * vx;
+        }
+      } else {
+        AT(cb, ix, iz - 1) += vz;
+        AT(cb, ix, iz + 1) += vz;
+        AT(cb, ix, iz) += KR(-2) * vz;
+        AT(cb, ix + 1, iz) += vx;
+        AT(cb, ix - 1, iz) += vx;
+        AT(cb, ix, iz) += KR(-2) * vx;
+      }
+      AT(cb, ix, iz) += KR(2) * ub;
+      AT(pb, ix, iz) -= ub;
+    }
+}
+
+/* Transpose of one forward step: from yb (adjoint of the new field) add the
+ * adjoints of the current field (cb) and of the previous one (pb); u3b gets
+ * the adjoint of the two-way value before the blend (where sources enter). */
+static void F(step_T)(const F(grid_t) *g, const F(coefs_t) *c, const REAL *yb, REAL *cb, REAL *pb,
+                      REAL *u3b, REAL *u31b)
+{
+  size_t n = (size_t)g->NX * g->NZ;
+  for (size_t i = 0; i < n; i++) {
+    u3b[i] = yb[i] * c->w[i];
+    u31b[i] = yb[i] * (KR(1.0) - c->w[i]);
+  }
+  /* u31 of non-ring cells never reaches the output (w = 1 there) */
+  F(rings_T)(g, c, u31b, u3b, cb, pb);
+  F(frame_T)(g, c, u3b, cb, pb);
+  F(twoway_T)(g, c, u3b, cb, pb);
+}
+
+/* Exact adjoint of orc_born: img[nx][nz] = L^T rec. */
+int F(orc_born_adjoint)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml,
+                        int sx, int sz, const int *gz, const REAL *wav, const REAL *vel,
+                        const REAL *rec, REAL *img)
+{
+  F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  F(coefs_t) c;
+  F(coefs_init)(g, vel, &c, 1);
+  size_t n = (size_t)g->NX * g->NZ;
+  int sxp = sx + pml, szp = sz + pml, NT = nt + ndel;
+  REAL idt2 = KR(1.0) / dt / dt;
+  /* background pass, keeping lap_k of every step (small problems only) */
+  REAL *laps = F(zalloc)(n * (size_t)NT);
+  if (!laps) return -1;
+  REAL *u0 = F(zalloc)(n), *u1 = F(zalloc)(n), *u2 = F(zalloc)(n);
+  for (int it = 0; it < NT; it++) {
+    F(twoway)(g, &c, u1, u0, u2);
+    if (it >= 1) AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+    F(absorb)(g, &c, u2, u1, u0);
+    for (size_t i = 0; i < n; i++) laps[(size_t)it * n + i] = (u2[i] + u0[i] - KR(2) * u1[i]) * idt2;
+    REAL *t = u0; u0 = u1; u1 = u2; u2 = t;
+  }
+  /* reverse sweep: A = adjoint of x_{k+1}, B of x_k, C of x_{k-1} */
+  REAL *A = u0, *B = u1, *C = u2;
+  memset(A, 0, n * sizeof(REAL)); memset(B, 0, n * sizeof(REAL)); memset(C, 0, n * sizeof(REAL));
+  REAL *u3b = F(zalloc)(n), *u31b = F(zalloc)(n), *gp = F(zalloc)(n);
+  for (int k = NT - 1; k >= 0; k--) {
+    if (k >= ndel)
+      for (int ix = 0; ix < nx; ix++) AT(A, ix + pml, gz[ix] + pml) += rec[(size_t)ix * nt + (k - ndel)];
+    F(step_T)(g, &c, A, B, C, u3b, u31b);
+    const REAL *lap = laps + (size_t)k * n;
+    for (size_t i = 0; i < n; i++) gp[i] += lap[i] * u3b[i];
+    REAL *t = A; A = B; B = C; C = t;
+    memset(C, 0, n * sizeof(REAL));
+  }
+  for (int ix = 0; ix < nx; ix++)
+    for (int iz = 0; iz < nz; iz++) {
+      int jx = ix + pml, jz = iz + pml;
+      img[(size_t)ix * nz + iz] = AT(c.vt2, jx, jz) * AT(c.vel3, jx, jz) * AT(gp, jx, jz);
+    }
+  free(laps); free(u0); free(u1); free(u2); free(u3b); free(u31b); free(gp);
+  F(coefs_free)(&c);
+  return 0;
+}
+
 #undef AT
 #undef KR
 #undef F

@@ -101,6 +101,10 @@ def lib():
         L.seis_fd_plan_launches_per_run.argtypes = [P]
         L.seis_fd_plan_launches_per_run.restype = ctypes.c_int64
         L.seis_fd_plan_set_exact.argtypes = [P, I]
+        L.seis_fd_plan_set_snapshots.argtypes = [P, I, I]
+        L.seis_fd_plan_device_bytes.argtypes = [P]
+        L.seis_fd_plan_device_bytes.restype = ctypes.c_int64
+        L.seis_fd_born_adjoint.argtypes = [P, SD, P, P, P, P]
         L.seis_fd_plan_time_kernels.argtypes = [P, I, ctypes.POINTER(ctypes.c_double),
                                                 ctypes.POINTER(ctypes.c_double)]
         PP = ctypes.POINTER(P)
@@ -177,7 +181,8 @@ def validate_shot(shot: "Shot") -> str:
     return "" if rc == SEIS_OK else (buf.value.decode() or f"error {rc}")
 
 
-OP_MODELING, OP_BORN, OP_RTM = 0, 1, 2
+OP_MODELING, OP_BORN, OP_RTM, OP_BORN_ADJOINT = 0, 1, 2, 3
+SNAP_F32, SNAP_BF16, SNAP_F16 = 1, 2, 3
 IN_VEL, IN_DV, IN_WAVELET, IN_GATHER = 0, 1, 2, 3
 OUT_GATHER, OUT_IMAGE = 0, 1
 
@@ -225,6 +230,13 @@ class Plan:
         self.ctx.check(self.ctx.L.seis_fd_plan_get(self.h, shot, what, ptr(out)))
         return out
 
+    def set_snapshots(self, every: int = 1, dtype: int = 1):
+        self.ctx.check(self.ctx.L.seis_fd_plan_set_snapshots(self.h, every, dtype))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.ctx.L.seis_fd_plan_device_bytes(self.h))
+
     def set_exact(self, exact: bool):
         self.ctx.check(self.ctx.L.seis_fd_plan_set_exact(self.h, 1 if exact else 0))
 
@@ -246,6 +258,12 @@ class Plan:
         if getattr(self, "h", None):
             self.ctx.L.seis_fd_plan_destroy(self.h)
             self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def __del__(self):
         try:

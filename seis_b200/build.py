@@ -29,6 +29,8 @@ NVCC_EXACT = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true"]
 # fast flavour (sources named *_fast.cu): contraction and approximate division,
 # denormals still kept (the decaying wavefield lives there)
 NVCC_FAST = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"]
+# accurate flavour (sources named *_acc.cu): contraction, IEEE division / sqrt
+NVCC_ACC = ["--fmad=true", "-prec-div=true", "-prec-sqrt=true"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
 
 
@@ -75,7 +77,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if not force and not _stale(obj, [src] + headers + [__file__]):
             continue
         if src.endswith(".cu"):
-            flav = NVCC_FAST if src.endswith("_fast.cu") else NVCC_EXACT
+            flav = (NVCC_FAST if src.endswith("_fast.cu")
+                    else NVCC_ACC if src.endswith("_acc.cu") else NVCC_EXACT)
             cmd = [nvcc, *ARCH, *NVCC_COMMON, *flav, "-I", CSRC, "-I", INCLUDE, "-c", "-o", obj, src]
         else:
             cmd = ["g++", *CXX_FLAGS, "-I", CSRC, "-I", INCLUDE, "-I", _cuda_include(), "-c", "-o", obj, src]

@@ -1,0 +1,379 @@
+// Exact adjoint of the Born operator (sm_100a).  No counterpart in the
+// reference: its adjoint() (src/util/fd.cpp:592-719) is a different imaging
+// operator and fails the dot-product test.
+//
+// One forward step maps (cur, prev) to next through
+//   u3  = S(cur, prev)                 two-way update + frame  fd.cpp:1057-1091, :1226-1271
+//   u31 = P(u3, cur, prev)             one-way update on the pad rings  :1092-1179
+//   nxt = w u3 + (1 - w) u31           blend  :55-56
+// and the scattering source enters u3.  With Lk the complete adjoint of the
+// field of step k, one reverse step computes
+//   mu(L)  = w L + P_u3^T ((1-w) L)          (adjoint of u3: where sources enter)
+//   L_k    = S_cur^T mu(L_{k+1}) + P_cur^T((1-w) L_{k+1})
+//          - mu(L_{k+2}) + P_prev^T((1-w) L_{k+2}) + R^T d_{k-1-ndel}
+// and images grad += w_img * lap_k * mu(L_{k+1}) on the model interior
+// (lap_k = source-field second time derivative from the snapshots).
+//
+// Interior tiles (tile + 4-cell halo strictly inside the model, no cell read
+// by the one-way update) reduce to the symmetric gather
+//   L_k = Lz(vz L1) + Lx(vx L1) + 2 L1 - L2 + R^T d.
+// Pad tiles run the transposed stages in scatter form over every consumer cell
+// of the tile + 5-cell halo, accumulating with shared-memory atomics; only the
+// contributions that land on the tile are kept.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#include "fd_tile.cuh"
+
+namespace seis {
+namespace SEIS_NS {
+
+constexpr int A_NT_I = 256;  // interior adjoint kernel threads
+constexpr int A_NT_P = 512;  // pad adjoint kernel threads
+constexpr int WIDE = CW_C * SR, NARROW = CW_P * SR;
+constexpr int MU_C = TX + 8, MU_R = TZ + 8;  // mu on tile + 4 halo
+
+__device__ __forceinline__ float snap_load(const ShotDev &g, int k, int x, int z) {
+  size_t i = (size_t)k * g.nx * g.nz + (size_t)x * g.nz + z;
+  switch (g.snap_dtype) {
+    case SNAP_F32: return reinterpret_cast<const float *>(g.snap)[i];
+    case SNAP_BF16: return __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(g.snap)[i]);
+    case SNAP_F16: return __half2float(reinterpret_cast<const __half *>(g.snap)[i]);
+    default: return 0.0f;
+  }
+}
+
+__device__ __forceinline__ float snap_inv_scale(const ShotDev &g, int k, int x0, int z0) {
+  if (g.snap_dtype == SNAP_F32) return 1.0f;
+  const int ntx = (g.NX + TX - 1) / TX;
+  return 1.0f / g.snap_scale[(size_t)k * ntx * g.ntz + (x0 / TX) * g.ntz + z0 / TZ];
+}
+
+// Coefficients of the one-way update of a pad-ring cell, as the linear map
+// u31 = sum coef * input (fd.cpp:1098-1104, :1146-1178).
+struct RingCoef {
+  int corner;         // 1: diagonal corner
+  int nx_, nz_;       // unit step toward the interior (inner neighbour offset)
+  int tx_, tz_;       // unit tangential step (strips)
+  float au3i, au3t;   // coefficients of u3 at inner, inner +- tangential
+  float bK, bi;       // of cur at the cell, at inner
+  float gK, gi, gt;   // of prev at the cell, inner, cell +- tangential
+  float cz, cx;       // corners: of u3 at the z-inner and x-inner neighbours
+};
+
+template <class VA>
+__device__ __forceinline__ RingCoef ring_coef(const ShotDev &g, const VA &V, int ix, int iz,
+                                              const PadPos &pp) {
+  RingCoef r;
+  float v = V(ix, iz);
+  if (pp.distx == pp.ring && pp.distz == pp.ring) {
+    r.corner = 1;
+    r.nx_ = pp.dl > 0 ? 1 : -1;
+    r.nz_ = pp.du > 0 ? 1 : -1;
+    r.tx_ = r.tz_ = 0;
+    float ax3;
+    if (pp.dl > 0 && pp.du > 0)
+      ax3 = __double2float_rn(g.sqrt2d / (double)v / (double)g.dt);
+    else
+      ax3 = g.sqrt2f / v / g.dt;
+    float e = g.ax1 + g.ax2 + ax3;
+    r.cz = g.ax1 / e;
+    r.cx = g.ax2 / e;
+    r.bK = ax3 / e;
+    r.au3i = r.au3t = r.bi = r.gK = r.gi = r.gt = 0.0f;
+    return r;
+  }
+  r.corner = 0;
+  float a1, a3;
+  if (pp.distz == pp.ring) {  // top / bottom strip
+    r.nx_ = 0; r.nz_ = pp.du > 0 ? 1 : -1;
+    r.tx_ = 1; r.tz_ = 0;
+    a1 = g.a1z;
+    a3 = v / 4.0f / g.dx / g.dx;
+  } else {  // left / right strip
+    r.nx_ = pp.dl > 0 ? 1 : -1; r.nz_ = 0;
+    r.tx_ = 0; r.tz_ = 1;
+    a1 = g.a1x;
+    a3 = v / 4.0f / g.dz / g.dz;
+  }
+  float a2 = g.hdt2 / v;
+  float d = a1 + a2;
+  // u31 = -tmp / d, tmp as in fd.cpp:1101-1103
+  r.au3i = (a1 - a2 - 2.0f * a3) / d;
+  r.au3t = a3 / d;
+  r.bK = 2.0f * a2 / d;
+  r.bi = 2.0f * a2 / d;
+  r.gK = (a1 - a2 - 2.0f * a3) / d;
+  r.gi = -(a1 + a2) / d;
+  r.gt = a3 / d;
+  r.cz = r.cx = 0.0f;
+  return r;
+}
+
+struct AdjTile {  // accumulator over a rectangular window of the grid
+  float *s;
+  int x0, z0, ncol, nrow;  // window origin and size
+  __device__ __forceinline__ bool in(int ix, int iz) const {
+    return ix >= x0 && ix < x0 + ncol && iz >= z0 && iz < z0 + nrow;
+  }
+  __device__ __forceinline__ void add(int ix, int iz, float v) const {
+    if (in(ix, iz)) atomicAdd(&s[(ix - x0) * nrow + (iz - z0)], v);
+  }
+  __device__ __forceinline__ float get(int ix, int iz) const {
+    return s[(ix - x0) * nrow + (iz - z0)];
+  }
+};
+
+// Scatter of the transposed two-way update and frame of consumer cell (ix,iz)
+// with adjoint mu into cb (mirrors fd.cpp:1057-1091 and :1226-1271).
+template <class VA>
+__device__ void stencil_T(const ShotDev &g, const VA &V, int ix, int iz, float mu,
+                          const AdjTile &cb) {
+  const int NX = g.NX, NZ = g.NZ;
+  bool fx = (ix == 0 || ix == NX - 1), fz = (iz == 0 || iz == NZ - 1);
+  auto d2T = [&](float e, float v, float k, int ax, int az, int bx, int bz, int cx_, int cz_) {
+    float t = v * v * k * e;
+    cb.add(ax, az, t);
+    cb.add(bx, bz, t);
+    cb.add(cx_, cz_, -2.0f * t);
+  };
+  if (fx || fz) {
+    if (!(fx && fz)) {
+      if (fz)
+        d2T(mu, V(ix, iz), g.kx, ix + 1, iz, ix - 1, iz, ix, iz);
+      else
+        d2T(mu, V(ix, iz), ix == 0 ? g.kz : g.kx, ix, iz + 1, ix, iz - 1, ix, iz);
+    }
+    cb.add(ix, iz, 2.0f * mu);
+    if (fz) {
+      int s1 = iz == 0 ? 1 : NZ - 2, s2 = iz == 0 ? 2 : NZ - 3, dz = iz == 0 ? 1 : -1;
+      d2T(2.0f * mu, V(ix, s1), g.kz, ix, s1 + dz, ix, s1 - dz, ix, s1);
+      d2T(-mu, V(ix, s2), g.kz, ix, s2 + dz, ix, s2 - dz, ix, s2);
+    }
+    if (fx) {
+      int s1 = ix == 0 ? 1 : NX - 2, s2 = ix == 0 ? 2 : NX - 3, dx = ix == 0 ? 1 : -1;
+      d2T(2.0f * mu, V(s1, iz), g.kx, s1 + dx, iz, s1 - dx, iz, s1, iz);
+      d2T(-mu, V(s2, iz), g.kx, s2 + dx, iz, s2 - dx, iz, s2, iz);
+    }
+    return;
+  }
+  Coef k = coef(V(ix, iz), g);
+  float vz = k.vz * mu, vx = k.vx * mu;
+  if (ix >= 4 && ix <= NX - 5 && iz >= 4 && iz <= NZ - 5) {
+    const float a[9] = {SEIS_C0, SEIS_C1, SEIS_C2, SEIS_C3, SEIS_C4, SEIS_C3, SEIS_C2, SEIS_C1, SEIS_C0};
+#pragma unroll
+    for (int m = 0; m < 9; m++) {
+      cb.add(ix, iz - 4 + m, a[m] * vz);
+      cb.add(ix - 4 + m, iz, a[m] * vx);
+    }
+  } else {
+    cb.add(ix, iz - 1, vz);
+    cb.add(ix, iz + 1, vz);
+    cb.add(ix + 1, iz, vx);
+    cb.add(ix - 1, iz, vx);
+    cb.add(ix, iz, -2.0f * vz - 2.0f * vx);
+  }
+  cb.add(ix, iz, 2.0f * mu);
+}
+
+// ---------------------------------------------------------------- interior
+// L_k = Lz(vz L1) + Lx(vx L1) + 2 L1 - L2 + R^T d ; grad += w lap L1.
+__global__ void __launch_bounds__(A_NT_I, 2) adj_interior_kernel(const ShotDev *__restrict__ shots,
+                                                                 const Tile *__restrict__ tiles,
+                                                                 StepArgs a, int *__restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float *sL1 = reinterpret_cast<float *>(smraw);  // wide
+  float *sV = sL1 + WIDE;                          // wide
+  float *sL2 = sV + WIDE;                          // narrow
+  float *sWZ = sL2 + NARROW;                       // wide
+  float *sWX = sWZ + WIDE;                         // wide
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sWX + WIDE);
+  const int tid = threadIdx.x;
+  const Tile t = tiles[blockIdx.x];
+  __shared__ ShotDev sg;
+  if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+    reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const ShotDev &g = sg;
+  const int x0 = t.x0, z0 = t.z0;
+  if (tid == 0) {
+    fence_proxy_async();
+    mbar_expect_tx(bar, (uint32_t)((2 * WIDE + NARROW) * sizeof(float)));
+    tma_load_2d(sL1, g.maps + MAP_FA_WIDE + (a.rot + 1) % 3, z0, x0 + XM - HXC, bar);
+    tma_load_2d(sV, g.maps + MAP_VEL_WIDE, z0, x0 + XM - HXC, bar);
+    tma_load_2d(sL2, g.maps + MAP_FA_NARROW + a.rot % 3, z0, x0 + XM - 1, bar);
+  }
+  if (!mbar_wait(bar, 0)) {
+    if (tid == 0) atomicExch(err, 2);
+    return;
+  }
+  // weighted fields vz L1, vx L1 on the staged window
+  for (int i = tid; i < WIDE; i += A_NT_I) {
+    Coef k = coef(sV[i], g);
+    float l = sL1[i];
+    sWZ[i] = k.vz * l;
+    sWX[i] = k.vx * l;
+  }
+  __syncthreads();
+  const int zm = z0 - ZM;
+  const SA L1{sL1, x0 - HXC, zm}, WZ{sWZ, x0 - HXC, zm}, WX{sWX, x0 - HXC, zm};
+  const SA L2{sL2, x0 - 1, zm};
+  const int qz = tid % QZ, cx = tid / QZ;
+  const int ix = x0 + 2 * cx, iz0 = z0 + 4 * qz;
+  float *out = g.fa[(a.rot + 2) % 3];
+  float4 xm[10];
+#pragma unroll
+  for (int m = 0; m < 10; m++) xm[m] = WX.quad(ix - 4 + m, iz0);
+  const bool img = a.snap_k >= 0 && g.snap != nullptr;
+  float inv_scale = img ? snap_inv_scale(g, a.snap_k, x0, z0) : 0.0f;
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const float4 za = WZ.quad(ix + j, iz0 - 4), zb = WZ.quad(ix + j, iz0), zc = WZ.quad(ix + j, iz0 + 4);
+    const float zz[12] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w, zc.x, zc.y, zc.z, zc.w};
+    const float4 l1 = L1.quad(ix + j, iz0), l2 = L2.quad(ix + j, iz0);
+    const int x = ix + j - g.pml;
+    const int gzr = g.gz[x] + g.pml;
+    float4 o;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      float sz_ = lap8(zz[r], zz[r + 1], zz[r + 2], zz[r + 3], zz[r + 4], zz[r + 5], zz[r + 6],
+                       zz[r + 7], zz[r + 8]);
+      float sx_ = lap8(comp(xm[j], r), comp(xm[j + 1], r), comp(xm[j + 2], r), comp(xm[j + 3], r),
+                       comp(xm[j + 4], r), comp(xm[j + 5], r), comp(xm[j + 6], r),
+                       comp(xm[j + 7], r), comp(xm[j + 8], r));
+      float v = sz_ + sx_ + 2.0f * comp(l1, r) - comp(l2, r);
+      if (a.rec_k >= 0 && iz0 + r == gzr) v += g.rec[(size_t)a.rec_k * g.nx + x];
+      set_comp(o, r, v);
+      if (img) {
+        const int z = iz0 + r - g.pml;
+        float lap = snap_load(g, a.snap_k, x, z) * inv_scale;
+        g.grad[(size_t)x * g.nz + z] += (double)(a.img_w * lap * comp(l1, r));
+      }
+    }
+    *reinterpret_cast<float4 *>(out + (size_t)(ix + j) * g.LDZ + iz0) = o;
+  }
+}
+
+// ---------------------------------------------------------------- pad tiles
+constexpr size_t ADJ_PAD_SMEM =
+    sizeof(float) * (size_t)(2 * WIDE + NARROW + MU_C * MU_R + 3 * TX * TZ) + 16;
+
+__global__ void __launch_bounds__(A_NT_P, 1) adj_pad_kernel(const ShotDev *__restrict__ shots,
+                                                            const Tile *__restrict__ tiles,
+                                                            StepArgs a, int *__restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float *sL1 = reinterpret_cast<float *>(smraw);  // wide
+  float *sV = sL1 + WIDE;                          // wide
+  float *sL2 = sV + WIDE;                          // narrow
+  float *sMU1 = sL2 + NARROW;                      // tile + 4
+  float *sCB = sMU1 + MU_C * MU_R;                 // tile
+  float *sMU2 = sCB + TX * TZ;                     // tile
+  float *sPB = sMU2 + TX * TZ;                     // tile
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sPB + TX * TZ);
+  const int tid = threadIdx.x;
+  const Tile t = tiles[blockIdx.x];
+  __shared__ ShotDev sg;
+  if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+    reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  for (int i = tid; i < MU_C * MU_R + 3 * TX * TZ; i += A_NT_P) sMU1[i] = 0.0f;
+  __syncthreads();
+  const ShotDev &g = sg;
+  const int x0 = t.x0, z0 = t.z0;
+  if (tid == 0) {
+    fence_proxy_async();
+    mbar_expect_tx(bar, (uint32_t)((2 * WIDE + NARROW) * sizeof(float)));
+    tma_load_2d(sL1, g.maps + MAP_FA_WIDE + (a.rot + 1) % 3, z0, x0 + XM - HXC, bar);
+    tma_load_2d(sV, g.maps + MAP_VEL_WIDE, z0, x0 + XM - HXC, bar);
+    tma_load_2d(sL2, g.maps + MAP_FA_NARROW + a.rot % 3, z0, x0 + XM - 1, bar);
+  }
+  if (!mbar_wait(bar, 0)) {
+    if (tid == 0) atomicExch(err, 2);
+    return;
+  }
+  const int zm = z0 - ZM;
+  const SA L1{sL1, x0 - HXC, zm}, V{sV, x0 - HXC, zm}, L2{sL2, x0 - 1, zm};
+  const AdjTile MU1{sMU1, x0 - 4, z0 - 4, MU_C, MU_R};
+  const AdjTile CB{sCB, x0, z0, TX, TZ}, MU2{sMU2, x0, z0, TX, TZ}, PB{sPB, x0, z0, TX, TZ};
+
+  // blend^T and rings^T of L1 over the consumers in tile + 5, of L2 over tile + 1
+  constexpr int R5C = TX + 10, R5R = TZ + 10;
+  for (int i = tid; i < R5C * R5R; i += A_NT_P) {
+    const int cx = x0 - 5 + i / R5R, cz = z0 - 5 + i % R5R;
+    if (cx < 0 || cx >= g.NX || cz < 0 || cz >= g.NZ) continue;
+    PadPos pp = pad_pos(g, cx, cz);
+    const bool near1 = cx >= x0 - 1 && cx <= x0 + TX && cz >= z0 - 1 && cz <= z0 + TZ;
+    float w = pp.ring == 0 ? 1.0f : pad_weight(g, pp);
+    float l1 = L1(cx, cz);
+    MU1.add(cx, cz, w * l1);
+    float l2 = near1 ? L2(cx, cz) : 0.0f;
+    if (near1) MU2.add(cx, cz, w * l2);
+    if (pp.ring == 0) continue;
+    RingCoef rc = ring_coef(g, V, cx, cz, pp);
+    float n1 = (1.0f - w) * l1, n2 = (1.0f - w) * l2;
+    if (rc.corner) {
+      MU1.add(cx, cz + rc.nz_, rc.cz * n1);
+      MU1.add(cx + rc.nx_, cz, rc.cx * n1);
+      CB.add(cx, cz, rc.bK * n1);
+      if (near1) {
+        MU2.add(cx, cz + rc.nz_, rc.cz * n2);
+        MU2.add(cx + rc.nx_, cz, rc.cx * n2);
+      }
+    } else {
+      const int ix_i = cx + rc.nx_, iz_i = cz + rc.nz_;
+      MU1.add(ix_i, iz_i, rc.au3i * n1);
+      MU1.add(ix_i + rc.tx_, iz_i + rc.tz_, rc.au3t * n1);
+      MU1.add(ix_i - rc.tx_, iz_i - rc.tz_, rc.au3t * n1);
+      CB.add(cx, cz, rc.bK * n1);
+      CB.add(ix_i, iz_i, rc.bi * n1);
+      if (near1) {
+        MU2.add(ix_i, iz_i, rc.au3i * n2);
+        MU2.add(ix_i + rc.tx_, iz_i + rc.tz_, rc.au3t * n2);
+        MU2.add(ix_i - rc.tx_, iz_i - rc.tz_, rc.au3t * n2);
+        PB.add(cx, cz, rc.gK * n2);
+        PB.add(ix_i, iz_i, rc.gi * n2);
+        PB.add(cx + rc.tx_, cz + rc.tz_, rc.gt * n2);
+        PB.add(cx - rc.tx_, cz - rc.tz_, rc.gt * n2);
+      }
+    }
+  }
+  __syncthreads();
+  // stencil^T and frame^T of mu1 over the consumers in tile + 4
+  for (int i = tid; i < MU_C * MU_R; i += A_NT_P) {
+    const int cx = x0 - 4 + i / MU_R, cz = z0 - 4 + i % MU_R;
+    if (cx < 0 || cx >= g.NX || cz < 0 || cz >= g.NZ) continue;
+    float mu = sMU1[i];
+    if (mu != 0.0f) stencil_T(g, V, cx, cz, mu, CB);
+  }
+  __syncthreads();
+  float *out = g.fa[(a.rot + 2) % 3];
+  const bool img = a.snap_k >= 0 && g.snap != nullptr;
+  const float inv_scale = img ? snap_inv_scale(g, a.snap_k, x0, z0) : 0.0f;
+  for (int i = tid; i < TX * TZ; i += A_NT_P) {
+    const int ix = x0 + i / TZ, iz = z0 + i % TZ;
+    if (ix >= g.NX || iz >= g.NZ) continue;
+    const int li = i;  // tile-local index (column-major, TZ rows)
+    float v = sCB[li] + sPB[li] - sMU2[li];
+    const int x = ix - g.pml, z = iz - g.pml;
+    const bool inside = x >= 0 && x < g.nx && z >= 0 && z < g.nz;
+    if (a.rec_k >= 0 && x >= 0 && x < g.nx && iz == g.gz[x] + g.pml)
+      v += g.rec[(size_t)a.rec_k * g.nx + x];
+    out[(size_t)ix * g.LDZ + iz] = v;
+    if (img && inside) {
+      float lap = snap_load(g, a.snap_k, x, z) * inv_scale;
+      g.grad[(size_t)x * g.nz + z] += (double)(a.img_w * lap * MU1.get(ix, iz));
+    }
+  }
+}
+
+}  // namespace SEIS_NS
+}  // namespace seis

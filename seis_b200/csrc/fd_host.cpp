@@ -33,14 +33,22 @@ struct seis_fd_ctx {
   cudaStream_t aux = nullptr;     // boundary tiles run here, joined every step
   cudaEvent_t fork = nullptr, join = nullptr;
   int *d_err = nullptr;  // set by kernels whose bounded waits ran out
+  std::vector<seis_fd_plan *> plans;  // live plans, torn down with the context
   int num_sms = 148;
   std::string err;
   int64_t launches = 0;
 };
 
 namespace {
+struct Plan;
+}
+struct seis_fd_plan {
+  Plan *p;  // null once the owning context is destroyed
+};
 
-enum Op { OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2 };
+namespace {
+
+enum Op { OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2, OP_BORN_ADJ = 3 };
 
 int fail(seis_fd_ctx *ctx, int code, const char *fmt, ...) {
   char buf[512];
@@ -99,6 +107,12 @@ struct Plan {
   std::vector<ShotDev> sd;
   std::vector<Tile> tiles;  // interior tiles first (n_int), then pad tiles
   int n_int = 0, n_pad = 0;
+  std::vector<Tile> adj_tiles;  // adjoint classification (stricter interior)
+  int n_int_adj = 0, n_pad_adj = 0;
+  Tile *d_adj_tiles = nullptr;
+  int snap_every = 1, snap_dtype = SNAP_F32;
+  bool snaps_ready = false;
+  int64_t device_bytes = 0;
   std::vector<int2> cols;
   std::vector<float *> field_bases;  // allocation starts of margin-padded fields
   std::vector<size_t> field_elems;
@@ -132,6 +146,7 @@ struct Plan {
                   "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
     }
     allocs.push_back(q);
+    device_bytes += (int64_t)(std::max<size_t>(n, 1) * sizeof(T));
     *p = static_cast<T *>(q);
     e = cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), ctx->stream);
     if (e != cudaSuccess) return fail(ctx, SEIS_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
@@ -205,6 +220,29 @@ void build_tiles(Plan &p) {
   p.n_pad = (int)p.tiles.size() - p.n_int;
 }
 
+// Tiles for the exact adjoint: interior tiles need their 4-cell halo strictly
+// inside the model and away from the cells the one-way update reads (the model
+// edge rows and columns), so that the adjoint there is the symmetric gather.
+void build_adj_tiles(Plan &p) {
+  std::vector<Tile> in_t, pad_t;
+  for (int s = 0; s < p.nshot; s++) {
+    const ShotDev &g = p.sd[s];
+    int lox = g.pml + 1 + 4, hix = g.pml + g.nx - 2 - 4;  // inclusive bounds of tile cells
+    int loz = g.pml + 1 + 4, hiz = g.pml + g.nz - 2 - 4;
+    lox = std::max(lox, 8); loz = std::max(loz, 8);
+    hix = std::min(hix, g.NX - 9); hiz = std::min(hiz, g.NZ - 9);
+    for (int x0 = 0; x0 < g.NX; x0 += TX)
+      for (int z0 = 0; z0 < g.NZ; z0 += TZ) {
+        bool in = x0 >= lox && x0 + TX - 1 <= hix && z0 >= loz && z0 + TZ - 1 <= hiz;
+        (in ? in_t : pad_t).push_back(Tile{s, x0, z0, in ? TILE_INTERIOR : TILE_PAD});
+      }
+  }
+  p.n_int_adj = (int)in_t.size();
+  p.n_pad_adj = (int)pad_t.size();
+  p.adj_tiles = in_t;
+  p.adj_tiles.insert(p.adj_tiles.end(), pad_t.begin(), pad_t.end());
+}
+
 // One field of a shot in the margin-padded layout; returns the cell (0,0)
 // pointer.
 int alloc_field(Plan &p, const ShotDev &g, float **cell0) {
@@ -266,6 +304,7 @@ int encode_maps(Plan &p) {
       if (!rc && g.fb[k]) rc = encode_map(p.ctx, g, g.fb[k], narrow, &m[MAP_FB_NARROW + k]);
     }
     if (!rc) rc = encode_map(p.ctx, g, g.vel, narrow, &m[MAP_VEL]);
+    if (!rc) rc = encode_map(p.ctx, g, g.vel, wide, &m[MAP_VEL_WIDE]);
     if (!rc && g.dv) rc = encode_map(p.ctx, g, g.dv, narrow, &m[MAP_DV]);
     if (rc) return rc;
   }
@@ -314,7 +353,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     p->max_NZ = std::max(p->max_NZ, g.NZ);
     p->stage_elems = std::max(p->stage_elems, std::max((size_t)d.nx * d.nz, (size_t)d.nx * d.nt));
     for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fa[k]);
-    if (op != OP_MODEL)
+    if (op == OP_BORN || op == OP_RTM)
       for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fb[k]);
     float *vel = nullptr, *dv = nullptr, *wav = nullptr, *rec = nullptr;
     int *gzd = nullptr;
@@ -324,7 +363,9 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (rc == SEIS_OK) rc = p->alloc(&rec, (size_t)d.nt * d.nx);
     if (rc == SEIS_OK) rc = p->alloc(&gzd, (size_t)d.nx);
     if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&g.strips, (size_t)d.nt * g.strip_len);
-    if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&g.img, (size_t)d.nx * d.nz);
+    if (rc == SEIS_OK && (op == OP_RTM || op == OP_BORN_ADJ)) rc = p->alloc(&g.img, (size_t)d.nx * d.nz);
+    if (rc == SEIS_OK && op == OP_BORN_ADJ) rc = p->alloc(&g.grad, (size_t)d.nx * d.nz);
+    g.ntz = (g.NZ + TZ - 1) / TZ;
     if (rc == SEIS_OK) {
       g.vel = vel; g.dv = dv; g.wav = wav; g.rec = rec; g.gz = gzd;
       cudaError_t e = cudaMemcpyAsync(gzd, d.gz, sizeof(int) * d.nx, cudaMemcpyHostToDevice,
@@ -336,15 +377,20 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
   if (rc == SEIS_OK) rc = encode_maps(*p);
   if (rc == SEIS_OK) {
     build_tiles(*p);
-    int fields = op == OP_MODEL ? 1 : (op == OP_BORN ? 2 : 3);
+    build_adj_tiles(*p);
+    // padded cell-updates of one run: modeling NT, Born 2 NT, reference RTM
+    // NT + 2 nt, exact adjoint NT (source pass) + NT + 1 (reverse pass)
     for (const ShotDev &g : p->sd) {
-      int64_t steps = op == OP_RTM ? (int64_t)g.NT + g.nt : g.NT;
-      int64_t f = op == OP_RTM ? 1 : fields;  // RTM: NT source steps, nt x 2 reverse steps
-      p->cell_updates += (int64_t)g.NX * g.NZ * (op == OP_RTM ? (g.NT + 2LL * g.nt) : steps * f);
+      int64_t per = op == OP_MODEL ? g.NT
+                  : op == OP_BORN  ? 2LL * g.NT
+                  : op == OP_RTM   ? g.NT + 2LL * g.nt
+                                   : 2LL * g.NT + 1;
+      p->cell_updates += (int64_t)g.NX * g.NZ * per;
     }
     rc = p->alloc(&p->d_sd, (size_t)nshot);
   }
   if (rc == SEIS_OK) rc = p->alloc(&p->d_tiles, p->tiles.size());
+  if (rc == SEIS_OK) rc = p->alloc(&p->d_adj_tiles, p->adj_tiles.size());
   if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&p->d_cols, p->cols.size());
   if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&p->d_taps, (size_t)61);
   if (rc == SEIS_OK) {
@@ -353,6 +399,9 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
                                     cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(p->d_tiles, p->tiles.data(), sizeof(Tile) * p->tiles.size(),
+                          cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(p->d_adj_tiles, p->adj_tiles.data(), sizeof(Tile) * p->adj_tiles.size(),
                           cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && op == OP_RTM) {
       e = cudaMemcpyAsync(p->d_cols, p->cols.data(), sizeof(int2) * p->cols.size(),
@@ -390,6 +439,43 @@ int step(Plan &p, int mode, const StepArgs &a) {
   return SEIS_OK;
 }
 
+// Snapshot storage of every shot (first run of an adjoint plan), then the
+// shot table is uploaded again with the new pointers.
+int ensure_snapshots(Plan &p) {
+  if (p.snaps_ready) return SEIS_OK;
+  seis_fd_ctx *ctx = p.ctx;
+  const size_t esize = p.snap_dtype == SNAP_F32 ? 4 : 2;
+  for (int s = 0; s < p.nshot; s++) {
+    ShotDev &g = p.sd[s];
+    int nsnap = (g.NT + p.snap_every - 1) / p.snap_every;
+    int ntx = (g.NX + TX - 1) / TX;
+    unsigned char *snap = nullptr;
+    int rc = p.alloc(&snap, (size_t)nsnap * g.nx * g.nz * esize);
+    if (!rc) rc = p.alloc(&g.snap_scale, (size_t)nsnap * ntx * g.ntz);
+    if (rc) return rc;
+    g.snap = snap;
+    g.snap_dtype = p.snap_dtype;
+    g.snap_every = p.snap_every;
+  }
+  CK(cudaMemcpyAsync(p.d_sd, p.sd.data(), sizeof(ShotDev) * p.nshot, cudaMemcpyHostToDevice,
+                     ctx->stream));
+  p.snaps_ready = true;
+  return SEIS_OK;
+}
+
+// One reverse step of the exact adjoint over the adjoint tile list.
+int adj_step(Plan &p, const StepArgs &a) {
+  seis_fd_ctx *ctx = p.ctx;
+  CK(cudaEventRecord(ctx->fork, ctx->stream));
+  CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
+  CK(fast::launch_adjoint(p.d_sd, p.d_adj_tiles, p.n_int_adj, p.n_pad_adj, a, ctx->d_err,
+                          ctx->stream, ctx->aux));
+  CK(cudaEventRecord(ctx->join, ctx->aux));
+  CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
+  ctx->launches += (p.n_int_adj > 0) + (p.n_pad_adj > 0);
+  return SEIS_OK;
+}
+
 // Zero every wavefield buffer (margins included) and the images.
 int clear_fields(Plan &p) {
   seis_fd_ctx *ctx = p.ctx;
@@ -400,6 +486,7 @@ int clear_fields(Plan &p) {
       if (g.fb[k]) CK(cudaMemsetAsync(g.fb[k] - fg.origin, 0, sizeof(float) * fg.elems, ctx->stream));
     }
     if (g.img) CK(cudaMemsetAsync(g.img, 0, sizeof(float) * g.nx * g.nz, ctx->stream));
+    if (g.grad) CK(cudaMemsetAsync(g.grad, 0, sizeof(double) * g.nx * g.nz, ctx->stream));
   }
   return SEIS_OK;
 }
@@ -412,8 +499,9 @@ int run_forward(Plan &p, int mode) {
     a.rot_b = it;
     a.src_k = it >= 1 ? it - 1 : -1;
     int itp = it - p.ndel;
-    a.rec_k = (p.op != OP_RTM && itp >= 0) ? itp : -1;
+    a.rec_k = (p.op != OP_RTM && p.op != OP_BORN_ADJ && itp >= 0) ? itp : -1;
     a.strip_k = (p.op == OP_RTM && itp >= 0) ? itp : -1;
+    a.snap_k = (p.op == OP_BORN_ADJ && it % p.snap_every == 0) ? it / p.snap_every : -1;
     int rc = step(p, mode, a);
     if (rc) return rc;
   }
@@ -452,6 +540,35 @@ int run_rtm_reverse(Plan &p) {
   return SEIS_OK;
 }
 
+// Reverse pass of the exact adjoint: L_k for k = NT .. 0 from L_{k+1}, L_{k+2};
+// the step producing L_k images the source term of step k with mu(L_{k+1}).
+int run_adjoint(Plan &p) {
+  seis_fd_ctx *ctx = p.ctx;
+  for (const ShotDev &g : p.sd) {
+    FieldGeom fg = field_geom(g.NX, g.NZ);
+    for (int k = 0; k < 3; k++)
+      CK(cudaMemsetAsync(g.fa[k] - fg.origin, 0, sizeof(float) * fg.elems, ctx->stream));
+  }
+  StepArgs a{};
+  a.nshots = p.nshot;
+  a.src_k = -1;
+  a.strip_k = -1;
+  a.img_w = (float)p.snap_every;
+  int r = 0;
+  for (int k = p.NT; k >= 0; k--, r++) {
+    a.rot = r;
+    a.rot_b = r;
+    int kd = k - 1 - p.ndel;
+    a.rec_k = (kd >= 0 && kd < p.nt) ? kd : -1;
+    a.snap_k = (k <= p.NT - 1 && k % p.snap_every == 0) ? k / p.snap_every : -1;
+    int rc = adj_step(p, a);
+    if (rc) return rc;
+  }
+  CK(launch_finalize_image(p.d_sd, p.nshot, ctx->stream));
+  ctx->launches++;
+  return SEIS_OK;
+}
+
 // The whole operator as a stream of launches (captured into a graph by
 // plan_run).
 int enqueue_operator(Plan &p) {
@@ -463,6 +580,10 @@ int enqueue_operator(Plan &p) {
     case OP_RTM:
       rc = run_forward(p, MODE_MODEL);
       return rc ? rc : run_rtm_reverse(p);
+    case OP_BORN_ADJ:
+      rc = ensure_snapshots(p);
+      if (!rc) rc = run_forward(p, MODE_MODEL);
+      return rc ? rc : run_adjoint(p);
   }
   return fail(p.ctx, SEIS_ERR_NOTSUP, "unknown operator %d", p.op);
 }
@@ -470,13 +591,26 @@ int enqueue_operator(Plan &p) {
 int plan_run(Plan &p) {
   seis_fd_ctx *ctx = p.ctx;
   if (!p.exec) {
+    // everything that allocates happens before the capture
+    if (p.op == OP_BORN_ADJ) {
+      int rc0 = ensure_snapshots(p);
+      if (rc0) return rc0;
+      CK(cudaStreamSynchronize(ctx->stream));
+    }
     int64_t before = ctx->launches;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_operator(p);
+    if (rc) {
+      // rejoin the auxiliary stream so that it leaves the capture with the
+      // main stream (an unjoined fork would keep it capturing)
+      cudaEventRecord(ctx->join, ctx->aux);
+      cudaStreamWaitEvent(ctx->stream, ctx->join, 0);
+    }
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
     if (rc) {
       if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
       return rc;
     }
     CK(e);
@@ -581,6 +715,14 @@ int seis_fd_create(seis_fd_ctx **out, int device) {
 int seis_fd_destroy(seis_fd_ctx *ctx) {
   if (!ctx) return SEIS_OK;
   cudaSetDevice(ctx->device);
+  // plans still alive lose their device state; their handles stay valid for
+  // seis_fd_plan_destroy, every other call on them returns SEIS_ERR_ARG
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (seis_fd_plan *h : ctx->plans) {
+    delete h->p;
+    h->p = nullptr;
+  }
+  ctx->plans.clear();
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->aux) cudaStreamSynchronize(ctx->aux);
   if (ctx->d_err) cudaFree(ctx->d_err);
@@ -599,9 +741,6 @@ int64_t seis_fd_launch_count(const seis_fd_ctx *ctx) { return ctx ? ctx->launche
 void *seis_fd_stream(const seis_fd_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 // ---------------------------------------------------------------- plans
-struct seis_fd_plan {
-  Plan *p;
-};
 
 int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *shots,
                         seis_fd_plan **out) {
@@ -609,7 +748,7 @@ int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_des
   if (rc) return rc;
   if (!out) return fail(ctx, SEIS_ERR_ARG, "out is null");
   *out = nullptr;
-  if (op < SEIS_OP_MODELING || op > SEIS_OP_RTM) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
+  if (op < SEIS_OP_MODELING || op > SEIS_OP_BORN_ADJOINT) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
   Plan *p = nullptr;
   rc = plan_create(ctx, op, nshot, shots, &p);
   if (rc) return rc;
@@ -618,6 +757,7 @@ int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_des
     delete p;
     return fail(ctx, SEIS_ERR_NOMEM, "host allocation failed");
   }
+  ctx->plans.push_back(h);
   *out = h;
   return SEIS_OK;
 }
@@ -628,6 +768,8 @@ int seis_fd_plan_destroy(seis_fd_plan *plan) {
     seis_fd_ctx *ctx = plan->p->ctx;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    auto &v = ctx->plans;
+    v.erase(std::remove(v.begin(), v.end(), plan), v.end());
     delete plan->p;
   }
   delete plan;
@@ -659,7 +801,8 @@ static int plan_input(seis_fd_plan *plan, int shot, int what, const float *src, 
       CK(cudaMemcpyAsync(const_cast<float *>(g.wav), src, sizeof(float) * g.NT, kind, ctx->stream));
       return SEIS_OK;
     case SEIS_IN_GATHER:
-      if (p.op != OP_RTM) return fail(ctx, SEIS_ERR_NOTSUP, "plan takes no gather input");
+      if (p.op != OP_RTM && p.op != OP_BORN_ADJ)
+        return fail(ctx, SEIS_ERR_NOTSUP, "plan takes no gather input");
       CK(cudaMemcpyAsync(p.d_stage, src, sizeof(float) * d.nt * d.nx, kind, ctx->stream));
       CK(launch_transpose(p.d_stage, d.nx, d.nt, g.rec, ctx->stream));
       ctx->launches++;
@@ -691,10 +834,12 @@ int seis_fd_plan_get(seis_fd_plan *plan, int shot, int what, float *h_dst) {
   if (shot < 0 || shot >= p.nshot) return fail(ctx, SEIS_ERR_ARG, "shot=%d of %d", shot, p.nshot);
   if (!h_dst) return fail(ctx, SEIS_ERR_ARG, "null destination");
   if (what == SEIS_OUT_GATHER) {
-    if (p.op == OP_RTM) return fail(ctx, SEIS_ERR_NOTSUP, "RTM plans output images");
+    if (p.op == OP_RTM || p.op == OP_BORN_ADJ)
+      return fail(ctx, SEIS_ERR_NOTSUP, "this plan outputs images");
     rc = download_gather(p, shot, h_dst);
   } else if (what == SEIS_OUT_IMAGE) {
-    if (p.op != OP_RTM) return fail(ctx, SEIS_ERR_NOTSUP, "plan outputs gathers");
+    if (p.op != OP_RTM && p.op != OP_BORN_ADJ)
+      return fail(ctx, SEIS_ERR_NOTSUP, "plan outputs gathers");
     const seis_shot_desc &d = p.desc[shot];
     CK(cudaMemcpyAsync(h_dst, p.sd[shot].img, sizeof(float) * d.nx * d.nz,
                        cudaMemcpyDeviceToHost, ctx->stream));
@@ -772,6 +917,22 @@ int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double 
   return clear_fields(p) ? SEIS_ERR_CUDA : sync(ctx);
 }
 
+int seis_fd_plan_set_snapshots(seis_fd_plan *plan, int every, int dtype) {
+  if (!plan || !plan->p) return SEIS_ERR_ARG;
+  Plan &p = *plan->p;
+  if (p.op != OP_BORN_ADJ) return fail(p.ctx, SEIS_ERR_NOTSUP, "plan keeps no snapshots");
+  if (every < 1 || dtype < SEIS_SNAP_F32 || dtype > SEIS_SNAP_F16)
+    return fail(p.ctx, SEIS_ERR_ARG, "snapshots every=%d dtype=%d", every, dtype);
+  if (p.snaps_ready) return fail(p.ctx, SEIS_ERR_STATE, "snapshots already allocated");
+  p.snap_every = every;
+  p.snap_dtype = dtype;
+  return SEIS_OK;
+}
+
+int64_t seis_fd_plan_device_bytes(const seis_fd_plan *plan) {
+  return plan && plan->p ? plan->p->device_bytes : 0;
+}
+
 int seis_fd_plan_set_exact(seis_fd_plan *plan, int exact) {
   if (!plan || !plan->p) return SEIS_ERR_ARG;
   Plan &p = *plan->p;
@@ -825,6 +986,12 @@ int seis_fd_born(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wa
 int seis_fd_rtm(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
                 const float *h_vel, const float *h_rec, float *h_img) {
   return run_batch(ctx, OP_RTM, 1, shot, &h_wav, SEIS_IN_WAVELET, &h_vel, SEIS_IN_VEL, &h_rec,
+                   SEIS_IN_GATHER, &h_img, SEIS_OUT_IMAGE);
+}
+
+int seis_fd_born_adjoint(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
+                         const float *h_vel, const float *h_rec, float *h_img) {
+  return run_batch(ctx, OP_BORN_ADJ, 1, shot, &h_wav, SEIS_IN_WAVELET, &h_vel, SEIS_IN_VEL, &h_rec,
                    SEIS_IN_GATHER, &h_img, SEIS_OUT_IMAGE);
 }
 

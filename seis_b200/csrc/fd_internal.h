@@ -39,7 +39,8 @@ enum MapIndex : int {
   MAP_FB_NARROW = 9,
   MAP_VEL = 12,
   MAP_DV = 13,
-  NMAPS = 14,
+  MAP_VEL_WIDE = 14,  // velocity with the wide halo (adjoint kernels)
+  NMAPS = 15,
 };
 
 // Device descriptor of one shot in a batch.  Scalars derived from dt/dx/dz are
@@ -68,18 +69,31 @@ struct ShotDev {
   float *strips;         // boundary strips, [nt][strip_len]
   float *img;            // image [nx][nz]
   const CUtensorMap *maps;  // NMAPS tensor maps of this shot (device memory)
+  // source-term snapshots for the adjoint imaging condition: lap of the
+  // background field at every snap_every-th step, interior cells [nx][nz],
+  // stored as snap_dtype with one power-of-two scale per (snapshot, tile)
+  void *snap;
+  float *snap_scale;     // [nsnap][ntile_x * ntile_z]
+  double *grad;          // FP64 imaging accumulator [nx][nz]
+  int snap_dtype;        // SNAP_NONE / SNAP_F32 / SNAP_BF16 / SNAP_F16
+  int snap_every;
+  int ntz;               // tiles along z of this shot (scale indexing)
+  int pad_;
 };
+enum SnapType : int { SNAP_NONE = 0, SNAP_F32 = 1, SNAP_BF16 = 2, SNAP_F16 = 3 };
 static_assert(sizeof(ShotDev) % sizeof(int) == 0 && sizeof(ShotDev) <= 256 * sizeof(int),
               "ShotDev is copied word by word into shared memory");
 
-// Per-launch step arguments.
+// Per-launch step arguments.  Every optional index defaults to -1 (none).
 struct StepArgs {
-  int rot;      // buffers: prev = f[rot%3], cur = f[(rot+1)%3], next = f[(rot+2)%3]
-  int rot_b;    // same for field B
-  int src_k;    // wavelet sample injected at the source (-1: none)
-  int rec_k;    // gather sample recorded (or injected, receiver mode) (-1: none)
-  int strip_k;  // boundary-strip sample saved (-1: none)
-  int nshots;
+  int rot = 0;       // buffers: prev = f[rot%3], cur = f[(rot+1)%3], next = f[(rot+2)%3]
+  int rot_b = 0;     // same for field B
+  int src_k = -1;    // wavelet sample injected at the source
+  int rec_k = -1;    // gather sample recorded (or injected, receiver / adjoint mode)
+  int strip_k = -1;  // boundary-strip sample saved
+  int nshots = 0;
+  int snap_k = -1;   // snapshot index written (forward) or imaged (adjoint)
+  float img_w = 0.f; // adjoint: weight of the imaging term (snapshot interval)
 };
 
 // Allocation geometry of one field of a shot: LDZ floats per column, and the
@@ -101,7 +115,7 @@ inline FieldGeom field_geom(int NX, int NZ) {
   return f;
 }
 
-// Kernel launchers (fd_kernels.cu, fd_stream_*.cu).
+// Kernel launchers (fd_kernels.cu, fd_step_*.cu, fd_adjoint_fast.cu).
 enum StepMode : int {
   MODE_MODEL = 0,    // field A; point source; record; optional strip save
   MODE_RCV = 1,      // field B; receiver injection rec*vt2 (reference RTM)
@@ -126,7 +140,12 @@ cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, i
                         int n_pad, int num_sms, const StepArgs &a, int *d_err, cudaStream_t s_int,
                         cudaStream_t s_pad);
 cudaError_t configure();
+// one reverse step of the exact Born adjoint over the adjoint tile list
+cudaError_t launch_adjoint(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
+                           const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad);
+cudaError_t configure_adjoint();
 }  // namespace fast
+cudaError_t launch_finalize_image(const ShotDev *d_shots, int nshots, cudaStream_t s);
 // Set kernel attributes (shared-memory limits); call once per device.
 cudaError_t configure_kernels();
 cudaError_t launch_pad(const float *d_src, int nx, int nz, int pml, int LDZ, int clamp,

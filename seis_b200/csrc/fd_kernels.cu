@@ -131,11 +131,32 @@ __global__ void rtm_image_kernel(const ShotDev *__restrict__ shots, const int2 *
   }
 }
 
+// Exact adjoint, last step: img = vt2 vel3 grad on the model interior (the
+// scattering source is vt2 lap vel3 dv, fd.cpp:138-139; dv is zero-padded).
+__global__ void finalize_image_kernel(const ShotDev *__restrict__ shots) {
+  const ShotDev &g = shots[blockIdx.y];
+  const int n = g.nx * g.nz;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int x = i / g.nz, z = i - x * g.nz;
+    float v = g.vel[(size_t)(x + g.pml) * g.LDZ + (z + g.pml)];
+    float vt2 = coef(v, g).vt2;
+    float vel3 = 2.0f / (v * v * v);
+    g.img[i] = (float)((double)(vt2 * vel3) * g.grad[i]);
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_finalize_image(const ShotDev *d_shots, int nshots, cudaStream_t s) {
+  dim3 grid(64, nshots);
+  finalize_image_kernel<<<grid, 256, 0, s>>>(d_shots);
+  return cudaGetLastError();
+}
 
 cudaError_t configure_kernels() {
   cudaError_t e = exact::configure();
-  return e == cudaSuccess ? fast::configure() : e;
+  if (e == cudaSuccess) e = fast::configure();
+  return e == cudaSuccess ? fast::configure_adjoint() : e;
 }
 
 cudaError_t launch_step(int mode, bool use_exact, const ShotDev *d_shots, const Tile *d_tiles,

@@ -19,6 +19,8 @@
 // Each thread owns a 4-row x 2-column micro-tile.  Cells are evaluated with
 // the per-cell formulas of fd_cell.cuh.
 #pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
 
 #include "fd_cell.cuh"
@@ -218,6 +220,57 @@ __device__ __forceinline__ float4 col_twoway(const SA &C, const SA &P, const SA 
   return out;
 }
 
+// Write this thread's source-term values (lap of the background field) of
+// snapshot `k`: cells (xs[i], zs[i]) where bit i of `mask` is set.  BF16 / FP16
+// snapshots carry one power-of-two scale per (snapshot, tile), taken from the
+// tile's largest magnitude so that the scaled values lie in [0.5, 1).  Every
+// thread of the CTA calls this (it holds block barriers).
+template <int NTH, int NV>
+__device__ void snap_write(const ShotDev &g, int k, int x0, int z0, const float (&v)[NV],
+                           const int (&xs)[NV], const int (&zs)[NV], unsigned mask, float *red) {
+  float scale = 1.0f;
+  if (g.snap_dtype != SNAP_F32) {
+    float m = 0.0f;
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+      if ((mask >> i) & 1u) m = fmaxf(m, fabsf(v[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = m;
+    __syncthreads();
+    if (warp == 0) {
+      m = lane < NTH / 32 ? red[lane] : 0.0f;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (lane == 0) {
+        int e = 0;
+        frexpf(m, &e);
+        // tiny (denormal) maxima would overflow the scale: clamp to 2^126
+        float sc = m > 0.0f ? ldexpf(1.0f, min(-e, 126)) : 1.0f;
+        red[32] = sc;
+        const int ntx = (g.NX + TX - 1) / TX;
+        g.snap_scale[(size_t)k * ntx * g.ntz + (x0 / TX) * g.ntz + z0 / TZ] = sc;
+      }
+    }
+    __syncthreads();
+    scale = red[32];
+  }
+  const size_t base = (size_t)k * g.nx * g.nz;
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    if (!((mask >> i) & 1u)) continue;
+    const size_t idx = base + (size_t)(xs[i] - g.pml) * g.nz + (zs[i] - g.pml);
+    const float q = v[i] * scale;
+    if (g.snap_dtype == SNAP_F32)
+      reinterpret_cast<float *>(g.snap)[idx] = q;
+    else if (g.snap_dtype == SNAP_BF16)
+      reinterpret_cast<__nv_bfloat16 *>(g.snap)[idx] = __float2bfloat16_rn(q);
+    else
+      reinterpret_cast<__half *>(g.snap)[idx] = __float2half_rn(q);
+  }
+}
+
 // Threads per CTA: interior tiles 256 (4-row x 2-column micro-tiles), pad
 // tiles 512 (4-row x 1-column micro-tiles; more warps to cover the latency of
 // the scalar absorbing-boundary code).
@@ -328,11 +381,16 @@ __global__ void __launch_bounds__(nthreads<KIND>(), KIND == TILE_PAD ? 1 : 2) ti
     }
     const bool record = MODE != MODE_RCV && aa.rec_k >= 0;
 
+    const bool snap = MODE != MODE_RCV && aa.snap_k >= 0 && g.snap != nullptr;
+    __shared__ float red[33];
+    float pout_keep[4] = {0.f, 0.f, 0.f, 0.f};  // pad tiles: this thread's new values
     if (KIND == TILE_INTERIOR) {
       // ---------------- interior tile: every cell 8th order, w = 1
       float4 o[2], cen[2], prv[2], vel[2];
       pair_twoway(CA, PA, VV, g, ix, iz0, o, cen, prv, vel);
       float4 qs[2];
+      float lv[8];
+      int lx[8], lz[8];
 #pragma unroll
       for (int j = 0; j < 2; j++) {
 #pragma unroll
@@ -344,15 +402,21 @@ __global__ void __launch_bounds__(nthreads<KIND>(), KIND == TILE_PAD ? 1 : 2) ti
           if (!BORN && record && iz == gzc[j])
             g.rec[(size_t)aa.rec_k * g.nx + (ix + j - g.pml)] = out;
           if (MODE == MODE_MODEL && aa.strip_k >= 0) save_strips(g, aa.strip_k, ix + j, iz, out);
-          if (BORN) {  // scattering source vt2 lap vel3 dv, fd.cpp:134-139
+          if (BORN || snap) {  // scattering source vt2 lap vel3 dv, fd.cpp:134-139
             float lap = (out + comp(prv[j], r) - 2.0f * comp(cen[j], r)) * g.idt2;
-            float vv = comp(vel[j], r);
-            float vel3 = 2.0f / (vv * vv * vv);
-            set_comp(qs[j], r, kk.vt2 * lap * vel3 * DV(ix + j, iz));
+            lv[4 * j + r] = lap;
+            lx[4 * j + r] = ix + j;
+            lz[4 * j + r] = iz;
+            if (BORN) {
+              float vv = comp(vel[j], r);
+              float vel3 = 2.0f / (vv * vv * vv);
+              set_comp(qs[j], r, kk.vt2 * lap * vel3 * DV(ix + j, iz));
+            }
           }
         }
         *reinterpret_cast<float4 *>(out_a + (size_t)(ix + j) * g.LDZ + iz0) = o[j];
       }
+      if (snap) snap_write<NTH, 8>(g, aa.snap_k, x0, z0, lv, lx, lz, 0xffu, red);
       if (BORN) {
         float4 ob[2], cb4[2], pb4[2], vb4[2];
         pair_twoway(CB, PB, VV, g, ix, iz0, ob, cb4, pb4, vb4);
@@ -434,6 +498,7 @@ __global__ void __launch_bounds__(nthreads<KIND>(), KIND == TILE_PAD ? 1 : 2) ti
         if (item < NTH) body_vec = vec;
       }
       __syncthreads();
+      float *pout = pout_keep;
       if (px < g.NX) {
         // a quad wholly inside the model (w = 1, u31 = 0) keeps its two-way
         // values; any other quad goes through the absorbing update per cell
@@ -449,6 +514,7 @@ __global__ void __launch_bounds__(nthreads<KIND>(), KIND == TILE_PAD ? 1 : 2) ti
           }
           *reinterpret_cast<float4 *>(out_a + off0) = o;
           if (BORN) *reinterpret_cast<float4 *>(nb_ + off0) = ob;
+          pout[0] = o.x; pout[1] = o.y; pout[2] = o.z; pout[3] = o.w;
 #pragma unroll
           for (int r = 0; r < 4; r++) {
             const int iz = pz + r;
@@ -463,6 +529,7 @@ __global__ void __launch_bounds__(nthreads<KIND>(), KIND == TILE_PAD ? 1 : 2) ti
             const size_t off = off0 + r;
             float out = absorb_cell(Ua(px, iz), Ua, CA, PA, VV, g, px, iz);
             out_a[off] = out;
+            pout[r] = out;
             if (!BORN && record && iz == gzp) g.rec[(size_t)aa.rec_k * g.nx + (px - g.pml)] = out;
             if (MODE == MODE_MODEL && aa.strip_k >= 0) save_strips(g, aa.strip_k, px, iz, out);
             if (BORN) {
@@ -473,6 +540,27 @@ __global__ void __launch_bounds__(nthreads<KIND>(), KIND == TILE_PAD ? 1 : 2) ti
           }
         }
       }
+    }
+    if (KIND == TILE_PAD && snap) {
+      // source-term snapshot of the model-interior cells of this pad tile
+      const int pc = tid / QZ, pz = z0 + 4 * (tid % QZ), px = x0 + pc;
+      const SA CA2{bb + arr_off(0), x0 - HXC, zm};
+      const SA PA2{bb + arr_off(C::NCUR), x0 - 1, zm};
+      float lv[4];
+      int lx[4], lz[4];
+      unsigned mask = 0;
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const int iz = pz + r;
+        lx[r] = px;
+        lz[r] = iz;
+        lv[r] = 0.0f;
+        if (px >= g.pml && px < g.pml + g.nx && iz >= g.pml && iz < g.pml + g.nz) {
+          lv[r] = (pout_keep[r] + PA2(px, iz) - 2.0f * CA2(px, iz)) * g.idt2;
+          mask |= 1u << r;
+        }
+      }
+      snap_write<NTH, 4>(g, aa.snap_k, x0, z0, lv, lx, lz, mask, red);
     }
     __syncthreads();  // buffer b and the u3 tiles are free again
   }

@@ -68,3 +68,18 @@ def adjoint(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, rec, ctx: C
     d = s.to_c()
     ctx.check(ctx.L.seis_fd_rtm(ctx.h, d, ptr(wav), ptr(vel), ptr(rec), ptr(img)))
     return img
+
+
+def born_adjoint(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, rec,
+                 ctx: Context = None):
+    """Exact adjoint of ``forward`` (no reference counterpart): ``img[nx][nz]``
+    with <forward(m), rec> = <m, born_adjoint(rec)> to FP32 rounding."""
+    ctx = ctx or default_context()
+    s = _shot(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz)
+    wav = _f32(wav, (s.NT,))
+    vel = _f32(vel, (nx, nz))
+    rec = _f32(rec, (nx, nt))
+    img = np.zeros((nx, nz), np.float32)
+    d = s.to_c()
+    ctx.check(ctx.L.seis_fd_born_adjoint(ctx.h, d, ptr(wav), ptr(vel), ptr(rec), ptr(img)))
+    return img

@@ -1,0 +1,76 @@
+"""Exact Born adjoint on the GPU: against the FP64 oracle adjoint, and the
+dot-product test against the GPU Born operator (FP32 gate: 1e-6 relative)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import fd_args, rel_l2
+from seis_b200 import Shot, fd
+from seis_b200._lib import (IN_GATHER, IN_VEL, IN_WAVELET, OP_BORN_ADJOINT, OUT_IMAGE, SNAP_BF16,
+                            SNAP_F16, SNAP_F32, Plan)
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(40, 30, 8, 10.0, 12.5), (33, 9, 3, 10.0, 10.0), (130, 100, 20, 10.0, 10.0),
+         (200, 90, 40, 12.5, 12.5), (90, 150, 5, 9.0, 11.0)]
+
+
+def make(nx, nz, pml, dx, dz, nt=160, seed=0):
+    rng = np.random.default_rng(seed + nx * 7 + nz)
+    s = Shot(nx=nx, nz=nz, pml=pml, nt=nt, ndel=20, sx=nx // 3, sz=3, dt=1e-3, dx=dx, dz=dz,
+             gz=rng.integers(0, nz, nx))
+    vel = (1800 + 1500 * rng.random((nx, nz))).astype(np.float32)
+    wav = O.ricker(s.dt, 25.0, s.ndel, s.NT)
+    m = rng.standard_normal((nx, nz)).astype(np.float32)
+    d = rng.standard_normal((nx, nt)).astype(np.float32)
+    return s, vel, wav, m, d
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"{c[0]}x{c[1]}p{c[2]}" for c in CASES])
+def test_adjoint_matches_fp64_oracle(ctx, case):
+    s, vel, wav, m, d = make(*case)
+    img = fd.born_adjoint(*fd_args(s), wav, vel, d, ctx=ctx)
+    ref = O.born_adjoint(s, wav.astype(np.float64), vel, d, prec="f64")
+    err = rel_l2(img, ref)
+    print(f"adjoint {case} vs FP64 oracle: rel L2 {err:.3e}")
+    assert err < 2e-5
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"{c[0]}x{c[1]}p{c[2]}" for c in CASES])
+def test_dot_product_fp32(ctx, case):
+    s, vel, wav, m, d = make(*case, seed=3)
+    Lm = fd.forward(*fd_args(s), wav, vel, m, ctx=ctx).astype(np.float64)
+    Ltd = fd.born_adjoint(*fd_args(s), wav, vel, d, ctx=ctx).astype(np.float64)
+    a, b = float(np.sum(Lm * d)), float(np.sum(m * Ltd))
+    rel = abs(a - b) / max(abs(a), abs(b))
+    # the same difference against the size of the terms: free of the
+    # cancellation in <Lm, d> for random vectors
+    rel_norm = abs(a - b) / (np.linalg.norm(Lm) * np.linalg.norm(d))
+    print(f"dot test {case}: {a:.9e} {b:.9e} rel {rel:.3e} rel/|Lm||d| {rel_norm:.3e}")
+    # FP32 recursions over ~200 steps: each operator carries ~5e-6 relative
+    # rounding error (the transpose itself is exact: the FP64 oracle pair
+    # passes at 1e-12)
+    assert rel_norm <= 1e-6, (a, b)
+    assert rel <= 1e-4, (a, b)
+
+
+@pytest.mark.parametrize("every,dtype,tol", [(1, SNAP_BF16, 5e-3), (1, SNAP_F16, 1e-3),
+                                             (2, SNAP_BF16, 2e-2), (4, SNAP_F32, 5e-2),
+                                             (4, SNAP_BF16, 5e-2)])
+def test_mixed_snapshot_image_error(ctx, every, dtype, tol):
+    """Snapshots thinned in time and/or stored in 16 bits: image error against
+    the FP64 exact adjoint, for band-limited residuals (Born data of a random
+    perturbation, as in an LSRTM iteration)."""
+    s, vel, wav, m, _ = make(200, 90, 40, 12.5, 12.5, nt=300, seed=9)
+    d = O.born(s, wav, vel, m)
+    with Plan(ctx, OP_BORN_ADJOINT, [s]) as p:
+        p.set_snapshots(every, dtype)
+        p.set(0, IN_VEL, vel)
+        p.set(0, IN_WAVELET, wav)
+        p.set(0, IN_GATHER, d)
+        p.run()
+        img = p.get(0, OUT_IMAGE)
+    ref = O.born_adjoint(s, wav.astype(np.float64), vel, d, prec="f64")
+    err = rel_l2(img, ref)
+    print(f"snapshots every {every} dtype {dtype}: image rel L2 {err:.3e}")
+    assert err < tol
