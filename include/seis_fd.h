@@ -190,6 +190,53 @@ int seis_fd_rtm_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
 int seis_fd_born_adjoint(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
                          const float *h_vel, const float *h_rec, float *h_img);
 
+/* ------------------------------------------------------- vector vocabulary */
+/* The CG vector operations of the reference's opern (src/util/arraymath.h),
+ * on device vectors of the context's device. */
+/* DOTPRODUCT (arraymath.h:230-299): *h_out = sum (double)(a[i] * b[i]). */
+int seis_fd_vec_dot(seis_fd_ctx *ctx, const float *d_a, const float *d_b, size_t n,
+                    double *h_out);
+/* ADDSCAL (arraymath.h:338-342): y = a x + b y, formed in double. */
+int seis_fd_vec_axpby(seis_fd_ctx *ctx, float *d_y, const float *d_x, double a, double b,
+                      size_t n);
+
+/* -------------------------------------------------------------- LSRTM (CG) */
+/* Least-squares RTM by conjugate gradient (CGLS) on a global model grid.  The
+ * reference declares this solver (Inversion::conope_MPI, cgsolver_MPI,
+ * src/lsrtm/inversion.h:81,87) but never defines it.
+ *   L m  = [ Born_s( m[x0_s .. x0_s + nx_s) ) ]_s      (forward, per shot)
+ *   L^T d = sum_s scatter_{x0_s}( BornAdjoint_s(d_s) )
+ * Shot s covers columns x0_s .. x0_s + nx_s - 1 of the nx x nz global grid and
+ * has the global nz.  The background velocity and wavelet are fixed: the
+ * adjoint's source-term snapshots are computed once and reused by every
+ * iteration.  Dot products, step lengths and residual norms are FP64. */
+typedef struct seis_fd_lsrtm seis_fd_lsrtm;
+typedef struct {
+  int snap_every;  /* source-term snapshot interval (default 1)            */
+  int snap_dtype;  /* SEIS_SNAP_* (default SEIS_SNAP_BF16)                 */
+  int exact;       /* Born kernels round like the reference (default 0)    */
+} seis_lsrtm_opts;
+
+int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot,
+                         const seis_shot_desc *shots, const int *x0,
+                         const seis_lsrtm_opts *opts, seis_fd_lsrtm **out);
+int seis_fd_lsrtm_destroy(seis_fd_lsrtm *ls);
+/* background velocity [nx][nz] of the global grid and wavelet [nt+ndel] */
+int seis_fd_lsrtm_set_background(seis_fd_lsrtm *ls, const float *h_v0, const float *h_wav);
+/* observed data of one shot, [nx_s][nt] */
+int seis_fd_lsrtm_set_data(seis_fd_lsrtm *ls, int shot, const float *h_d);
+/* Start CGLS from m = 0: r = d, s = L^T r, p = s.  *h_rr = |r|^2 (may be null). */
+int seis_fd_lsrtm_reset(seis_fd_lsrtm *ls, double *h_rr);
+/* niter CGLS iterations (one L and one L^T each); h_rr[i] = |r|^2 after
+ * iteration i (h_rr may be null).  Enqueued without host round trips; returns
+ * after the last iteration completes. */
+int seis_fd_lsrtm_iterate(seis_fd_lsrtm *ls, int niter, double *h_rr);
+/* current model [nx][nz] */
+int seis_fd_lsrtm_model(seis_fd_lsrtm *ls, float *h_m);
+/* padded cell-updates of one iteration (Born + adjoint reverse pass) */
+int64_t seis_fd_lsrtm_cell_updates(const seis_fd_lsrtm *ls);
+int64_t seis_fd_lsrtm_device_bytes(const seis_fd_lsrtm *ls);
+
 #ifdef __cplusplus
 }
 #endif

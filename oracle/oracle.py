@@ -188,5 +188,47 @@ def born_adjoint(shot, wav, vel, rec, prec="f64"):
     return img
 
 
+def lsrtm_cgls(nx, nz, shots, x0, wav, v0, dobs, niter, prec="f64"):
+    """CGLS on the global model (the solver the reference declares as
+    Inversion::conope_MPI / cgsolver_MPI, src/lsrtm/inversion.h:81,87, without
+    a definition), built from the oracle's Born operator and its exact
+    transpose, in FP64.  Shot k covers model columns x0[k] .. x0[k]+nx_k-1.
+    Returns (model, |d|^2, [|r|^2 after each iteration])."""
+    f = np.float64
+    wav = np.asarray(wav, f)
+    subs = [slice(x, x + s.nx) for s, x in zip(shots, x0)]
+
+    def L(m):
+        return [born(s, wav, v0[c], m[c], prec=prec).astype(f) for s, c in zip(shots, subs)]
+
+    def LT(r):
+        out = np.zeros((nx, nz), f)
+        for s, c, rk in zip(shots, subs, r):
+            out[c] += born_adjoint(s, wav, v0[c], rk, prec=prec)
+        return out
+
+    def ddot(a, b):
+        return float(sum(np.sum(x * y) for x, y in zip(a, b)))
+
+    m = np.zeros((nx, nz), f)
+    r = [np.asarray(d, f).copy() for d in dobs]
+    rr0 = ddot(r, r)
+    sg = LT(r)
+    p = sg.copy()
+    gamma = float(np.sum(sg * sg))
+    hist = []
+    for _ in range(niter):
+        q = L(p)
+        alpha = gamma / ddot(q, q)
+        m += alpha * p
+        r = [rk - alpha * qk for rk, qk in zip(r, q)]
+        hist.append(ddot(r, r))
+        sg = LT(r)
+        gnew = float(np.sum(sg * sg))
+        p = sg + (gnew / gamma) * p
+        gamma = gnew
+    return m, rr0, hist
+
+
 def ref_set_threads(n: int):
     ref_lib().ref_set_threads(_I(n))

@@ -65,6 +65,11 @@ class Shot:
         return d
 
 
+class LsrtmOptsC(ctypes.Structure):
+    _fields_ = [("snap_every", ctypes.c_int), ("snap_dtype", ctypes.c_int),
+                ("exact", ctypes.c_int)]
+
+
 _lib = None
 
 
@@ -113,6 +118,21 @@ def lib():
         L.seis_fd_rtm_batch.argtypes = [P, I, SD, PP, PP, PP, PP]
         L.seis_fd_born.argtypes = [P, SD, P, P, P, P]
         L.seis_fd_rtm.argtypes = [P, SD, P, P, P, P]
+        L.seis_fd_vec_dot.argtypes = [P, P, P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)]
+        L.seis_fd_vec_axpby.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_size_t]
+        L.seis_fd_lsrtm_create.argtypes = [P, I, I, I, SD, ctypes.POINTER(I),
+                                           ctypes.POINTER(LsrtmOptsC), PP]
+        L.seis_fd_lsrtm_destroy.argtypes = [P]
+        L.seis_fd_lsrtm_set_background.argtypes = [P, P, P]
+        L.seis_fd_lsrtm_set_data.argtypes = [P, I, P]
+        L.seis_fd_lsrtm_reset.argtypes = [P, P]
+        L.seis_fd_lsrtm_iterate.argtypes = [P, I, P]
+        L.seis_fd_lsrtm_model.argtypes = [P, P]
+        L.seis_fd_lsrtm_cell_updates.argtypes = [P]
+        L.seis_fd_lsrtm_cell_updates.restype = ctypes.c_int64
+        L.seis_fd_lsrtm_device_bytes.argtypes = [P]
+        L.seis_fd_lsrtm_device_bytes.restype = ctypes.c_int64
         _lib = L
     return _lib
 
@@ -298,3 +318,86 @@ def batch(ctx: Context, op: int, shots, wavs, vels, third=None):
         rc = fn(ctx.h, n, descs, pw, pv, pt, po)
     ctx.check(rc)
     return outs
+
+
+class Lsrtm:
+    """Least-squares RTM by CGLS on a global nx x nz grid (seis_fd_lsrtm_*).
+
+    Shot k covers columns x0[k] .. x0[k] + shots[k].nx - 1 of the model.
+    """
+
+    def __init__(self, ctx: Context, nx: int, nz: int, shots, x0, snap_every: int = 1,
+                 snap_dtype: int = None, exact: bool = False):
+        self.ctx, self.nx, self.nz, self.shots = ctx, nx, nz, list(shots)
+        self._descs = shot_array(self.shots)
+        self._x0 = (ctypes.c_int * len(self.shots))(*[int(v) for v in x0])
+        o = LsrtmOptsC(snap_every, SNAP_BF16 if snap_dtype is None else snap_dtype,
+                       1 if exact else 0)
+        h = ctypes.c_void_p()
+        ctx.check(ctx.L.seis_fd_lsrtm_create(ctx.h, nx, nz, len(self.shots), self._descs,
+                                             self._x0, ctypes.byref(o), ctypes.byref(h)))
+        self.h = h
+
+    def set_background(self, v0: np.ndarray, wav: np.ndarray):
+        v = np.ascontiguousarray(v0, np.float32)
+        w = np.ascontiguousarray(wav, np.float32)
+        assert v.shape == (self.nx, self.nz)
+        self.ctx.check(self.ctx.L.seis_fd_lsrtm_set_background(self.h, ptr(v), ptr(w)))
+
+    def set_data(self, shot: int, d: np.ndarray):
+        a = np.ascontiguousarray(d, np.float32)
+        s = self.shots[shot]
+        assert a.shape == (s.nx, s.nt)
+        self.ctx.check(self.ctx.L.seis_fd_lsrtm_set_data(self.h, shot, ptr(a)))
+
+    def reset(self) -> float:
+        rr = ctypes.c_double()
+        self.ctx.check(self.ctx.L.seis_fd_lsrtm_reset(self.h, ctypes.byref(rr)))
+        return rr.value
+
+    def iterate(self, niter: int = 1) -> np.ndarray:
+        rr = np.zeros(niter, np.float64)
+        self.ctx.check(self.ctx.L.seis_fd_lsrtm_iterate(self.h, niter, ptr(rr)))
+        return rr
+
+    def model(self) -> np.ndarray:
+        m = np.zeros((self.nx, self.nz), np.float32)
+        self.ctx.check(self.ctx.L.seis_fd_lsrtm_model(self.h, ptr(m)))
+        return m
+
+    @property
+    def cell_updates(self) -> int:
+        return int(self.ctx.L.seis_fd_lsrtm_cell_updates(self.h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.ctx.L.seis_fd_lsrtm_device_bytes(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.seis_fd_lsrtm_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def vec_dot(ctx: Context, a_ptr: int, b_ptr: int, n: int) -> float:
+    out = ctypes.c_double()
+    ctx.check(ctx.L.seis_fd_vec_dot(ctx.h, ctypes.c_void_p(a_ptr), ctypes.c_void_p(b_ptr), n,
+                                    ctypes.byref(out)))
+    return out.value
+
+
+def vec_axpby(ctx: Context, y_ptr: int, x_ptr: int, a: float, b: float, n: int):
+    ctx.check(ctx.L.seis_fd_vec_axpby(ctx.h, ctypes.c_void_p(y_ptr), ctypes.c_void_p(x_ptr),
+                                      a, b, n))

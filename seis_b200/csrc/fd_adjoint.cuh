@@ -18,8 +18,13 @@
 // by the one-way update) reduce to the symmetric gather
 //   L_k = Lz(vz L1) + Lx(vx L1) + 2 L1 - L2 + R^T d.
 // Pad tiles run the transposed stages in scatter form over every consumer cell
-// of the tile + 5-cell halo, accumulating with shared-memory atomics; only the
-// contributions that land on the tile are kept.
+// of the tile + 5-cell halo; only the contributions that land on the tile are
+// kept.  The scatter accumulates in 64-bit fixed point (shared-memory integer
+// atomics, whose sum does not depend on the order of the adds), so the
+// adjoint is bit-for-bit repeatable.  The tile's scale is 2^(49 - e) for
+// inputs below 2^e: every accumulator stays below 2^62 (a target collects at
+// most ~2^12 times the largest input) and the resolution is 2^-49 of the
+// tile's largest input.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -112,19 +117,38 @@ __device__ __forceinline__ RingCoef ring_coef(const ShotDev &g, const VA &V, int
   return r;
 }
 
-struct AdjTile {  // accumulator over a rectangular window of the grid
-  float *s;
+struct AdjTile {  // fixed-point accumulator over a rectangular window of the grid
+  long long *s;
   int x0, z0, ncol, nrow;  // window origin and size
+  float scale;             // value -> fixed point (a power of two)
+  double inv;              // fixed point -> value
   __device__ __forceinline__ bool in(int ix, int iz) const {
     return ix >= x0 && ix < x0 + ncol && iz >= z0 && iz < z0 + nrow;
   }
   __device__ __forceinline__ void add(int ix, int iz, float v) const {
-    if (in(ix, iz)) atomicAdd(&s[(ix - x0) * nrow + (iz - z0)], v);
+    if (in(ix, iz))
+      atomicAdd(reinterpret_cast<unsigned long long *>(&s[(ix - x0) * nrow + (iz - z0)]),
+                (unsigned long long)__float2ll_rn(v * scale));
   }
   __device__ __forceinline__ float get(int ix, int iz) const {
-    return s[(ix - x0) * nrow + (iz - z0)];
+    return (float)((double)s[(ix - x0) * nrow + (iz - z0)] * inv);
   }
 };
+
+// largest |value| over n staged floats, reduced across the block
+template <int NTH>
+__device__ float block_amax(const float *a, int n, const float *b, int nb, float *red) {
+  float m = 0.0f;
+  for (int i = threadIdx.x; i < n; i += NTH) m = fmaxf(m, fabsf(a[i]));
+  for (int i = threadIdx.x; i < nb; i += NTH) m = fmaxf(m, fabsf(b[i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  m = 0.0f;
+#pragma unroll
+  for (int w = 0; w < NTH / 32; w++) m = fmaxf(m, red[w]);
+  return m;
+}
 
 // Scatter of the transposed two-way update and frame of consumer cell (ix,iz)
 // with adjoint mu into cb (mirrors fd.cpp:1057-1091 and :1226-1271).
@@ -261,8 +285,10 @@ __global__ void __launch_bounds__(A_NT_I, 2) adj_interior_kernel(const ShotDev *
 }
 
 // ---------------------------------------------------------------- pad tiles
+constexpr size_t ADJ_PAD_F32 = sizeof(float) * (size_t)(2 * WIDE + NARROW);
+static_assert(ADJ_PAD_F32 % 8 == 0, "fixed-point accumulators must be 8-byte aligned");
 constexpr size_t ADJ_PAD_SMEM =
-    sizeof(float) * (size_t)(2 * WIDE + NARROW + MU_C * MU_R + 3 * TX * TZ) + 16;
+    ADJ_PAD_F32 + sizeof(long long) * (size_t)(MU_C * MU_R + 3 * TX * TZ) + 16;
 
 __global__ void __launch_bounds__(A_NT_P, 1) adj_pad_kernel(const ShotDev *__restrict__ shots,
                                                             const Tile *__restrict__ tiles,
@@ -271,11 +297,12 @@ __global__ void __launch_bounds__(A_NT_P, 1) adj_pad_kernel(const ShotDev *__res
   float *sL1 = reinterpret_cast<float *>(smraw);  // wide
   float *sV = sL1 + WIDE;                          // wide
   float *sL2 = sV + WIDE;                          // narrow
-  float *sMU1 = sL2 + NARROW;                      // tile + 4
-  float *sCB = sMU1 + MU_C * MU_R;                 // tile
-  float *sMU2 = sCB + TX * TZ;                     // tile
-  float *sPB = sMU2 + TX * TZ;                     // tile
+  long long *sMU1 = reinterpret_cast<long long *>(sL2 + NARROW);  // tile + 4
+  long long *sCB = sMU1 + MU_C * MU_R;             // tile
+  long long *sMU2 = sCB + TX * TZ;                 // tile
+  long long *sPB = sMU2 + TX * TZ;                 // tile
   uint64_t *bar = reinterpret_cast<uint64_t *>(sPB + TX * TZ);
+  __shared__ float red[A_NT_P / 32];
   const int tid = threadIdx.x;
   const Tile t = tiles[blockIdx.x];
   __shared__ ShotDev sg;
@@ -285,7 +312,7 @@ __global__ void __launch_bounds__(A_NT_P, 1) adj_pad_kernel(const ShotDev *__res
     mbar_init(bar, 1);
     fence_barrier_init();
   }
-  for (int i = tid; i < MU_C * MU_R + 3 * TX * TZ; i += A_NT_P) sMU1[i] = 0.0f;
+  for (int i = tid; i < MU_C * MU_R + 3 * TX * TZ; i += A_NT_P) sMU1[i] = 0;
   __syncthreads();
   const ShotDev &g = sg;
   const int x0 = t.x0, z0 = t.z0;
@@ -302,8 +329,14 @@ __global__ void __launch_bounds__(A_NT_P, 1) adj_pad_kernel(const ShotDev *__res
   }
   const int zm = z0 - ZM;
   const SA L1{sL1, x0 - HXC, zm}, V{sV, x0 - HXC, zm}, L2{sL2, x0 - 1, zm};
-  const AdjTile MU1{sMU1, x0 - 4, z0 - 4, MU_C, MU_R};
-  const AdjTile CB{sCB, x0, z0, TX, TZ}, MU2{sMU2, x0, z0, TX, TZ}, PB{sPB, x0, z0, TX, TZ};
+  int e;
+  frexpf(block_amax<A_NT_P>(sL1, WIDE, sL2, NARROW, red), &e);  // inputs below 2^e
+  const int se = min(49 - e, 126);
+  const float scale = ldexpf(1.0f, se);
+  const double inv = ldexp(1.0, -se);
+  const AdjTile MU1{sMU1, x0 - 4, z0 - 4, MU_C, MU_R, scale, inv};
+  const AdjTile CB{sCB, x0, z0, TX, TZ, scale, inv}, MU2{sMU2, x0, z0, TX, TZ, scale, inv},
+      PB{sPB, x0, z0, TX, TZ, scale, inv};
 
   // blend^T and rings^T of L1 over the consumers in tile + 5, of L2 over tile + 1
   constexpr int R5C = TX + 10, R5R = TZ + 10;
@@ -351,8 +384,7 @@ __global__ void __launch_bounds__(A_NT_P, 1) adj_pad_kernel(const ShotDev *__res
   for (int i = tid; i < MU_C * MU_R; i += A_NT_P) {
     const int cx = x0 - 4 + i / MU_R, cz = z0 - 4 + i % MU_R;
     if (cx < 0 || cx >= g.NX || cz < 0 || cz >= g.NZ) continue;
-    float mu = sMU1[i];
-    if (mu != 0.0f) stencil_T(g, V, cx, cz, mu, CB);
+    if (sMU1[i] != 0) stencil_T(g, V, cx, cz, (float)((double)sMU1[i] * inv), CB);
   }
   __syncthreads();
   float *out = g.fa[(a.rot + 2) % 3];
@@ -362,7 +394,7 @@ __global__ void __launch_bounds__(A_NT_P, 1) adj_pad_kernel(const ShotDev *__res
     const int ix = x0 + i / TZ, iz = z0 + i % TZ;
     if (ix >= g.NX || iz >= g.NZ) continue;
     const int li = i;  // tile-local index (column-major, TZ rows)
-    float v = sCB[li] + sPB[li] - sMU2[li];
+    float v = (float)((double)(sCB[li] + sPB[li] - sMU2[li]) * inv);
     const int x = ix - g.pml, z = iz - g.pml;
     const bool inside = x >= 0 && x < g.nx && z >= 0 && z < g.nz;
     if (a.rec_k >= 0 && x >= 0 && x < g.nx && iz == g.gz[x] + g.pml)

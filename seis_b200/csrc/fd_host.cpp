@@ -34,6 +34,8 @@ struct seis_fd_ctx {
   cudaEvent_t fork = nullptr, join = nullptr;
   int *d_err = nullptr;  // set by kernels whose bounded waits ran out
   std::vector<seis_fd_plan *> plans;  // live plans, torn down with the context
+  double *d_partial = nullptr;        // DOT_PARTS partial sums of a dot product
+  double *d_scalar = nullptr;         // one FP64 result
   int num_sms = 148;
   std::string err;
   int64_t launches = 0;
@@ -111,7 +113,8 @@ struct Plan {
   int n_int_adj = 0, n_pad_adj = 0;
   Tile *d_adj_tiles = nullptr;
   int snap_every = 1, snap_dtype = SNAP_F32;
-  bool snaps_ready = false;
+  bool snaps_ready = false;  // storage allocated
+  bool snaps_valid = false;  // storage holds the source terms of the current inputs
   int64_t device_bytes = 0;
   std::vector<int2> cols;
   std::vector<float *> field_bases;  // allocation starts of margin-padded fields
@@ -540,6 +543,15 @@ int run_rtm_reverse(Plan &p) {
   return SEIS_OK;
 }
 
+// Forward pass of the background field keeping the source-term snapshots
+// (adjoint plans); reused by every later run until the velocity or the
+// wavelet changes.
+int source_pass(Plan &p) {
+  int rc = run_forward(p, MODE_MODEL);
+  if (!rc) p.snaps_valid = true;
+  return rc;
+}
+
 // Reverse pass of the exact adjoint: L_k for k = NT .. 0 from L_{k+1}, L_{k+2};
 // the step producing L_k images the source term of step k with mu(L_{k+1}).
 int run_adjoint(Plan &p) {
@@ -582,7 +594,7 @@ int enqueue_operator(Plan &p) {
       return rc ? rc : run_rtm_reverse(p);
     case OP_BORN_ADJ:
       rc = ensure_snapshots(p);
-      if (!rc) rc = run_forward(p, MODE_MODEL);
+      if (!rc && !p.snaps_valid) rc = source_pass(p);
       return rc ? rc : run_adjoint(p);
   }
   return fail(p.ctx, SEIS_ERR_NOTSUP, "unknown operator %d", p.op);
@@ -597,6 +609,13 @@ int plan_run(Plan &p) {
       if (rc0) return rc0;
       CK(cudaStreamSynchronize(ctx->stream));
     }
+  }
+  // the source pass runs outside the graph, only when its inputs changed
+  if (p.op == OP_BORN_ADJ && !p.snaps_valid) {
+    int rc0 = source_pass(p);
+    if (rc0) return rc0;
+  }
+  if (!p.exec) {
     int64_t before = ctx->launches;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_operator(p);
@@ -703,6 +722,8 @@ int seis_fd_create(seis_fd_ctx **out, int device) {
   if (e == cudaSuccess)
     e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_partial, sizeof(double) * DOT_PARTS);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_scalar, sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, sizeof(int));
   if (e != cudaSuccess) {
     seis_fd_destroy(ctx);
@@ -726,6 +747,8 @@ int seis_fd_destroy(seis_fd_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->aux) cudaStreamSynchronize(ctx->aux);
   if (ctx->d_err) cudaFree(ctx->d_err);
+  if (ctx->d_partial) cudaFree(ctx->d_partial);
+  if (ctx->d_scalar) cudaFree(ctx->d_scalar);
   if (ctx->fork) cudaEventDestroy(ctx->fork);
   if (ctx->join) cudaEventDestroy(ctx->join);
   if (ctx->aux) cudaStreamDestroy(ctx->aux);
@@ -787,6 +810,7 @@ static int plan_input(seis_fd_plan *plan, int shot, int what, const float *src, 
   const seis_shot_desc &d = p.desc[shot];
   ShotDev &g = p.sd[shot];
   cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (what == SEIS_IN_VEL || what == SEIS_IN_WAVELET) p.snaps_valid = false;
   switch (what) {
     case SEIS_IN_VEL:
     case SEIS_IN_DV: {
@@ -1014,6 +1038,293 @@ int seis_fd_rtm_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
                       const float *const *h_rec, float *const *h_img) {
   return run_batch(ctx, OP_RTM, nshot, shots, h_wav, SEIS_IN_WAVELET, h_vel, SEIS_IN_VEL, h_rec,
                    SEIS_IN_GATHER, h_img, SEIS_OUT_IMAGE);
+}
+
+// ------------------------------------------------------------ vector ops
+int seis_fd_vec_dot(seis_fd_ctx *ctx, const float *d_a, const float *d_b, size_t n,
+                    double *h_out) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (!d_a || !d_b || !h_out) return fail(ctx, SEIS_ERR_ARG, "null pointer");
+  CK(launch_dot(d_a, d_b, n, ctx->d_partial, ctx->d_scalar, 0, ctx->stream));
+  ctx->launches += 2;
+  CK(cudaMemcpyAsync(h_out, ctx->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  return sync(ctx);
+}
+
+int seis_fd_vec_axpby(seis_fd_ctx *ctx, float *d_y, const float *d_x, double a, double b,
+                      size_t n) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (!d_y || !d_x) return fail(ctx, SEIS_ERR_ARG, "null pointer");
+  CK(launch_axpby(d_y, d_x, a, b, n, ctx->stream));
+  ctx->launches++;
+  return sync(ctx);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ LSRTM
+struct seis_fd_lsrtm {
+  seis_fd_ctx *ctx = nullptr;
+  int nx = 0, nz = 0, nshot = 0, nt = 0;
+  std::vector<seis_shot_desc> shots;
+  std::vector<std::vector<int>> gz;
+  std::vector<int> x0;
+  seis_fd_plan born{nullptr}, adj{nullptr};
+  std::vector<void *> allocs;
+  float *m = nullptr, *p = nullptr, *s = nullptr;  // model-space vectors [nx][nz]
+  float *dobs = nullptr, *r = nullptr;             // data space, per shot [nt][nx_s]
+  std::vector<size_t> doff;                        // offset of shot s in data space
+  size_t ndata = 0;
+  double *sc = nullptr;  // FP64 scalars: 0 gamma, 1 |q|^2, 2 alpha, 3 gamma_new, 4 beta
+  double *rr = nullptr;  // |r|^2 per iteration
+  int rr_cap = 0;
+  bool ready = false;    // reset done
+  int64_t device_bytes = 0;
+  ~seis_fd_lsrtm() {
+    if (born.p) delete born.p;
+    if (adj.p) delete adj.p;
+    for (void *q : allocs) cudaFree(q);
+  }
+  template <class T>
+  int alloc(T **out, size_t n) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, e == cudaErrorMemoryAllocation ? SEIS_ERR_NOMEM : SEIS_ERR_CUDA,
+                  "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    }
+    allocs.push_back(q);
+    device_bytes += (int64_t)(std::max<size_t>(n, 1) * sizeof(T));
+    *out = static_cast<T *>(q);
+    e = cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), ctx->stream);
+    return e == cudaSuccess ? SEIS_OK : fail(ctx, SEIS_ERR_CUDA, "cudaMemset failed");
+  }
+};
+
+namespace {
+
+// s = L^T r: adjoint plan over the residuals, per-shot images scattered into
+// the global grid.
+int lsrtm_adjoint(seis_fd_lsrtm &L) {
+  seis_fd_ctx *ctx = L.ctx;
+  size_t nm = (size_t)L.nx * L.nz;
+  int rc = plan_run(*L.adj.p);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(L.s, 0, sizeof(float) * nm, ctx->stream));
+  for (int k = 0; k < L.nshot; k++) {
+    const ShotDev &g = L.adj.p->sd[k];
+    CK(launch_add(L.s + (size_t)L.x0[k] * L.nz, g.img, (size_t)g.nx * g.nz, ctx->stream));
+    ctx->launches++;
+  }
+  return SEIS_OK;
+}
+
+// q = L p into the Born plan's gathers.
+int lsrtm_forward(seis_fd_lsrtm &L) {
+  for (int k = 0; k < L.nshot; k++) {
+    int rc = plan_input(&L.born, k, SEIS_IN_DV, L.p + (size_t)L.x0[k] * L.nz, true);
+    if (rc) return rc;
+  }
+  return plan_run(*L.born.p);
+}
+
+// out = sum over shots of <a_s, b_s> in data space; a from the Born plan's
+// gathers when `from_q`, else the residual.
+int data_dot(seis_fd_lsrtm &L, bool q_left, bool q_right, double *out) {
+  seis_fd_ctx *ctx = L.ctx;
+  for (int k = 0; k < L.nshot; k++) {
+    const float *q = L.born.p->sd[k].rec, *r = L.r + L.doff[k];
+    size_t n = (size_t)L.shots[k].nx * L.nt;
+    CK(launch_dot(q_left ? q : r, q_right ? q : r, n, ctx->d_partial, out, k > 0, ctx->stream));
+    ctx->launches += 2;
+  }
+  return SEIS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot, const seis_shot_desc *shots,
+                         const int *x0, const seis_lsrtm_opts *opts, seis_fd_lsrtm **out) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (!out || !shots || !x0 || nshot < 1 || nx < 1 || nz < 1)
+    return fail(ctx, SEIS_ERR_ARG, "lsrtm: bad arguments");
+  *out = nullptr;
+  for (int k = 0; k < nshot; k++) {
+    if (shots[k].nz != nz || x0[k] < 0 || x0[k] + shots[k].nx > nx)
+      return fail(ctx, SEIS_ERR_ARG, "lsrtm: shot %d aperture [%d, %d) x nz %d outside %d x %d",
+                  k, x0[k], x0[k] + shots[k].nx, shots[k].nz, nx, nz);
+  }
+  seis_lsrtm_opts o{1, SEIS_SNAP_BF16, 0};
+  if (opts) o = *opts;
+  seis_fd_lsrtm *L = new (std::nothrow) seis_fd_lsrtm();
+  if (!L) return fail(ctx, SEIS_ERR_NOMEM, "host allocation failed");
+  L->ctx = ctx;
+  L->nx = nx; L->nz = nz; L->nshot = nshot; L->nt = shots[0].nt;
+  L->shots.assign(shots, shots + nshot);
+  L->x0.assign(x0, x0 + nshot);
+  Plan *pb = nullptr, *pa = nullptr;
+  rc = plan_create(ctx, OP_BORN, nshot, shots, &pb);
+  if (!rc) rc = plan_create(ctx, OP_BORN_ADJ, nshot, shots, &pa);
+  L->born.p = pb;
+  L->adj.p = pa;
+  if (!rc) {
+    pb->exact = o.exact != 0;
+    seis_fd_plan h{pa};
+    rc = seis_fd_plan_set_snapshots(&h, o.snap_every, o.snap_dtype);
+  }
+  size_t nm = (size_t)nx * nz;
+  if (!rc) rc = L->alloc(&L->m, nm);
+  if (!rc) rc = L->alloc(&L->p, nm);
+  if (!rc) rc = L->alloc(&L->s, nm);
+  for (int k = 0; k < nshot; k++) {
+    L->doff.push_back(L->ndata);
+    L->ndata += (size_t)shots[k].nx * L->nt;
+  }
+  if (!rc) rc = L->alloc(&L->dobs, L->ndata);
+  if (!rc) rc = L->alloc(&L->r, L->ndata);
+  if (!rc) rc = L->alloc(&L->sc, 8);
+  if (!rc) {
+    L->rr_cap = 4096;
+    rc = L->alloc(&L->rr, (size_t)L->rr_cap);
+  }
+  if (!rc) {
+    // the adjoint plan reads its receiver data straight from the residual
+    for (int k = 0; k < nshot; k++) pa->sd[k].rec = L->r + L->doff[k];
+    cudaError_t e = cudaMemcpyAsync(pa->d_sd, pa->sd.data(), sizeof(ShotDev) * nshot,
+                                    cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = fail(ctx, SEIS_ERR_CUDA, "lsrtm setup: %s", cudaGetErrorString(e));
+  }
+  if (rc) {
+    delete L;
+    return rc;
+  }
+  *out = L;
+  return SEIS_OK;
+}
+
+int seis_fd_lsrtm_destroy(seis_fd_lsrtm *L) {
+  if (!L) return SEIS_OK;
+  cudaSetDevice(L->ctx->device);
+  cudaStreamSynchronize(L->ctx->stream);
+  delete L;
+  return SEIS_OK;
+}
+
+int seis_fd_lsrtm_set_background(seis_fd_lsrtm *L, const float *h_v0, const float *h_wav) {
+  if (!L) return SEIS_ERR_ARG;
+  int rc = begin(L->ctx);
+  if (rc) return rc;
+  if (!h_v0 || !h_wav) return fail(L->ctx, SEIS_ERR_ARG, "null array");
+  for (int k = 0; k < L->nshot && !rc; k++) {
+    const float *sub = h_v0 + (size_t)L->x0[k] * L->nz;  // aperture columns are contiguous
+    rc = plan_input(&L->born, k, SEIS_IN_VEL, sub, false);
+    if (!rc) rc = plan_input(&L->born, k, SEIS_IN_WAVELET, h_wav, false);
+    if (!rc) rc = plan_input(&L->adj, k, SEIS_IN_VEL, sub, false);
+    if (!rc) rc = plan_input(&L->adj, k, SEIS_IN_WAVELET, h_wav, false);
+  }
+  L->ready = false;
+  return rc ? rc : sync(L->ctx);
+}
+
+int seis_fd_lsrtm_set_data(seis_fd_lsrtm *L, int shot, const float *h_d) {
+  if (!L) return SEIS_ERR_ARG;
+  seis_fd_ctx *ctx = L->ctx;
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (shot < 0 || shot >= L->nshot || !h_d) return fail(ctx, SEIS_ERR_ARG, "shot %d", shot);
+  const int nxs = L->shots[shot].nx;
+  Plan &pb = *L->born.p;
+  CK(cudaMemcpyAsync(pb.d_stage, h_d, sizeof(float) * nxs * L->nt, cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(launch_transpose(pb.d_stage, nxs, L->nt, L->dobs + L->doff[shot], ctx->stream));
+  ctx->launches++;
+  L->ready = false;
+  return sync(ctx);
+}
+
+int seis_fd_lsrtm_reset(seis_fd_lsrtm *L, double *h_rr) {
+  if (!L) return SEIS_ERR_ARG;
+  seis_fd_ctx *ctx = L->ctx;
+  int rc = begin(ctx);
+  if (rc) return rc;
+  size_t nm = (size_t)L->nx * L->nz;
+  CK(cudaMemsetAsync(L->m, 0, sizeof(float) * nm, ctx->stream));
+  CK(cudaMemcpyAsync(L->r, L->dobs, sizeof(float) * L->ndata, cudaMemcpyDeviceToDevice,
+                     ctx->stream));
+  rc = lsrtm_adjoint(*L);  // s = L^T r
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(L->p, L->s, sizeof(float) * nm, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(launch_dot(L->s, L->s, nm, ctx->d_partial, L->sc + 0, 0, ctx->stream));  // gamma
+  ctx->launches += 2;
+  rc = data_dot(*L, false, false, L->rr);  // |r|^2
+  if (rc) return rc;
+  if (h_rr)
+    CK(cudaMemcpyAsync(h_rr, L->rr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  L->ready = true;
+  return sync(ctx);
+}
+
+int seis_fd_lsrtm_iterate(seis_fd_lsrtm *L, int niter, double *h_rr) {
+  if (!L) return SEIS_ERR_ARG;
+  seis_fd_ctx *ctx = L->ctx;
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (!L->ready) return fail(ctx, SEIS_ERR_STATE, "lsrtm: call seis_fd_lsrtm_reset first");
+  if (niter < 1 || niter > L->rr_cap) return fail(ctx, SEIS_ERR_ARG, "niter=%d", niter);
+  size_t nm = (size_t)L->nx * L->nz;
+  double *gamma = L->sc + 0, *qq = L->sc + 1, *alpha = L->sc + 2, *gnew = L->sc + 3,
+         *beta = L->sc + 4;
+  for (int it = 0; it < niter && !rc; it++) {
+    rc = lsrtm_forward(*L);                                        // q = L p
+    if (!rc) rc = data_dot(*L, true, true, qq);                    // |q|^2
+    if (rc) break;
+    CK(launch_ratio(gamma, qq, alpha, ctx->stream));               // alpha = gamma / |q|^2
+    CK(launch_axpby_dev(L->m, L->p, alpha, 1.0, nullptr, 1.0, nm, ctx->stream));  // m += a p
+    for (int k = 0; k < L->nshot; k++)                              // r -= a q
+      CK(launch_axpby_dev(L->r + L->doff[k], L->born.p->sd[k].rec, alpha, -1.0, nullptr, 1.0,
+                          (size_t)L->shots[k].nx * L->nt, ctx->stream));
+    ctx->launches += 2 + L->nshot;
+    rc = data_dot(*L, false, false, L->rr + it);                   // |r|^2
+    if (!rc) rc = lsrtm_adjoint(*L);                               // s = L^T r
+    if (rc) break;
+    CK(launch_dot(L->s, L->s, nm, ctx->d_partial, gnew, 0, ctx->stream));  // |s|^2
+    CK(launch_ratio(gnew, gamma, beta, ctx->stream));              // beta = gnew / gamma
+    CK(cudaMemcpyAsync(gamma, gnew, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(launch_axpby_dev(L->p, L->s, nullptr, 1.0, beta, 1.0, nm, ctx->stream));  // p = s + b p
+    ctx->launches += 5;
+  }
+  if (rc) return rc;
+  if (h_rr)
+    CK(cudaMemcpyAsync(h_rr, L->rr, sizeof(double) * niter, cudaMemcpyDeviceToHost, ctx->stream));
+  return sync(ctx);
+}
+
+int seis_fd_lsrtm_model(seis_fd_lsrtm *L, float *h_m) {
+  if (!L || !h_m) return SEIS_ERR_ARG;
+  seis_fd_ctx *ctx = L->ctx;
+  int rc = begin(ctx);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h_m, L->m, sizeof(float) * L->nx * L->nz, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  return sync(ctx);
+}
+
+int64_t seis_fd_lsrtm_cell_updates(const seis_fd_lsrtm *L) {
+  if (!L) return 0;
+  int64_t c = 0;
+  for (const ShotDev &g : L->born.p->sd) c += (int64_t)g.NX * g.NZ * (2LL * g.NT + g.NT + 1);
+  return c;
+}
+
+int64_t seis_fd_lsrtm_device_bytes(const seis_fd_lsrtm *L) {
+  return L ? L->device_bytes + L->born.p->device_bytes + L->adj.p->device_bytes : 0;
 }
 
 }  // extern "C"

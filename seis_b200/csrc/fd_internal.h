@@ -146,6 +146,17 @@ cudaError_t launch_adjoint(const ShotDev *d_shots, const Tile *d_tiles, int n_in
 cudaError_t configure_adjoint();
 }  // namespace fast
 cudaError_t launch_finalize_image(const ShotDev *d_shots, int nshots, cudaStream_t s);
+
+// Vector operations of the CG solver (fd_vec.cu).  A dot product needs a
+// scratch array of DOT_PARTS doubles for its per-CTA partial sums.
+constexpr int DOT_PARTS = 1184;
+cudaError_t launch_dot(const float *a, const float *b, size_t n, double *partial, double *out,
+                       int accumulate, cudaStream_t s);
+cudaError_t launch_axpby(float *y, const float *x, double a, double b, size_t n, cudaStream_t s);
+cudaError_t launch_axpby_dev(float *y, const float *x, const double *sa, double fa,
+                             const double *sb, double fb, size_t n, cudaStream_t s);
+cudaError_t launch_add(float *y, const float *x, size_t n, cudaStream_t s);
+cudaError_t launch_ratio(const double *num, const double *den, double *out, cudaStream_t s);
 // Set kernel attributes (shared-memory limits); call once per device.
 cudaError_t configure_kernels();
 cudaError_t launch_pad(const float *d_src, int nx, int nz, int pml, int LDZ, int clamp,

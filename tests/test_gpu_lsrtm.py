@@ -1,0 +1,96 @@
+"""LSRTM by CGLS on the GPU against the FP64 oracle CGLS (same operators,
+same global model, shots on overlapping apertures)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import rel_l2
+from seis_b200 import Shot
+from seis_b200._lib import SNAP_BF16, SNAP_F32, Lsrtm
+
+pytestmark = pytest.mark.gpu
+
+
+def survey(nx=96, nz=60, nsx=48, nshot=3, pml=12, nt=260, seed=4):
+    rng = np.random.default_rng(seed)
+    x0 = [int(round(k * (nx - nsx) / max(nshot - 1, 1))) for k in range(nshot)]
+    shots = [Shot(nx=nsx, nz=nz, pml=pml, nt=nt, ndel=25, sx=nsx // 2, sz=2, dt=1e-3, dx=10.0,
+                  dz=10.0, gz=np.full(nsx, 1)) for _ in range(nshot)]
+    z = np.arange(nz)
+    v0 = np.broadcast_to(1900.0 + 12.0 * z, (nx, nz)).astype(np.float32).copy()
+    m_true = np.zeros((nx, nz), np.float32)
+    m_true[:, nz // 2] = 150.0
+    m_true[nx // 3:nx // 3 + 10, nz // 3] = -100.0
+    wav = O.ricker(1e-3, 25.0, 25, nt + 25)
+    dobs = [O.born(s, wav, v0[x:x + s.nx], m_true[x:x + s.nx]) for s, x in zip(shots, x0)]
+    return nx, nz, shots, x0, wav, v0, m_true, dobs
+
+
+def run_gpu(ctx, sv, niter, **kw):
+    nx, nz, shots, x0, wav, v0, _, dobs = sv
+    with Lsrtm(ctx, nx, nz, shots, x0, **kw) as ls:
+        ls.set_background(v0, wav)
+        for k, d in enumerate(dobs):
+            ls.set_data(k, d)
+        rr0 = ls.reset()
+        hist = ls.iterate(niter)
+        return ls.model(), rr0, hist
+
+
+def test_lsrtm_matches_fp64_cgls(ctx):
+    sv = survey()
+    nx, nz, shots, x0, wav, v0, _, dobs = sv
+    niter = 4
+    m_ref, rr0_ref, hist_ref = O.lsrtm_cgls(nx, nz, shots, x0, wav, v0, dobs, niter)
+    m, rr0, hist = run_gpu(ctx, sv, niter, snap_dtype=SNAP_F32, exact=True)
+    print("rr0", rr0, rr0_ref)
+    print("gpu ", hist / rr0)
+    print("fp64", np.array(hist_ref) / rr0_ref)
+    assert abs(rr0 - rr0_ref) <= 1e-6 * rr0_ref
+    assert np.all(np.diff(hist) < 0) and hist[0] < rr0
+    np.testing.assert_allclose(hist / rr0, np.array(hist_ref) / rr0_ref, rtol=2e-3, atol=1e-5)
+    err = rel_l2(m, m_ref)
+    print("model rel L2 vs FP64 CGLS", err)
+    assert err < 2e-3
+
+
+def test_lsrtm_bf16_snapshots_and_repeat(ctx):
+    """The default configuration (BF16 snapshots, fast kernels) follows the FP64
+    solver closely, and a reset reproduces the same iterates bit for bit."""
+    sv = survey(seed=5)
+    nx, nz, shots, x0, wav, v0, _, dobs = sv
+    niter = 3
+    m_ref, rr0_ref, hist_ref = O.lsrtm_cgls(nx, nz, shots, x0, wav, v0, dobs, niter)
+    nx, nz, shots, x0, wav, v0, _, dobs = sv
+    with Lsrtm(ctx, nx, nz, shots, x0, snap_dtype=SNAP_BF16) as ls:
+        ls.set_background(v0, wav)
+        for k, d in enumerate(dobs):
+            ls.set_data(k, d)
+        rr0 = ls.reset()
+        h1 = ls.iterate(niter)
+        m1 = ls.model()
+        ls.reset()
+        h2 = ls.iterate(niter)
+        m2 = ls.model()
+    assert np.array_equal(h1, h2) and np.array_equal(m1, m2)
+    np.testing.assert_allclose(h1 / rr0, np.array(hist_ref) / rr0_ref, rtol=2e-2, atol=1e-4)
+    assert rel_l2(m1, m_ref) < 2e-2
+
+
+def test_vector_ops_match_opern(ctx):
+    """seis_fd_vec_dot / seis_fd_vec_axpby follow DOTPRODUCT (FP32 product,
+    FP64 sum) and ADDSCAL (formed in double) of src/util/arraymath.h."""
+    import torch
+    from seis_b200._lib import vec_axpby, vec_dot
+    rng = np.random.default_rng(1)
+    for n in (1, 1000, 3_000_001):
+        a = rng.standard_normal(n).astype(np.float32)
+        b = rng.standard_normal(n).astype(np.float32)
+        ta, tb = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+        torch.cuda.synchronize()
+        got = vec_dot(ctx, ta.data_ptr(), tb.data_ptr(), n)
+        want = float(np.sum((a * b).astype(np.float64)))
+        assert abs(got - want) <= 1e-12 * np.sum(np.abs(a * b).astype(np.float64))
+        vec_axpby(ctx, tb.data_ptr(), ta.data_ptr(), 0.3, -1.7, n)
+        want_y = (0.3 * a.astype(np.float64) - 1.7 * b.astype(np.float64)).astype(np.float32)
+        assert np.array_equal(tb.cpu().numpy(), want_y)
