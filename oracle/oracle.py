@@ -176,13 +176,15 @@ def rtm(shot, wav, vel, rec, prec="f32", impl="oracle"):
     return img
 
 
-def born_adjoint(shot, wav, vel, rec, prec="f64"):
+def born_adjoint(shot, wav, vel, rec, prec="f64", every=1):
     """Image [nx][nz] of the exact transpose of ``born`` (the library's own
-    adjoint; the reference has no exact adjoint to compare with)."""
+    adjoint; the reference has no exact adjoint to compare with).  With
+    ``every`` > 1 the imaging sum keeps every ``every``-th step of the source
+    term plus the last one, with trapezoid weights."""
     dt, (gz, wav, vel, rec) = _prep(shot, prec, "oracle", wav, vel, rec)
     img = np.zeros((shot.nx, shot.nz), dt)
-    rc = getattr(oracle_lib(), f"orc_born_adjoint_{prec}")(*_common_args(shot, prec), _ptr(gz),
-                                                           _ptr(wav), _ptr(vel), _ptr(rec), _ptr(img))
+    rc = getattr(oracle_lib(), f"orc_born_adjoint_thin_{prec}")(
+        *_common_args(shot, prec), _ptr(gz), _ptr(wav), _ptr(vel), _ptr(rec), _I(every), _ptr(img))
     if rc != 0:
         raise RuntimeError(f"oracle born_adjoint failed ({rc})")
     return img

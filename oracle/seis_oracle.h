@@ -35,7 +35,11 @@ extern "C" {
                   const R *rec, R *img);                                        \
   int orc_born_adjoint_##S(R dt, R dx, R dz, int nt, int ndel, int nx, int nz,  \
                            int pml, int sx, int sz, const int *gz,              \
-                           const R *wav, const R *vel, const R *rec, R *img);
+                           const R *wav, const R *vel, const R *rec, R *img);   \
+  int orc_born_adjoint_thin_##S(R dt, R dx, R dz, int nt, int ndel, int nx,     \
+                                int nz, int pml, int sx, int sz, const int *gz, \
+                                const R *wav, const R *vel, const R *rec,       \
+                                int every, R *img);
 
 SEIS_ORACLE_DECL(float, f32)
 SEIS_ORACLE_DECL(double, f64)

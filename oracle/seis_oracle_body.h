@@ -684,11 +684,27 @@ static void F(step_T)(const F(grid_t) *g, const F(coefs_t) *c, const REAL *yb, R
   F(twoway_T)(g, c, u3b, cb, pb);
 }
 
-/* Exact adjoint of orc_born: img[nx][nz] = L^T rec. */
-int F(orc_born_adjoint)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml,
-                        int sx, int sz, const int *gz, const REAL *wav, const REAL *vel,
-                        const REAL *rec, REAL *img)
+/* Weight of step k in the imaging sum over k = 0..K when only every m-th
+ * step (and step K) of the source term is kept: trapezoid weights over the
+ * kept steps, plus 1/2 at each end, summing to K + 1 (1 everywhere for m = 1).
+ * This is the library's own thinning rule, restated. */
+static double F(thin_weight)(int k, int K, int m)
 {
+  if (m == 1) return 1.0;
+  if (k % m != 0 && k != K) return 0.0;
+  int prev = k == 0 ? k : (k % m == 0 ? k - m : (K / m) * m);
+  int next = k == K ? k : (k + m < K ? k + m : K);
+  return 0.5 * (double)(next - prev + (k == 0) + (k == K));
+}
+
+/* Exact adjoint of orc_born: img[nx][nz] = L^T rec.  With every > 1 the
+ * imaging sum keeps only the thinned steps (weights above): the same
+ * operator with the source term sampled as the library samples it. */
+int F(orc_born_adjoint_thin)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz,
+                             int pml, int sx, int sz, const int *gz, const REAL *wav,
+                             const REAL *vel, const REAL *rec, int every, REAL *img)
+{
+  if (every < 1) return -2;
   F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
   const F(grid_t) *g = &gg;
   F(coefs_t) c;
@@ -716,7 +732,9 @@ int F(orc_born_adjoint)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int
       for (int ix = 0; ix < nx; ix++) AT(A, ix + pml, gz[ix] + pml) += rec[(size_t)ix * nt + (k - ndel)];
     F(step_T)(g, &c, A, B, C, u3b, u31b);
     const REAL *lap = laps + (size_t)k * n;
-    for (size_t i = 0; i < n; i++) gp[i] += lap[i] * u3b[i];
+    const REAL wk = (REAL)F(thin_weight)(k, NT - 1, every);
+    if (wk != KR(0))
+      for (size_t i = 0; i < n; i++) gp[i] += wk * lap[i] * u3b[i];
     REAL *t = A; A = B; B = C; C = t;
     memset(C, 0, n * sizeof(REAL));
   }
@@ -728,6 +746,14 @@ int F(orc_born_adjoint)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int
   free(laps); free(u0); free(u1); free(u2); free(u3b); free(u31b); free(gp);
   F(coefs_free)(&c);
   return 0;
+}
+
+int F(orc_born_adjoint)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml,
+                        int sx, int sz, const int *gz, const REAL *wav, const REAL *vel,
+                        const REAL *rec, REAL *img)
+{
+  return F(orc_born_adjoint_thin)(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, rec,
+                                  1, img);
 }
 
 #undef AT

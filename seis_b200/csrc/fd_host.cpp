@@ -442,6 +442,28 @@ int step(Plan &p, int mode, const StepArgs &a) {
   return SEIS_OK;
 }
 
+// Snapshot schedule of the adjoint imaging sum  sum_{k=0..K} f(k), K = NT-1,
+// f(k) = lap_k * mu(L_{k+1}).  Every m-th step is stored, and step K as well;
+// the stored steps t_0 = 0 < t_1 < ... < t_J = K carry trapezoid weights
+//   w_j = (t_{j+1} - t_{j-1}) / 2  (+ 1/2 at each end),
+// which sum to K + 1 and reduce to 1 for m = 1.  Against plain m-fold
+// weights this removes the first-order end error of a wavefield that is
+// still live at the last step.
+int snap_slot(int k, int K, int m) {
+  if (k < 0 || k > K) return -1;
+  if (k % m == 0) return k / m;
+  return k == K ? K / m + 1 : -1;
+}
+
+int snap_count(int K, int m) { return K / m + 1 + (K % m != 0); }
+
+float snap_weight(int k, int K, int m) {
+  if (m == 1) return 1.0f;
+  const int prev = k == 0 ? k : (k % m == 0 ? k - m : (K / m) * m);
+  const int next = k == K ? k : std::min(k + m, K);
+  return 0.5f * (float)(next - prev + (k == 0) + (k == K));
+}
+
 // Snapshot storage of every shot (first run of an adjoint plan), then the
 // shot table is uploaded again with the new pointers.
 int ensure_snapshots(Plan &p) {
@@ -450,7 +472,7 @@ int ensure_snapshots(Plan &p) {
   const size_t esize = p.snap_dtype == SNAP_F32 ? 4 : 2;
   for (int s = 0; s < p.nshot; s++) {
     ShotDev &g = p.sd[s];
-    int nsnap = (g.NT + p.snap_every - 1) / p.snap_every;
+    int nsnap = snap_count(g.NT - 1, p.snap_every);
     int ntx = (g.NX + TX - 1) / TX;
     unsigned char *snap = nullptr;
     int rc = p.alloc(&snap, (size_t)nsnap * g.nx * g.nz * esize);
@@ -504,7 +526,7 @@ int run_forward(Plan &p, int mode) {
     int itp = it - p.ndel;
     a.rec_k = (p.op != OP_RTM && p.op != OP_BORN_ADJ && itp >= 0) ? itp : -1;
     a.strip_k = (p.op == OP_RTM && itp >= 0) ? itp : -1;
-    a.snap_k = (p.op == OP_BORN_ADJ && it % p.snap_every == 0) ? it / p.snap_every : -1;
+    a.snap_k = p.op == OP_BORN_ADJ ? snap_slot(it, p.NT - 1, p.snap_every) : -1;
     int rc = step(p, mode, a);
     if (rc) return rc;
   }
@@ -565,14 +587,14 @@ int run_adjoint(Plan &p) {
   a.nshots = p.nshot;
   a.src_k = -1;
   a.strip_k = -1;
-  a.img_w = (float)p.snap_every;
   int r = 0;
   for (int k = p.NT; k >= 0; k--, r++) {
     a.rot = r;
     a.rot_b = r;
     int kd = k - 1 - p.ndel;
     a.rec_k = (kd >= 0 && kd < p.nt) ? kd : -1;
-    a.snap_k = (k <= p.NT - 1 && k % p.snap_every == 0) ? k / p.snap_every : -1;
+    a.snap_k = snap_slot(k, p.NT - 1, p.snap_every);
+    a.img_w = a.snap_k >= 0 ? snap_weight(k, p.NT - 1, p.snap_every) : 0.0f;
     int rc = adj_step(p, a);
     if (rc) return rc;
   }
