@@ -196,6 +196,23 @@ int seis_fd_born_adjoint(seis_fd_ctx *ctx, const seis_shot_desc *shot, const flo
 /* DOTPRODUCT (arraymath.h:230-299): *h_out = sum (double)(a[i] * b[i]). */
 int seis_fd_vec_dot(seis_fd_ctx *ctx, const float *d_a, const float *d_b, size_t n,
                     double *h_out);
+/* No counterpart in the reference.  The same dot product for callers that
+ * cannot allocate device memory (an application that owns the whole device
+ * budget, a plugin that must not bypass its host's memory pool, a loop that
+ * cannot afford the synchronisation cudaMalloc/cudaFree may cause): no
+ * context, no allocation.  *d_out (device memory) = sum (double)(a[i] * b[i]),
+ * FP32 products and FP64 sum as above, enqueued on `stream` (a cudaStream_t;
+ * null = legacy default stream) of the current device; the call returns once
+ * the work is enqueued.  Its scratch, 16384 partial sums (128 KiB) in a fixed
+ * array inside the library, limits n to SEIS_DOT_NOALLOC_MAX_N elements;
+ * larger n returns SEIS_ERR_ARG.  The first call on a device looks up that
+ * array's device address; make it before any stream capture.  All calls on a
+ * device share the array: calls whose GPU work overlaps (e.g. on two streams
+ * without ordering between them) race and give wrong sums.  A message for
+ * any error goes to err (err_len bytes, may be null). */
+#define SEIS_DOT_NOALLOC_MAX_N ((size_t)16384 * 4096)
+int seis_fd_vec_dot_noalloc(const float *d_a, const float *d_b, size_t n, double *d_out,
+                            void *stream, char *err, size_t err_len);
 /* ADDSCAL (arraymath.h:338-342): y = a x + b y, formed in double. */
 int seis_fd_vec_axpby(seis_fd_ctx *ctx, float *d_y, const float *d_x, double a, double b,
                       size_t n);
