@@ -1,29 +1,38 @@
 """Benchmark of the B200 FD engine -- one JSON line on stdout (rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload born_lsrtm]
+                    [--nt NT]
 
-Workload ``born_lsrtm`` (default): linearised Born modeling of all 32 shots of
-the 1200x400 LSRTM survey (10 m grid, pml 40, nt 5000 + 94 delay steps,
-dt 0.8 ms, 20 Hz Ricker, full-aperture receivers at gz=1), i.e. the forward
-half of one LSRTM CG iteration.  One step = one batched Born run of the 32
-shots (two fields advanced per time step).  Metric: padded grid cell-updates
-per second (Gcell/s), whole job.
+Workload ``lsrtm_iter`` (default): one least-squares RTM CG iteration (CGLS)
+on the 32-shot survey of the 1200x400 model (10 m grid, pml 40, nt 5000 + 94
+delay steps, dt 0.8 ms, 20 Hz Ricker, full-aperture receivers at gz=1):
+Born modeling of all 32 shots (two fields per step), the exact adjoint of all
+32 shots (one field per step, imaging from BF16 source snapshots kept every 4
+steps) and the FP64 CG vector algebra.  The background velocity is fixed, so
+the source snapshots are computed once when the solver is reset and reused by
+every iteration.  One step = one CG iteration.  Metric: padded grid
+cell-updates per second (Gcell/s), whole job; ``ms_per_step`` is the LSRTM
+iteration time.
 
-* ``value``: device-resident inputs, CUDA-event timed graph replays.
-* ``e2e``: the same through the public plan API with host buffers: every step
-  uploads velocity, perturbation and wavelet of every shot from pinned memory
-  and downloads every gather.
-* ``roofline``: the interior-tile kernel (dominant), algorithmic bytes per
-  launch (16 B per field-update: read prev, cur, vel; write next -- the Born
-  kernel also reads dv, counted inside 16 B x 2 fields) over its mean
+* ``value``: device-resident solver state, CUDA-event timed iterations.
+* ``e2e``: the public LSRTM API with host buffers, every step: background and
+  wavelet upload, observed data of every shot uploaded from pinned memory,
+  reset (source pass + first adjoint), one iteration, model download; its
+  Gcell/s counts every cell-update of that work.
+* ``plain_fp32``: the same iteration on the plain path -- one shot per plan
+  and launch sequence, FP32 source snapshots at every step recomputed for
+  every shot (32 shots' snapshots do not fit in HBM), timed on a sample of
+  shots and scaled to 32.
+* ``roofline``: the kernel with the largest share of the iteration,
+  algorithmic bytes per launch (16 B per field cell-update: read prev, cur,
+  velocity, write next; Born's dv read is inside its 2 x 16 B) over its mean
   CUDA-event duration, against the measured HBM copy bandwidth.
-* ``cpu_baseline``: the reference's own ``forward`` (src/util/fd.cpp:81-177,
-  compiled from its sources into oracle/_ref) on one shot of the workload with
-  the time loop cut to a bounded number of steps, all host threads.
+* ``cpu_baseline``: the reference's own ``forward`` and ``adjoint``
+  (src/util/fd.cpp:81-177, :592-719, compiled from its sources into
+  oracle/_ref) on shot 0 with the time loop cut short, all host threads,
+  expressed as this iteration's cell-updates per second.
 
-Under torchrun (N > 1) every rank runs its own 32-shot survey (weak scaling);
-there is no data-path collective in this workload.
+Under torchrun (N > 1) every rank runs its own 32-shot survey (weak scaling).
 """
 from __future__ import annotations
 
@@ -135,48 +144,69 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
-def workload(name: str, rank: int):
+def workload(name: str, rank: int, nt: int = 5000):
     from seis_b200 import synth
-    if name == "born_lsrtm":
-        return synth.lsrtm()
+    if name == "lsrtm_iter":
+        return synth.lsrtm(nt=nt)
     raise SystemExit(f"unknown workload {name}")
 
 
-def cpu_baseline(sv, steps_cap: int = 300):
-    """Reference `forward` (compiled from its own sources) on shot 0 of the
-    survey, time loop cut to `steps_cap` recorded samples."""
+SNAP_EVERY = 4
+
+
+def iteration_cells(shots) -> int:
+    """Cell-updates of one CG iteration: Born (2 fields x NT steps) and the
+    exact adjoint's reverse pass (1 field x NT+1 steps) of every shot."""
+    return sum((s.nx + 2 * s.pml) * (s.nz + 2 * s.pml) * (3 * s.NT + 1) for s in shots)
+
+
+def reset_cells(shots) -> int:
+    """Cell-updates of a solver reset: source pass (NT) + one adjoint (NT+1)."""
+    return sum((s.nx + 2 * s.pml) * (s.nz + 2 * s.pml) * (2 * s.NT + 1) for s in shots)
+
+
+def cpu_baseline(sv, steps_cap: int = 150):
+    """The reference's `forward` (Born) and `adjoint` (RTM), compiled from its
+    own sources, on shot 0 with the recorded time samples cut to `steps_cap`;
+    rate = this library's cell-updates of one CG iteration for that shot and
+    step count (3 NT + 1 per padded cell) over the reference's Born + adjoint
+    time, i.e. the reference's speed on the same job."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    s0 = sv.shots[0]
     from seis_b200 import Shot
+    s0 = sv.shots[0]
     s = Shot(nx=s0.nx, nz=s0.nz, pml=s0.pml, nt=steps_cap, ndel=s0.ndel, sx=s0.sx, sz=s0.sz,
              dt=s0.dt, dx=s0.dx, dz=s0.dz, gz=s0.gz)
     wav = sv.wavelet()[:s.NT]
     vel, dv = sv.sub(sv.vel0, 0), sv.sub(sv.dv, 0)
     kind = "reference" if O.ref_available() else "port"
     cores = len(os.sched_getaffinity(0))
+    impl = "ref" if kind == "reference" else "oracle"
     if kind == "reference":
         O.ref_set_threads(cores)
-    t = time.perf_counter()
-    if kind == "reference":
-        O.born(s, wav, vel, dv, impl="ref")
     else:
         cores = 1
-        O.born(s, wav, vel, dv)
-    dt = time.perf_counter() - t
-    cells = 2 * (s.nx + 2 * s.pml) * (s.nz + 2 * s.pml) * s.NT
+    t = time.perf_counter()
+    rec = O.born(s, wav, vel, dv, impl=impl)
+    t_born = time.perf_counter() - t
+    t = time.perf_counter()
+    O.rtm(s, wav, vel, rec, impl=impl)
+    t_adj = time.perf_counter() - t
+    dt = t_born + t_adj
+    cells = iteration_cells([s])
     return {"value": cells / dt / 1e9, "unit": "Gcell/s", "cores": cores, "kind": kind,
-            "sample": f"Born of shot 0 ({s.nx}x{s.nz}, pml {s.pml}), {s.NT} of {s0.NT} steps, "
-                      f"{dt:.2f} s"}
+            "sample": f"forward (Born) {t_born:.2f} s + adjoint (RTM) {t_adj:.2f} s of shot 0 "
+                      f"({s.nx}x{s.nz}, pml {s.pml}), {s.NT} of {s0.NT} steps; the reference has "
+                      f"no CG, so one iteration = these two calls per shot"}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    sv = workload(args.workload, rank)
+    sv = workload(args.workload, rank, args.nt)
     vals = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(sv, steps_cap=120 if i < args.warmup else 200)
+        r = cpu_baseline(sv, steps_cap=40 if i < args.warmup else 150)
         if i >= args.warmup:
             vals.append(r["value"])
     v = statistics.median(vals)
@@ -190,14 +220,95 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def observed_data(ctx, sv):
+    """Synthetic observed data: Born gathers of the true perturbation over the
+    background, exact-rounding kernels."""
+    from seis_b200._lib import IN_DV, IN_VEL, IN_WAVELET, OP_BORN, OUT_GATHER, Plan
+    wav = sv.wavelet()
+    with Plan(ctx, OP_BORN, sv.shots) as p:
+        for i in range(len(sv.shots)):
+            p.set(i, IN_VEL, sv.sub(sv.vel0, i))
+            p.set(i, IN_DV, sv.sub(sv.dv, i))
+            p.set(i, IN_WAVELET, wav)
+        p.run()
+        return [p.get(i, OUT_GATHER) for i in range(len(sv.shots))]
+
+
+def kernel_roofline(ctx, sv, iter_ms):
+    """Per-kernel CUDA-event durations of the Born and adjoint step kernels
+    (separate plans over the same shots), their share of one iteration, and
+    the roofline of the kernel with the largest share."""
+    from seis_b200._lib import IN_VEL, IN_WAVELET, OP_BORN, OP_BORN_ADJOINT, Plan
+    wav = sv.wavelet()
+    NT = sv.shots[0].NT
+    rows = []
+    for op, name, launches in ((OP_BORN, "born", NT), (OP_BORN_ADJOINT, "adjoint", NT + 1)):
+        with Plan(ctx, op, sv.shots) as p:
+            for i in range(len(sv.shots)):
+                p.set(i, IN_VEL, sv.sub(sv.vel0, i))
+                p.set(i, IN_WAVELET, wav)
+            p.time_kernels(20)
+            ms, by = p.time_kernels(200)
+        for k, kname in ((0, "interior"), (1, "pad")):
+            rows.append({"kernel": f"{name}_{kname}", "ms": ms[k], "bytes": by[k],
+                         "launches_per_iter": launches,
+                         "share": ms[k] * launches / iter_ms})
+        rows.append({"kernel": f"{name}_step", "ms": ms[2], "launches_per_iter": launches,
+                     "share": ms[2] * launches / iter_ms})
+    kern = [r for r in rows if "bytes" in r]
+    top = max(kern, key=lambda r: r["ms"] * r["launches_per_iter"])
+    return top, rows
+
+
+def plain_fp32(ctx, sv, dobs, nsample: int = 2):
+    """One CG iteration on the plain path, timed on `nsample` shots and scaled
+    to the survey: per shot, one single-shot Born plan run and one single-shot
+    adjoint plan run with FP32 snapshots at every step (recomputed per shot)."""
+    import torch
+    from seis_b200._lib import (IN_DV, IN_GATHER, IN_VEL, IN_WAVELET, OP_BORN, OP_BORN_ADJOINT,
+                                SNAP_F32, Plan)
+    wav = sv.wavelet()
+    p0 = np.zeros((sv.nx, sv.nz), np.float32) + 1.0
+    with Plan(ctx, OP_BORN, [sv.shots[0]]) as pb, Plan(ctx, OP_BORN_ADJOINT, [sv.shots[0]]) as pa:
+        pa.set_snapshots(1, SNAP_F32)
+        stream = torch.cuda.ExternalStream(ctx.stream_ptr)
+
+        def shot(i):
+            pb.set(0, IN_VEL, sv.sub(sv.vel0, i))
+            pb.set(0, IN_WAVELET, wav)
+            pb.set(0, IN_DV, sv.sub(p0, i))
+            pb.run()
+            pa.set(0, IN_VEL, sv.sub(sv.vel0, i))
+            pa.set(0, IN_WAVELET, wav)
+            pa.set(0, IN_GATHER, dobs[i])
+            pa.run()
+            pa.sync()
+
+        shot(0)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record(stream)
+        for i in range(1, 1 + nsample):
+            shot(i)
+        stop.record(stream)
+        stop.synchronize()
+        per_shot = start.elapsed_time(stop) / nsample
+    return {"iter_ms": per_shot * len(sv.shots), "per_shot_ms": per_shot, "sampled_shots": nsample,
+            "how": "one shot per plan and graph; Born run, then adjoint with FP32 snapshots at "
+                   "every step, source pass recomputed per shot; sample scaled to all shots"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="born_lsrtm")
+    ap.add_argument("--workload", default="lsrtm_iter")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--nt", type=int, default=5000,
+                    help="recorded time samples (a shorter loop of the same launches, for profiling)")
     args = ap.parse_args()
     rank, world, local = dist_init()
     if args.impl == "reference":
@@ -207,95 +318,109 @@ def main():
 
     import torch
     from seis_b200 import Context
-    from seis_b200._lib import IN_DV, IN_VEL, IN_WAVELET, OP_BORN, OUT_GATHER, Plan, ptr
+    from seis_b200._lib import SNAP_BF16, Lsrtm
 
     torch.cuda.set_device(local)
-    sv = workload(args.workload, rank)
+    sv = workload(args.workload, rank, args.nt)
     shots = sv.shots
     ctx = Context(local)
-    plan = Plan(ctx, OP_BORN, shots)
     wav = sv.wavelet()
-    vels = [sv.sub(sv.vel0, i) for i in range(len(shots))]
-    dvs = [sv.sub(sv.dv, i) for i in range(len(shots))]
-    for i in range(len(shots)):
-        plan.set(i, IN_VEL, vels[i])
-        plan.set(i, IN_DV, dvs[i])
-        plan.set(i, IN_WAVELET, wav)
-    cells = plan.cell_updates
+    dobs = observed_data(ctx, sv)
+    ls = Lsrtm(ctx, sv.nx, sv.nz, shots, sv.x0, snap_every=SNAP_EVERY, snap_dtype=SNAP_BF16)
+    ls.set_background(sv.vel0, wav)
+    for i, d in enumerate(dobs):
+        ls.set_data(i, d)
+    rr0 = ls.reset()
+    cells = iteration_cells(shots)
+    assert cells == ls.cell_updates, (cells, ls.cell_updates)
 
-    # ---- device-resident: graph replays timed with CUDA events on the
+    # ---- device-resident: CG iterations timed with CUDA events on the
     # library's stream
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local))
-    for _ in range(args.warmup):
-        plan.run()
-    plan.sync()
+    rr_warm = ls.iterate(args.warmup) if args.warmup > 0 else []
+    launches0 = ctx.launches
     barrier(world)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rr = []
     with Clocks(local) as clk:
         torch.cuda.synchronize()
         start.record(stream)
         for _ in range(args.steps):
-            plan.run()
+            rr.extend(ls.iterate(1).tolist())
         stop.record(stream)
         stop.synchronize()
         torch.cuda.synchronize()
     clocks = clk.summary()
+    launches = ctx.launches - launches0
     ms_per_step = start.elapsed_time(stop) / args.steps
     ms_per_step = max_over_ranks(ms_per_step, world)
     value = cells * world / (ms_per_step / 1e3) / 1e9
 
-    # ---- end to end through the plan API with pinned host buffers
-    pin = lambda a: torch.from_numpy(a).pin_memory()
-    h_vel = [pin(v) for v in vels]
-    h_dv = [pin(d) for d in dvs]
-    h_wav = pin(wav)
-    h_rec = [torch.empty((s.nx, s.nt), dtype=torch.float32).pin_memory() for s in shots]
+    # ---- end to end through the public LSRTM API with pinned host buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    h_v0, h_wav = pin(sv.vel0), pin(wav)
+    h_d = [pin(d) for d in dobs]
+    h_m = torch.empty((sv.nx, sv.nz), dtype=torch.float32).pin_memory()
+    h_rr = torch.empty(2, dtype=torch.float64)
     L = ctx.L
+    import ctypes
 
     def e2e_step():
+        ctx.check(L.seis_fd_lsrtm_set_background(ls.h, h_v0.data_ptr(), h_wav.data_ptr()))
         for i in range(len(shots)):
-            ctx.check(L.seis_fd_plan_set(plan.h, i, IN_VEL, h_vel[i].data_ptr()))
-            ctx.check(L.seis_fd_plan_set(plan.h, i, IN_DV, h_dv[i].data_ptr()))
-            ctx.check(L.seis_fd_plan_set(plan.h, i, IN_WAVELET, h_wav.data_ptr()))
-        plan.run()
-        for i in range(len(shots)):
-            ctx.check(L.seis_fd_plan_get(plan.h, i, OUT_GATHER, h_rec[i].data_ptr()))
+            ctx.check(L.seis_fd_lsrtm_set_data(ls.h, i, h_d[i].data_ptr()))
+        ctx.check(L.seis_fd_lsrtm_reset(ls.h, ctypes.c_void_p(h_rr.data_ptr())))
+        ctx.check(L.seis_fd_lsrtm_iterate(ls.h, 1, ctypes.c_void_p(h_rr.data_ptr() + 8)))
+        ctx.check(L.seis_fd_lsrtm_model(ls.h, h_m.data_ptr()))
 
-    e2e_step()
+    e2e_steps = max(1, args.steps // 2)
     barrier(world)
     t0 = time.perf_counter()
-    for _ in range(max(1, args.steps // 2)):
+    for _ in range(e2e_steps):
         e2e_step()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / max(1, args.steps // 2)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
     e2e_ms = max_over_ranks(e2e_ms, world)
-    h2d = sum(v.nbytes + d.nbytes + wav.nbytes for v, d in zip(vels, dvs))
-    d2h = sum(s.nx * s.nt * 4 for s in shots)
+    e2e_cells = cells + reset_cells(shots)
+    h2d = sv.vel0.nbytes + wav.nbytes + sum(d.nbytes for d in dobs)
+    d2h = h_m.numel() * 4 + 16
+    dev_bytes = ls.device_bytes
+    ls.close()
 
-    # ---- roofline of the dominant kernel
-    ms, by = plan.time_kernels(200)
+    # ---- roofline of the kernel with the largest share, plain FP32 path
+    top, rows = kernel_roofline(ctx, sv, ms_per_step)
     hbm, src = peaks()
-    ach = by[0] / (ms[0] * 1e-3) / 1e9
+    ach = top["bytes"] / (top["ms"] * 1e-3) / 1e9
+    plain = None if args.no_plain else plain_fp32(ctx, sv, dobs)
     line = {
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": args.workload, "shots_per_gpu": len(shots), "grid": "1200x400 pml 40",
-                   "nt": shots[0].nt, "ndel": shots[0].ndel, "fields": 2,
-                   "cell_updates_per_step": cells, "l2": "inputs larger than L2 "
-                   f"({(sum(v.nbytes for v in vels) * 8) / 2**20:.0f} MiB working set)"},
-        "e2e": {"value": cells * world / (e2e_ms / 1e3) / 1e9, "unit": "Gcell/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "data": "synthetic (layered + faulted 1200x400 model; observed data = Born of the true "
+                "perturbation)",
+        "config": {"workload": args.workload, "shots_per_gpu": len(shots),
+                   "grid": "1200x400 at 10 m, pml 40", "nt": shots[0].nt, "ndel": shots[0].ndel,
+                   "snapshots": f"BF16 every {SNAP_EVERY} steps, per-tile scale",
+                   "cell_updates_per_step": cells, "lsrtm_iter_ms": ms_per_step,
+                   "device_bytes": dev_bytes,
+                   "l2": "inputs larger than L2: fields, snapshots and data of 32 shots "
+                         f"({dev_bytes / 2**30:.1f} GiB resident)",
+                   "residual": {"rr0": rr0, "after_warmup": list(map(float, rr_warm)),
+                                "timed": rr}},
+        "e2e": {"value": e2e_cells * world / (e2e_ms / 1e3) / 1e9, "unit": "Gcell/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                "cell_updates_per_step": e2e_cells},
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                     "frac": ach / hbm, "traffic": None, "kernel": "interior_kernel<BORN>",
-                     "peak_source": src, "interior_ms": ms[0], "boundary_ms": ms[1],
-                     "step_ms": ms[2]},
-        "gpu_launches": plan.launches_per_run * args.steps,
+                     "frac": ach / hbm, "traffic": None, "kernel": top["kernel"],
+                     "peak_source": src, "kernel_ms": top["ms"], "share": top["share"],
+                     "kernels": rows},
+        "plain_fp32": plain,
+        "gpu_launches": launches,
         "clocks": clocks,
     }
+    if plain:
+        line["config"]["speedup_vs_plain_fp32"] = plain["iter_ms"] / ms_per_step
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sv)
-    plan.close()
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

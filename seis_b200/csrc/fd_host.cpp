@@ -125,6 +125,8 @@ struct Plan {
   ShotDev *d_sd = nullptr;
   Tile *d_tiles = nullptr;
   int2 *d_cols = nullptr;
+  std::vector<PadChunk> chunks;  // pad cells of the batch (absorbing kernel)
+  PadChunk *d_chunks = nullptr;
   float *d_taps = nullptr;
   float *d_stage = nullptr;  // staging for unpadded uploads / transposes
   size_t stage_elems = 0;
@@ -204,8 +206,11 @@ void build_tiles(Plan &p) {
   size_t most = 0;
   for (int s = 0; s < p.nshot; s++) {
     const ShotDev &g = p.sd[s];
-    int lox = std::max(g.pml, 4), hix = std::min(g.pml + g.nx, g.NX - 4);
-    int loz = std::max(g.pml, 4), hiz = std::min(g.pml + g.nz, g.NZ - 4);
+    // interior tiles keep one cell off the model edge: the one-way update of
+    // the first pad ring reads the two-way values of the edge cells, which
+    // only pad tiles keep
+    int lox = std::max(g.pml + 1, 4), hix = std::min(g.pml + g.nx - 1, g.NX - 4);
+    int loz = std::max(g.pml + 1, 4), hiz = std::min(g.pml + g.nz - 1, g.NZ - 4);
     for (int x0 = 0; x0 < g.NX; x0 += TX)
       for (int z0 = 0; z0 < g.NZ; z0 += TZ) {
         bool in = x0 >= lox && x0 + TX <= hix && z0 >= loz && z0 + TZ <= hiz;
@@ -221,6 +226,27 @@ void build_tiles(Plan &p) {
   p.n_int = 0;
   for (const Tile &t : p.tiles) p.n_int += t.kind == TILE_INTERIOR;
   p.n_pad = (int)p.tiles.size() - p.n_int;
+  // pad cells: left and right blocks over the full height, top and bottom
+  // blocks over the model columns, cut into rectangles of at most
+  // ABS_NT * ABS_CPT cells (z fastest)
+  p.chunks.clear();
+  constexpr int CH = ABS_NT * ABS_CPT;
+  auto block = [&](int s, int xa, int xb, int za, int zb) {
+    const int R = zb - za, Cn = xb - xa;
+    if (R <= 0 || Cn <= 0) return;
+    const int k = (R + CH - 1) / CH, nrows = (R + k - 1) / k;
+    const int ncols = std::max(1, CH / nrows);
+    for (int x = xa; x < xb; x += ncols)
+      for (int z = za; z < zb; z += nrows)
+        p.chunks.push_back(PadChunk{s, x, z, std::min(ncols, xb - x), std::min(nrows, zb - z)});
+  };
+  for (int s = 0; s < p.nshot; s++) {
+    const ShotDev &g = p.sd[s];
+    block(s, 0, g.pml, 0, g.NZ);
+    block(s, g.pml + g.nx, g.NX, 0, g.NZ);
+    block(s, g.pml, g.pml + g.nx, 0, g.pml);
+    block(s, g.pml, g.pml + g.nx, g.pml + g.nz, g.NZ);
+  }
 }
 
 // Tiles for the exact adjoint: interior tiles need their 4-cell halo strictly
@@ -358,6 +384,8 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fa[k]);
     if (op == OP_BORN || op == OP_RTM)
       for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fb[k]);
+    if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.u3s[0]);
+    if (rc == SEIS_OK && op == OP_BORN) rc = alloc_field(*p, g, &g.u3s[1]);
     float *vel = nullptr, *dv = nullptr, *wav = nullptr, *rec = nullptr;
     int *gzd = nullptr;
     if (rc == SEIS_OK) rc = alloc_field(*p, g, &vel);
@@ -394,6 +422,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
   }
   if (rc == SEIS_OK) rc = p->alloc(&p->d_tiles, p->tiles.size());
   if (rc == SEIS_OK) rc = p->alloc(&p->d_adj_tiles, p->adj_tiles.size());
+  if (rc == SEIS_OK) rc = p->alloc(&p->d_chunks, p->chunks.size());
   if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&p->d_cols, p->cols.size());
   if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&p->d_taps, (size_t)61);
   if (rc == SEIS_OK) {
@@ -405,6 +434,9 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
                           cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(p->d_adj_tiles, p->adj_tiles.data(), sizeof(Tile) * p->adj_tiles.size(),
+                          cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !p->chunks.empty())
+      e = cudaMemcpyAsync(p->d_chunks, p->chunks.data(), sizeof(PadChunk) * p->chunks.size(),
                           cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && op == OP_RTM) {
       e = cudaMemcpyAsync(p->d_cols, p->cols.data(), sizeof(int2) * p->cols.size(),
@@ -434,11 +466,14 @@ int step(Plan &p, int mode, const StepArgs &a) {
   seis_fd_ctx *ctx = p.ctx;
   CK(cudaEventRecord(ctx->fork, ctx->stream));
   CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
-  CK(launch_step(mode, p.exact, p.d_sd, p.d_tiles, p.n_int, p.n_pad, ctx->num_sms, a, ctx->d_err,
+  StepArgs b = a;
+  b.chunks = p.d_chunks;
+  b.nchunks = (int)p.chunks.size();
+  CK(launch_step(mode, p.exact, p.d_sd, p.d_tiles, p.n_int, p.n_pad, ctx->num_sms, b, ctx->d_err,
                  ctx->stream, ctx->aux));
   CK(cudaEventRecord(ctx->join, ctx->aux));
   CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
-  ctx->launches += (p.n_int > 0) + (p.n_pad > 0);
+  ctx->launches += (p.n_int > 0) + (p.n_pad > 0) + (p.n_pad > 0 && b.nchunks > 0);
   return SEIS_OK;
 }
 
@@ -919,31 +954,44 @@ int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double 
   int fields = p.op == OP_BORN ? 2 : 1;
   cudaEvent_t ev[5];
   for (auto &e : ev) CK(cudaEventCreate(&e));
+  // adjoint plans time the reverse-step kernels (no imaging term)
+  const bool adj = p.op == OP_BORN_ADJ;
+  const std::vector<Tile> &tl = adj ? p.adj_tiles : p.tiles;
+  const int n_int = adj ? p.n_int_adj : p.n_int, n_pad = adj ? p.n_pad_adj : p.n_pad;
+  const Tile *d_tl = adj ? p.d_adj_tiles : p.d_tiles;
   int64_t cells_int = 0, cells_pad = 0;
-  for (size_t i = 0; i < p.tiles.size(); i++) {
-    const Tile &t = p.tiles[i];
+  for (size_t i = 0; i < tl.size(); i++) {
+    const Tile &t = tl[i];
     const ShotDev &g = p.sd[t.shot];
     int64_t c = (int64_t)std::min(TX, g.NX - t.x0) * std::min(TZ, g.NZ - t.z0);
-    ((int)i < p.n_int ? cells_int : cells_pad) += c;
+    ((int)i < n_int ? cells_int : cells_pad) += c;
   }
   StepArgs a{};
   a.nshots = p.nshot;
   a.strip_k = -1;
+  a.chunks = p.d_chunks;
+  a.nchunks = (int)p.chunks.size();
   double t_int = 0, t_pad = 0, t_step = 0;
   for (int k = 0; k < steps; k++) {
     a.rot = k; a.rot_b = k;
     int it = k % p.NT;
     a.src_k = it >= 1 ? it - 1 : -1;
-    a.rec_k = it - p.ndel >= 0 && p.op != OP_RTM ? it - p.ndel : -1;
+    a.rec_k = it - p.ndel >= 0 && p.op != OP_RTM && !adj ? it - p.ndel : -1;
     // interior kernel on the main stream, pad kernel on the auxiliary one,
     // concurrently, each bracketed by events on its own stream
     CK(cudaEventRecord(ev[0], ctx->stream));
     CK(cudaStreamWaitEvent(ctx->aux, ev[0], 0));
     CK(cudaEventRecord(ev[2], ctx->aux));
-    CK(launch_step(mode, p.exact, p.d_sd, p.d_tiles, p.n_int, 0, ctx->num_sms, a, ctx->d_err,
-                   ctx->stream, ctx->aux));
-    CK(launch_step(mode, p.exact, p.d_sd, p.d_tiles + p.n_int, 0, p.n_pad, ctx->num_sms, a,
-                   ctx->d_err, ctx->stream, ctx->aux));
+    if (adj) {
+      CK(fast::launch_adjoint(p.d_sd, d_tl, n_int, 0, a, ctx->d_err, ctx->stream, ctx->aux));
+      CK(fast::launch_adjoint(p.d_sd, d_tl + n_int, 0, n_pad, a, ctx->d_err, ctx->stream,
+                              ctx->aux));
+    } else {
+      CK(launch_step(mode, p.exact, p.d_sd, d_tl, n_int, 0, ctx->num_sms, a, ctx->d_err,
+                     ctx->stream, ctx->aux));
+      CK(launch_step(mode, p.exact, p.d_sd, d_tl + n_int, 0, n_pad, ctx->num_sms, a,
+                     ctx->d_err, ctx->stream, ctx->aux));
+    }
     CK(cudaEventRecord(ev[1], ctx->stream));
     CK(cudaEventRecord(ev[3], ctx->aux));
     CK(cudaStreamWaitEvent(ctx->stream, ev[3], 0));
@@ -954,7 +1002,7 @@ int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double 
     CK(cudaEventElapsedTime(&a2, ev[2], ev[3]));
     CK(cudaEventElapsedTime(&a3, ev[0], ev[4]));
     t_int += a1; t_pad += a2; t_step += a3;
-    ctx->launches += 2;
+    ctx->launches += 2 + (!adj && n_pad > 0 && a.nchunks > 0);
   }
   for (auto &e : ev) cudaEventDestroy(e);
   ms[0] = t_int / steps; ms[1] = t_pad / steps; ms[2] = t_step / steps;

@@ -20,12 +20,22 @@ constexpr int XM = 16;
 constexpr int LAYERS = 4;   // boundary layers kept for reconstruction
 
 enum TileKind : int {
-  TILE_INTERIOR = 0,  // every cell inside the model and 8th order: no absorbing terms
-  TILE_PAD = 1,       // touches the pad, the frame or the low-order rings
+  TILE_INTERIOR = 0,  // every cell inside the model, 8th order and off the model's edge
+                      // rows / columns (which the one-way update of the pad reads)
+  TILE_PAD = 1,       // touches the pad, the frame, the low-order rings or the model edge
 };
 
 struct Tile {
   int shot, x0, z0, kind;
+};
+
+// A rectangle of pad cells (one shot, ncols x nrows cells, z fastest) given to
+// one CTA of the absorbing-boundary kernel (ABS_NT threads, ABS_CPT cells
+// each); ncols * nrows <= ABS_NT * ABS_CPT.
+constexpr int ABS_NT = 256;
+constexpr int ABS_CPT = 4;
+struct PadChunk {
+  int shot, x0, z0, ncols, nrows;
 };
 
 // 2-D TMA tensor maps of one shot (each describes one margin-padded field
@@ -79,6 +89,10 @@ struct ShotDev {
   int snap_every;
   int ntz;               // tiles along z of this shot (scale indexing)
   int pad_;
+  // two-way values of the cells of pad tiles before the absorbing blend
+  // (field A or the receiver field; Born: [1] = scattered field), read by the
+  // absorbing-boundary kernel
+  float *u3s[2];
 };
 enum SnapType : int { SNAP_NONE = 0, SNAP_F32 = 1, SNAP_BF16 = 2, SNAP_F16 = 3 };
 static_assert(sizeof(ShotDev) % sizeof(int) == 0 && sizeof(ShotDev) <= 256 * sizeof(int),
@@ -94,6 +108,8 @@ struct StepArgs {
   int nshots = 0;
   int snap_k = -1;   // snapshot index written (forward) or imaged (adjoint)
   float img_w = 0.f; // adjoint: weight of the imaging term (snapshot interval)
+  const PadChunk *chunks = nullptr;  // pad cells of the batch (absorbing kernel)
+  int nchunks = 0;
 };
 
 // Allocation geometry of one field of a shot: LDZ floats per column, and the

@@ -7,32 +7,25 @@ namespace seis {
 namespace SEIS_NS {
 
 namespace {
-int g_ctas[3][2] = {{0, 0}, {0, 0}, {0, 0}};
-
 template <int MODE, int KIND>
 cudaError_t setup() {
-  cudaError_t e = cudaFuncSetAttribute(tile_kernel<MODE, KIND>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)TCfg<MODE, KIND>::bytes);
-  if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_ctas[MODE][KIND], tile_kernel<MODE, KIND>,
-                                                      nthreads<KIND>(), TCfg<MODE, KIND>::bytes);
-  return e;
+  return cudaFuncSetAttribute(tile_kernel<MODE, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)TCfg<MODE, KIND>::bytes);
 }
 
+// Interior tiles on s_int; pad tiles and then the absorbing kernel on s_pad
+// (it reads the pad tiles' two-way values).
 template <int MODE>
 cudaError_t launch_t(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
-                     int num_sms, const StepArgs &a, int *d_err, cudaStream_t s_int,
-                     cudaStream_t s_pad) {
+                     const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad) {
   if (n_int > 0)
-    tile_kernel<MODE, TILE_INTERIOR>
-        <<<n_int, nthreads<TILE_INTERIOR>(), TCfg<MODE, TILE_INTERIOR>::bytes, s_int>>>(
-        d_shots, d_tiles, n_int, a, d_err);
+    tile_kernel<MODE, TILE_INTERIOR><<<n_int, NT_T, TCfg<MODE, TILE_INTERIOR>::bytes, s_int>>>(
+        d_shots, d_tiles, a, d_err);
   if (n_pad > 0) {
-    int grid = num_sms * (g_ctas[MODE][TILE_PAD] > 0 ? g_ctas[MODE][TILE_PAD] : 1);
-    grid = grid < n_pad ? grid : n_pad;
-    tile_kernel<MODE, TILE_PAD><<<grid, nthreads<TILE_PAD>(), TCfg<MODE, TILE_PAD>::bytes, s_pad>>>(
-        d_shots, d_tiles + n_int, n_pad, a, d_err);
+    tile_kernel<MODE, TILE_PAD><<<n_pad, NT_T, TCfg<MODE, TILE_PAD>::bytes, s_pad>>>(
+        d_shots, d_tiles + n_int, a, d_err);
+    if (a.nchunks > 0)
+      absorb_kernel<MODE><<<a.nchunks, ABS_NT, 0, s_pad>>>(d_shots, a.chunks, a);
   }
   return cudaGetLastError();
 }
@@ -53,11 +46,11 @@ cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, i
                         cudaStream_t s_pad) {
   switch (mode) {
     case MODE_MODEL:
-      return launch_t<MODE_MODEL>(d_shots, d_tiles, n_int, n_pad, num_sms, a, d_err, s_int, s_pad);
+      return launch_t<MODE_MODEL>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
     case MODE_RCV:
-      return launch_t<MODE_RCV>(d_shots, d_tiles, n_int, n_pad, num_sms, a, d_err, s_int, s_pad);
+      return launch_t<MODE_RCV>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
     case MODE_BORN:
-      return launch_t<MODE_BORN>(d_shots, d_tiles, n_int, n_pad, num_sms, a, d_err, s_int, s_pad);
+      return launch_t<MODE_BORN>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
     default:
       return cudaErrorInvalidValue;
   }

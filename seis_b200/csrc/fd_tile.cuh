@@ -1,23 +1,22 @@
-// Time-step kernel of the 2-D acoustic FD engine (sm_100a): persistent CTAs
-// over a tile list, double-buffered bulk-copy staging.
+// Time-step kernels of the 2-D acoustic FD engine (sm_100a).
 //
-// One launch advances every shot of a batch by one time step.  The padded grid
-// of every shot is cut into TX x TZ tiles; each persistent CTA walks the tile
-// list with stride gridDim.x.  While it computes tile i, the column segments of
-// tile i+1 (current field with a 5-column / 8-row halo; previous field,
-// velocity and -- for Born -- perturbation with a 1-column / 8-row halo) are in
-// flight into the other shared-memory buffer as 2-D TMA tensor copies
-// (cp.async.bulk.tensor, one per array, one mbarrier per buffer, no multicast).
-//
-// Per tile, two paths (uniform per CTA):
-//  * interior tiles (every cell inside the model and in the 8th-order region):
-//    vector two-way update from shared memory; the absorbing blend is the
-//    identity there (w = 1, u31 = 0; src/util/fd.cpp:55-56);
-//  * pad tiles: the two-way field on tile + 1 halo into shared memory (frame,
-//    low-order rings and injections included), then the one-way update and
-//    blend per pad cell (processBoundary, fd.cpp:1053-1180).
-// Each thread owns a 4-row x 2-column micro-tile.  Cells are evaluated with
-// the per-cell formulas of fd_cell.cuh.
+// One step of a batch is two launches over the tile list plus one over the
+// pad cells:
+//  * tile_kernel<MODE, TILE_INTERIOR>: tiles whose every cell is a model cell
+//    in the 8th-order region; the absorbing blend is the identity there
+//    (w = 1, u31 = 0; src/util/fd.cpp:55-56);
+//  * tile_kernel<MODE, TILE_PAD>: tiles touching the pad, the frame, the
+//    low-order rings or the model edge: the same two-way update (the frame
+//    and low-order cells by the per-cell formula), model cells finished as in
+//    the interior, and the two-way value u3 of every cell kept in the shot's
+//    scratch field;
+//  * absorb_kernel<MODE>: every pad cell, the one-way update from u3 and the
+//    blend (processBoundary, fd.cpp:1092-1179), elementwise from global
+//    memory (no halo exchange, no barrier).
+// Tile kernels: one 32 x 64 tile per CTA, 2-D TMA tensor copies of the
+// current field (5-column / 8-row halo), the previous field, the velocity and,
+// for Born, the perturbation (1-column / 8-row halo) into shared memory (one
+// mbarrier, no multicast); each thread owns a 4-row x 2-column micro-tile.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -33,21 +32,16 @@ constexpr int QZ = TZ / 4;         // row quads per column (16)
 constexpr int SR = TZ + 2 * ZM;    // staged rows per column (80)
 constexpr int CW_C = TX + 2 * HXC; // staged columns of the current fields (42)
 constexpr int CW_P = TX + 2;       // staged columns of the other arrays (34)
-constexpr int U3R = TZ + 2, U3C = TX + 2;
 
-// KIND = TILE_INTERIOR: one interior tile per CTA, one staging buffer (many
-// CTAs per SM hide the copy latency).  KIND = TILE_PAD: persistent CTAs over
-// the pad tiles, two staging buffers (tile i+1 in flight while tile i computes).
+// Staged arrays of one tile (one buffer, one tile per CTA: several CTAs per SM
+// hide the copy latency).
 template <int MODE, int KIND>
 struct TCfg {
   static constexpr bool BORN = MODE == MODE_BORN;
   static constexpr int NCUR = BORN ? 2 : 1;   // arrays staged with the wide halo
   static constexpr int NOTH = BORN ? 4 : 2;   // prev, vel [, prev B, dv]
   static constexpr int BUF = (NCUR * CW_C + NOTH * CW_P) * SR;  // floats per buffer
-  static constexpr int NBUF = KIND == TILE_PAD ? 2 : 1;
-  static constexpr int NU3 = KIND == TILE_PAD ? (BORN ? 2 : 1) : 0;
-  static constexpr size_t bytes =
-      sizeof(float) * (size_t)(NBUF * BUF + NU3 * U3R * U3C) + 16 * 2;
+  static constexpr size_t bytes = sizeof(float) * (size_t)BUF + 16;
 };
 
 // ---- PTX helpers: mbarrier + bulk asynchronous copy global -> shared
@@ -119,14 +113,6 @@ struct SA {
   }
   __device__ __forceinline__ float4 quad(int ix, int iz) const {
     return *reinterpret_cast<const float4 *>(s + (ix - x0h) * SR + (iz - z0m));
-  }
-};
-
-struct U3Tile {  // two-way field on tile + 1 halo
-  float *s;
-  int x0, z0;
-  __device__ __forceinline__ float &operator()(int ix, int iz) const {
-    return s[(ix - x0 + 1) * U3R + (iz - z0 + 1)];
   }
 };
 
@@ -271,51 +257,49 @@ __device__ void snap_write(const ShotDev &g, int k, int x0, int z0, const float 
   }
 }
 
-// Threads per CTA: interior tiles 256 (4-row x 2-column micro-tiles), pad
-// tiles 512 (4-row x 1-column micro-tiles; more warps to cover the latency of
-// the scalar absorbing-boundary code).
-template <int KIND>
-__host__ __device__ constexpr int nthreads() {
-  return KIND == TILE_PAD ? 512 : NT_T;
-}
+// Global-memory accessor of one field by padded-grid coordinates.
+struct GA {
+  const float *p;  // cell (0, 0)
+  int ldz;
+  __device__ __forceinline__ float operator()(int ix, int iz) const {
+    return __ldg(p + (size_t)ix * ldz + iz);
+  }
+};
 
 template <int MODE, int KIND>
-__global__ void __launch_bounds__(nthreads<KIND>(), KIND == TILE_PAD ? 1 : 2) tile_kernel(
-    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, int ntiles, StepArgs a,
-    int *__restrict__ err) {
+__global__ void __launch_bounds__(NT_T, 2) tile_kernel(const ShotDev *__restrict__ shots,
+                                                       const Tile *__restrict__ tiles, StepArgs a,
+                                                       int *__restrict__ err) {
   using C = TCfg<MODE, KIND>;
-  constexpr int NTH = nthreads<KIND>();
   constexpr bool BORN = C::BORN;
+  constexpr bool PAD = KIND == TILE_PAD;
   extern __shared__ __align__(128) unsigned char smraw[];
-  float *buf0 = reinterpret_cast<float *>(smraw);
-  float *su3a = buf0 + C::NBUF * C::BUF;
-  float *su3b = su3a + U3R * U3C;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(su3a + C::NU3 * U3R * U3C);
+  float *bb = reinterpret_cast<float *>(smraw);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(bb + C::BUF);
+  __shared__ ShotDev sg;
+  __shared__ float red[33];
   const int tid = threadIdx.x;
-
+  const Tile t = tiles[blockIdx.x];
+  if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+    reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
   if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    mbar_init(bar, 1);
     fence_barrier_init();
   }
   __syncthreads();
+  const ShotDev &g = sg;
 
-  // staged arrays within a buffer: cur A [, cur B] (wide halo), then
-  // prev A, vel [, prev B, dv] (narrow halo)
-  auto arr_off = [](int arr) -> int {  // float offset of array `arr` in a buffer
+  // staged arrays: cur A [, cur B] (wide halo), then prev A, vel [, prev B, dv]
+  auto arr_off = [](int arr) -> int {
     return arr < C::NCUR ? arr * CW_C * SR : C::NCUR * CW_C * SR + (arr - C::NCUR) * CW_P * SR;
   };
   // One 2-D tensor copy per staged array: rows [z0 - ZM, z0 + TZ + ZM) of
   // columns [x0 - halo, x0 + TX + halo), addressed from the allocation start
   // (row + ZM, column + XM), so coordinates are never negative and the row
   // coordinate is a multiple of TZ (16-byte aligned).
-  auto issue = [&](int ti, int b) {
-    if (tid != 0) return;
-    const Tile t = tiles[ti];
-    const ShotDev &g = shots[t.shot];
-    float *dst0 = buf0 + b * C::BUF;
+  if (tid == 0) {
     fence_proxy_async();
-    mbar_expect_tx(&bar[b], (uint32_t)(C::BUF * sizeof(float)));
+    mbar_expect_tx(bar, (uint32_t)(C::BUF * sizeof(float)));
     const int ra = a.rot % 3, rca = (a.rot + 1) % 3, rb = a.rot_b % 3, rcb = (a.rot_b + 1) % 3;
     int maps[6];
     if (MODE == MODE_RCV) {
@@ -326,254 +310,234 @@ __global__ void __launch_bounds__(nthreads<KIND>(), KIND == TILE_PAD ? 1 : 2) ti
       maps[0] = MAP_FA_WIDE + rca; maps[1] = MAP_FB_WIDE + rcb; maps[2] = MAP_FA_NARROW + ra;
       maps[3] = MAP_VEL; maps[4] = MAP_FB_NARROW + rb; maps[5] = MAP_DV;
     }
-    const int row = t.z0;  // (z0 - ZM) + ZM
 #pragma unroll
     for (int arr = 0; arr < C::NCUR + C::NOTH; arr++) {
       const int col = t.x0 + XM - (arr < C::NCUR ? HXC : 1);
-      tma_load_2d(dst0 + arr_off(arr), g.maps + maps[arr], row, col, &bar[b]);
+      tma_load_2d(bb + arr_off(arr), g.maps + maps[arr], t.z0, col, bar);
+    }
+  }
+  if (!mbar_wait(bar, 0)) {
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+
+  StepArgs aa = a;
+  if (MODE != MODE_RCV && aa.rec_k >= g.nt) aa.rec_k = -1;
+  float *na = g.fa[(a.rot + 2) % 3];
+  float *nb_ = g.fb[(a.rot_b + 2) % 3];
+  float *out_a = MODE == MODE_RCV ? nb_ : na;
+  const int x0 = t.x0, z0 = t.z0;
+  const int zm = z0 - ZM;
+  const SA CA{bb + arr_off(0), x0 - HXC, zm};
+  const SA CB{bb + arr_off(BORN ? 1 : 0), x0 - HXC, zm};
+  const SA PA{bb + arr_off(C::NCUR), x0 - 1, zm};
+  const SA VV{bb + arr_off(C::NCUR + 1), x0 - 1, zm};
+  const SA PB{bb + arr_off(BORN ? C::NCUR + 2 : C::NCUR), x0 - 1, zm};
+  const SA DV{bb + arr_off(BORN ? C::NCUR + 3 : C::NCUR + 1), x0 - 1, zm};
+  const int qz = tid % QZ, cx = tid / QZ;  // micro-tile: rows 4qz.., columns 2cx, 2cx+1
+  const int ix = x0 + 2 * cx, iz0 = z0 + 4 * qz;
+  const bool record = MODE != MODE_RCV && aa.rec_k >= 0;
+  const bool snap = MODE != MODE_RCV && aa.snap_k >= 0 && g.snap != nullptr;
+
+  auto in_grid = [&](int cxj, int iz) { return !PAD || (cxj < g.NX && iz < g.NZ); };
+  auto model = [&](int cxj, int iz) {
+    return !PAD || (cxj >= g.pml && cxj < g.pml + g.nx && iz >= g.pml && iz < g.pml + g.nz);
+  };
+
+  // One micro-tile (columns qx, qx+1, rows qz0 .. qz0+3): two-way values,
+  // injection, model cells finished (w = 1), every u3 of a pad tile kept.
+  // `vec`: all eight cells in the 8th-order region (vector path from shared
+  // memory); otherwise cell by cell with the general formula (frame,
+  // low-order rings, cells past the grid skipped).  lv/mask: source-term
+  // values of the model cells for the snapshot.
+  auto quad = [&](int qx, int qz0, bool vec, float (&lv)[8], int (&lx)[8], int (&lz)[8],
+                  unsigned &mask) {
+    auto twoway = [&](const SA &Cc, const SA &Pp, float4 o[2], float4 cen[2], float4 prv[2],
+                      float4 vel[2]) {
+      if (vec) {
+        pair_twoway(Cc, Pp, VV, g, qx, qz0, o, cen, prv, vel);
+        return;
+      }
+      // low-order ring cells (modeling2D_low, fd.cpp:1226-1241) from vector
+      // loads of the column and its x neighbours; frame cells and any
+      // 8th-order cell of a mixed micro-tile by the general formula
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        o[j] = cen[j] = prv[j] = vel[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        const int cxj = qx + j;
+        if (PAD && cxj >= g.NX) continue;
+        const float4 c4 = Cc.quad(cxj, qz0), l4 = Cc.quad(cxj - 1, qz0), r4 = Cc.quad(cxj + 1, qz0);
+        const float cm = Cc(cxj, qz0 - 1), cp = Cc(cxj, qz0 + 4);
+        const float4 p4 = Pp.quad(cxj, qz0), v4 = VV.quad(cxj, qz0);
+        cen[j] = c4;
+        prv[j] = p4;
+        vel[j] = v4;
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const int iz = qz0 + r;
+          if (!in_grid(cxj, iz)) continue;
+          const bool frame = cxj == 0 || cxj == g.NX - 1 || iz == 0 || iz == g.NZ - 1;
+          const bool high = cxj >= 4 && cxj <= g.NX - 5 && iz >= 4 && iz <= g.NZ - 5;
+          float u;
+          if (frame || high) {
+            u = twoway_cell(Cc, Pp, VV, g, cxj, iz);
+          } else {
+            const float c = comp(c4, r);
+            const float zm1 = r == 0 ? cm : comp(c4, r - 1), zp1 = r == 3 ? cp : comp(c4, r + 1);
+            Coef k = coef(comp(v4, r), g);
+            const float uzz = zm1 + zp1 - 2.0f * c;
+            const float uxx = comp(r4, r) + comp(l4, r) - 2.0f * c;
+            u = k.vz * uzz + k.vx * uxx + 2.0f * c - comp(p4, r);
+          }
+          set_comp(o[j], r, u);
+        }
+      }
+    };
+    // a column quad wholly in the grid (or wholly in the model) is stored as
+    // one vector; the other cells of a pad tile one by one
+    auto quad_in = [&](int cxj) { return !PAD || (cxj < g.NX && qz0 + 3 < g.NZ); };
+    auto quad_model = [&](int cxj) {
+      return !PAD || (cxj >= g.pml && cxj < g.pml + g.nx && qz0 >= g.pml && qz0 + 3 < g.pml + g.nz);
+    };
+    int gzq[2];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      int x = qx + j - g.pml;
+      gzq[j] = (x >= 0 && x < g.nx) ? g.gz[x] + g.pml : -1;
+    }
+    float4 o[2], cen[2], prv[2], vel[2];
+    twoway(CA, PA, o, cen, prv, vel);
+    float4 qs[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const int cxj = qx + j;
+      float4 u4 = o[j];
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const int iz = qz0 + r;
+        lv[4 * j + r] = 0.0f;
+        lx[4 * j + r] = cxj;
+        lz[4 * j + r] = iz;
+        if (!in_grid(cxj, iz)) continue;
+        Coef kk = coef(comp(vel[j], r), g);
+        const float u = inject<MODE>(g, aa, cxj, iz, gzq[j], comp(o[j], r), kk.vt2);
+        set_comp(u4, r, u);
+        if (PAD && !quad_in(cxj)) g.u3s[0][(size_t)cxj * g.LDZ + iz] = u;
+        if (!model(cxj, iz)) continue;  // pad cell: finished by absorb_kernel
+        const float out = u + 0.0f;
+        set_comp(o[j], r, out);
+        if (PAD && !quad_model(cxj)) out_a[(size_t)cxj * g.LDZ + iz] = out;
+        if (!BORN && record && iz == gzq[j])
+          g.rec[(size_t)aa.rec_k * g.nx + (cxj - g.pml)] = out;
+        if (MODE == MODE_MODEL && aa.strip_k >= 0) save_strips(g, aa.strip_k, cxj, iz, out);
+        if (BORN || snap) {  // scattering source vt2 lap vel3 dv, fd.cpp:134-139
+          float lap = (out + comp(prv[j], r) - 2.0f * comp(cen[j], r)) * g.idt2;
+          lv[4 * j + r] = lap;
+          mask |= 1u << (4 * j + r);
+          if (BORN) {
+            float vv = comp(vel[j], r);
+            float vel3 = 2.0f / (vv * vv * vv);
+            set_comp(qs[j], r, kk.vt2 * lap * vel3 * DV(cxj, iz));
+          }
+        }
+      }
+      if (PAD && quad_in(cxj))
+        *reinterpret_cast<float4 *>(g.u3s[0] + (size_t)cxj * g.LDZ + qz0) = u4;
+      if (quad_model(cxj)) *reinterpret_cast<float4 *>(out_a + (size_t)cxj * g.LDZ + qz0) = o[j];
+    }
+    if (BORN) {
+      float4 ob[2], cb4[2], pb4[2], vb4[2];
+      twoway(CB, PB, ob, cb4, pb4, vb4);
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const int cxj = qx + j;
+        float4 u4 = ob[j];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+          const int iz = qz0 + r;
+          if (!in_grid(cxj, iz)) continue;
+          const float u = comp(ob[j], r) + comp(qs[j], r);
+          set_comp(u4, r, u);
+          if (PAD && !quad_in(cxj)) g.u3s[1][(size_t)cxj * g.LDZ + iz] = u;
+          if (!model(cxj, iz)) continue;
+          const float out = u + 0.0f;
+          set_comp(ob[j], r, out);
+          if (PAD && !quad_model(cxj)) nb_[(size_t)cxj * g.LDZ + iz] = out;
+          if (record && iz == gzq[j]) g.rec[(size_t)aa.rec_k * g.nx + (cxj - g.pml)] = out;
+        }
+        if (PAD && quad_in(cxj))
+          *reinterpret_cast<float4 *>(g.u3s[1] + (size_t)cxj * g.LDZ + qz0) = u4;
+        if (quad_model(cxj)) *reinterpret_cast<float4 *>(nb_ + (size_t)cxj * g.LDZ + qz0) = ob[j];
+      }
     }
   };
 
-  const int qz = tid % QZ, cx = tid / QZ;  // micro-tile: rows 4qz.., columns 2cx, 2cx+1
-  int it = 0;
-  int ti = blockIdx.x;
-  const int stride = C::NBUF == 2 ? (int)gridDim.x : ntiles;  // interior: one tile per CTA
-  if (ti < ntiles) issue(ti, 0);
-  bool ok = true;
-  for (; ti < ntiles; ti += stride, it++) {
-    const int b = C::NBUF == 2 ? (it & 1) : 0;
-    const int tn = ti + stride;
-    if (C::NBUF == 2 && tn < ntiles) issue(tn, b ^ 1);
-    if (!mbar_wait(&bar[b], (uint32_t)(C::NBUF == 2 ? ((it >> 1) & 1) : (it & 1)))) {
-      ok = false;
-      break;
-    }
-    const Tile t = tiles[ti];
-    // the shot descriptor in shared memory: its fields cannot alias the
-    // global stores below, so they are loaded once per use site, not reloaded
-    __shared__ ShotDev sg;
-    __syncthreads();  // the previous tile's readers of sg are done
-    if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
-      reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
-    __syncthreads();
-    const ShotDev &g = sg;
-    StepArgs aa = a;
-    if (MODE != MODE_RCV && aa.rec_k >= g.nt) aa.rec_k = -1;
-    float *na = g.fa[(a.rot + 2) % 3];
-    float *nb_ = g.fb[(a.rot_b + 2) % 3];
-    float *out_a = MODE == MODE_RCV ? nb_ : na;
-    const float *bb = buf0 + b * C::BUF;
-    const int x0 = t.x0, z0 = t.z0;
-    const int zm = z0 - ZM;
-    const SA CA{bb + arr_off(0), x0 - HXC, zm};
-    const SA CB{bb + arr_off(BORN ? 1 : 0), x0 - HXC, zm};
-    const SA PA{bb + arr_off(C::NCUR), x0 - 1, zm};
-    const SA VV{bb + arr_off(C::NCUR + 1), x0 - 1, zm};
-    const SA PB{bb + arr_off(BORN ? C::NCUR + 2 : C::NCUR), x0 - 1, zm};
-    const SA DV{bb + arr_off(BORN ? C::NCUR + 3 : C::NCUR + 1), x0 - 1, zm};
-    const int ix = x0 + 2 * cx, iz0 = z0 + 4 * qz;
-    // receiver rows of this thread's two columns
-    int gzc[2];
+  float lv[8];
+  int lx[8], lz[8];
+  unsigned mask = 0;
+  if (!PAD) {
+    float (&l0)[8] = *reinterpret_cast<float(*)[8]>(lv);
+    int (&x0_)[8] = *reinterpret_cast<int(*)[8]>(lx);
+    int (&z0_)[8] = *reinterpret_cast<int(*)[8]>(lz);
+    quad(ix, iz0, true, l0, x0_, z0_, mask);
+    if (snap) snap_write<NT_T, 8>(g, aa.snap_k, x0, z0, l0, x0_, z0_, mask, red);
+  } else {
+    float (&l1)[8] = *reinterpret_cast<float(*)[8]>(lv);
+    int (&x1)[8] = *reinterpret_cast<int(*)[8]>(lx);
+    int (&z1)[8] = *reinterpret_cast<int(*)[8]>(lz);
+    const bool vecq = ix >= 4 && ix + 1 <= g.NX - 5 && iz0 >= 4 && iz0 + 3 <= g.NZ - 5;
+    if (ix < g.NX && iz0 < g.NZ) quad(ix, iz0, vecq, l1, x1, z1, mask);
+    else
 #pragma unroll
-    for (int j = 0; j < 2; j++) {
-      int x = ix + j - g.pml;
-      gzc[j] = (x >= 0 && x < g.nx) ? g.gz[x] + g.pml : -1;
-    }
-    const bool record = MODE != MODE_RCV && aa.rec_k >= 0;
-
-    const bool snap = MODE != MODE_RCV && aa.snap_k >= 0 && g.snap != nullptr;
-    __shared__ float red[33];
-    float pout_keep[4] = {0.f, 0.f, 0.f, 0.f};  // pad tiles: this thread's new values
-    if (KIND == TILE_INTERIOR) {
-      // ---------------- interior tile: every cell 8th order, w = 1
-      float4 o[2], cen[2], prv[2], vel[2];
-      pair_twoway(CA, PA, VV, g, ix, iz0, o, cen, prv, vel);
-      float4 qs[2];
-      float lv[8];
-      int lx[8], lz[8];
-#pragma unroll
-      for (int j = 0; j < 2; j++) {
-#pragma unroll
-        for (int r = 0; r < 4; r++) {
-          const int iz = iz0 + r;
-          Coef kk = coef(comp(vel[j], r), g);
-          float out = inject<MODE>(g, aa, ix + j, iz, gzc[j], comp(o[j], r), kk.vt2) + 0.0f;
-          set_comp(o[j], r, out);
-          if (!BORN && record && iz == gzc[j])
-            g.rec[(size_t)aa.rec_k * g.nx + (ix + j - g.pml)] = out;
-          if (MODE == MODE_MODEL && aa.strip_k >= 0) save_strips(g, aa.strip_k, ix + j, iz, out);
-          if (BORN || snap) {  // scattering source vt2 lap vel3 dv, fd.cpp:134-139
-            float lap = (out + comp(prv[j], r) - 2.0f * comp(cen[j], r)) * g.idt2;
-            lv[4 * j + r] = lap;
-            lx[4 * j + r] = ix + j;
-            lz[4 * j + r] = iz;
-            if (BORN) {
-              float vv = comp(vel[j], r);
-              float vel3 = 2.0f / (vv * vv * vv);
-              set_comp(qs[j], r, kk.vt2 * lap * vel3 * DV(ix + j, iz));
-            }
-          }
-        }
-        *reinterpret_cast<float4 *>(out_a + (size_t)(ix + j) * g.LDZ + iz0) = o[j];
+      for (int k = 0; k < 8; k++) {
+        lv[k] = 0.0f;
+        lx[k] = ix;
+        lz[k] = iz0;
       }
-      if (snap) snap_write<NTH, 8>(g, aa.snap_k, x0, z0, lv, lx, lz, 0xffu, red);
-      if (BORN) {
-        float4 ob[2], cb4[2], pb4[2], vb4[2];
-        pair_twoway(CB, PB, VV, g, ix, iz0, ob, cb4, pb4, vb4);
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-#pragma unroll
-          for (int r = 0; r < 4; r++) {
-            float out = (comp(ob[j], r) + comp(qs[j], r)) + 0.0f;
-            set_comp(ob[j], r, out);
-            if (record && iz0 + r == gzc[j])
-              g.rec[(size_t)aa.rec_k * g.nx + (ix + j - g.pml)] = out;
-          }
-          *reinterpret_cast<float4 *>(nb_ + (size_t)(ix + j) * g.LDZ + iz0) = ob[j];
-        }
-      }
-    } else {
-      // ---------------- pad tile: two-way field on tile + 1 halo
-      // thread: column x0 + pc, rows pz .. pz+3
-      const int pc = tid / QZ, pz = z0 + 4 * (tid % QZ), px = x0 + pc;
-      const U3Tile Ua{su3a, x0, z0}, Ub{su3b, x0, z0};
-      int gzp;
-      {
-        int x = px - g.pml;
-        gzp = (x >= 0 && x < g.nx) ? g.gz[x] + g.pml : -1;
-      }
-      // items: NTH body quads (one per thread, its own), 2 x QZ halo-column
-      // quads, 2 x (TX + 2) halo-row cells (the halo rows include the four
-      // diagonal corners, which the one-way update of a tile-corner strip cell
-      // reads)
-      constexpr int NITEM = NTH + 2 * QZ + 2 * (TX + 2);
-      float4 ua = make_float4(0.f, 0.f, 0.f, 0.f), ub = ua;
-      bool body_vec = false;
-      for (int item = tid; item < NITEM; item += NTH) {
-        int c0, cz0, nrow;
-        if (item < NTH) {
-          c0 = px; cz0 = pz; nrow = 4;
-        } else if (item < NTH + 2 * QZ) {
-          int h = item - NTH;
-          c0 = h < QZ ? x0 - 1 : x0 + TX;
-          cz0 = z0 + 4 * (h % QZ);
-          nrow = 4;
-        } else {
-          int h = item - NTH - 2 * QZ;
-          c0 = x0 - 1 + (h % (TX + 2));
-          cz0 = h < TX + 2 ? z0 - 1 : z0 + TZ;
-          nrow = 1;
-        }
-        if (c0 < 0 || c0 >= g.NX) continue;
-        const bool vec = nrow == 4 && c0 >= 4 && c0 <= g.NX - 5 && cz0 >= 4 && cz0 + 3 <= g.NZ - 5;
-        float4 va, vb, cen, prv, vel;
-        if (vec) {
-          va = col_twoway(CA, PA, VV, g, c0, cz0, cen, prv, vel);
-          if (BORN) vb = col_twoway(CB, PB, VV, g, c0, cz0, cen, prv, vel);
-        }
-        int x = c0 - g.pml;
-        const int gz_ = (x >= 0 && x < g.nx) ? g.gz[x] + g.pml : -1;
-        for (int r = 0; r < nrow; r++) {
-          const int iz = cz0 + r;
-          if (iz < 0 || iz >= g.NZ) continue;
-          const float v = VV(c0, iz);
-          Coef kk = coef(v, g);
-          float u = vec ? comp(va, r) : twoway_cell(CA, PA, VV, g, c0, iz);
-          u = inject<MODE>(g, aa, c0, iz, gz_, u, kk.vt2);
-          Ua(c0, iz) = u;
-          if (item < NTH) set_comp(ua, r, u);
-          if (BORN) {
-            float qv = 0.0f;
-            int z = iz - g.pml;
-            if (x >= 0 && x < g.nx && z >= 0 && z < g.nz) {  // dv is zero in the pad
-              float lap = ((u + 0.0f) + PA(c0, iz) - 2.0f * CA(c0, iz)) * g.idt2;
-              float vel3 = 2.0f / (v * v * v);
-              qv = kk.vt2 * lap * vel3 * DV(c0, iz);
-            }
-            float ubv = (vec ? comp(vb, r) : twoway_cell(CB, PB, VV, g, c0, iz)) + qv;
-            Ub(c0, iz) = ubv;
-            if (item < NTH) set_comp(ub, r, ubv);
-          }
-        }
-        if (item < NTH) body_vec = vec;
-      }
-      __syncthreads();
-      float *pout = pout_keep;
-      if (px < g.NX) {
-        // a quad wholly inside the model (w = 1, u31 = 0) keeps its two-way
-        // values; any other quad goes through the absorbing update per cell
-        const bool inside = body_vec && px >= g.pml && px < g.pml + g.nx && pz >= g.pml &&
-                            pz + 3 < g.pml + g.nz;
-        const size_t off0 = (size_t)px * g.LDZ + pz;
-        if (inside) {
-          float4 o = ua, ob = ub;
-#pragma unroll
-          for (int r = 0; r < 4; r++) {
-            set_comp(o, r, comp(ua, r) + 0.0f);
-            if (BORN) set_comp(ob, r, comp(ub, r) + 0.0f);
-          }
-          *reinterpret_cast<float4 *>(out_a + off0) = o;
-          if (BORN) *reinterpret_cast<float4 *>(nb_ + off0) = ob;
-          pout[0] = o.x; pout[1] = o.y; pout[2] = o.z; pout[3] = o.w;
-#pragma unroll
-          for (int r = 0; r < 4; r++) {
-            const int iz = pz + r;
-            const float rv = BORN ? comp(ob, r) : comp(o, r);
-            if (record && iz == gzp) g.rec[(size_t)aa.rec_k * g.nx + (px - g.pml)] = rv;
-            if (MODE == MODE_MODEL && aa.strip_k >= 0) save_strips(g, aa.strip_k, px, iz, comp(o, r));
-          }
-        } else {
-          for (int r = 0; r < 4; r++) {
-            const int iz = pz + r;
-            if (iz >= g.NZ) break;
-            const size_t off = off0 + r;
-            float out = absorb_cell(Ua(px, iz), Ua, CA, PA, VV, g, px, iz);
-            out_a[off] = out;
-            pout[r] = out;
-            if (!BORN && record && iz == gzp) g.rec[(size_t)aa.rec_k * g.nx + (px - g.pml)] = out;
-            if (MODE == MODE_MODEL && aa.strip_k >= 0) save_strips(g, aa.strip_k, px, iz, out);
-            if (BORN) {
-              float ob = absorb_cell(Ub(px, iz), Ub, CB, PB, VV, g, px, iz);
-              nb_[off] = ob;
-              if (record && iz == gzp) g.rec[(size_t)aa.rec_k * g.nx + (px - g.pml)] = ob;
-            }
-          }
-        }
-      }
-    }
-    if (KIND == TILE_PAD && snap) {
-      // source-term snapshot of the model-interior cells of this pad tile
-      const int pc = tid / QZ, pz = z0 + 4 * (tid % QZ), px = x0 + pc;
-      const SA CA2{bb + arr_off(0), x0 - HXC, zm};
-      const SA PA2{bb + arr_off(C::NCUR), x0 - 1, zm};
-      float lv[4];
-      int lx[4], lz[4];
-      unsigned mask = 0;
-#pragma unroll
-      for (int r = 0; r < 4; r++) {
-        const int iz = pz + r;
-        lx[r] = px;
-        lz[r] = iz;
-        lv[r] = 0.0f;
-        if (px >= g.pml && px < g.pml + g.nx && iz >= g.pml && iz < g.pml + g.nz) {
-          lv[r] = (pout_keep[r] + PA2(px, iz) - 2.0f * CA2(px, iz)) * g.idt2;
-          mask |= 1u << r;
-        }
-      }
-      snap_write<NTH, 4>(g, aa.snap_k, x0, z0, lv, lx, lz, mask, red);
-    }
-    __syncthreads();  // buffer b and the u3 tiles are free again
+    if (snap) snap_write<NT_T, 8>(g, aa.snap_k, x0, z0, l1, x1, z1, mask, red);
   }
-  if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
-    // let every copy already issued land before the CTA's shared memory goes
-    // away: the current tile's buffer and, if issued, the next tile's
-    if (C::NBUF == 2) {
-      mbar_wait(&bar[it & 1], (uint32_t)((it >> 1) & 1));
-      if (ti + stride < ntiles) mbar_wait(&bar[(it + 1) & 1], (uint32_t)(((it + 1) >> 1) & 1));
-    } else {
-      mbar_wait(&bar[0], (uint32_t)(it & 1));
-    }
+}
+
+// Absorbing boundary of the pad cells: one-way update from the two-way values
+// kept by the pad tiles, and the blend (fd.cpp:1092-1179, :55-56).  Each
+// thread takes ABS_CPT cells of its chunk (z fastest, stride ABS_NT) and
+// forms all of them before storing any, so their loads overlap; every input
+// is read-only during the launch.
+template <int MODE>
+__global__ void __launch_bounds__(ABS_NT) absorb_kernel(const ShotDev *__restrict__ shots,
+                                                        const PadChunk *__restrict__ chunks,
+                                                        StepArgs a) {
+  const PadChunk c = chunks[blockIdx.x];
+  const ShotDev &g = shots[c.shot];
+  const int ldz = g.LDZ;
+  const GA V{g.vel, ldz};
+  const int ra = MODE == MODE_RCV ? a.rot_b : a.rot;
+  float *const *FA = MODE == MODE_RCV ? g.fb : g.fa;
+  const GA UA{g.u3s[0], ldz}, CA{FA[(ra + 1) % 3], ldz}, PA{FA[ra % 3], ldz};
+  float *outa = FA[(ra + 2) % 3];
+  const int rb = a.rot_b;
+  const GA UB{g.u3s[1], ldz}, CB{g.fb[(rb + 1) % 3], ldz}, PB{g.fb[rb % 3], ldz};
+  float *outb = g.fb[(rb + 2) % 3];
+  float va[ABS_CPT], vb[ABS_CPT];
+  size_t off[ABS_CPT];
+  bool act[ABS_CPT];
+#pragma unroll
+  for (int k = 0; k < ABS_CPT; k++) {
+    const int flat = threadIdx.x + k * ABS_NT;
+    const int col = flat / c.nrows, row = flat - col * c.nrows;
+    act[k] = col < c.ncols;
+    const int ix = c.x0 + (act[k] ? col : 0), iz = c.z0 + (act[k] ? row : 0);
+    off[k] = (size_t)ix * ldz + iz;
+    va[k] = vb[k] = 0.0f;
+    if (!act[k]) continue;
+    va[k] = absorb_cell(UA(ix, iz), UA, CA, PA, V, g, ix, iz);
+    if (MODE == MODE_BORN) vb[k] = absorb_cell(UB(ix, iz), UB, CB, PB, V, g, ix, iz);
+  }
+#pragma unroll
+  for (int k = 0; k < ABS_CPT; k++) {
+    if (!act[k]) continue;
+    outa[off[k]] = va[k];
+    if (MODE == MODE_BORN) outb[off[k]] = vb[k];
   }
 }
 
