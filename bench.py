@@ -244,6 +244,8 @@ def kernel_roofline(ctx, sv, iter_ms):
     rows = []
     for op, name, launches in ((OP_BORN, "born", NT), (OP_BORN_ADJOINT, "adjoint", NT + 1)):
         with Plan(ctx, op, sv.shots) as p:
+            if op == OP_BORN:
+                p.set_exact(False)  # the solver's Born operator runs the fast build
             for i in range(len(sv.shots)):
                 p.set(i, IN_VEL, sv.sub(sv.vel0, i))
                 p.set(i, IN_WAVELET, wav)

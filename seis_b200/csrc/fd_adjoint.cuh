@@ -17,14 +17,16 @@
 // Interior tiles (tile + 4-cell halo strictly inside the model, no cell read
 // by the one-way update) reduce to the symmetric gather
 //   L_k = Lz(vz L1) + Lx(vx L1) + 2 L1 - L2 + R^T d.
-// Pad tiles run the transposed stages in scatter form over every consumer cell
-// of the tile + 5-cell halo; only the contributions that land on the tile are
-// kept.  The scatter accumulates in 64-bit fixed point (shared-memory integer
-// atomics, whose sum does not depend on the order of the adds), so the
-// adjoint is bit-for-bit repeatable.  The tile's scale is 2^(49 - e) for
-// inputs below 2^e: every accumulator stays below 2^62 (a target collects at
-// most ~2^12 times the largest input) and the resolution is 2^-49 of the
-// tile's largest input.
+// Pad tiles: mu(L1) = w L1 + ringsT((1-w) L1) and the ring terms of cur and
+// prev are scattered from every ring cell of the tile + 5-cell halo; the
+// transposed two-way stencil is then a gather of vz mu, vx mu over the 8th-order
+// consumers (as in the interior), plus a scatter from the low-order and frame
+// consumers of the outer 4 cells.  Scatters accumulate in 64-bit fixed point
+// (shared-memory integer atomics, whose sum does not depend on the order of
+// the adds), so the adjoint is bit-for-bit repeatable.  The tile's scale is
+// 2^(49 - e) for inputs below 2^e: every accumulator stays below 2^62 (a
+// target collects at most ~2^12 times the largest input) and the resolution
+// is 2^-49 of the tile's largest input.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -36,7 +38,7 @@ namespace seis {
 namespace SEIS_NS {
 
 constexpr int A_NT_I = 256;  // interior adjoint kernel threads
-constexpr int A_NT_P = 512;  // pad adjoint kernel threads
+constexpr int A_NT_P = 256;  // pad adjoint kernel threads
 constexpr int WIDE = CW_C * SR, NARROW = CW_P * SR;
 constexpr int MU_C = TX + 8, MU_R = TZ + 8;  // mu on tile + 4 halo
 
@@ -285,34 +287,48 @@ __global__ void __launch_bounds__(A_NT_I, 2) adj_interior_kernel(const ShotDev *
 }
 
 // ---------------------------------------------------------------- pad tiles
+// shared memory: staged L1, V (wide), L2 (narrow); MU1 (fixed point, tile + 4);
+// ACC (fixed point, tile: ring terms of cur and prev minus mu(L2), and the
+// frame-band stencil scatter); WZ, WX = vz mu, vx mu of the 8th-order
+// consumers (float, tile + 4)
 constexpr size_t ADJ_PAD_F32 = sizeof(float) * (size_t)(2 * WIDE + NARROW);
-static_assert(ADJ_PAD_F32 % 8 == 0, "fixed-point accumulators must be 8-byte aligned");
-constexpr size_t ADJ_PAD_SMEM =
-    ADJ_PAD_F32 + sizeof(long long) * (size_t)(MU_C * MU_R + 3 * TX * TZ) + 16;
+static_assert(ADJ_PAD_F32 % 16 == 0, "fixed-point accumulators must be 16-byte aligned");
+constexpr size_t ADJ_PAD_SMEM = ADJ_PAD_F32 + sizeof(long long) * (size_t)(MU_C * MU_R + TX * TZ) +
+                                sizeof(float) * (size_t)(2 * MU_C * MU_R) + 16;
 
-__global__ void __launch_bounds__(A_NT_P, 1) adj_pad_kernel(const ShotDev *__restrict__ shots,
+struct MA {  // float array over tile + 4, column stride MU_R
+  const float *s;
+  int x0h, z0h;
+  __device__ __forceinline__ float operator()(int ix, int iz) const {
+    return s[(ix - x0h) * MU_R + (iz - z0h)];
+  }
+  __device__ __forceinline__ float4 quad(int ix, int iz) const {
+    return *reinterpret_cast<const float4 *>(s + (ix - x0h) * MU_R + (iz - z0h));
+  }
+};
+
+__global__ void __launch_bounds__(A_NT_P, 2) adj_pad_kernel(const ShotDev *__restrict__ shots,
                                                             const Tile *__restrict__ tiles,
                                                             StepArgs a, int *__restrict__ err) {
   extern __shared__ __align__(128) unsigned char smraw[];
   float *sL1 = reinterpret_cast<float *>(smraw);  // wide
   float *sV = sL1 + WIDE;                          // wide
   float *sL2 = sV + WIDE;                          // narrow
-  long long *sMU1 = reinterpret_cast<long long *>(sL2 + NARROW);  // tile + 4
-  long long *sCB = sMU1 + MU_C * MU_R;             // tile
-  long long *sMU2 = sCB + TX * TZ;                 // tile
-  long long *sPB = sMU2 + TX * TZ;                 // tile
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sPB + TX * TZ);
+  long long *sMU1 = reinterpret_cast<long long *>(smraw + ADJ_PAD_F32);  // tile + 4
+  long long *sACC = sMU1 + MU_C * MU_R;                                  // tile
+  float *sWZ = reinterpret_cast<float *>(sACC + TX * TZ);                // tile + 4
+  float *sWX = sWZ + MU_C * MU_R;                                        // tile + 4
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sWX + MU_C * MU_R);
   __shared__ float red[A_NT_P / 32];
+  __shared__ ShotDev sg;
   const int tid = threadIdx.x;
   const Tile t = tiles[blockIdx.x];
-  __shared__ ShotDev sg;
   if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
     reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
   if (tid == 0) {
     mbar_init(bar, 1);
     fence_barrier_init();
   }
-  for (int i = tid; i < MU_C * MU_R + 3 * TX * TZ; i += A_NT_P) sMU1[i] = 0;
   __syncthreads();
   const ShotDev &g = sg;
   const int x0 = t.x0, z0 = t.z0;
@@ -327,6 +343,7 @@ __global__ void __launch_bounds__(A_NT_P, 1) adj_pad_kernel(const ShotDev *__res
     if (tid == 0) atomicExch(err, 2);
     return;
   }
+  const int NX = g.NX, NZ = g.NZ;
   const int zm = z0 - ZM;
   const SA L1{sL1, x0 - HXC, zm}, V{sV, x0 - HXC, zm}, L2{sL2, x0 - 1, zm};
   int e;
@@ -335,74 +352,131 @@ __global__ void __launch_bounds__(A_NT_P, 1) adj_pad_kernel(const ShotDev *__res
   const float scale = ldexpf(1.0f, se);
   const double inv = ldexp(1.0, -se);
   const AdjTile MU1{sMU1, x0 - 4, z0 - 4, MU_C, MU_R, scale, inv};
-  const AdjTile CB{sCB, x0, z0, TX, TZ, scale, inv}, MU2{sMU2, x0, z0, TX, TZ, scale, inv},
-      PB{sPB, x0, z0, TX, TZ, scale, inv};
+  const AdjTile ACC{sACC, x0, z0, TX, TZ, scale, inv};
+  auto fix = [&](float v) { return __float2ll_rn(v * scale); };
+  auto is8 = [&](int cx, int cz) { return cx >= 4 && cx <= NX - 5 && cz >= 4 && cz <= NZ - 5; };
 
-  // blend^T and rings^T of L1 over the consumers in tile + 5, of L2 over tile + 1
+  // blendT of the cells themselves: MU1 = w L1 on tile + 4, ACC = -w L2 on
+  // the tile (plain stores: each cell once)
+  for (int i = tid; i < MU_C * MU_R; i += A_NT_P) {
+    const int cx = x0 - 4 + i / MU_R, cz = z0 - 4 + i % MU_R;
+    long long m = 0;
+    if (cx >= 0 && cx < NX && cz >= 0 && cz < NZ) {
+      PadPos pp = pad_pos(g, cx, cz);
+      const float w = pp.ring == 0 ? 1.0f : pad_weight(g, pp);
+      m = fix(w * L1(cx, cz));
+    }
+    sMU1[i] = m;
+  }
+  for (int i = tid; i < TX * TZ; i += A_NT_P) {
+    const int cx = x0 + i / TZ, cz = z0 + i % TZ;
+    long long m = 0;
+    if (cx < NX && cz < NZ) {
+      PadPos pp = pad_pos(g, cx, cz);
+      const float w = pp.ring == 0 ? 1.0f : pad_weight(g, pp);
+      m = -fix(w * L2(cx, cz));
+    }
+    sACC[i] = m;
+  }
+  __syncthreads();
+
+  // ringsT of the pad cells of tile + 5: (1 - w) L1 through the one-way
+  // update's u3, cur and prev terms, (1 - w) L2 through its prev terms and
+  // (minus) its u3 terms
   constexpr int R5C = TX + 10, R5R = TZ + 10;
   for (int i = tid; i < R5C * R5R; i += A_NT_P) {
     const int cx = x0 - 5 + i / R5R, cz = z0 - 5 + i % R5R;
-    if (cx < 0 || cx >= g.NX || cz < 0 || cz >= g.NZ) continue;
+    if (cx < 0 || cx >= NX || cz < 0 || cz >= NZ) continue;
     PadPos pp = pad_pos(g, cx, cz);
-    const bool near1 = cx >= x0 - 1 && cx <= x0 + TX && cz >= z0 - 1 && cz <= z0 + TZ;
-    float w = pp.ring == 0 ? 1.0f : pad_weight(g, pp);
-    float l1 = L1(cx, cz);
-    MU1.add(cx, cz, w * l1);
-    float l2 = near1 ? L2(cx, cz) : 0.0f;
-    if (near1) MU2.add(cx, cz, w * l2);
     if (pp.ring == 0) continue;
+    const bool near1 = cx >= x0 - 1 && cx <= x0 + TX && cz >= z0 - 1 && cz <= z0 + TZ;
+    const float w = pad_weight(g, pp);
     RingCoef rc = ring_coef(g, V, cx, cz, pp);
-    float n1 = (1.0f - w) * l1, n2 = (1.0f - w) * l2;
+    const float n1 = (1.0f - w) * L1(cx, cz), n2 = near1 ? (1.0f - w) * L2(cx, cz) : 0.0f;
     if (rc.corner) {
       MU1.add(cx, cz + rc.nz_, rc.cz * n1);
       MU1.add(cx + rc.nx_, cz, rc.cx * n1);
-      CB.add(cx, cz, rc.bK * n1);
+      ACC.add(cx, cz, rc.bK * n1);
       if (near1) {
-        MU2.add(cx, cz + rc.nz_, rc.cz * n2);
-        MU2.add(cx + rc.nx_, cz, rc.cx * n2);
+        ACC.add(cx, cz + rc.nz_, -(rc.cz * n2));
+        ACC.add(cx + rc.nx_, cz, -(rc.cx * n2));
       }
     } else {
       const int ix_i = cx + rc.nx_, iz_i = cz + rc.nz_;
       MU1.add(ix_i, iz_i, rc.au3i * n1);
       MU1.add(ix_i + rc.tx_, iz_i + rc.tz_, rc.au3t * n1);
       MU1.add(ix_i - rc.tx_, iz_i - rc.tz_, rc.au3t * n1);
-      CB.add(cx, cz, rc.bK * n1);
-      CB.add(ix_i, iz_i, rc.bi * n1);
+      ACC.add(cx, cz, rc.bK * n1);
+      ACC.add(ix_i, iz_i, rc.bi * n1);
       if (near1) {
-        MU2.add(ix_i, iz_i, rc.au3i * n2);
-        MU2.add(ix_i + rc.tx_, iz_i + rc.tz_, rc.au3t * n2);
-        MU2.add(ix_i - rc.tx_, iz_i - rc.tz_, rc.au3t * n2);
-        PB.add(cx, cz, rc.gK * n2);
-        PB.add(ix_i, iz_i, rc.gi * n2);
-        PB.add(cx + rc.tx_, cz + rc.tz_, rc.gt * n2);
-        PB.add(cx - rc.tx_, cz - rc.tz_, rc.gt * n2);
+        ACC.add(ix_i, iz_i, -(rc.au3i * n2));
+        ACC.add(ix_i + rc.tx_, iz_i + rc.tz_, -(rc.au3t * n2));
+        ACC.add(ix_i - rc.tx_, iz_i - rc.tz_, -(rc.au3t * n2));
+        ACC.add(cx, cz, rc.gK * n2);
+        ACC.add(ix_i, iz_i, rc.gi * n2);
+        ACC.add(cx + rc.tx_, cz + rc.tz_, rc.gt * n2);
+        ACC.add(cx - rc.tx_, cz - rc.tz_, rc.gt * n2);
       }
     }
   }
   __syncthreads();
-  // stencil^T and frame^T of mu1 over the consumers in tile + 4
+
+  // stencilT: vz mu, vx mu of the 8th-order consumers for the gather; the
+  // low-order and frame consumers (outer 4 cells) scatter
   for (int i = tid; i < MU_C * MU_R; i += A_NT_P) {
     const int cx = x0 - 4 + i / MU_R, cz = z0 - 4 + i % MU_R;
-    if (cx < 0 || cx >= g.NX || cz < 0 || cz >= g.NZ) continue;
-    if (sMU1[i] != 0) stencil_T(g, V, cx, cz, (float)((double)sMU1[i] * inv), CB);
+    float wz = 0.0f, wx = 0.0f;
+    if (cx >= 0 && cx < NX && cz >= 0 && cz < NZ && sMU1[i] != 0) {
+      const float mu = (float)((double)sMU1[i] * inv);
+      if (is8(cx, cz)) {
+        Coef k = coef(V(cx, cz), g);
+        wz = k.vz * mu;
+        wx = k.vx * mu;
+      } else {
+        stencil_T(g, V, cx, cz, mu, ACC);
+      }
+    }
+    sWZ[i] = wz;
+    sWX[i] = wx;
   }
   __syncthreads();
+
+  // L_k = gather + ACC + R^T d on the tile; grad += w lap mu(L1)
+  const MA WZ{sWZ, x0 - 4, z0 - 4}, WX{sWX, x0 - 4, z0 - 4};
+  const int qz = tid % QZ, cxp = tid / QZ;
+  const int ix = x0 + 2 * cxp, iz0 = z0 + 4 * qz;
   float *out = g.fa[(a.rot + 2) % 3];
   const bool img = a.snap_k >= 0 && g.snap != nullptr;
   const float inv_scale = img ? snap_inv_scale(g, a.snap_k, x0, z0) : 0.0f;
-  for (int i = tid; i < TX * TZ; i += A_NT_P) {
-    const int ix = x0 + i / TZ, iz = z0 + i % TZ;
-    if (ix >= g.NX || iz >= g.NZ) continue;
-    const int li = i;  // tile-local index (column-major, TZ rows)
-    float v = (float)((double)(sCB[li] + sPB[li] - sMU2[li]) * inv);
-    const int x = ix - g.pml, z = iz - g.pml;
-    const bool inside = x >= 0 && x < g.nx && z >= 0 && z < g.nz;
-    if (a.rec_k >= 0 && x >= 0 && x < g.nx && iz == g.gz[x] + g.pml)
-      v += g.rec[(size_t)a.rec_k * g.nx + x];
-    out[(size_t)ix * g.LDZ + iz] = v;
-    if (img && inside) {
-      float lap = snap_load(g, a.snap_k, x, z) * inv_scale;
-      g.grad[(size_t)x * g.nz + z] += (double)(a.img_w * lap * MU1.get(ix, iz));
+  float4 xm[10];
+#pragma unroll
+  for (int m = 0; m < 10; m++) xm[m] = WX.quad(ix - 4 + m, iz0);
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int cx = ix + j;
+    if (cx >= NX) continue;
+    const float4 za = WZ.quad(cx, iz0 - 4), zb = WZ.quad(cx, iz0), zc = WZ.quad(cx, iz0 + 4);
+    const float zz[12] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w, zc.x, zc.y, zc.z, zc.w};
+    const int x = cx - g.pml;
+    const int gzr = (x >= 0 && x < g.nx) ? g.gz[x] + g.pml : -1;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int cz = iz0 + r;
+      if (cz >= NZ) break;
+      const float sz_ = lap8(zz[r], zz[r + 1], zz[r + 2], zz[r + 3], zz[r + 4], zz[r + 5],
+                             zz[r + 6], zz[r + 7], zz[r + 8]);
+      const float sx_ = lap8(comp(xm[j], r), comp(xm[j + 1], r), comp(xm[j + 2], r),
+                             comp(xm[j + 3], r), comp(xm[j + 4], r), comp(xm[j + 5], r),
+                             comp(xm[j + 6], r), comp(xm[j + 7], r), comp(xm[j + 8], r));
+      const float mu = MU1.get(cx, cz);
+      float v = sz_ + sx_ + (is8(cx, cz) ? 2.0f * mu : 0.0f) + ACC.get(cx, cz);
+      if (a.rec_k >= 0 && cz == gzr) v += g.rec[(size_t)a.rec_k * g.nx + x];
+      out[(size_t)cx * g.LDZ + cz] = v;
+      const int z = cz - g.pml;
+      if (img && x >= 0 && x < g.nx && z >= 0 && z < g.nz) {
+        float lap = snap_load(g, a.snap_k, x, z) * inv_scale;
+        g.grad[(size_t)x * g.nz + z] += (double)(a.img_w * lap * mu);
+      }
     }
   }
 }

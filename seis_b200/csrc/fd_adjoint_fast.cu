@@ -1,6 +1,7 @@
-// Exact-adjoint kernels.  Built with multiply-add contraction (the adjoint has
-// no reference rounding to reproduce) but IEEE division, so that the one-way
-// coefficients it transposes are the forward's correctly rounded ones.
+// Exact-adjoint kernels, built like the fast step kernels (multiply-add
+// contraction, approximate division): the adjoint transposes the fast Born
+// operator that the LSRTM solver applies, so it carries the same coefficient
+// rounding; it has no reference rounding to reproduce.
 #define SEIS_NS fast
 #include "fd_adjoint.cuh"
 
