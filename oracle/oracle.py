@@ -234,3 +234,74 @@ def lsrtm_cgls(nx, nz, shots, x0, wav, v0, dobs, niter, prec="f64"):
 
 def ref_set_threads(n: int):
     ref_lib().ref_set_threads(_I(n))
+
+
+class RefInversion:
+    """The reference's own Inversion object (src/lsrtm/inversion.cpp, compiled
+    into oracle/_ref) with ns shots: sources sc [ns][2] (x, z), receivers
+    gx/gz lists per shot; exposes its geometry members on flat arrays."""
+
+    def __init__(self, sc, gxs, gzs, dx, dz, dt, fr, velfx, nx, nz, nt, delay=0, lpad=0, rpad=0):
+        L = ref_lib()
+        V, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+        L.ref_inv_create.restype = V
+        L.ref_inv_create.argtypes = [I, I, V, V, V, F, F, F, F, F, I, I, I, I, I, I]
+        L.ref_inv_destroy.argtypes = [V]
+        L.ref_inv_getvel.argtypes = [V, I, V, I, I, F, ctypes.POINTER(F), ctypes.POINTER(I), V,
+                                     ctypes.c_size_t]
+        L.ref_inv_getigz.argtypes = [V, F, I, I, V]
+        L.ref_inv_swapreord.argtypes = [V, V, I, I, I, V, F, I, I]
+        L.ref_inv_swapmodel.argtypes = [V, V, V, F, F, I, I, I, I, I]
+        L.ref_inv_removedirect.argtypes = [V, V, V, I]
+        self.L = L
+        ns = len(gxs)
+        self.ng = np.array([len(g) for g in gxs], np.int32)
+        self.ngmax = int(self.ng.max())
+        gc = np.zeros((ns, 2, self.ngmax), np.float32)
+        for i, (gx, gz) in enumerate(zip(gxs, gzs)):
+            gc[i, 0, :len(gx)] = gx
+            gc[i, 1, :len(gz)] = gz
+        self._sc = np.ascontiguousarray(sc, np.float32)
+        self._gc = gc
+        self.nt, self.nx, self.nz = nt, nx, nz
+        self.h = L.ref_inv_create(ns, self.ngmax, _ptr(self.ng), _ptr(self._sc), _ptr(gc), dx, dz, dt,
+                                  fr, velfx, nx, nz, nt, delay, lpad, rpad)
+
+    def close(self):
+        if self.h:
+            self.L.ref_inv_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def getvel(self, is_, vel, velfx):
+        vel = np.ascontiguousarray(vel, np.float32)
+        nx, nz = vel.shape
+        cap = 1 << 24
+        out = np.zeros(cap, np.float32)
+        fx, n = ctypes.c_float(), ctypes.c_int()
+        rc = self.L.ref_inv_getvel(self.h, is_, _ptr(vel), nz, nx, velfx, ctypes.byref(fx),
+                                   ctypes.byref(n), _ptr(out), cap)
+        if rc != 0:
+            raise RuntimeError("reference getVel failed")
+        return fx.value, n.value, out[:n.value * nz].reshape(n.value, nz).copy()
+
+    def getigz(self, fx_sub, nx_sub, is_):
+        out = np.zeros(nx_sub, np.int32)
+        if self.L.ref_inv_getigz(self.h, fx_sub, nx_sub, is_, _ptr(out)) != 0:
+            raise RuntimeError("reference getIgz failed")
+        return out
+
+    def swapreord(self, csg, is_, rec, fx, adj):
+        if self.L.ref_inv_swapreord(self.h, _ptr(csg), is_, csg.shape[0], csg.shape[1], _ptr(rec),
+                                    fx, rec.shape[0], 1 if adj else 0) != 0:
+            raise RuntimeError("reference swapReord failed")
+
+    def swapmodel(self, m, d, mfx, dfx, add):
+        if self.L.ref_inv_swapmodel(self.h, _ptr(m), _ptr(d), mfx, dfx, m.shape[1], m.shape[0],
+                                    d.shape[1], d.shape[0], 1 if add else 0) != 0:
+            raise RuntimeError("reference swapModel failed")
+
+    def removedirect(self, csg, v, is_):
+        if self.L.ref_inv_removedirect(self.h, _ptr(csg), _ptr(v), is_) != 0:
+            raise RuntimeError("reference removeDirect failed")
