@@ -224,7 +224,7 @@ int seis_fd_vec_axpby(seis_fd_ctx *ctx, float *d_y, const float *d_x, double a, 
  *   L m  = [ Born_s( m[x0_s .. x0_s + nx_s) ) ]_s      (forward, per shot)
  *   L^T d = sum_s scatter_{x0_s}( BornAdjoint_s(d_s) )
  * Shot s covers columns x0_s .. x0_s + nx_s - 1 of the nx x nz global grid and
- * has the global nz.  The background velocity and wavelet are fixed: the
+ * has the global nz (seis_fd_lsrtm_create_mapped: any non-decreasing map).  The background velocity and wavelet are fixed: the
  * adjoint's source-term snapshots are computed once and reused by every
  * iteration.  Dot products, step lengths and residual norms are FP64. */
 typedef struct seis_fd_lsrtm seis_fd_lsrtm;
@@ -237,6 +237,13 @@ typedef struct {
 int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot,
                          const seis_shot_desc *shots, const int *x0,
                          const seis_lsrtm_opts *opts, seis_fd_lsrtm **out);
+/* Same with an explicit column map: colmap holds, shot after shot, the model
+ * column of each of the shot's nx_s sub-grid columns (non-decreasing, as the
+ * aperture extraction of the shot driver clamps at the model edges); L^T
+ * scatters through the transpose of that map. */
+int seis_fd_lsrtm_create_mapped(seis_fd_ctx *ctx, int nx, int nz, int nshot,
+                                const seis_shot_desc *shots, const int *colmap,
+                                const seis_lsrtm_opts *opts, seis_fd_lsrtm **out);
 int seis_fd_lsrtm_destroy(seis_fd_lsrtm *ls);
 /* background velocity [nx][nz] of the global grid and wavelet [nt+ndel] */
 int seis_fd_lsrtm_set_background(seis_fd_lsrtm *ls, const float *h_v0, const float *h_wav);

@@ -31,6 +31,10 @@ int seis_geom_aperture(float sx, const float *gx, int ng, float dx, int lpad, in
 int seis_geom_extract(const float *model, int nz, int nx, float fx, float dx, float fx_sub,
                       int nx_sub, float *sub);
 
+/* The model column each sub-grid column copies in seis_geom_extract:
+ * cols[nx_sub], non-decreasing. */
+int seis_geom_extract_columns(int nx, float fx, float dx, float fx_sub, int nx_sub, int *cols);
+
 /* Receiver depth index per sub-grid column (Inversion::getIgz,
  * inversion.cpp:600-625): 0 where no receiver lies, else the depth sample
  * of the (last) receiver in the column.  nz = model depth samples (range

@@ -190,23 +190,25 @@ def born_adjoint(shot, wav, vel, rec, prec="f64", every=1):
     return img
 
 
-def lsrtm_cgls(nx, nz, shots, x0, wav, v0, dobs, niter, prec="f64"):
+def lsrtm_cgls(nx, nz, shots, x0, wav, v0, dobs, niter, prec="f64", cols=None):
     """CGLS on the global model (the solver the reference declares as
     Inversion::conope_MPI / cgsolver_MPI, src/lsrtm/inversion.h:81,87, without
     a definition), built from the oracle's Born operator and its exact
-    transpose, in FP64.  Shot k covers model columns x0[k] .. x0[k]+nx_k-1.
-    Returns (model, |d|^2, [|r|^2 after each iteration])."""
+    transpose, in FP64.  Shot k covers model columns x0[k] .. x0[k]+nx_k-1, or
+    the columns cols[k] (a sub-grid column map, repeated columns summed by the
+    transpose).  Returns (model, |d|^2, [|r|^2 after each iteration])."""
     f = np.float64
     wav = np.asarray(wav, f)
-    subs = [slice(x, x + s.nx) for s, x in zip(shots, x0)]
+    if cols is None:
+        cols = [np.arange(x, x + s.nx) for s, x in zip(shots, x0)]
 
     def L(m):
-        return [born(s, wav, v0[c], m[c], prec=prec).astype(f) for s, c in zip(shots, subs)]
+        return [born(s, wav, v0[c], m[c], prec=prec).astype(f) for s, c in zip(shots, cols)]
 
     def LT(r):
         out = np.zeros((nx, nz), f)
-        for s, c, rk in zip(shots, subs, r):
-            out[c] += born_adjoint(s, wav, v0[c], rk, prec=prec)
+        for s, c, rk in zip(shots, cols, r):
+            np.add.at(out, c, born_adjoint(s, wav, v0[c], rk, prec=prec))
         return out
 
     def ddot(a, b):
@@ -305,3 +307,45 @@ class RefInversion:
     def removedirect(self, csg, v, is_):
         if self.L.ref_inv_removedirect(self.h, _ptr(csg), _ptr(v), is_) != 0:
             raise RuntimeError("reference removeDirect failed")
+
+
+_PARAM_INTS = ("nthread", "ns", "ngmax", "nx", "nz", "nt", "npml", "delay", "delaycal", "mask",
+               "maxiter", "lpad", "rpad", "planeTag", "sbegin", "send")
+_PARAM_FLOATS = ("dx", "dz", "dt", "fr", "velfx")
+_PARAM_STRINGS = ("precsg", "wdir", "v0file", "vfile", "coordfile", "maskfile")
+
+
+def ref_read_params(path):
+    """The reference's Inversion::readParamFile (src/lsrtm/inversion.cpp:38-88)
+    on a file: dict of the values it reads, or None where it would exit."""
+    L = ref_lib()
+    L.ref_param_read.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    ints = np.zeros(16, np.int32)
+    floats = np.zeros(5, np.float32)
+    strs = ctypes.create_string_buffer(256 * 6)
+    if L.ref_param_read(path.encode(), _ptr(ints), _ptr(floats), strs) != 0:
+        return None
+    out = dict(zip(_PARAM_INTS, map(int, ints)))
+    out.update(zip(_PARAM_FLOATS, map(np.float32, floats)))
+    raw = strs.raw
+    out.update((k, raw[256 * i:256 * (i + 1)].split(b"\0")[0].decode())
+               for i, k in enumerate(_PARAM_STRINGS))
+    return out
+
+
+def ref_read_coords(path, ngmax):
+    """The reference's Coords readers (src/util/coord.cpp): ns, ng, sc, gc."""
+    L = ref_lib()
+    L.ref_coords_count.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    L.ref_coords_read.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_void_p]
+    ns = np.zeros(1, np.int32)
+    if L.ref_coords_count(path.encode(), _ptr(ns)) != 0:
+        raise RuntimeError("reference countShots failed")
+    ns = int(ns[0])
+    ng = np.zeros(ns, np.int32)
+    sc = np.zeros((ns, 2), np.float32)
+    gc = np.zeros((ns, 2, ngmax), np.float32)
+    if L.ref_coords_read(path.encode(), ns, ngmax, _ptr(ng), _ptr(sc), _ptr(gc)) != 0:
+        raise RuntimeError("reference Coords failed")
+    return ns, ng, sc, gc

@@ -185,9 +185,16 @@ int ref_coords_read(const char *file, int ns, int ngmax, int *ng, float *sc, flo
       sc[2 * is] = s[is][0];
       sc[2 * is + 1] = s[is][1];
     }
-    float ***g = MyAlloc<float>::alc(ngmax, 2, ns);
+    // getConfig lets getReceivers size the array itself (max of ng)
+    float ***g = 0;
     Coords::getReceivers(file, ns, n, g);
-    std::memcpy(gc, g[0][0], sizeof(float) * (size_t)ns * 2 * ngmax);
+    int ngm = 0;
+    for (int is = 0; is < ns; is++) ngm = n[is] > ngm ? n[is] : ngm;
+    for (size_t i = 0; i < (size_t)ns * 2 * ngmax; i++) gc[i] = -1e10f;
+    for (int is = 0; is < ns; is++)
+      for (int k = 0; k < 2; k++)
+        for (int ig = 0; ig < ngm && ig < ngmax; ig++)
+          gc[((size_t)is * 2 + k) * ngmax + ig] = g[is][k][ig];
     MyAlloc<int>::free(n);
     MyAlloc<float>::free(s);
     MyAlloc<float>::free(g);

@@ -1140,7 +1140,12 @@ struct seis_fd_lsrtm {
   int nx = 0, nz = 0, nshot = 0, nt = 0;
   std::vector<seis_shot_desc> shots;
   std::vector<std::vector<int>> gz;
-  std::vector<int> x0;
+  // model column of every sub-grid column of every shot (non-decreasing)
+  std::vector<std::vector<int>> cmap;
+  std::vector<size_t> cmap_off, range_off;
+  std::vector<int> g0, gcount;  // model columns g0 .. g0 + gcount - 1 a shot touches
+  int *d_cmap = nullptr;
+  int2 *d_ranges = nullptr;
   seis_fd_plan born{nullptr}, adj{nullptr};
   std::vector<void *> allocs;
   float *m = nullptr, *p = nullptr, *s = nullptr;  // model-space vectors [nx][nz]
@@ -1186,19 +1191,26 @@ int lsrtm_adjoint(seis_fd_lsrtm &L) {
   CK(cudaMemsetAsync(L.s, 0, sizeof(float) * nm, ctx->stream));
   for (int k = 0; k < L.nshot; k++) {
     const ShotDev &g = L.adj.p->sd[k];
-    CK(launch_add(L.s + (size_t)L.x0[k] * L.nz, g.img, (size_t)g.nx * g.nz, ctx->stream));
+    CK(launch_scatter_cols(L.s, L.nz, L.d_ranges + L.range_off[k], L.g0[k], L.gcount[k], g.img,
+                           ctx->stream));
     ctx->launches++;
   }
   return SEIS_OK;
 }
 
-// q = L p into the Born plan's gathers.
+// q = L p into the Born plan's gathers: each shot's perturbation is its
+// sub-grid of p (column map), padded into the plan.
 int lsrtm_forward(seis_fd_lsrtm &L) {
+  seis_fd_ctx *ctx = L.ctx;
+  Plan &pb = *L.born.p;
   for (int k = 0; k < L.nshot; k++) {
-    int rc = plan_input(&L.born, k, SEIS_IN_DV, L.p + (size_t)L.x0[k] * L.nz, true);
-    if (rc) return rc;
+    const ShotDev &g = pb.sd[k];
+    CK(launch_gather_cols(L.p, L.nz, L.d_cmap + L.cmap_off[k], g.nx, pb.d_stage, ctx->stream));
+    CK(launch_pad(pb.d_stage, g.nx, g.nz, g.pml, g.LDZ, false, const_cast<float *>(g.dv),
+                  ctx->stream));
+    ctx->launches += 2;
   }
-  return plan_run(*L.born.p);
+  return plan_run(pb);
 }
 
 // out = sum over shots of <a_s, b_s> in data space; a from the Born plan's
@@ -1218,17 +1230,25 @@ int data_dot(seis_fd_lsrtm &L, bool q_left, bool q_right, double *out) {
 
 extern "C" {
 
-int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot, const seis_shot_desc *shots,
-                         const int *x0, const seis_lsrtm_opts *opts, seis_fd_lsrtm **out) {
+int seis_fd_lsrtm_create_mapped(seis_fd_ctx *ctx, int nx, int nz, int nshot,
+                                const seis_shot_desc *shots, const int *colmap,
+                                const seis_lsrtm_opts *opts, seis_fd_lsrtm **out) {
   int rc = begin(ctx);
   if (rc) return rc;
-  if (!out || !shots || !x0 || nshot < 1 || nx < 1 || nz < 1)
+  if (!out || !shots || !colmap || nshot < 1 || nx < 1 || nz < 1)
     return fail(ctx, SEIS_ERR_ARG, "lsrtm: bad arguments");
   *out = nullptr;
+  size_t off = 0;
   for (int k = 0; k < nshot; k++) {
-    if (shots[k].nz != nz || x0[k] < 0 || x0[k] + shots[k].nx > nx)
-      return fail(ctx, SEIS_ERR_ARG, "lsrtm: shot %d aperture [%d, %d) x nz %d outside %d x %d",
-                  k, x0[k], x0[k] + shots[k].nx, shots[k].nz, nx, nz);
+    if (shots[k].nz != nz)
+      return fail(ctx, SEIS_ERR_ARG, "lsrtm: shot %d has nz %d, the model %d", k, shots[k].nz, nz);
+    for (int ix = 0; ix < shots[k].nx; ix++) {
+      const int c = colmap[off + ix];
+      if (c < 0 || c >= nx || (ix > 0 && c < colmap[off + ix - 1]))
+        return fail(ctx, SEIS_ERR_ARG,
+                    "lsrtm: shot %d column map must be non-decreasing within [0, %d)", k, nx);
+    }
+    off += shots[k].nx;
   }
   seis_lsrtm_opts o{1, SEIS_SNAP_BF16, 0};
   if (opts) o = *opts;
@@ -1237,7 +1257,25 @@ int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot, const seis
   L->ctx = ctx;
   L->nx = nx; L->nz = nz; L->nshot = nshot; L->nt = shots[0].nt;
   L->shots.assign(shots, shots + nshot);
-  L->x0.assign(x0, x0 + nshot);
+  std::vector<int2> ranges;
+  off = 0;
+  for (int k = 0; k < nshot; k++) {
+    const int n = shots[k].nx;
+    L->cmap.emplace_back(colmap + off, colmap + off + n);
+    L->cmap_off.push_back(off);
+    off += n;
+    const std::vector<int> &m = L->cmap.back();
+    L->g0.push_back(m[0]);
+    L->gcount.push_back(m[n - 1] - m[0] + 1);
+    L->range_off.push_back(ranges.size());
+    const size_t base = ranges.size();
+    ranges.resize(base + (size_t)L->gcount.back(), make_int2(0, -1));
+    for (int ix = 0; ix < n; ix++) {
+      int2 &r = ranges[base + (m[ix] - m[0])];
+      if (r.y < r.x) r.x = ix;
+      r.y = ix;
+    }
+  }
   Plan *pb = nullptr, *pa = nullptr;
   rc = plan_create(ctx, OP_BORN, nshot, shots, &pb);
   if (!rc) rc = plan_create(ctx, OP_BORN_ADJ, nshot, shots, &pa);
@@ -1245,6 +1283,7 @@ int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot, const seis
   L->adj.p = pa;
   if (!rc) {
     pb->exact = o.exact != 0;
+    pa->exact = o.exact != 0;
     seis_fd_plan h{pa};
     rc = seis_fd_plan_set_snapshots(&h, o.snap_every, o.snap_dtype);
   }
@@ -1263,11 +1302,19 @@ int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot, const seis
     L->rr_cap = 4096;
     rc = L->alloc(&L->rr, (size_t)L->rr_cap);
   }
+  if (!rc) rc = L->alloc(&L->d_cmap, off);
+  if (!rc) rc = L->alloc(&L->d_ranges, ranges.size());
   if (!rc) {
     // the adjoint plan reads its receiver data straight from the residual
     for (int k = 0; k < nshot; k++) pa->sd[k].rec = L->r + L->doff[k];
     cudaError_t e = cudaMemcpyAsync(pa->d_sd, pa->sd.data(), sizeof(ShotDev) * nshot,
                                     cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(L->d_cmap, colmap, sizeof(int) * off, cudaMemcpyHostToDevice,
+                          ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(L->d_ranges, ranges.data(), sizeof(int2) * ranges.size(),
+                          cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) rc = fail(ctx, SEIS_ERR_CUDA, "lsrtm setup: %s", cudaGetErrorString(e));
   }
@@ -1277,6 +1324,22 @@ int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot, const seis
   }
   *out = L;
   return SEIS_OK;
+}
+
+int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot, const seis_shot_desc *shots,
+                         const int *x0, const seis_lsrtm_opts *opts, seis_fd_lsrtm **out) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (!out || !shots || !x0 || nshot < 1 || nx < 1 || nz < 1)
+    return fail(ctx, SEIS_ERR_ARG, "lsrtm: bad arguments");
+  std::vector<int> map;
+  for (int k = 0; k < nshot; k++) {
+    if (x0[k] < 0 || x0[k] + shots[k].nx > nx)
+      return fail(ctx, SEIS_ERR_ARG, "lsrtm: shot %d aperture [%d, %d) outside %d columns", k,
+                  x0[k], x0[k] + shots[k].nx, nx);
+    for (int ix = 0; ix < shots[k].nx; ix++) map.push_back(x0[k] + ix);
+  }
+  return seis_fd_lsrtm_create_mapped(ctx, nx, nz, nshot, shots, map.data(), opts, out);
 }
 
 int seis_fd_lsrtm_destroy(seis_fd_lsrtm *L) {
@@ -1292,12 +1355,17 @@ int seis_fd_lsrtm_set_background(seis_fd_lsrtm *L, const float *h_v0, const floa
   int rc = begin(L->ctx);
   if (rc) return rc;
   if (!h_v0 || !h_wav) return fail(L->ctx, SEIS_ERR_ARG, "null array");
+  std::vector<float> sub;
   for (int k = 0; k < L->nshot && !rc; k++) {
-    const float *sub = h_v0 + (size_t)L->x0[k] * L->nz;  // aperture columns are contiguous
-    rc = plan_input(&L->born, k, SEIS_IN_VEL, sub, false);
+    const std::vector<int> &m = L->cmap[k];
+    sub.resize(m.size() * (size_t)L->nz);
+    for (size_t ix = 0; ix < m.size(); ix++)
+      std::memcpy(sub.data() + ix * L->nz, h_v0 + (size_t)m[ix] * L->nz, sizeof(float) * L->nz);
+    rc = plan_input(&L->born, k, SEIS_IN_VEL, sub.data(), false);
     if (!rc) rc = plan_input(&L->born, k, SEIS_IN_WAVELET, h_wav, false);
-    if (!rc) rc = plan_input(&L->adj, k, SEIS_IN_VEL, sub, false);
+    if (!rc) rc = plan_input(&L->adj, k, SEIS_IN_VEL, sub.data(), false);
     if (!rc) rc = plan_input(&L->adj, k, SEIS_IN_WAVELET, h_wav, false);
+    if (!rc) rc = sync(L->ctx);  // the host sub-grid is reused by the next shot
   }
   L->ready = false;
   return rc ? rc : sync(L->ctx);

@@ -172,6 +172,10 @@ cudaError_t launch_axpby(float *y, const float *x, double a, double b, size_t n,
 cudaError_t launch_axpby_dev(float *y, const float *x, const double *sa, double fa,
                              const double *sb, double fb, size_t n, cudaStream_t s);
 cudaError_t launch_add(float *y, const float *x, size_t n, cudaStream_t s);
+cudaError_t launch_gather_cols(const float *src, int nz, const int *map, int nxs, float *dst,
+                               cudaStream_t s);
+cudaError_t launch_scatter_cols(float *dst, int nz, const int2 *ranges, int g0, int ncols,
+                                const float *img, cudaStream_t s);
 cudaError_t launch_ratio(const double *num, const double *den, double *out, cudaStream_t s);
 // Set kernel attributes (shared-memory limits); call once per device.
 cudaError_t configure_kernels();

@@ -78,6 +78,35 @@ __global__ void ratio_kernel(const double *num, const double *den, double *out) 
   *out = *den != 0.0 ? *num / *den : 0.0;
 }
 
+// dst[ix][iz] = src[map[ix]][iz]: the sub-grid of a model by its column map
+__global__ void gather_cols_kernel(const float *__restrict__ src, int nz, const int *__restrict__ map,
+                                   int nxs, float *__restrict__ dst) {
+  const size_t n = (size_t)nxs * nz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t ix = i / nz, iz = i - ix * nz;
+    dst[i] = src[(size_t)map[ix] * nz + iz];
+  }
+}
+
+// transpose of the gather: model column g0 + c collects the sub-grid columns
+// ranges[c].x .. ranges[c].y (the map is non-decreasing, so each preimage is
+// a range), summed in column order
+__global__ void scatter_cols_kernel(float *__restrict__ dst, int nz, const int2 *__restrict__ ranges,
+                                    int g0, int ncols, const float *__restrict__ img) {
+  const size_t n = (size_t)ncols * nz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t c = i / nz, iz = i - c * nz;
+    const int2 r = ranges[c];
+    if (r.y < r.x) continue;
+    float acc = img[(size_t)r.x * nz + iz];
+    for (int ix = r.x + 1; ix <= r.y; ix++) acc += img[(size_t)ix * nz + iz];
+    const size_t o = ((size_t)g0 + c) * nz + iz;
+    dst[o] = dst[o] + acc;
+  }
+}
+
 int grid_for(size_t n) {
   return (int)std::min<size_t>((n + VT - 1) / VT, (size_t)DOT_PARTS);
 }
@@ -105,6 +134,19 @@ cudaError_t launch_axpby_dev(float *y, const float *x, const double *sa, double 
 
 cudaError_t launch_add(float *y, const float *x, size_t n, cudaStream_t s) {
   add_kernel<<<std::max(1, grid_for(n)), VT, 0, s>>>(y, x, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_cols(const float *src, int nz, const int *map, int nxs, float *dst,
+                               cudaStream_t s) {
+  gather_cols_kernel<<<std::max(1, grid_for((size_t)nxs * nz)), VT, 0, s>>>(src, nz, map, nxs, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_cols(float *dst, int nz, const int2 *ranges, int g0, int ncols,
+                                const float *img, cudaStream_t s) {
+  scatter_cols_kernel<<<std::max(1, grid_for((size_t)ncols * nz)), VT, 0, s>>>(dst, nz, ranges, g0,
+                                                                              ncols, img);
   return cudaGetLastError();
 }
 

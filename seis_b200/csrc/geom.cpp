@@ -7,6 +7,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "seis_fd.h"
 
@@ -42,19 +43,30 @@ int seis_geom_aperture(float sx, const float *gx, int ng, float dx, int lpad, in
   return *nx_sub >= 1 ? SEIS_OK : SEIS_ERR_ARG;
 }
 
-int seis_geom_extract(const float *model, int nz, int nx, float fx, float dx, float fx_sub,
-                      int nx_sub, float *sub) {
-  if (!model || !sub || nz < 1 || nx < 1 || nx_sub < 1 || !(dx > 0.0f)) return SEIS_ERR_ARG;
+int seis_geom_extract_columns(int nx, float fx, float dx, float fx_sub, int nx_sub, int *cols) {
+  if (!cols || nx < 1 || nx_sub < 1 || !(dx > 0.0f)) return SEIS_ERR_ARG;
   const float lo = fx + dx;                            // :564
   const float hi = fx + (float)(nx - 1) * dx - dx;     // :565
   for (int ix = 0; ix < nx_sub; ix++) {
     const float x = fx_sub + (float)ix * dx;           // :572-573
+    if (x != x) return SEIS_ERR_ARG;                   // :594-597
     float at = x;
     if (!(x >= lo && x <= hi)) at = x < lo ? lo : hi;  // :579-593 (clamp)
     const int col = (int)((at - fx) / dx);
     if (col < 0 || col >= nx) return SEIS_ERR_ARG;
-    std::memcpy(sub + (size_t)ix * nz, model + (size_t)col * nz, sizeof(float) * nz);
+    cols[ix] = col;
   }
+  return SEIS_OK;
+}
+
+int seis_geom_extract(const float *model, int nz, int nx, float fx, float dx, float fx_sub,
+                      int nx_sub, float *sub) {
+  if (!model || !sub || nz < 1 || nx < 1 || nx_sub < 1 || !(dx > 0.0f)) return SEIS_ERR_ARG;
+  std::vector<int> cols((size_t)nx_sub);
+  int rc = seis_geom_extract_columns(nx, fx, dx, fx_sub, nx_sub, cols.data());
+  if (rc) return rc;
+  for (int ix = 0; ix < nx_sub; ix++)
+    std::memcpy(sub + (size_t)ix * nz, model + (size_t)cols[ix] * nz, sizeof(float) * nz);
   return SEIS_OK;
 }
 

@@ -23,6 +23,7 @@ def _setup():
         return L
     L.seis_geom_aperture.argtypes = [_F, _P, _I, _F, _I, _I, ctypes.POINTER(_F), ctypes.POINTER(_I)]
     L.seis_geom_extract.argtypes = [_P, _I, _I, _F, _F, _F, _I, _P]
+    L.seis_geom_extract_columns.argtypes = [_I, _F, _F, _F, _I, _P]
     L.seis_geom_receiver_rows.argtypes = [_P, _P, _I, _F, _I, _F, _F, _I, _P]
     L.seis_geom_source_index.argtypes = [_F, _F, _F, _F, _F, ctypes.POINTER(_I), ctypes.POINTER(_I)]
     L.seis_geom_reorder.argtypes = [_P, _I, _I, _P, _P, _F, _I, _F, _I]
@@ -63,6 +64,14 @@ def extract(model, fx, dx, fx_sub, nx_sub):
     out = np.zeros((nx_sub, m.shape[1]), np.float32)
     _ok(L.seis_geom_extract(_p(m), m.shape[1], m.shape[0], fx, dx, fx_sub, nx_sub, _p(out)),
         "extract")
+    return out
+
+
+def extract_columns(nx, fx, dx, fx_sub, nx_sub):
+    """Model column each sub-grid column copies (non-decreasing)."""
+    L = _setup()
+    out = np.zeros(nx_sub, np.int32)
+    _ok(L.seis_geom_extract_columns(nx, fx, dx, fx_sub, nx_sub, _p(out)), "extract_columns")
     return out
 
 
