@@ -323,7 +323,12 @@ def main():
     from seis_b200._lib import SNAP_BF16, Lsrtm
 
     torch.cuda.set_device(local)
-    sv = workload(args.workload, rank, args.nt)
+    from seis_b200.shards import DeviceEngine, ShardedCGLS, nccl_reduce, shard_shots
+    # N ranks: a survey of 32 N shots, 32 per rank, image and CG sums all-reduced
+    full = workload(args.workload, rank, args.nt) if world == 1 else \
+        __import__("seis_b200.synth", fromlist=["lsrtm"]).lsrtm(nshots=32 * world, nt=args.nt)
+    mine = shard_shots([full.cell_updates_of(i) for i in range(len(full.shots))], world)[rank]
+    sv = full.subset(mine)
     shots = sv.shots
     ctx = Context(local)
     wav = sv.wavelet()
@@ -332,14 +337,16 @@ def main():
     ls.set_background(sv.vel0, wav)
     for i, d in enumerate(dobs):
         ls.set_data(i, d)
-    rr0 = ls.reset()
+    eng = DeviceEngine(ls)
+    cg = ShardedCGLS(eng, nccl_reduce(eng))
+    rr0 = cg.reset()
     cells = iteration_cells(shots)
     assert cells == ls.cell_updates, (cells, ls.cell_updates)
 
     # ---- device-resident: CG iterations timed with CUDA events on the
     # library's stream
-    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local))
-    rr_warm = ls.iterate(args.warmup) if args.warmup > 0 else []
+    stream = eng.stream
+    rr_warm = cg.iterate(args.warmup) if args.warmup > 0 else []
     launches0 = ctx.launches
     barrier(world)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -348,7 +355,7 @@ def main():
         torch.cuda.synchronize()
         start.record(stream)
         for _ in range(args.steps):
-            rr.extend(ls.iterate(1).tolist())
+            rr.extend(cg.iterate(1))
         stop.record(stream)
         stop.synchronize()
         torch.cuda.synchronize()
@@ -371,8 +378,8 @@ def main():
         ctx.check(L.seis_fd_lsrtm_set_background(ls.h, h_v0.data_ptr(), h_wav.data_ptr()))
         for i in range(len(shots)):
             ctx.check(L.seis_fd_lsrtm_set_data(ls.h, i, h_d[i].data_ptr()))
-        ctx.check(L.seis_fd_lsrtm_reset(ls.h, ctypes.c_void_p(h_rr.data_ptr())))
-        ctx.check(L.seis_fd_lsrtm_iterate(ls.h, 1, ctypes.c_void_p(h_rr.data_ptr() + 8)))
+        h_rr[0] = cg.reset()
+        h_rr[1] = cg.iterate(1)[0]
         ctx.check(L.seis_fd_lsrtm_model(ls.h, h_m.data_ptr()))
 
     e2e_steps = max(1, args.steps // 2)
@@ -382,7 +389,7 @@ def main():
         e2e_step()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
     e2e_ms = max_over_ranks(e2e_ms, world)
-    e2e_cells = cells + reset_cells(shots)
+    e2e_cells = (cells + reset_cells(shots)) * world
     h2d = sv.vel0.nbytes + wav.nbytes + sum(d.nbytes for d in dobs)
     d2h = h_m.numel() * 4 + 16
     dev_bytes = ls.device_bytes
@@ -392,7 +399,7 @@ def main():
     top, rows = kernel_roofline(ctx, sv, ms_per_step)
     hbm, src = peaks()
     ach = top["bytes"] / (top["ms"] * 1e-3) / 1e9
-    plain = None if args.no_plain else plain_fp32(ctx, sv, dobs)
+    plain = None if (args.no_plain or world > 1) else plain_fp32(ctx, sv, dobs)
     line = {
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -400,6 +407,9 @@ def main():
         "data": "synthetic (layered + faulted 1200x400 model; observed data = Born of the true "
                 "perturbation)",
         "config": {"workload": args.workload, "shots_per_gpu": len(shots),
+                   "shots_total": len(full.shots),
+                   "exchange": "per CG iteration: NCCL all-reduce of the image and 2 FP64 sums"
+                               if world > 1 else "none",
                    "grid": "1200x400 at 10 m, pml 40", "nt": shots[0].nt, "ndel": shots[0].ndel,
                    "snapshots": f"BF16 every {SNAP_EVERY} steps, per-tile scale",
                    "cell_updates_per_step": cells, "lsrtm_iter_ms": ms_per_step,
@@ -408,7 +418,7 @@ def main():
                          f"({dev_bytes / 2**30:.1f} GiB resident)",
                    "residual": {"rr0": rr0, "after_warmup": list(map(float, rr_warm)),
                                 "timed": rr}},
-        "e2e": {"value": e2e_cells * world / (e2e_ms / 1e3) / 1e9, "unit": "Gcell/s",
+        "e2e": {"value": e2e_cells / (e2e_ms / 1e3) / 1e9, "unit": "Gcell/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "cell_updates_per_step": e2e_cells},
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",

@@ -255,6 +255,19 @@ int seis_fd_lsrtm_reset(seis_fd_lsrtm *ls, double *h_rr);
  * iteration i (h_rr may be null).  Enqueued without host round trips; returns
  * after the last iteration completes. */
 int seis_fd_lsrtm_iterate(seis_fd_lsrtm *ls, int niter, double *h_rr);
+/* The three phases of one iteration, for a solver whose shots are spread
+ * over several devices (one solver per rank, each with its own shots and the
+ * same model grid).  Each phase is enqueued on the context's stream and leaves
+ * this rank's partial sums in the caller's device buffers; the caller sums
+ * them over the ranks in place (e.g. an NCCL all-reduce on that stream) before
+ * the next phase reads them.  On one device nothing needs summing:
+ *   reset   = phase_reset(s, rr), phase_direction(s, first = 1)
+ *   iterate = phase_forward(qq), phase_update(qq, s, rr), phase_direction(s, 0)
+ * d_s: [nx][nz] float; d_qq, d_rr: one double. */
+int seis_fd_lsrtm_phase_reset(seis_fd_lsrtm *ls, float *d_s, double *d_rr);
+int seis_fd_lsrtm_phase_forward(seis_fd_lsrtm *ls, double *d_qq);
+int seis_fd_lsrtm_phase_update(seis_fd_lsrtm *ls, const double *d_qq, float *d_s, double *d_rr);
+int seis_fd_lsrtm_phase_direction(seis_fd_lsrtm *ls, const float *d_s, int first);
 /* current model [nx][nz] */
 int seis_fd_lsrtm_model(seis_fd_lsrtm *ls, float *h_m);
 /* padded cell-updates of one iteration (Born + adjoint reverse pass) */

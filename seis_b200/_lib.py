@@ -124,6 +124,12 @@ def lib():
         L.seis_fd_lsrtm_create.argtypes = [P, I, I, I, SD, ctypes.POINTER(I),
                                            ctypes.POINTER(LsrtmOptsC), PP]
         L.seis_fd_lsrtm_destroy.argtypes = [P]
+        L.seis_fd_lsrtm_create_mapped.argtypes = [P, I, I, I, SD, ctypes.POINTER(I),
+                                                  ctypes.POINTER(LsrtmOptsC), PP]
+        L.seis_fd_lsrtm_phase_reset.argtypes = [P, P, P]
+        L.seis_fd_lsrtm_phase_forward.argtypes = [P, P]
+        L.seis_fd_lsrtm_phase_update.argtypes = [P, P, P, P]
+        L.seis_fd_lsrtm_phase_direction.argtypes = [P, P, I]
         L.seis_fd_lsrtm_set_background.argtypes = [P, P, P]
         L.seis_fd_lsrtm_set_data.argtypes = [P, I, P]
         L.seis_fd_lsrtm_reset.argtypes = [P, P]
@@ -326,17 +332,40 @@ class Lsrtm:
     Shot k covers columns x0[k] .. x0[k] + shots[k].nx - 1 of the model.
     """
 
-    def __init__(self, ctx: Context, nx: int, nz: int, shots, x0, snap_every: int = 1,
-                 snap_dtype: int = None, exact: bool = False):
+    def __init__(self, ctx: Context, nx: int, nz: int, shots, x0=None, snap_every: int = 1,
+                 snap_dtype: int = None, exact: bool = False, colmaps=None):
+        """Shot k covers columns x0[k] .. x0[k] + nx_k - 1, or the model columns
+        colmaps[k] (one per sub-grid column, non-decreasing)."""
         self.ctx, self.nx, self.nz, self.shots = ctx, nx, nz, list(shots)
         self._descs = shot_array(self.shots)
-        self._x0 = (ctypes.c_int * len(self.shots))(*[int(v) for v in x0])
         o = LsrtmOptsC(snap_every, SNAP_BF16 if snap_dtype is None else snap_dtype,
                        1 if exact else 0)
         h = ctypes.c_void_p()
-        ctx.check(ctx.L.seis_fd_lsrtm_create(ctx.h, nx, nz, len(self.shots), self._descs,
-                                             self._x0, ctypes.byref(o), ctypes.byref(h)))
+        if colmaps is None:
+            self._x0 = (ctypes.c_int * len(self.shots))(*[int(v) for v in x0])
+            ctx.check(ctx.L.seis_fd_lsrtm_create(ctx.h, nx, nz, len(self.shots), self._descs,
+                                                 self._x0, ctypes.byref(o), ctypes.byref(h)))
+        else:
+            flat = np.concatenate([np.asarray(c, np.int32) for c in colmaps])
+            self._map = (ctypes.c_int * len(flat))(*[int(v) for v in flat])
+            ctx.check(ctx.L.seis_fd_lsrtm_create_mapped(ctx.h, nx, nz, len(self.shots),
+                                                        self._descs, self._map, ctypes.byref(o),
+                                                        ctypes.byref(h)))
         self.h = h
+
+    # phases of one iteration on device buffers (pointers as integers), for
+    # solvers spread over several devices; see include/seis_fd.h
+    def phase_reset(self, d_s: int, d_rr: int):
+        self.ctx.check(self.ctx.L.seis_fd_lsrtm_phase_reset(self.h, d_s, d_rr))
+
+    def phase_forward(self, d_qq: int):
+        self.ctx.check(self.ctx.L.seis_fd_lsrtm_phase_forward(self.h, d_qq))
+
+    def phase_update(self, d_qq: int, d_s: int, d_rr: int):
+        self.ctx.check(self.ctx.L.seis_fd_lsrtm_phase_update(self.h, d_qq, d_s, d_rr))
+
+    def phase_direction(self, d_s: int, first: bool):
+        self.ctx.check(self.ctx.L.seis_fd_lsrtm_phase_direction(self.h, d_s, 1 if first else 0))
 
     def set_background(self, v0: np.ndarray, wav: np.ndarray):
         v = np.ascontiguousarray(v0, np.float32)

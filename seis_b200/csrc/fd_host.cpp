@@ -1387,25 +1387,96 @@ int seis_fd_lsrtm_set_data(seis_fd_lsrtm *L, int shot, const float *h_d) {
   return sync(ctx);
 }
 
-int seis_fd_lsrtm_reset(seis_fd_lsrtm *L, double *h_rr) {
-  if (!L) return SEIS_ERR_ARG;
+// ---- the phases of a CGLS iteration.  Each leaves this solver's partial
+// sums in the caller's device buffers; the next phase reads them summed (over
+// the ranks of a solver spread across devices, or as they are on one).
+
+// m = 0, r = d, s = L^T r, rr = |r|^2
+int seis_fd_lsrtm_phase_reset(seis_fd_lsrtm *L, float *d_s, double *d_rr) {
+  if (!L || !d_s || !d_rr) return SEIS_ERR_ARG;
   seis_fd_ctx *ctx = L->ctx;
   int rc = begin(ctx);
   if (rc) return rc;
-  size_t nm = (size_t)L->nx * L->nz;
+  const size_t nm = (size_t)L->nx * L->nz;
   CK(cudaMemsetAsync(L->m, 0, sizeof(float) * nm, ctx->stream));
   CK(cudaMemcpyAsync(L->r, L->dobs, sizeof(float) * L->ndata, cudaMemcpyDeviceToDevice,
                      ctx->stream));
-  rc = lsrtm_adjoint(*L);  // s = L^T r
+  rc = data_dot(*L, false, false, d_rr);
+  if (!rc) rc = lsrtm_adjoint(*L);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(L->p, L->s, sizeof(float) * nm, cudaMemcpyDeviceToDevice, ctx->stream));
-  CK(launch_dot(L->s, L->s, nm, ctx->d_partial, L->sc + 0, 0, ctx->stream));  // gamma
+  if (d_s != L->s)
+    CK(cudaMemcpyAsync(d_s, L->s, sizeof(float) * nm, cudaMemcpyDeviceToDevice, ctx->stream));
+  L->ready = true;
+  return SEIS_OK;
+}
+
+// q = L p, qq = |q|^2
+int seis_fd_lsrtm_phase_forward(seis_fd_lsrtm *L, double *d_qq) {
+  if (!L || !d_qq) return SEIS_ERR_ARG;
+  int rc = begin(L->ctx);
+  if (rc) return rc;
+  if (!L->ready) return fail(L->ctx, SEIS_ERR_STATE, "lsrtm: reset first");
+  rc = lsrtm_forward(*L);
+  return rc ? rc : data_dot(*L, true, true, d_qq);
+}
+
+// alpha = gamma / qq, m += alpha p, r -= alpha q, rr = |r|^2, s = L^T r
+int seis_fd_lsrtm_phase_update(seis_fd_lsrtm *L, const double *d_qq, float *d_s, double *d_rr) {
+  if (!L || !d_qq || !d_s || !d_rr) return SEIS_ERR_ARG;
+  seis_fd_ctx *ctx = L->ctx;
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (!L->ready) return fail(ctx, SEIS_ERR_STATE, "lsrtm: reset first");
+  const size_t nm = (size_t)L->nx * L->nz;
+  double *gamma = L->sc + 0, *alpha = L->sc + 2;
+  CK(launch_ratio(gamma, d_qq, alpha, ctx->stream));
+  CK(launch_axpby_dev(L->m, L->p, alpha, 1.0, nullptr, 1.0, nm, ctx->stream));
+  for (int k = 0; k < L->nshot; k++)
+    CK(launch_axpby_dev(L->r + L->doff[k], L->born.p->sd[k].rec, alpha, -1.0, nullptr, 1.0,
+                        (size_t)L->shots[k].nx * L->nt, ctx->stream));
+  ctx->launches += 2 + L->nshot;
+  rc = data_dot(*L, false, false, d_rr);
+  if (!rc) rc = lsrtm_adjoint(*L);
+  if (rc) return rc;
+  if (d_s != L->s)
+    CK(cudaMemcpyAsync(d_s, L->s, sizeof(float) * nm, cudaMemcpyDeviceToDevice, ctx->stream));
+  return SEIS_OK;
+}
+
+// s = the summed image, gamma' = |s|^2; first: gamma = gamma', p = s; else
+// beta = gamma' / gamma, gamma = gamma', p = s + beta p
+int seis_fd_lsrtm_phase_direction(seis_fd_lsrtm *L, const float *d_s, int first) {
+  if (!L || !d_s) return SEIS_ERR_ARG;
+  seis_fd_ctx *ctx = L->ctx;
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (!L->ready) return fail(ctx, SEIS_ERR_STATE, "lsrtm: reset first");
+  const size_t nm = (size_t)L->nx * L->nz;
+  double *gamma = L->sc + 0, *gnew = L->sc + 3, *beta = L->sc + 4;
+  if (d_s != L->s)
+    CK(cudaMemcpyAsync(L->s, d_s, sizeof(float) * nm, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(launch_dot(L->s, L->s, nm, ctx->d_partial, gnew, 0, ctx->stream));
   ctx->launches += 2;
-  rc = data_dot(*L, false, false, L->rr);  // |r|^2
+  if (first) {
+    CK(cudaMemcpyAsync(gamma, gnew, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(L->p, L->s, sizeof(float) * nm, cudaMemcpyDeviceToDevice, ctx->stream));
+    return SEIS_OK;
+  }
+  CK(launch_ratio(gnew, gamma, beta, ctx->stream));
+  CK(cudaMemcpyAsync(gamma, gnew, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(launch_axpby_dev(L->p, L->s, nullptr, 1.0, beta, 1.0, nm, ctx->stream));
+  ctx->launches += 2;
+  return SEIS_OK;
+}
+
+int seis_fd_lsrtm_reset(seis_fd_lsrtm *L, double *h_rr) {
+  if (!L) return SEIS_ERR_ARG;
+  seis_fd_ctx *ctx = L->ctx;
+  int rc = seis_fd_lsrtm_phase_reset(L, L->s, L->rr);
+  if (!rc) rc = seis_fd_lsrtm_phase_direction(L, L->s, 1);
   if (rc) return rc;
   if (h_rr)
     CK(cudaMemcpyAsync(h_rr, L->rr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  L->ready = true;
   return sync(ctx);
 }
 
@@ -1416,27 +1487,11 @@ int seis_fd_lsrtm_iterate(seis_fd_lsrtm *L, int niter, double *h_rr) {
   if (rc) return rc;
   if (!L->ready) return fail(ctx, SEIS_ERR_STATE, "lsrtm: call seis_fd_lsrtm_reset first");
   if (niter < 1 || niter > L->rr_cap) return fail(ctx, SEIS_ERR_ARG, "niter=%d", niter);
-  size_t nm = (size_t)L->nx * L->nz;
-  double *gamma = L->sc + 0, *qq = L->sc + 1, *alpha = L->sc + 2, *gnew = L->sc + 3,
-         *beta = L->sc + 4;
+  double *qq = L->sc + 1;
   for (int it = 0; it < niter && !rc; it++) {
-    rc = lsrtm_forward(*L);                                        // q = L p
-    if (!rc) rc = data_dot(*L, true, true, qq);                    // |q|^2
-    if (rc) break;
-    CK(launch_ratio(gamma, qq, alpha, ctx->stream));               // alpha = gamma / |q|^2
-    CK(launch_axpby_dev(L->m, L->p, alpha, 1.0, nullptr, 1.0, nm, ctx->stream));  // m += a p
-    for (int k = 0; k < L->nshot; k++)                              // r -= a q
-      CK(launch_axpby_dev(L->r + L->doff[k], L->born.p->sd[k].rec, alpha, -1.0, nullptr, 1.0,
-                          (size_t)L->shots[k].nx * L->nt, ctx->stream));
-    ctx->launches += 2 + L->nshot;
-    rc = data_dot(*L, false, false, L->rr + it);                   // |r|^2
-    if (!rc) rc = lsrtm_adjoint(*L);                               // s = L^T r
-    if (rc) break;
-    CK(launch_dot(L->s, L->s, nm, ctx->d_partial, gnew, 0, ctx->stream));  // |s|^2
-    CK(launch_ratio(gnew, gamma, beta, ctx->stream));              // beta = gnew / gamma
-    CK(cudaMemcpyAsync(gamma, gnew, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-    CK(launch_axpby_dev(L->p, L->s, nullptr, 1.0, beta, 1.0, nm, ctx->stream));  // p = s + b p
-    ctx->launches += 5;
+    rc = seis_fd_lsrtm_phase_forward(L, qq);
+    if (!rc) rc = seis_fd_lsrtm_phase_update(L, qq, L->s, L->rr + it);
+    if (!rc) rc = seis_fd_lsrtm_phase_direction(L, L->s, 0);
   }
   if (rc) return rc;
   if (h_rr)

@@ -73,6 +73,16 @@ class Survey:
         """Aperture sub-model of shot s (columns x0 .. x0+nx)."""
         return np.ascontiguousarray(a[self.x0[s]:self.x0[s] + self.shots[s].nx], np.float32)
 
+    def cell_updates_of(self, i: int) -> int:
+        s = self.shots[i]
+        return (s.nx + 2 * s.pml) * (s.nz + 2 * s.pml) * s.NT
+
+    def subset(self, idx) -> "Survey":
+        """The same survey restricted to shots idx."""
+        idx = list(idx)
+        return Survey(self.name, self.nx, self.nz, self.dx, self.dz, self.dt, self.nt, self.fr,
+                      self.vel, self.vel0, [self.shots[i] for i in idx], [self.x0[i] for i in idx])
+
     def cell_updates(self, fields: int = 1) -> int:
         return sum((s.nx + 2 * s.pml) * (s.nz + 2 * s.pml) * s.NT for s in self.shots) * fields
 

@@ -94,3 +94,24 @@ def test_vector_ops_match_opern(ctx):
         vec_axpby(ctx, tb.data_ptr(), ta.data_ptr(), 0.3, -1.7, n)
         want_y = (0.3 * a.astype(np.float64) - 1.7 * b.astype(np.float64)).astype(np.float32)
         assert np.array_equal(tb.cpu().numpy(), want_y)
+
+
+def test_phase_loop_reproduces_iterate(ctx):
+    """The sharded CG loop on one device (nothing to sum) gives the same
+    iterates as seis_fd_lsrtm_iterate, bit for bit."""
+    from seis_b200.shards import DeviceEngine, ShardedCGLS
+    sv = survey(seed=6)
+    nx, nz, shots, x0, wav, v0, _, dobs = sv
+    with Lsrtm(ctx, nx, nz, shots, x0) as ls:
+        ls.set_background(v0, wav)
+        for k, d in enumerate(dobs):
+            ls.set_data(k, d)
+        rr0 = ls.reset()
+        h1 = ls.iterate(3)
+        m1 = ls.model()
+        cg = ShardedCGLS(DeviceEngine(ls), lambda b: None)
+        rr0b = cg.reset()
+        h2 = cg.iterate(3)
+        m2 = ls.model()
+    assert rr0 == rr0b
+    assert np.array_equal(h1, np.array(h2)) and np.array_equal(m1, m2)
