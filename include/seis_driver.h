@@ -71,6 +71,11 @@ int seis_driver_born(seis_driver *d, const float *h_dv);
  * [nx][nz]. */
 int seis_driver_rtm(seis_driver *d, int born_data, float *h_img);
 
+/* illum_MPI (inversion.cpp:207-290): source illumination of every shot over
+ * the v0file background, through swapModel into the global grid, written to
+ * wdir ILLUM<is>.dat and summed into h_ss [nx][nz]. */
+int seis_driver_illum(seis_driver *d, float *h_ss);
+
 /* Least-squares RTM by CGLS over all shots: L = Born on each aperture
  * sub-grid, L^T its exact adjoint scattered back through the transpose of the
  * sub-grid extraction; observed data from precsg<is>.dat or BORN<is>.dat

@@ -100,6 +100,16 @@ int seis_fd_born(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wa
 int seis_fd_rtm(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
                 const float *h_vel, const float *h_rec, float *h_img);
 
+/* illum (src/util/fd.cpp:275-339): h_ss[nx][nz] = sum over it > ndel of the
+ * blended source field squared, accumulated step by step in FP32 (the
+ * illumination of the reference's illum_MPI, inversion.cpp:207-290).
+ * shot->gz may be NULL (receivers play no part). */
+int seis_fd_illum(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
+                  const float *h_vel, float *h_ss);
+int seis_fd_illum_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
+                        const float *const *h_wav, const float *const *h_vel,
+                        float *const *h_ss);
+
 /* ---------------------------------------------------------- shot batches */
 /* A plan is a batch of shots resident on the device.  It replaces the
  * reference's MPI shot farm (masterRun + worker loops,
@@ -113,6 +123,8 @@ int seis_fd_rtm(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav
 #define SEIS_OP_RTM 2      /* adjoint, reference RTM (fd.cpp:592-719)       */
 #define SEIS_OP_BORN_ADJOINT 3 /* exact adjoint of SEIS_OP_BORN (no reference
                                   counterpart): gather -> image             */
+#define SEIS_OP_ILLUM 4    /* illum, source illumination (fd.cpp:275-339):
+                              wavelet, velocity -> image [nx][nz]           */
 
 #define SEIS_IN_VEL 0      /* [nx][nz] velocity of the shot's model         */
 #define SEIS_IN_DV 1       /* [nx][nz] velocity perturbation (SEIS_OP_BORN) */

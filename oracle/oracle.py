@@ -146,6 +146,20 @@ def modeling(shot, wav, vel, prec="f32", impl="oracle"):
     return rec
 
 
+def illum(shot, wav, vel, prec="f32", impl="oracle"):
+    """Source illumination [nx][nz] of ``illum`` (src/util/fd.cpp:275-339)."""
+    dt, (gz, wav, vel) = _prep(shot, prec, impl, wav, vel)
+    ss = np.zeros((shot.nx, shot.nz), dt)
+    if impl == "ref":
+        rc = ref_lib().ref_illum(*_common_args(shot, None), _ptr(wav), _ptr(vel), _ptr(ss))
+    else:
+        rc = getattr(oracle_lib(), f"orc_illum_{prec}")(*_common_args(shot, prec), _ptr(wav),
+                                                        _ptr(vel), _ptr(ss))
+    if rc != 0:
+        raise RuntimeError(f"oracle illum failed ({rc})")
+    return ss
+
+
 def born(shot, wav, vel, dv, prec="f32", impl="oracle"):
     """Scattered gather [nx][nt] of ``forward`` (src/util/fd.cpp:81-177)."""
     dt, (gz, wav, vel, dv) = _prep(shot, prec, impl, wav, vel, dv)

@@ -351,6 +351,36 @@ int F(orc_modeling)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz,
   return 0;
 }
 
+/* illum, src/util/fd.cpp:275-339: ss[nx][nz] = sum over it > ndel of the
+ * blended source field squared, accumulated in REAL step by step. */
+int F(orc_illum)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml, int sx,
+                 int sz, const REAL *wav, const REAL *vel, REAL *ss)
+{
+  F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  F(coefs_t) c;
+  F(coefs_init)(g, vel, &c, 0);
+  size_t n = (size_t)g->NX * g->NZ;
+  REAL *u0 = F(zalloc)(n), *u1 = F(zalloc)(n), *u2 = F(zalloc)(n);
+  int sxp = sx + pml, szp = sz + pml, NT = nt + ndel;
+  for (size_t i = 0; i < (size_t)nx * nz; i++) ss[i] = KR(0);
+  for (int it = 0; it < NT; it++) {
+    F(twoway)(g, &c, u1, u0, u2);
+    if (it >= 1) AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+    F(absorb)(g, &c, u2, u1, u0);
+    if (it > ndel)  /* fd.cpp:318 */
+      for (int ix = 0; ix < nx; ix++)
+        for (int iz = 0; iz < nz; iz++) {
+          REAL u = AT(u2, ix + pml, iz + pml);
+          ss[(size_t)ix * nz + iz] += u * u;
+        }
+    REAL *t = u0; u0 = u1; u1 = u2; u2 = t;
+  }
+  free(u0); free(u1); free(u2);
+  F(coefs_free)(&c);
+  return 0;
+}
+
 /* forward (Born), src/util/fd.cpp:81-177.  Scattering source
  * vt2 lap vel3 dv with lap = (u2 + u0 - 2 u1)/dt^2 of the blended background. */
 int F(orc_born)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml, int sx,

@@ -105,6 +105,23 @@ int ref_modeling(float dt, float dx, float dz, int nt, int ndel, int nx, int nz,
   return 0;
 }
 
+/* illum (src/util/fd.cpp:275-339): ss_out [nx][nz] */
+int ref_illum(float dt, float dx, float dz, int nt, int ndel, int nx, int nz, int pml, int sx,
+              int sz, const float *wav, const float *vel, float *ss_out) {
+  QuietCout q(g_verbose);
+  try {
+    float **v = to2d(vel, nz, nx);
+    float **ss = illum(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, const_cast<float *>(wav), v);
+    from2d(ss_out, ss, nz, nx);
+    MyAlloc<float>::free(ss);
+    MyAlloc<float>::free(v);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return -1;
+  }
+  return 0;
+}
+
 /* forward, Born modeling (src/util/fd.cpp:81-177): rec_out [nx][nt] */
 int ref_born(float dt, float dx, float dz, int nt, int ndel, int nx, int nz,
              int pml, int sx, int sz, const int *gz, const float *wav,

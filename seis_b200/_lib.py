@@ -118,6 +118,8 @@ def lib():
         L.seis_fd_rtm_batch.argtypes = [P, I, SD, PP, PP, PP, PP]
         L.seis_fd_born.argtypes = [P, SD, P, P, P, P]
         L.seis_fd_rtm.argtypes = [P, SD, P, P, P, P]
+        L.seis_fd_illum.argtypes = [P, SD, P, P, P]
+        L.seis_fd_illum_batch.argtypes = [P, I, SD, PP, PP, PP]
         L.seis_fd_vec_dot.argtypes = [P, P, P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)]
         L.seis_fd_vec_axpby.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double,
                                         ctypes.c_size_t]
@@ -207,7 +209,7 @@ def validate_shot(shot: "Shot") -> str:
     return "" if rc == SEIS_OK else (buf.value.decode() or f"error {rc}")
 
 
-OP_MODELING, OP_BORN, OP_RTM, OP_BORN_ADJOINT = 0, 1, 2, 3
+OP_MODELING, OP_BORN, OP_RTM, OP_BORN_ADJOINT, OP_ILLUM = 0, 1, 2, 3, 4
 SNAP_F32, SNAP_BF16, SNAP_F16 = 1, 2, 3
 IN_VEL, IN_DV, IN_WAVELET, IN_GATHER = 0, 1, 2, 3
 OUT_GATHER, OUT_IMAGE = 0, 1
@@ -309,13 +311,15 @@ def batch(ctx: Context, op: int, shots, wavs, vels, third=None):
     descs = shot_array(shots)
     wavs = [np.ascontiguousarray(w, np.float32) for w in wavs]
     vels = [np.ascontiguousarray(v, np.float32) for v in vels]
-    if op == OP_RTM:
+    if op in (OP_RTM, OP_ILLUM):
         outs = [np.zeros((s.nx, s.nz), np.float32) for s in shots]
     else:
         outs = [np.zeros((s.nx, s.nt), np.float32) for s in shots]
     pw, pv, po = _ptr_list(wavs), _ptr_list(vels), _ptr_list(outs)
     n = len(shots)
-    if op == OP_MODELING:
+    if op == OP_ILLUM:
+        rc = ctx.L.seis_fd_illum_batch(ctx.h, n, descs, pw, pv, po)
+    elif op == OP_MODELING:
         rc = ctx.L.seis_fd_modeling_batch(ctx.h, n, descs, pw, pv, po)
     else:
         thirds = [np.ascontiguousarray(t, np.float32) for t in third]

@@ -581,6 +581,50 @@ int seis_driver_rtm(seis_driver *d, int born_data, float *h_img) {
   });
 }
 
+int seis_driver_illum(seis_driver *d, float *h_ss) {
+  if (!d || !h_ss) return SEIS_ERR_ARG;
+  const seis_params &p = d->p;
+  int rc = SEIS_OK;
+  const std::vector<float> v0 = load_model(d, p.v0file, &rc);
+  if (rc) return rc;
+  const size_t nm = (size_t)p.nx * p.nz;
+  std::memset(h_ss, 0, sizeof(float) * nm);
+  const std::vector<float> wav = wavelet(p);
+  return in_batches(d, 0, p.ns, [&](int s0, int n) {
+    std::vector<ShotGeom> g((size_t)n);
+    std::vector<std::vector<float>> vel((size_t)n), ss((size_t)n);
+    std::vector<seis_shot_desc> desc;
+    std::vector<const float *> pw, pv;
+    std::vector<float *> po;
+    for (int k = 0; k < n; k++) {
+      int r = shot_geom(*d, s0 + k, &g[k]);
+      if (r) return dfail(d, r, "shot %d geometry", s0 + k);
+      vel[k] = sub_grid(v0.data(), p, g[k]);
+      ss[k].assign((size_t)g[k].nx * p.nz, 0.0f);
+    }
+    for (int k = 0; k < n; k++) {
+      desc.push_back(g[k].desc);
+      pw.push_back(wav.data());
+      pv.push_back(vel[k].data());
+      po.push_back(ss[k].data());
+    }
+    int r = seis_fd_illum_batch(d->ctx, n, desc.data(), pw.data(), pv.data(), po.data());
+    if (r) return dfail(d, r, "illum: %s", seis_fd_last_error(d->ctx));
+    std::vector<float> tmp(nm);
+    for (int k = 0; k < n; k++) {  // illum_MPI, inversion.cpp:257-260, :271-282
+      const int is = s0 + k;
+      r = seis_geom_swap_model(ss[k].data(), tmp.data(), g[k].fx, p.velfx, p.nz, g[k].nx, p.nz,
+                               p.nx, p.dx, 0);
+      if (r) return dfail(d, r, "shot %d illumination scatter", is);
+      const std::string name = std::string(p.wdir) + "ILLUM" + std::to_string(is) + ".dat";
+      if (!write_file(name, tmp.data(), nm))
+        return dfail(d, SEIS_ERR_ARG, "cannot write %s", name.c_str());
+      for (size_t i = 0; i < nm; i++) h_ss[i] = tmp[i] + h_ss[i];
+    }
+    return SEIS_OK;
+  });
+}
+
 int seis_driver_lsrtm(seis_driver *d, int born_data, int niter, const seis_lsrtm_opts *opts,
                       float *h_img, double *h_rr) {
   if (!d || !h_img || niter < 0) return SEIS_ERR_ARG;

@@ -382,8 +382,14 @@ __global__ void __launch_bounds__(A_NT_P, 2) adj_pad_kernel(const ShotDev *__res
 
   // ringsT of the pad cells of tile + 5: (1 - w) L1 through the one-way
   // update's u3, cur and prev terms, (1 - w) L2 through its prev terms and
-  // (minus) its u3 terms
+  // (minus) its u3 terms.  Terms that land on the same cell are summed before
+  // the fixed-point add; cells at least 2 inside both windows skip the
+  // window test.
   constexpr int R5C = TX + 10, R5R = TZ + 10;
+  auto addu = [&](long long *base, int ncol, int x0w, int z0w, int nrow, int ix, int iz, float v) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(&base[(ix - x0w) * nrow + (iz - z0w)]),
+              (unsigned long long)fix(v));
+  };
   for (int i = tid; i < R5C * R5R; i += A_NT_P) {
     const int cx = x0 - 5 + i / R5R, cz = z0 - 5 + i % R5R;
     if (cx < 0 || cx >= NX || cz < 0 || cz >= NZ) continue;
@@ -393,29 +399,54 @@ __global__ void __launch_bounds__(A_NT_P, 2) adj_pad_kernel(const ShotDev *__res
     const float w = pad_weight(g, pp);
     RingCoef rc = ring_coef(g, V, cx, cz, pp);
     const float n1 = (1.0f - w) * L1(cx, cz), n2 = near1 ? (1.0f - w) * L2(cx, cz) : 0.0f;
+    // deep: every target (distance <= 1) inside the tile (ACC) and tile + 4 (MU1)
+    const bool deep = cx >= x0 + 1 && cx <= x0 + TX - 2 && cz >= z0 + 1 && cz <= z0 + TZ - 2;
     if (rc.corner) {
-      MU1.add(cx, cz + rc.nz_, rc.cz * n1);
-      MU1.add(cx + rc.nx_, cz, rc.cx * n1);
-      ACC.add(cx, cz, rc.bK * n1);
-      if (near1) {
-        ACC.add(cx, cz + rc.nz_, -(rc.cz * n2));
-        ACC.add(cx + rc.nx_, cz, -(rc.cx * n2));
+      if (deep) {
+        addu(sMU1, MU_C, x0 - 4, z0 - 4, MU_R, cx, cz + rc.nz_, rc.cz * n1);
+        addu(sMU1, MU_C, x0 - 4, z0 - 4, MU_R, cx + rc.nx_, cz, rc.cx * n1);
+        addu(sACC, TX, x0, z0, TZ, cx, cz, rc.bK * n1);
+        addu(sACC, TX, x0, z0, TZ, cx, cz + rc.nz_, -(rc.cz * n2));
+        addu(sACC, TX, x0, z0, TZ, cx + rc.nx_, cz, -(rc.cx * n2));
+      } else {
+        MU1.add(cx, cz + rc.nz_, rc.cz * n1);
+        MU1.add(cx + rc.nx_, cz, rc.cx * n1);
+        ACC.add(cx, cz, rc.bK * n1);
+        if (near1) {
+          ACC.add(cx, cz + rc.nz_, -(rc.cz * n2));
+          ACC.add(cx + rc.nx_, cz, -(rc.cx * n2));
+        }
       }
     } else {
       const int ix_i = cx + rc.nx_, iz_i = cz + rc.nz_;
-      MU1.add(ix_i, iz_i, rc.au3i * n1);
-      MU1.add(ix_i + rc.tx_, iz_i + rc.tz_, rc.au3t * n1);
-      MU1.add(ix_i - rc.tx_, iz_i - rc.tz_, rc.au3t * n1);
-      ACC.add(cx, cz, rc.bK * n1);
-      ACC.add(ix_i, iz_i, rc.bi * n1);
-      if (near1) {
-        ACC.add(ix_i, iz_i, -(rc.au3i * n2));
-        ACC.add(ix_i + rc.tx_, iz_i + rc.tz_, -(rc.au3t * n2));
-        ACC.add(ix_i - rc.tx_, iz_i - rc.tz_, -(rc.au3t * n2));
-        ACC.add(cx, cz, rc.gK * n2);
-        ACC.add(ix_i, iz_i, rc.gi * n2);
-        ACC.add(cx + rc.tx_, cz + rc.tz_, rc.gt * n2);
-        ACC.add(cx - rc.tx_, cz - rc.tz_, rc.gt * n2);
+      const float at = rc.au3t * n1, mt = -(rc.au3t * n2), gt = rc.gt * n2;
+      const float self = rc.bK * n1 + rc.gK * n2;
+      const float inner = rc.bi * n1 - rc.au3i * n2 + rc.gi * n2;
+      if (deep) {
+        addu(sMU1, MU_C, x0 - 4, z0 - 4, MU_R, ix_i, iz_i, rc.au3i * n1);
+        addu(sMU1, MU_C, x0 - 4, z0 - 4, MU_R, ix_i + rc.tx_, iz_i + rc.tz_, at);
+        addu(sMU1, MU_C, x0 - 4, z0 - 4, MU_R, ix_i - rc.tx_, iz_i - rc.tz_, at);
+        addu(sACC, TX, x0, z0, TZ, cx, cz, self);
+        addu(sACC, TX, x0, z0, TZ, ix_i, iz_i, inner);
+        addu(sACC, TX, x0, z0, TZ, ix_i + rc.tx_, iz_i + rc.tz_, mt);
+        addu(sACC, TX, x0, z0, TZ, ix_i - rc.tx_, iz_i - rc.tz_, mt);
+        addu(sACC, TX, x0, z0, TZ, cx + rc.tx_, cz + rc.tz_, gt);
+        addu(sACC, TX, x0, z0, TZ, cx - rc.tx_, cz - rc.tz_, gt);
+      } else {
+        MU1.add(ix_i, iz_i, rc.au3i * n1);
+        MU1.add(ix_i + rc.tx_, iz_i + rc.tz_, at);
+        MU1.add(ix_i - rc.tx_, iz_i - rc.tz_, at);
+        if (near1) {
+          ACC.add(cx, cz, self);
+          ACC.add(ix_i, iz_i, inner);
+          ACC.add(ix_i + rc.tx_, iz_i + rc.tz_, mt);
+          ACC.add(ix_i - rc.tx_, iz_i - rc.tz_, mt);
+          ACC.add(cx + rc.tx_, cz + rc.tz_, gt);
+          ACC.add(cx - rc.tx_, cz - rc.tz_, gt);
+        } else {
+          ACC.add(cx, cz, rc.bK * n1);
+          ACC.add(ix_i, iz_i, rc.bi * n1);
+        }
       }
     }
   }

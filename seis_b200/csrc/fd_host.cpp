@@ -50,7 +50,7 @@ struct seis_fd_plan {
 
 namespace {
 
-enum Op { OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2, OP_BORN_ADJ = 3 };
+enum Op { OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2, OP_BORN_ADJ = 3, OP_ILLUM = 4 };
 
 int fail(seis_fd_ctx *ctx, int code, const char *fmt, ...) {
   char buf[512];
@@ -394,7 +394,9 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (rc == SEIS_OK) rc = p->alloc(&rec, (size_t)d.nt * d.nx);
     if (rc == SEIS_OK) rc = p->alloc(&gzd, (size_t)d.nx);
     if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&g.strips, (size_t)d.nt * g.strip_len);
-    if (rc == SEIS_OK && (op == OP_RTM || op == OP_BORN_ADJ)) rc = p->alloc(&g.img, (size_t)d.nx * d.nz);
+    if (rc == SEIS_OK && (op == OP_RTM || op == OP_BORN_ADJ || op == OP_ILLUM))
+      rc = p->alloc(&g.img, (size_t)d.nx * d.nz);
+    if (op == OP_ILLUM) g.illum = g.img;
     if (rc == SEIS_OK && op == OP_BORN_ADJ) rc = p->alloc(&g.grad, (size_t)d.nx * d.nz);
     g.ntz = (g.NZ + TZ - 1) / TZ;
     if (rc == SEIS_OK) {
@@ -412,7 +414,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     // padded cell-updates of one run: modeling NT, Born 2 NT, reference RTM
     // NT + 2 nt, exact adjoint NT (source pass) + NT + 1 (reverse pass)
     for (const ShotDev &g : p->sd) {
-      int64_t per = op == OP_MODEL ? g.NT
+      int64_t per = (op == OP_MODEL || op == OP_ILLUM) ? g.NT
                   : op == OP_BORN  ? 2LL * g.NT
                   : op == OP_RTM   ? g.NT + 2LL * g.nt
                                    : 2LL * g.NT + 1;
@@ -559,7 +561,8 @@ int run_forward(Plan &p, int mode) {
     a.rot_b = it;
     a.src_k = it >= 1 ? it - 1 : -1;
     int itp = it - p.ndel;
-    a.rec_k = (p.op != OP_RTM && p.op != OP_BORN_ADJ && itp >= 0) ? itp : -1;
+    a.rec_k = (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_ILLUM && itp >= 0) ? itp : -1;
+    a.illum_on = p.op == OP_ILLUM && it > p.ndel;  // fd.cpp:318
     a.strip_k = (p.op == OP_RTM && itp >= 0) ? itp : -1;
     a.snap_k = p.op == OP_BORN_ADJ ? snap_slot(it, p.NT - 1, p.snap_every) : -1;
     int rc = step(p, mode, a);
@@ -653,6 +656,7 @@ int enqueue_operator(Plan &p) {
       rc = ensure_snapshots(p);
       if (!rc && !p.snaps_valid) rc = source_pass(p);
       return rc ? rc : run_adjoint(p);
+    case OP_ILLUM: return run_forward(p, MODE_MODEL);
   }
   return fail(p.ctx, SEIS_ERR_NOTSUP, "unknown operator %d", p.op);
 }
@@ -828,7 +832,7 @@ int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_des
   if (rc) return rc;
   if (!out) return fail(ctx, SEIS_ERR_ARG, "out is null");
   *out = nullptr;
-  if (op < SEIS_OP_MODELING || op > SEIS_OP_BORN_ADJOINT) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
+  if (op < SEIS_OP_MODELING || op > SEIS_OP_ILLUM) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
   Plan *p = nullptr;
   rc = plan_create(ctx, op, nshot, shots, &p);
   if (rc) return rc;
@@ -915,11 +919,11 @@ int seis_fd_plan_get(seis_fd_plan *plan, int shot, int what, float *h_dst) {
   if (shot < 0 || shot >= p.nshot) return fail(ctx, SEIS_ERR_ARG, "shot=%d of %d", shot, p.nshot);
   if (!h_dst) return fail(ctx, SEIS_ERR_ARG, "null destination");
   if (what == SEIS_OUT_GATHER) {
-    if (p.op == OP_RTM || p.op == OP_BORN_ADJ)
+    if (p.op == OP_RTM || p.op == OP_BORN_ADJ || p.op == OP_ILLUM)
       return fail(ctx, SEIS_ERR_NOTSUP, "this plan outputs images");
     rc = download_gather(p, shot, h_dst);
   } else if (what == SEIS_OUT_IMAGE) {
-    if (p.op != OP_RTM && p.op != OP_BORN_ADJ)
+    if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_ILLUM)
       return fail(ctx, SEIS_ERR_NOTSUP, "plan outputs gathers");
     const seis_shot_desc &d = p.desc[shot];
     CK(cudaMemcpyAsync(h_dst, p.sd[shot].img, sizeof(float) * d.nx * d.nz,
@@ -1075,6 +1079,27 @@ int seis_fd_born(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wa
                  const float *h_vel, const float *h_dv, float *h_rec) {
   return run_batch(ctx, OP_BORN, 1, shot, &h_wav, SEIS_IN_WAVELET, &h_vel, SEIS_IN_VEL, &h_dv,
                    SEIS_IN_DV, &h_rec, SEIS_OUT_GATHER);
+}
+
+int seis_fd_illum(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
+                  const float *h_vel, float *h_ss) {
+  return seis_fd_illum_batch(ctx, 1, shot, &h_wav, &h_vel, &h_ss);
+}
+
+int seis_fd_illum_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
+                        const float *const *h_wav, const float *const *h_vel,
+                        float *const *h_ss) {
+  // the receivers play no part: a shot without them gets surface rows
+  if (!shots || nshot < 1) return begin(ctx) ? SEIS_ERR_ARG : fail(ctx, SEIS_ERR_ARG, "no shots");
+  std::vector<seis_shot_desc> d(shots, shots + nshot);
+  std::vector<std::vector<int>> zero((size_t)nshot);
+  for (int s = 0; s < nshot; s++)
+    if (!d[s].gz) {
+      zero[s].assign((size_t)std::max(d[s].nx, 0), 0);
+      d[s].gz = zero[s].data();
+    }
+  return run_batch(ctx, OP_ILLUM, nshot, d.data(), h_wav, SEIS_IN_WAVELET, h_vel, SEIS_IN_VEL,
+                   nullptr, -1, h_ss, SEIS_OUT_IMAGE);
 }
 
 int seis_fd_rtm(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,

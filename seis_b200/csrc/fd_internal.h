@@ -93,6 +93,7 @@ struct ShotDev {
   // (field A or the receiver field; Born: [1] = scattered field), read by the
   // absorbing-boundary kernel
   float *u3s[2];
+  float *illum;          // source illumination [nx][nz] (illumination plans)
 };
 enum SnapType : int { SNAP_NONE = 0, SNAP_F32 = 1, SNAP_BF16 = 2, SNAP_F16 = 3 };
 static_assert(sizeof(ShotDev) % sizeof(int) == 0 && sizeof(ShotDev) <= 256 * sizeof(int),
@@ -108,6 +109,7 @@ struct StepArgs {
   int nshots = 0;
   int snap_k = -1;   // snapshot index written (forward) or imaged (adjoint)
   float img_w = 0.f; // adjoint: weight of the imaging term (snapshot interval)
+  int illum_on = 0;  // add the square of every model cell's new value to g.illum
   const PadChunk *chunks = nullptr;  // pad cells of the batch (absorbing kernel)
   int nchunks = 0;
 };

@@ -430,6 +430,10 @@ __global__ void __launch_bounds__(NT_T, 2) tile_kernel(const ShotDev *__restrict
         if (!BORN && record && iz == gzq[j])
           g.rec[(size_t)aa.rec_k * g.nx + (cxj - g.pml)] = out;
         if (MODE == MODE_MODEL && aa.strip_k >= 0) save_strips(g, aa.strip_k, cxj, iz, out);
+        if (MODE == MODE_MODEL && aa.illum_on) {  // illum, fd.cpp:317-319
+          float *ss = g.illum + (size_t)(cxj - g.pml) * g.nz + (iz - g.pml);
+          *ss = *ss + out * out;
+        }
         if (BORN || snap) {  // scattering source vt2 lap vel3 dv, fd.cpp:134-139
           float lap = (out + comp(prv[j], r) - 2.0f * comp(cen[j], r)) * g.idt2;
           lv[4 * j + r] = lap;

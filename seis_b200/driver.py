@@ -8,7 +8,7 @@ same files with the same rules, and ``modeling``, ``born``, ``rtm`` follow
 the same file names and raw float32 layouts; ``lsrtm`` is the CG solver the
 reference declares (``cgsolver_MPI``) but does not define.
 
-    python -m seis_b200.driver PARAM_FILE {modeling|born|rtm|lsrtm} [options]
+    python -m seis_b200.driver PARAM_FILE {modeling|born|rtm|lsrtm|illum} [options]
 """
 from __future__ import annotations
 
@@ -56,6 +56,7 @@ def _setup():
     L.seis_driver_modeling.argtypes = [_P, _P]
     L.seis_driver_born.argtypes = [_P, _P]
     L.seis_driver_rtm.argtypes = [_P, _I, _P]
+    L.seis_driver_illum.argtypes = [_P, _P]
     L.seis_driver_lsrtm.argtypes = [_P, _I, _I, ctypes.POINTER(LsrtmOptsC), _P, _P]
     L._driver_ready = True
     return L
@@ -130,6 +131,12 @@ class Driver:
         self._run(self.L.seis_driver_rtm(self.h, 1 if born_data else 0, img.ctypes.data), "rtm")
         return img
 
+    def illum(self) -> np.ndarray:
+        """Source illumination [nx][nz] of all shots (illum_MPI)."""
+        ss = np.zeros((self.params.nx, self.params.nz), np.float32)
+        self._run(self.L.seis_driver_illum(self.h, ss.ctypes.data), "illum")
+        return ss
+
     def lsrtm(self, niter: int, born_data: bool = False, snap_every: int = 1,
               snap_dtype: int = SNAP_BF16, exact: bool = False):
         """(model [nx][nz], [|d|^2, |r|^2 per iteration]) of CGLS over all shots."""
@@ -161,7 +168,7 @@ class Driver:
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m seis_b200.driver", description=__doc__.split("\n")[0])
     ap.add_argument("param_file")
-    ap.add_argument("op", choices=["modeling", "born", "rtm", "lsrtm"])
+    ap.add_argument("op", choices=["modeling", "born", "rtm", "lsrtm", "illum"])
     ap.add_argument("--dv", help="perturbation [nx][nz] float32 file (born)")
     ap.add_argument("--born-data", action="store_true", help="rtm/lsrtm from BORN<is>.dat")
     ap.add_argument("--niter", type=int, default=None, help="lsrtm iterations (default maxiter)")
@@ -178,6 +185,8 @@ def main(argv=None):
         else:
             if a.op == "rtm":
                 img = d.rtm(a.born_data)
+            elif a.op == "illum":
+                img = d.illum()
             else:
                 img, rr = d.lsrtm(a.niter if a.niter is not None else p.maxiter, a.born_data)
                 for i, r in enumerate(rr):

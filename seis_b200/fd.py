@@ -44,6 +44,18 @@ def modeling(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, ctx: Conte
     return rec
 
 
+def illum(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, wav, vel, ctx: Context = None):
+    """Source illumination ``ss[nx][nz]`` (reference ``illum``, src/util/fd.cpp:275-339)."""
+    ctx = ctx or default_context()
+    s = _shot(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, np.zeros(nx, np.int32))
+    wav = _f32(wav, (s.NT,))
+    vel = _f32(vel, (nx, nz))
+    ss = np.zeros((nx, nz), np.float32)
+    d = s.to_c()
+    ctx.check(ctx.L.seis_fd_illum(ctx.h, d, ptr(wav), ptr(vel), ptr(ss)))
+    return ss
+
+
 def forward(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, dv, ctx: Context = None):
     """Born gather ``rec[nx][nt]`` (reference ``forward``, src/util/fd.cpp:81-177)."""
     ctx = ctx or default_context()

@@ -160,3 +160,21 @@ def test_driver_lsrtm_matches_fp64_cgls(ctx, survey):
     err = rel_l2(m, m_ref)
     print("driver LSRTM model vs FP64 CGLS", err)
     assert err < 2e-3
+
+
+def test_driver_illum_matches_reference_pipeline(ctx, survey):
+    tmp, v, v0, shots = survey
+    ref = reference(shots, v)
+    wav = O.ricker(DT, FR, DELAY + DELAYCAL, NT + DELAYCAL, impl="ref")
+    with Driver(ctx, str(tmp / "param.txt"), batch=2) as d:
+        ss = d.illum()
+    want = np.zeros((NX, NZ), np.float32)
+    for is_ in range(len(shots)):
+        fx, nxs, sub, shot = shot_of(ref, is_, shots, v0)
+        sssub = O.illum(shot, wav, sub, impl="ref")
+        tmpimg = np.zeros((NX, NZ), np.float32)
+        ref.swapmodel(np.ascontiguousarray(sssub), tmpimg, fx, 0.0, add=False)
+        got = np.fromfile(tmp / "WDIR" / f"ILLUM{is_}.dat", np.float32).reshape(NX, NZ)
+        assert np.array_equal(got, tmpimg), f"shot {is_} illumination"
+        want = tmpimg + want
+    assert np.array_equal(ss, want)

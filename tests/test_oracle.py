@@ -62,3 +62,10 @@ def test_restatement_matches_reference_random():
     assert np.array_equal(O.modeling(s, wav, vel), rec)
     assert np.array_equal(O.born(s, wav, vel, dv), O.born(s, wav, vel, dv, impl="ref"))
     assert np.array_equal(O.rtm(s, wav, vel, rec), O.rtm(s, wav, vel, rec, impl="ref"))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("g", CASES, ids=golden_ids())
+def test_illum_restatement_matches_reference(g):
+    """illum (src/util/fd.cpp:275-339): the C restatement bit for bit."""
+    assert np.array_equal(O.illum(g.shot, g.wav, g.vel), O.illum(g.shot, g.wav, g.vel, impl="ref"))
