@@ -49,7 +49,7 @@ int seis_coords_read(const char *file, int ns, int ngmax, int *ng, float *sc, fl
 typedef struct seis_driver seis_driver;
 
 /* Reads the parameter and coordinate files; batch = shots per device batch
- * (0: all). */
+ * (0: all).  ctx may be NULL for the host-only steps (plane-wave preparation). */
 int seis_driver_create(seis_fd_ctx *ctx, const char *param_file, int batch, seis_driver **out);
 int seis_driver_destroy(seis_driver *d);
 const seis_params *seis_driver_params(const seis_driver *d);
@@ -75,6 +75,15 @@ int seis_driver_rtm(seis_driver *d, int born_data, float *h_img);
  * the v0file background, through swapModel into the global grid, written to
  * wdir ILLUM<is>.dat and summed into h_ss [nx][nz]. */
 int seis_driver_illum(seis_driver *d, float *h_ss);
+
+/* planeWavePrepare (inversion.cpp:808-912): for each of the np wavenumbers
+ * p = pmin + k dp, the phase-encoded areal source (every shot's wavelet
+ * rotated by p times its x through the 201-tap Hilbert filter, harmonic,
+ * InitInversion.cpp:141-150, added at its column) and the phase-encoded data
+ * (every trace of every precsg<is>.dat likewise, moved to its model column and
+ * summed), written to wdir PLANE_S_NEW<k>.dat ([nx][nt+delaycal]) and
+ * PLANE_R_NEW<k>.dat ([nx][nt]).  Requires planeTag. */
+int seis_driver_plane_prepare(seis_driver *d);
 
 /* Least-squares RTM by CGLS over all shots: L = Born on each aperture
  * sub-grid, L^T its exact adjoint scattered back through the transpose of the

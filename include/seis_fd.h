@@ -79,6 +79,11 @@ void *seis_fd_stream(const seis_fd_ctx *ctx);
 /* rickerWavelet (src/util/wavelet.cpp:7-18): out[n], (1-2 tmp t^2) exp(-tmp t^2)
  * with tmp = pi^2 fr^2 formed in double, t = (i - delay) dt.  No device. */
 int seis_fd_ricker(float dt, float fr, int delay, int n, float *out);
+/* Hilbert<float>(half).apply (src/filter/hilbert.h:22-70): out[n] = the
+ * (2 half + 1)-tap Hamming-tapered Hilbert FIR of in[n], convolved in full and
+ * cut to n.  Host only. */
+int seis_fd_hilbert(const float *in, float *out, int n, int half);
+
 /* Argument checks of one shot without touching a device: 0 or SEIS_ERR_ARG,
  * with the reason copied into msg[msg_len] when msg is not null. */
 int seis_fd_validate_shot(const seis_shot_desc *shot, char *msg, size_t msg_len);
@@ -110,6 +115,14 @@ int seis_fd_illum_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots
                         const float *const *h_wav, const float *const *h_vel,
                         float *const *h_ss);
 
+/* forwordPlane (src/util/fd.cpp:178-274): Born modeling with the areal
+ * source h_sou[nx][nt+ndel] injected at row shot->sz of every model column
+ * (a plane-wave or phase-encoded source, see seis_driver_plane_prepare) and
+ * receivers at rows shot->gz (the reference takes one row for all).
+ * shot->sx is not used.  h_rec[nx][nt]. */
+int seis_fd_born_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_sou,
+                       const float *h_vel, const float *h_dv, float *h_rec);
+
 /* ---------------------------------------------------------- shot batches */
 /* A plan is a batch of shots resident on the device.  It replaces the
  * reference's MPI shot farm (masterRun + worker loops,
@@ -125,11 +138,14 @@ int seis_fd_illum_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots
                                   counterpart): gather -> image             */
 #define SEIS_OP_ILLUM 4    /* illum, source illumination (fd.cpp:275-339):
                               wavelet, velocity -> image [nx][nz]           */
+#define SEIS_OP_BORN_PLANE 5 /* forwordPlane, Born with an areal source
+                                (fd.cpp:178-274): source, velocity, dv -> gather */
 
 #define SEIS_IN_VEL 0      /* [nx][nz] velocity of the shot's model         */
 #define SEIS_IN_DV 1       /* [nx][nz] velocity perturbation (SEIS_OP_BORN) */
 #define SEIS_IN_WAVELET 2  /* [nt+ndel] source wavelet                      */
 #define SEIS_IN_GATHER 3   /* [nx][nt] receiver data (SEIS_OP_RTM)          */
+#define SEIS_IN_SOURCE 4   /* [nx][nt+ndel] areal source at row sz (plane-wave ops) */
 #define SEIS_OUT_GATHER 0  /* [nx][nt] recorded gather                      */
 #define SEIS_OUT_IMAGE 1   /* [nx][nz] image                                */
 

@@ -146,6 +146,25 @@ def modeling(shot, wav, vel, prec="f32", impl="oracle"):
     return rec
 
 
+def born_plane(shot, sou, vel, dv, gz, prec="f32", impl="oracle"):
+    """Scattered gather [nx][nt] of ``forwordPlane`` (src/util/fd.cpp:178-274):
+    areal source sou [nx][nt+ndel] at row shot.sz, receivers at row gz."""
+    dt, (_, sou, vel, dv) = _prep(shot, prec, impl, sou, vel, dv)
+    rec = np.zeros((shot.nx, shot.nt), dt)
+    R = _real(prec) if impl != "ref" else ctypes.c_float
+    s = shot
+    args = [R(s.dt), R(s.dx), R(s.dz), _I(s.nt), _I(s.ndel), _I(s.nx), _I(s.nz), _I(s.pml),
+            _I(s.sz), _I(int(gz))]
+    if impl == "ref":
+        rc = ref_lib().ref_born_plane(*args, _ptr(sou), _ptr(vel), _ptr(dv), _ptr(rec))
+    else:
+        rc = getattr(oracle_lib(), f"orc_born_plane_{prec}")(*args, _ptr(sou), _ptr(vel), _ptr(dv),
+                                                             _ptr(rec))
+    if rc != 0:
+        raise RuntimeError(f"oracle born_plane failed ({rc})")
+    return rec
+
+
 def illum(shot, wav, vel, prec="f32", impl="oracle"):
     """Source illumination [nx][nz] of ``illum`` (src/util/fd.cpp:275-339)."""
     dt, (gz, wav, vel) = _prep(shot, prec, impl, wav, vel)
@@ -363,3 +382,23 @@ def ref_read_coords(path, ngmax):
     if L.ref_coords_read(path.encode(), ns, ngmax, _ptr(ng), _ptr(sc), _ptr(gc)) != 0:
         raise RuntimeError("reference Coords failed")
     return ns, ng, sc, gc
+
+
+def ref_plane_prepare(param_file):
+    """The reference's Inversion::planeWavePrepare on a parameter file's survey."""
+    L = ref_lib()
+    L.ref_plane_prepare.argtypes = [ctypes.c_char_p]
+    if L.ref_plane_prepare(str(param_file).encode()) != 0:
+        raise RuntimeError("reference planeWavePrepare failed")
+
+
+def ref_harmonic(x, kx, sx):
+    """The reference's harmonic() on one trace (InitInversion.cpp:141-150)."""
+    L = ref_lib()
+    L.ref_harmonic.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_float,
+                               ctypes.c_float]
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.zeros_like(x)
+    if L.ref_harmonic(_ptr(x), _ptr(out), len(x), kx, sx) != 0:
+        raise RuntimeError("reference harmonic failed")
+    return out

@@ -383,8 +383,12 @@ int F(orc_illum)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, in
 
 /* forward (Born), src/util/fd.cpp:81-177.  Scattering source
  * vt2 lap vel3 dv with lap = (u2 + u0 - 2 u1)/dt^2 of the blended background. */
-int F(orc_born)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml, int sx,
-                int sz, const int *gz, const REAL *wav, const REAL *vel, const REAL *dv, REAL *rec)
+/* Born core: a point source wav at (sx, sz), or (sou != NULL) the areal source
+ * of forwordPlane, sou[ix][it] injected at every model column of row sz
+ * (src/util/fd.cpp:221-225). */
+static int F(born_core)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml,
+                        int sx, int sz, const int *gz, const REAL *wav, const REAL *sou,
+                        const REAL *vel, const REAL *dv, REAL *rec)
 {
   F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
   const F(grid_t) *g = &gg;
@@ -399,7 +403,13 @@ int F(orc_born)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int
   int sxp = sx + pml, szp = sz + pml, NT = nt + ndel;
   for (int it = 0; it < NT; it++) {
     F(twoway)(g, &c, u1, u0, u2);
-    if (it >= 1) AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+    if (it >= 1) {
+      if (sou)
+        for (int ix = 0; ix < nx; ix++)
+          AT(u2, ix + pml, szp) += AT(c.vt2, ix + pml, szp) * sou[(size_t)ix * NT + (it - 1)];
+      else
+        AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+    }
     F(absorb)(g, &c, u2, u1, u0);
     F(twoway)(g, &c, b1, b0, b2);
     for (size_t i = 0; i < n; i++) {
@@ -415,6 +425,25 @@ int F(orc_born)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int
   free(u0); free(u1); free(u2); free(b0); free(b1); free(b2); free(dvp);
   F(coefs_free)(&c);
   return 0;
+}
+
+int F(orc_born)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml, int sx,
+                int sz, const int *gz, const REAL *wav, const REAL *vel, const REAL *dv, REAL *rec)
+{
+  return F(born_core)(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, NULL, vel, dv, rec);
+}
+
+/* forwordPlane, src/util/fd.cpp:178-274: Born with the areal source
+ * sou[nx][nt+ndel] at row sz and every receiver at row gz. */
+int F(orc_born_plane)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml,
+                      int sz, int gz, const REAL *sou, const REAL *vel, const REAL *dv, REAL *rec)
+{
+  int *g = (int *)malloc(sizeof(int) * (size_t)(nx > 0 ? nx : 1));
+  if (!g) return -1;
+  for (int ix = 0; ix < nx; ix++) g[ix] = gz;
+  int rc = F(born_core)(dt, dx, dz, nt, ndel, nx, nz, pml, 0, sz, g, NULL, sou, vel, dv, rec);
+  free(g);
+  return rc;
 }
 
 /* SaveAtBoundary, src/util/fd.cpp:1181-1225: the 4 outermost interior rows

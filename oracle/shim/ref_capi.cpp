@@ -105,6 +105,40 @@ int ref_modeling(float dt, float dx, float dz, int nt, int ndel, int nx, int nz,
   return 0;
 }
 
+/* forwordPlane (src/util/fd.cpp:178-274): sou [nx][nt+ndel], rec_out [nx][nt] */
+int ref_born_plane(float dt, float dx, float dz, int nt, int ndel, int nx, int nz, int pml,
+                   int sz, int gz, const float *sou, const float *vel, const float *dv,
+                   float *rec_out) {
+  QuietCout q(g_verbose);
+  try {
+    float **v = to2d(vel, nz, nx);
+    float **d = to2d(dv, nz, nx);
+    float **s = to2d(sou, nt + ndel, nx);
+    float **rec = forwordPlane(dt, dx, dz, nt, ndel, nx, nz, pml, sz, gz, v, s, d);
+    from2d(rec_out, rec, nt, nx);
+    MyAlloc<float>::free(rec);
+    MyAlloc<float>::free(v);
+    MyAlloc<float>::free(d);
+    MyAlloc<float>::free(s);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return -1;
+  }
+  return 0;
+}
+
+/* harmonic (src/util/InitInversion.cpp:141-150): phase rotation of a trace by
+ * kx x through the 201-tap Hilbert filter */
+int ref_harmonic(const float *in, float *out, int nt, float kx, float x) {
+  try {
+    harmonic(const_cast<float *>(in), out, nt, kx, x);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return -1;
+  }
+  return 0;
+}
+
 /* illum (src/util/fd.cpp:275-339): ss_out [nx][nz] */
 int ref_illum(float dt, float dx, float dz, int nt, int ndel, int nx, int nz, int pml, int sx,
               int sz, const float *wav, const float *vel, float *ss_out) {

@@ -9,7 +9,9 @@
  * fields are reachable.  A failed reference check() throws (ref_shim.cpp);
  * every entry point turns that into a -1 return.
  */
+#include <cstdlib>
 #include <cstring>
+#include <iostream>
 #include <string>
 #include <vector>
 
@@ -161,6 +163,23 @@ int ref_param_read(const char *file, int *ints, float *floats, char *strs) {
   } catch (...) {
     return -1;
   }
+}
+
+/* planeWavePrepare (inversion.cpp:808-912) of a parameter file's survey: reads
+ * its precsg<is>.dat files and writes PLANE_S_NEW / PLANE_R_NEW into its wdir. */
+int ref_plane_prepare(const char *param_file) {
+  std::streambuf *keep = getenv("SEIS_REF_VERBOSE") ? std::cout.rdbuf() : std::cout.rdbuf(nullptr);
+  int rc = 0;
+  try {
+    Inversion v(0, 1);
+    v.readParamFile(param_file);
+    v.getConfig();
+    v.planeWavePrepare();
+  } catch (...) {
+    rc = -1;
+  }
+  std::cout.rdbuf(keep);
+  return rc;
 }
 
 /* Coords: number of shots, then receivers per shot, sources and receivers

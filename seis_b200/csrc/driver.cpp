@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cctype>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -394,7 +395,7 @@ int observed(seis_driver *d, int is, int born_data, const float *v0, const ShotG
 extern "C" {
 
 int seis_driver_create(seis_fd_ctx *ctx, const char *param_file, int batch, seis_driver **out) {
-  if (!ctx || !param_file || !out) return SEIS_ERR_ARG;
+  if (!param_file || !out) return SEIS_ERR_ARG;
   *out = nullptr;
   seis_driver *d = new (std::nothrow) seis_driver();
   if (!d) return SEIS_ERR_NOMEM;
@@ -434,6 +435,7 @@ const seis_params *seis_driver_params(const seis_driver *d) { return d ? &d->p :
 
 int seis_driver_modeling(seis_driver *d, const float *h_v) {
   if (!d) return SEIS_ERR_ARG;
+  if (!d->ctx) return dfail(d, SEIS_ERR_STATE, "driver created without a device context");
   const seis_params &p = d->p;
   int rc = SEIS_OK;
   std::vector<float> vfile;
@@ -482,6 +484,7 @@ int seis_driver_modeling(seis_driver *d, const float *h_v) {
 
 int seis_driver_born(seis_driver *d, const float *h_dv) {
   if (!d || !h_dv) return SEIS_ERR_ARG;
+  if (!d->ctx) return dfail(d, SEIS_ERR_STATE, "driver created without a device context");
   const seis_params &p = d->p;
   int rc = SEIS_OK;
   const std::vector<float> v0 = load_model(d, p.v0file, &rc);
@@ -528,6 +531,7 @@ int seis_driver_born(seis_driver *d, const float *h_dv) {
 
 int seis_driver_rtm(seis_driver *d, int born_data, float *h_img) {
   if (!d || !h_img) return SEIS_ERR_ARG;
+  if (!d->ctx) return dfail(d, SEIS_ERR_STATE, "driver created without a device context");
   const seis_params &p = d->p;
   int rc = SEIS_OK;
   const std::vector<float> v0 = load_model(d, p.v0file, &rc);
@@ -583,6 +587,7 @@ int seis_driver_rtm(seis_driver *d, int born_data, float *h_img) {
 
 int seis_driver_illum(seis_driver *d, float *h_ss) {
   if (!d || !h_ss) return SEIS_ERR_ARG;
+  if (!d->ctx) return dfail(d, SEIS_ERR_STATE, "driver created without a device context");
   const seis_params &p = d->p;
   int rc = SEIS_OK;
   const std::vector<float> v0 = load_model(d, p.v0file, &rc);
@@ -625,9 +630,67 @@ int seis_driver_illum(seis_driver *d, float *h_ss) {
   });
 }
 
+int seis_driver_plane_prepare(seis_driver *d) {
+  if (!d) return SEIS_ERR_ARG;
+  const seis_params &p = d->p;
+  if (!p.planeTag) return dfail(d, SEIS_ERR_STATE, "planeTag is 0");
+  const int NT = p.nt + p.delaycal;
+  const int hb = 100;  // Hilbert<float> hl(100), InitInversion.cpp:145
+  const std::vector<float> wav = wavelet(p);
+  std::vector<float> hwav((size_t)NT);
+  seis_fd_hilbert(wav.data(), hwav.data(), NT, hb);
+  // each trace and its Hilbert transform, once for all wavenumbers
+  std::vector<std::vector<float>> data((size_t)p.ns), hdata((size_t)p.ns);
+  float sxmax = d->sc[0];
+  for (int is = 0; is < p.ns; is++) {
+    const size_t n = (size_t)d->ng[is] * p.nt;
+    data[is].resize(n);
+    hdata[is].resize(n);
+    if (!read_file(d->csg_name(is), data[is].data(), n))
+      return dfail(d, SEIS_ERR_ARG, "cannot read %s", d->csg_name(is).c_str());
+    for (int ig = 0; ig < d->ng[is]; ig++)
+      seis_fd_hilbert(data[is].data() + (size_t)ig * p.nt, hdata[is].data() + (size_t)ig * p.nt,
+                      p.nt, hb);
+    sxmax = sxmax < d->sc[2 * is] ? d->sc[2 * is] : sxmax;  // :840-843
+  }
+  const float xlo = (float)((double)p.velfx - 0.0001 * (double)p.dx);  // :862
+  std::vector<float> sou((size_t)p.nx * NT), rec((size_t)p.nx * p.nt), tr((size_t)p.nx * p.nt);
+  std::vector<float> tw((size_t)NT), csgn;
+  for (int k = 0; k < p.np; k++) {
+    std::fill(sou.begin(), sou.end(), 0.0f);
+    std::fill(rec.begin(), rec.end(), 0.0f);
+    const float kx = p.pmin + (float)k * p.dp;  // :860
+    for (int is = 0; is < p.ns; is++) {
+      const float sx = d->sc[2 * is];
+      if (!((sx - xlo) >= 0.0f && (sxmax - sx) >= 0.0f))
+        return dfail(d, SEIS_ERR_ARG, "shot %d x outside [velfx, largest source x]", is);
+      // harmonic(), InitInversion.cpp:141-150: cos/sin of the float phase
+      const float cn = std::cos(kx * sx), sn = std::sin(kx * sx);
+      for (int it = 0; it < NT; it++) tw[it] = cn * wav[it] - sn * hwav[it];
+      const int isx = (int)((sx - p.velfx) / p.dx + 0.001f);  // :879
+      if (isx < 0 || isx >= p.nx) return dfail(d, SEIS_ERR_ARG, "shot %d column %d", is, isx);
+      float *col = sou.data() + (size_t)isx * NT;
+      for (int it = 0; it < NT; it++) col[it] = col[it] + tw[it];
+      const size_t n = data[is].size();
+      csgn.resize(n);
+      for (size_t i = 0; i < n; i++) csgn[i] = cn * data[is][i] - sn * hdata[is][i];
+      int r = seis_geom_reorder(csgn.data(), d->ng[is], p.nt, d->gx(is), tr.data(), p.velfx,
+                                p.nx, p.dx, 0);
+      if (r) return dfail(d, r, "shot %d traces", is);
+      for (size_t i = 0; i < rec.size(); i++) rec[i] = tr[i] + rec[i];  // :897
+    }
+    const std::string sn_ = std::string(p.wdir) + "PLANE_S_NEW" + std::to_string(k) + ".dat";
+    const std::string rn_ = std::string(p.wdir) + "PLANE_R_NEW" + std::to_string(k) + ".dat";
+    if (!write_file(sn_, sou.data(), sou.size()) || !write_file(rn_, rec.data(), rec.size()))
+      return dfail(d, SEIS_ERR_ARG, "cannot write %s", sn_.c_str());
+  }
+  return SEIS_OK;
+}
+
 int seis_driver_lsrtm(seis_driver *d, int born_data, int niter, const seis_lsrtm_opts *opts,
                       float *h_img, double *h_rr) {
   if (!d || !h_img || niter < 0) return SEIS_ERR_ARG;
+  if (!d->ctx) return dfail(d, SEIS_ERR_STATE, "driver created without a device context");
   const seis_params &p = d->p;
   int rc = SEIS_OK;
   const std::vector<float> v0 = load_model(d, p.v0file, &rc);

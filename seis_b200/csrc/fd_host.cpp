@@ -50,7 +50,7 @@ struct seis_fd_plan {
 
 namespace {
 
-enum Op { OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2, OP_BORN_ADJ = 3, OP_ILLUM = 4 };
+enum Op { OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2, OP_BORN_ADJ = 3, OP_ILLUM = 4, OP_BORN_PLANE = 5 };
 
 int fail(seis_fd_ctx *ctx, int code, const char *fmt, ...) {
   char buf[512];
@@ -381,15 +381,22 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     p->max_strip = std::max(p->max_strip, g.strip_len);
     p->max_NZ = std::max(p->max_NZ, g.NZ);
     p->stage_elems = std::max(p->stage_elems, std::max((size_t)d.nx * d.nz, (size_t)d.nx * d.nt));
+    if (op == OP_BORN_PLANE)
+      p->stage_elems = std::max(p->stage_elems, (size_t)d.nx * (d.nt + d.ndel));
     for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fa[k]);
-    if (op == OP_BORN || op == OP_RTM)
+    if (op == OP_BORN || op == OP_RTM || op == OP_BORN_PLANE)
       for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fb[k]);
     if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.u3s[0]);
-    if (rc == SEIS_OK && op == OP_BORN) rc = alloc_field(*p, g, &g.u3s[1]);
+    if (rc == SEIS_OK && (op == OP_BORN || op == OP_BORN_PLANE)) rc = alloc_field(*p, g, &g.u3s[1]);
     float *vel = nullptr, *dv = nullptr, *wav = nullptr, *rec = nullptr;
     int *gzd = nullptr;
     if (rc == SEIS_OK) rc = alloc_field(*p, g, &vel);
-    if (rc == SEIS_OK && op == OP_BORN) rc = alloc_field(*p, g, &dv);
+    if (rc == SEIS_OK && (op == OP_BORN || op == OP_BORN_PLANE)) rc = alloc_field(*p, g, &dv);
+    if (rc == SEIS_OK && op == OP_BORN_PLANE) {
+      float *sou = nullptr;
+      rc = p->alloc(&sou, (size_t)g.NT * d.nx);
+      g.sou = sou;
+    }
     if (rc == SEIS_OK) rc = p->alloc(&wav, (size_t)g.NT);
     if (rc == SEIS_OK) rc = p->alloc(&rec, (size_t)d.nt * d.nx);
     if (rc == SEIS_OK) rc = p->alloc(&gzd, (size_t)d.nx);
@@ -415,7 +422,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     // NT + 2 nt, exact adjoint NT (source pass) + NT + 1 (reverse pass)
     for (const ShotDev &g : p->sd) {
       int64_t per = (op == OP_MODEL || op == OP_ILLUM) ? g.NT
-                  : op == OP_BORN  ? 2LL * g.NT
+                  : (op == OP_BORN || op == OP_BORN_PLANE) ? 2LL * g.NT
                   : op == OP_RTM   ? g.NT + 2LL * g.nt
                                    : 2LL * g.NT + 1;
       p->cell_updates += (int64_t)g.NX * g.NZ * per;
@@ -657,6 +664,7 @@ int enqueue_operator(Plan &p) {
       if (!rc && !p.snaps_valid) rc = source_pass(p);
       return rc ? rc : run_adjoint(p);
     case OP_ILLUM: return run_forward(p, MODE_MODEL);
+    case OP_BORN_PLANE: return run_forward(p, MODE_BORN);
   }
   return fail(p.ctx, SEIS_ERR_NOTSUP, "unknown operator %d", p.op);
 }
@@ -832,7 +840,7 @@ int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_des
   if (rc) return rc;
   if (!out) return fail(ctx, SEIS_ERR_ARG, "out is null");
   *out = nullptr;
-  if (op < SEIS_OP_MODELING || op > SEIS_OP_ILLUM) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
+  if (op < SEIS_OP_MODELING || op > SEIS_OP_BORN_PLANE) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
   Plan *p = nullptr;
   rc = plan_create(ctx, op, nshot, shots, &p);
   if (rc) return rc;
@@ -884,6 +892,12 @@ static int plan_input(seis_fd_plan *plan, int shot, int what, const float *src, 
     }
     case SEIS_IN_WAVELET:
       CK(cudaMemcpyAsync(const_cast<float *>(g.wav), src, sizeof(float) * g.NT, kind, ctx->stream));
+      return SEIS_OK;
+    case SEIS_IN_SOURCE:
+      if (!g.sou) return fail(ctx, SEIS_ERR_NOTSUP, "plan takes no areal source");
+      CK(cudaMemcpyAsync(p.d_stage, src, sizeof(float) * d.nx * g.NT, kind, ctx->stream));
+      CK(launch_transpose(p.d_stage, d.nx, g.NT, const_cast<float *>(g.sou), ctx->stream));
+      ctx->launches++;
       return SEIS_OK;
     case SEIS_IN_GATHER:
       if (p.op != OP_RTM && p.op != OP_BORN_ADJ)
@@ -1079,6 +1093,33 @@ int seis_fd_born(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wa
                  const float *h_vel, const float *h_dv, float *h_rec) {
   return run_batch(ctx, OP_BORN, 1, shot, &h_wav, SEIS_IN_WAVELET, &h_vel, SEIS_IN_VEL, &h_dv,
                    SEIS_IN_DV, &h_rec, SEIS_OUT_GATHER);
+}
+
+int seis_fd_hilbert(const float *in, float *out, int n, int half) {
+  if (!in || !out || n < 0 || half < 1) return SEIS_ERR_ARG;
+  std::vector<float> h((size_t)(2 * half + 1));
+  hilbert_taps(h.data(), half);
+  // a full convolution cut to the input length, summed in increasing input
+  // index; a tap of exactly zero adds nothing (hilbert.h:42-54)
+  for (int k = 0; k < n; k++) {
+    const int i0 = std::max(0, k - half), i1 = std::min(n - 1, k + half);
+    float acc = 0.0f;
+    for (int i = i0; i <= i1; i++) {
+      const float hk = h[(size_t)(k - i + half)];
+      if (hk != 0.0f) acc += in[i] * hk;
+    }
+    out[k] = acc;
+  }
+  return SEIS_OK;
+}
+
+int seis_fd_born_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_sou,
+                       const float *h_vel, const float *h_dv, float *h_rec) {
+  if (!shot) return begin(ctx) ? SEIS_ERR_ARG : fail(ctx, SEIS_ERR_ARG, "null shot");
+  seis_shot_desc d = *shot;
+  d.sx = d.nx / 2;  // the areal source has no point position
+  return run_batch(ctx, OP_BORN_PLANE, 1, &d, &h_sou, SEIS_IN_SOURCE, &h_vel, SEIS_IN_VEL,
+                   &h_dv, SEIS_IN_DV, &h_rec, SEIS_OUT_GATHER);
 }
 
 int seis_fd_illum(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,

@@ -94,6 +94,7 @@ struct ShotDev {
   // absorbing-boundary kernel
   float *u3s[2];
   float *illum;          // source illumination [nx][nz] (illumination plans)
+  const float *sou;      // areal source [NT][nx] at row szp (plane-wave plans), else null
 };
 enum SnapType : int { SNAP_NONE = 0, SNAP_F32 = 1, SNAP_BF16 = 2, SNAP_F16 = 3 };
 static_assert(sizeof(ShotDev) % sizeof(int) == 0 && sizeof(ShotDev) <= 256 * sizeof(int),

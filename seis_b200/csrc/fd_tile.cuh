@@ -123,7 +123,14 @@ template <int MODE>
 __device__ __forceinline__ float inject(const ShotDev &g, const StepArgs &a, int ix, int iz,
                                         int gzc, float u3, float vt2) {
   if (MODE != MODE_RCV) {
-    if (a.src_k >= 0 && ix == g.sxp && iz == g.szp) u3 = u3 + vt2 * g.wav[a.src_k];
+    if (a.src_k >= 0) {
+      if (g.sou) {  // areal source of forwordPlane, fd.cpp:221-225
+        if (iz == g.szp && ix >= g.pml && ix < g.pml + g.nx)
+          u3 = u3 + vt2 * g.sou[(size_t)a.src_k * g.nx + (ix - g.pml)];
+      } else if (ix == g.sxp && iz == g.szp) {
+        u3 = u3 + vt2 * g.wav[a.src_k];
+      }
+    }
   } else if (a.rec_k >= 0 && iz == gzc) {
     u3 = u3 + g.rec[(size_t)a.rec_k * g.nx + (ix - g.pml)] * vt2;
   }

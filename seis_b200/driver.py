@@ -57,6 +57,7 @@ def _setup():
     L.seis_driver_born.argtypes = [_P, _P]
     L.seis_driver_rtm.argtypes = [_P, _I, _P]
     L.seis_driver_illum.argtypes = [_P, _P]
+    L.seis_driver_plane_prepare.argtypes = [_P]
     L.seis_driver_lsrtm.argtypes = [_P, _I, _I, ctypes.POINTER(LsrtmOptsC), _P, _P]
     L._driver_ready = True
     return L
@@ -100,19 +101,28 @@ def read_coords(path: str, ngmax: int = None):
 class Driver:
     """A parameter file's survey on one device context."""
 
-    def __init__(self, ctx: Context, param_file: str, batch: int = 0):
+    def __init__(self, ctx, param_file: str, batch: int = 0):
+        """ctx: a Context, or None for the host-only steps (plane_prepare)."""
         self.ctx = ctx
         self.L = _setup()
         h = _P()
-        rc = self.L.seis_driver_create(ctx.h, param_file.encode(), batch, ctypes.byref(h))
+        rc = self.L.seis_driver_create(ctx.h if ctx is not None else None, param_file.encode(),
+                                       batch, ctypes.byref(h))
         if rc:
             raise SeisError(f"{param_file}: driver setup failed ({rc})")
         self.h = h
-        self.params = self.L.seis_driver_params(h).contents
+        # a copy: it outlives the driver
+        self.params = Params.from_buffer_copy(self.L.seis_driver_params(h).contents)
 
     def _run(self, rc, what):
         if rc:
-            raise SeisError(f"{what} failed ({rc}): {self.ctx.L.seis_fd_last_error(self.ctx.h)}")
+            msg = self.ctx.L.seis_fd_last_error(self.ctx.h) if self.ctx is not None else b""
+            raise SeisError(f"{what} failed ({rc}): {msg}")
+
+    def plane_prepare(self):
+        """Phase-encoded sources and data PLANE_S_NEW<k>.dat / PLANE_R_NEW<k>.dat
+        (planeWavePrepare); host only."""
+        self._run(self.L.seis_driver_plane_prepare(self.h), "plane_prepare")
 
     def modeling(self, v: np.ndarray = None):
         """Synthetic gathers precsg<is>.dat of v [nx][nz] (None: the vfile model)."""

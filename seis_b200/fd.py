@@ -44,6 +44,20 @@ def modeling(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, ctx: Conte
     return rec
 
 
+def forward_plane(dt, dx, dz, nt, ndel, nx, nz, pml, sz, gz, vel, sou, dv, ctx: Context = None):
+    """Born gather ``rec[nx][nt]`` of the areal source ``sou[nx][nt+ndel]`` at row sz,
+    receivers at row gz (reference ``forwordPlane``, src/util/fd.cpp:178-274)."""
+    ctx = ctx or default_context()
+    s = _shot(dt, dx, dz, nt, ndel, nx, nz, pml, nx // 2, sz, np.full(nx, gz, np.int32))
+    sou = _f32(sou, (nx, s.NT))
+    vel = _f32(vel, (nx, nz))
+    dv = _f32(dv, (nx, nz))
+    rec = np.zeros((nx, nt), np.float32)
+    d = s.to_c()
+    ctx.check(ctx.L.seis_fd_born_plane(ctx.h, d, ptr(sou), ptr(vel), ptr(dv), ptr(rec)))
+    return rec
+
+
 def illum(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, wav, vel, ctx: Context = None):
     """Source illumination ``ss[nx][nz]`` (reference ``illum``, src/util/fd.cpp:275-339)."""
     ctx = ctx or default_context()

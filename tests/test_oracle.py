@@ -69,3 +69,14 @@ def test_restatement_matches_reference_random():
 def test_illum_restatement_matches_reference(g):
     """illum (src/util/fd.cpp:275-339): the C restatement bit for bit."""
     assert np.array_equal(O.illum(g.shot, g.wav, g.vel), O.illum(g.shot, g.wav, g.vel, impl="ref"))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("g", CASES, ids=golden_ids())
+def test_born_plane_restatement_matches_reference(g):
+    """forwordPlane (src/util/fd.cpp:178-274): the C restatement bit for bit."""
+    rng = np.random.default_rng(1)
+    sou = np.outer(rng.standard_normal(g.shot.nx), g.wav).astype(np.float32)
+    gz = int(g.shot.gz[0])
+    assert np.array_equal(O.born_plane(g.shot, sou, g.vel, g.dv, gz),
+                          O.born_plane(g.shot, sou, g.vel, g.dv, gz, impl="ref"))
