@@ -123,6 +123,15 @@ int seis_fd_illum_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots
 int seis_fd_born_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_sou,
                        const float *h_vel, const float *h_dv, float *h_rec);
 
+/* adjointPlane (src/util/fd.cpp:787-921): RTM of the areal source
+ * h_sou[nx][nt+ndel] at row shot->sz with the gather h_rec[nx][nt] at rows
+ * shot->gz; the receiver field is back-propagated first keeping its boundary
+ * layers, then re-propagated beside the source field; FaQi imaging.  Gather
+ * samples at negative time indices, which the reference reads outside its
+ * array (fd.cpp:834, :873), are skipped.  h_img[nx][nz]. */
+int seis_fd_rtm_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_sou,
+                      const float *h_vel, const float *h_rec, float *h_img);
+
 /* ---------------------------------------------------------- shot batches */
 /* A plan is a batch of shots resident on the device.  It replaces the
  * reference's MPI shot farm (masterRun + worker loops,
@@ -140,6 +149,8 @@ int seis_fd_born_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float
                               wavelet, velocity -> image [nx][nz]           */
 #define SEIS_OP_BORN_PLANE 5 /* forwordPlane, Born with an areal source
                                 (fd.cpp:178-274): source, velocity, dv -> gather */
+#define SEIS_OP_RTM_PLANE 6  /* adjointPlane, RTM of an areal source
+                                (fd.cpp:787-921): source, velocity, gather -> image */
 
 #define SEIS_IN_VEL 0      /* [nx][nz] velocity of the shot's model         */
 #define SEIS_IN_DV 1       /* [nx][nz] velocity perturbation (SEIS_OP_BORN) */

@@ -165,6 +165,25 @@ def born_plane(shot, sou, vel, dv, gz, prec="f32", impl="oracle"):
     return rec
 
 
+def rtm_plane(shot, sou, vel, rec, gz, prec="f32", impl="oracle"):
+    """Image [nx][nz] of ``adjointPlane`` (src/util/fd.cpp:787-921): areal source
+    sou [nx][nt+ndel] at row shot.sz, receivers rec [nx][nt] at row gz."""
+    dt, (_, sou, vel, rec) = _prep(shot, prec, impl, sou, vel, rec)
+    img = np.zeros((shot.nx, shot.nz), dt)
+    R = _real(prec) if impl != "ref" else ctypes.c_float
+    s = shot
+    args = [R(s.dt), R(s.dx), R(s.dz), _I(s.nt), _I(s.ndel), _I(s.nx), _I(s.nz), _I(s.pml),
+            _I(s.sz), _I(int(gz))]
+    if impl == "ref":
+        rc = ref_lib().ref_rtm_plane(*args, _ptr(sou), _ptr(vel), _ptr(rec), _ptr(img))
+    else:
+        rc = getattr(oracle_lib(), f"orc_rtm_plane_{prec}")(*args, _ptr(sou), _ptr(vel),
+                                                            _ptr(rec), _ptr(img))
+    if rc != 0:
+        raise RuntimeError(f"oracle rtm_plane failed ({rc})")
+    return img
+
+
 def illum(shot, wav, vel, prec="f32", impl="oracle"):
     """Source illumination [nx][nz] of ``illum`` (src/util/fd.cpp:275-339)."""
     dt, (gz, wav, vel) = _prep(shot, prec, impl, wav, vel)

@@ -546,6 +546,72 @@ int F(orc_rtm)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int 
   return 0;
 }
 
+/* adjointPlane, src/util/fd.cpp:787-921: RTM of the areal source sou[nx][NT]
+ * at row sz with receivers at row gz.  The receiver field is propagated back
+ * first, keeping its boundary layers per step, then re-propagated forward in
+ * step with the source field from those layers; imaging is FaQi alone.  The
+ * reference's receiver injections run for negative sample indices too (a stray
+ * ';' after the guard, fd.cpp:834, :873) and read outside rec there; this
+ * restatement skips those samples, which equals the reference whenever the
+ * memory it reads there holds zeros. */
+int F(orc_rtm_plane)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml, int sz,
+                     int gz, const REAL *sou, const REAL *vel, const REAL *rec, REAL *img)
+{
+  F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  F(coefs_t) c;
+  F(coefs_init)(g, vel, &c, 1);
+  int NT = nt + ndel, szp = sz + pml, gzp = gz + pml;
+  size_t n = (size_t)g->NX * g->NZ, sl = F(strip_len)(g);
+  REAL *u0 = F(zalloc)(n), *u1 = F(zalloc)(n), *u2 = F(zalloc)(n);
+  REAL *b0 = F(zalloc)(n), *b1 = F(zalloc)(n), *b2 = F(zalloc)(n);
+  REAL *lap = F(zalloc)(n), *imgp = F(zalloc)(n);
+  REAL *store = F(zalloc)(sl * (size_t)NT);
+  REAL *h = F(zalloc)(61), *uh = F(zalloc)((size_t)g->NZ), *rh = F(zalloc)((size_t)g->NZ);
+  F(hilbert_taps)(30, h);
+  REAL idt2 = KR(1.0) / dt / dt;
+  /* receiver side, back in time (:829-845) */
+  for (int it = NT - 1; it >= 0; it--) {
+    int itp = it - ndel;
+    F(twoway)(g, &c, b1, b2, b0);
+    if (itp >= 0)
+      for (int ix = 0; ix < nx; ix++)
+        AT(b0, ix + pml, gzp) += rec[(size_t)ix * nt + itp] * AT(c.vt2, ix + pml, gzp);
+    F(absorb)(g, &c, b0, b1, b2);
+    F(strips)(g, b1, store + sl * (size_t)it, 1);
+    REAL *t = b2; b2 = b1; b1 = b0; b0 = t;
+  }
+  { REAL *t = b0; b0 = b1; b1 = b2; b2 = t; }  /* :846-850 */
+  memset(b2, 0, n * sizeof(REAL));
+  /* source forward, receiver re-propagated from its layers (:853-893) */
+  for (int it = 2; it < NT; it++) {
+    F(twoway)(g, &c, u1, u0, u2);
+    for (int ix = 0; ix < nx; ix++)
+      AT(u2, ix + pml, szp) += AT(c.vt2, ix + pml, szp) * sou[(size_t)ix * NT + (it - 1)];
+    F(absorb)(g, &c, u2, u1, u0);
+    for (size_t i = 0; i < n; i++) lap[i] = (u2[i] + u0[i] - KR(2) * u1[i]) * idt2;
+    int itp = it - ndel - 1;
+    if (itp >= 0)
+      for (int ix = 0; ix < nx; ix++)
+        AT(b0, ix + pml, gzp) -= rec[(size_t)ix * nt + itp] * AT(c.vt2, ix + pml, gzp);
+    F(twoway)(g, &c, b1, b0, b2);
+    F(absorb)(g, &c, b2, b1, b0);
+    if (it - ndel > 0) {
+      for (size_t i = 0; i < n; i++) lap[i] = lap[i] * c.vel3[i];
+      F(faqi)(g, h, lap, b2, imgp, uh, rh);
+    }
+    REAL *t = u0; u0 = u1; u1 = u2; u2 = t;
+    t = b0; b0 = b1; b1 = b2; b2 = t;
+    F(strips)(g, b1, store + sl * (size_t)it, 0);
+  }
+  for (int ix = 0; ix < nx; ix++)
+    for (int iz = 0; iz < nz; iz++) img[(size_t)ix * nz + iz] = AT(imgp, ix + pml, iz + pml);
+  free(u0); free(u1); free(u2); free(b0); free(b1); free(b2); free(lap); free(imgp);
+  free(store); free(h); free(uh); free(rh);
+  F(coefs_free)(&c);
+  return 0;
+}
+
 /* ---------------------------------------------------------------------------
  * Exact adjoint of the Born operator above (no counterpart in the reference,
  * whose adjoint() is a different imaging operator).  Every stage of one

@@ -8,6 +8,7 @@
  * t fastest.  Every call copies into MyAlloc arrays, calls the reference, and
  * copies the result out.  Return value: 0 ok, -1 if the reference threw.
  */
+#include <vector>
 #include "ref_shim.h"
 #include <cstring>
 #include <stdexcept>
@@ -119,6 +120,33 @@ int ref_born_plane(float dt, float dx, float dz, int nt, int ndel, int nx, int n
     MyAlloc<float>::free(rec);
     MyAlloc<float>::free(v);
     MyAlloc<float>::free(d);
+    MyAlloc<float>::free(s);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return -1;
+  }
+  return 0;
+}
+
+/* adjointPlane (src/util/fd.cpp:787-921): sou [nx][nt+ndel], rec [nx][nt],
+ * img_out [nx][nz].  The reference reads rec at negative sample indices
+ * (fd.cpp:834, :873); the gather is laid out after ndel + 2 zero samples so
+ * that those reads stay inside this allocation. */
+int ref_rtm_plane(float dt, float dx, float dz, int nt, int ndel, int nx, int nz, int pml, int sz,
+                  int gz, const float *sou, const float *vel, const float *rec, float *img_out) {
+  QuietCout q(g_verbose);
+  try {
+    float **v = to2d(vel, nz, nx);
+    float **s = to2d(sou, nt + ndel, nx);
+    const size_t pad = (size_t)ndel + 2;
+    std::vector<float> block(pad + (size_t)nx * nt, 0.0f);
+    std::copy(rec, rec + (size_t)nx * nt, block.begin() + pad);
+    std::vector<float *> rows((size_t)nx);
+    for (int ix = 0; ix < nx; ix++) rows[ix] = block.data() + pad + (size_t)ix * nt;
+    float **img = adjointPlane(dt, dx, dz, nt, ndel, nx, nz, pml, sz, gz, v, s, rows.data());
+    from2d(img_out, img, nz, nx);
+    MyAlloc<float>::free(img);
+    MyAlloc<float>::free(v);
     MyAlloc<float>::free(s);
   } catch (const std::exception &e) {
     std::fprintf(stderr, "%s\n", e.what());

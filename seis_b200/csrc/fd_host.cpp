@@ -50,7 +50,10 @@ struct seis_fd_plan {
 
 namespace {
 
-enum Op { OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2, OP_BORN_ADJ = 3, OP_ILLUM = 4, OP_BORN_PLANE = 5 };
+enum Op {
+  OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2, OP_BORN_ADJ = 3, OP_ILLUM = 4, OP_BORN_PLANE = 5,
+  OP_RTM_PLANE = 6
+};
 
 int fail(seis_fd_ctx *ctx, int code, const char *fmt, ...) {
   char buf[512];
@@ -381,10 +384,10 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     p->max_strip = std::max(p->max_strip, g.strip_len);
     p->max_NZ = std::max(p->max_NZ, g.NZ);
     p->stage_elems = std::max(p->stage_elems, std::max((size_t)d.nx * d.nz, (size_t)d.nx * d.nt));
-    if (op == OP_BORN_PLANE)
+    if (op == OP_BORN_PLANE || op == OP_RTM_PLANE)
       p->stage_elems = std::max(p->stage_elems, (size_t)d.nx * (d.nt + d.ndel));
     for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fa[k]);
-    if (op == OP_BORN || op == OP_RTM || op == OP_BORN_PLANE)
+    if (op == OP_BORN || op == OP_RTM || op == OP_BORN_PLANE || op == OP_RTM_PLANE)
       for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fb[k]);
     if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.u3s[0]);
     if (rc == SEIS_OK && (op == OP_BORN || op == OP_BORN_PLANE)) rc = alloc_field(*p, g, &g.u3s[1]);
@@ -392,7 +395,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     int *gzd = nullptr;
     if (rc == SEIS_OK) rc = alloc_field(*p, g, &vel);
     if (rc == SEIS_OK && (op == OP_BORN || op == OP_BORN_PLANE)) rc = alloc_field(*p, g, &dv);
-    if (rc == SEIS_OK && op == OP_BORN_PLANE) {
+    if (rc == SEIS_OK && (op == OP_BORN_PLANE || op == OP_RTM_PLANE)) {
       float *sou = nullptr;
       rc = p->alloc(&sou, (size_t)g.NT * d.nx);
       g.sou = sou;
@@ -401,7 +404,9 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (rc == SEIS_OK) rc = p->alloc(&rec, (size_t)d.nt * d.nx);
     if (rc == SEIS_OK) rc = p->alloc(&gzd, (size_t)d.nx);
     if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&g.strips, (size_t)d.nt * g.strip_len);
-    if (rc == SEIS_OK && (op == OP_RTM || op == OP_BORN_ADJ || op == OP_ILLUM))
+    if (rc == SEIS_OK && op == OP_RTM_PLANE)  // boundary layers of every step (fd.cpp:812-815)
+      rc = p->alloc(&g.strips, (size_t)g.NT * g.strip_len);
+    if (rc == SEIS_OK && (op == OP_RTM || op == OP_BORN_ADJ || op == OP_ILLUM || op == OP_RTM_PLANE))
       rc = p->alloc(&g.img, (size_t)d.nx * d.nz);
     if (op == OP_ILLUM) g.illum = g.img;
     if (rc == SEIS_OK && op == OP_BORN_ADJ) rc = p->alloc(&g.grad, (size_t)d.nx * d.nz);
@@ -424,6 +429,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
       int64_t per = (op == OP_MODEL || op == OP_ILLUM) ? g.NT
                   : (op == OP_BORN || op == OP_BORN_PLANE) ? 2LL * g.NT
                   : op == OP_RTM   ? g.NT + 2LL * g.nt
+                  : op == OP_RTM_PLANE ? g.NT + 2LL * (g.NT - 2)
                                    : 2LL * g.NT + 1;
       p->cell_updates += (int64_t)g.NX * g.NZ * per;
     }
@@ -432,8 +438,9 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
   if (rc == SEIS_OK) rc = p->alloc(&p->d_tiles, p->tiles.size());
   if (rc == SEIS_OK) rc = p->alloc(&p->d_adj_tiles, p->adj_tiles.size());
   if (rc == SEIS_OK) rc = p->alloc(&p->d_chunks, p->chunks.size());
-  if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&p->d_cols, p->cols.size());
-  if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&p->d_taps, (size_t)61);
+  const bool imaging = op == OP_RTM || op == OP_RTM_PLANE;
+  if (rc == SEIS_OK && imaging) rc = p->alloc(&p->d_cols, p->cols.size());
+  if (rc == SEIS_OK && imaging) rc = p->alloc(&p->d_taps, (size_t)61);
   if (rc == SEIS_OK) {
     cudaStream_t st = ctx->stream;
     cudaError_t e = cudaMemcpyAsync(p->d_sd, p->sd.data(), sizeof(ShotDev) * nshot,
@@ -447,7 +454,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (e == cudaSuccess && !p->chunks.empty())
       e = cudaMemcpyAsync(p->d_chunks, p->chunks.data(), sizeof(PadChunk) * p->chunks.size(),
                           cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && op == OP_RTM) {
+    if (e == cudaSuccess && imaging) {
       e = cudaMemcpyAsync(p->d_cols, p->cols.data(), sizeof(int2) * p->cols.size(),
                           cudaMemcpyHostToDevice, st);
       float taps[61];
@@ -610,6 +617,64 @@ int run_rtm_reverse(Plan &p) {
   return SEIS_OK;
 }
 
+// adjointPlane (fd.cpp:787-921).  Pass 1 propagates the receiver field back
+// in time from zero, injecting the gather and keeping the boundary layers of
+// every step's current field; pass 2 runs the areal-source field forward from
+// step 2 and, in step with it, the receiver field again from its two last
+// pass-1 states, taking the gather off at the receiver rows and restoring the
+// kept layers, imaging with FaQi alone.  Gather samples at negative indices
+// are skipped (the reference reads outside its array there, fd.cpp:834, :873).
+int run_rtm_plane(Plan &p) {
+  seis_fd_ctx *ctx = p.ctx;
+  for (const ShotDev &g : p.sd)
+    CK(cudaMemsetAsync(g.strips, 0, sizeof(float) * (size_t)g.NT * g.strip_len, ctx->stream));
+  const int NT = p.NT, ndel = p.ndel;
+  StepArgs a{};
+  a.nshots = p.nshot;
+  a.src_k = -1;
+  for (int j = 0; j < NT; j++) {  // pass 1, it = NT-1 .. 0 (fd.cpp:829-845)
+    const int it = NT - 1 - j;
+    a.rot_b = j;
+    a.rec_k = it - ndel >= 0 ? it - ndel : -1;
+    a.strip_k = it - 1 >= 0 ? it - 1 : -1;  // the new field is the next step's current
+    int rc = step(p, MODE_RCV, a);
+    if (rc) return rc;
+  }
+  // fd.cpp:846-850: (prev, cur, new) = (R0, R1, 0) for pass 2 with the buffers
+  // in rotation order r0, r0+1, r0+2: R1 moves into the buffer after R0's
+  const int r0 = NT + 1;
+  for (const ShotDev &g : p.sd) {
+    FieldGeom fg = field_geom(g.NX, g.NZ);
+    float *b_r1 = g.fb[NT % 3] - fg.origin, *b_next = g.fb[(r0 + 1) % 3] - fg.origin;
+    CK(cudaMemcpyAsync(b_next, b_r1, sizeof(float) * fg.elems, cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    CK(cudaMemsetAsync(b_r1, 0, sizeof(float) * fg.elems, ctx->stream));
+  }
+  for (int it = 2; it < NT; it++) {  // pass 2 (fd.cpp:853-893)
+    const int k = it - 2;
+    CK(launch_plane_rcv_prep(p.d_sd, p.nshot, p.max_strip, r0 + k, k > 0 ? it - 1 : -1,
+                             it - ndel - 1 >= 0 ? it - ndel - 1 : -1, ctx->stream));
+    ctx->launches++;
+    StepArgs sa{};
+    sa.nshots = p.nshot;
+    sa.rot = k;
+    sa.src_k = it - 1;
+    int rc = step(p, MODE_MODEL, sa);
+    if (rc) return rc;
+    StepArgs ra{};
+    ra.nshots = p.nshot;
+    ra.rot_b = r0 + k;
+    rc = step(p, MODE_RCV, ra);
+    if (rc) return rc;
+    if (it - ndel > 0) {
+      CK(launch_rtm_image(p.d_sd, p.d_cols, (int)p.cols.size(), k, r0 + k, p.max_NZ, p.d_taps,
+                          ctx->stream, 1));
+      ctx->launches++;
+    }
+  }
+  return SEIS_OK;
+}
+
 // Forward pass of the background field keeping the source-term snapshots
 // (adjoint plans); reused by every later run until the velocity or the
 // wavelet changes.
@@ -665,6 +730,7 @@ int enqueue_operator(Plan &p) {
       return rc ? rc : run_adjoint(p);
     case OP_ILLUM: return run_forward(p, MODE_MODEL);
     case OP_BORN_PLANE: return run_forward(p, MODE_BORN);
+    case OP_RTM_PLANE: return run_rtm_plane(p);
   }
   return fail(p.ctx, SEIS_ERR_NOTSUP, "unknown operator %d", p.op);
 }
@@ -840,7 +906,7 @@ int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_des
   if (rc) return rc;
   if (!out) return fail(ctx, SEIS_ERR_ARG, "out is null");
   *out = nullptr;
-  if (op < SEIS_OP_MODELING || op > SEIS_OP_BORN_PLANE) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
+  if (op < SEIS_OP_MODELING || op > SEIS_OP_RTM_PLANE) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
   Plan *p = nullptr;
   rc = plan_create(ctx, op, nshot, shots, &p);
   if (rc) return rc;
@@ -900,7 +966,7 @@ static int plan_input(seis_fd_plan *plan, int shot, int what, const float *src, 
       ctx->launches++;
       return SEIS_OK;
     case SEIS_IN_GATHER:
-      if (p.op != OP_RTM && p.op != OP_BORN_ADJ)
+      if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_RTM_PLANE)
         return fail(ctx, SEIS_ERR_NOTSUP, "plan takes no gather input");
       CK(cudaMemcpyAsync(p.d_stage, src, sizeof(float) * d.nt * d.nx, kind, ctx->stream));
       CK(launch_transpose(p.d_stage, d.nx, d.nt, g.rec, ctx->stream));
@@ -933,11 +999,11 @@ int seis_fd_plan_get(seis_fd_plan *plan, int shot, int what, float *h_dst) {
   if (shot < 0 || shot >= p.nshot) return fail(ctx, SEIS_ERR_ARG, "shot=%d of %d", shot, p.nshot);
   if (!h_dst) return fail(ctx, SEIS_ERR_ARG, "null destination");
   if (what == SEIS_OUT_GATHER) {
-    if (p.op == OP_RTM || p.op == OP_BORN_ADJ || p.op == OP_ILLUM)
+    if (p.op == OP_RTM || p.op == OP_BORN_ADJ || p.op == OP_ILLUM || p.op == OP_RTM_PLANE)
       return fail(ctx, SEIS_ERR_NOTSUP, "this plan outputs images");
     rc = download_gather(p, shot, h_dst);
   } else if (what == SEIS_OUT_IMAGE) {
-    if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_ILLUM)
+    if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_ILLUM && p.op != OP_RTM_PLANE)
       return fail(ctx, SEIS_ERR_NOTSUP, "plan outputs gathers");
     const seis_shot_desc &d = p.desc[shot];
     CK(cudaMemcpyAsync(h_dst, p.sd[shot].img, sizeof(float) * d.nx * d.nz,
@@ -1120,6 +1186,15 @@ int seis_fd_born_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float
   d.sx = d.nx / 2;  // the areal source has no point position
   return run_batch(ctx, OP_BORN_PLANE, 1, &d, &h_sou, SEIS_IN_SOURCE, &h_vel, SEIS_IN_VEL,
                    &h_dv, SEIS_IN_DV, &h_rec, SEIS_OUT_GATHER);
+}
+
+int seis_fd_rtm_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_sou,
+                      const float *h_vel, const float *h_rec, float *h_img) {
+  if (!shot) return begin(ctx) ? SEIS_ERR_ARG : fail(ctx, SEIS_ERR_ARG, "null shot");
+  seis_shot_desc d = *shot;
+  d.sx = d.nx / 2;  // the areal source has no point position
+  return run_batch(ctx, OP_RTM_PLANE, 1, &d, &h_sou, SEIS_IN_SOURCE, &h_vel, SEIS_IN_VEL,
+                   &h_rec, SEIS_IN_GATHER, &h_img, SEIS_OUT_IMAGE);
 }
 
 int seis_fd_illum(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,

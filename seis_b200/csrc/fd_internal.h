@@ -189,6 +189,9 @@ cudaError_t launch_transpose(const float *d_src, int rows, int cols, float *d_ds
 cudaError_t launch_rtm_restore(const ShotDev *d_shots, int nshots, int max_strip, int rot,
                                int it, cudaStream_t s);
 cudaError_t launch_rtm_image(const ShotDev *d_shots, const int2 *d_cols, int ncols, int rot,
-                             int rot_b, int max_nz, const float *d_taps, cudaStream_t s);
+                             int rot_b, int max_nz, const float *d_taps, cudaStream_t s,
+                             int faqi_only = 0);
+cudaError_t launch_plane_rcv_prep(const ShotDev *d_shots, int nshots, int max_strip, int rot_b,
+                                  int strip_k, int rec_k, cudaStream_t s);
 
 }  // namespace seis

@@ -87,13 +87,49 @@ __global__ void rtm_restore_kernel(const ShotDev *__restrict__ shots, int nshots
   cur[(size_t)ix * g.LDZ + iz] = src[i];
 }
 
+// Before a re-propagation step of the plane-wave receiver field
+// (adjointPlane, fd.cpp:870-893): the boundary layers kept for sample strip_k
+// restored into the current field, and the receiver samples rec_k (times vt2)
+// taken off the previous field at the receiver rows.  Either part is skipped
+// when its index is negative.
+__global__ void plane_rcv_prep_kernel(const ShotDev *__restrict__ shots, int nshots, int rot_b,
+                                      int strip_k, int rec_k) {
+  const int s = blockIdx.y;
+  if (s >= nshots) return;
+  const ShotDev &g = shots[s];
+  float *prev = g.fb[rot_b % 3];
+  float *cur = g.fb[(rot_b + 1) % 3];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (rec_k >= 0 && i < g.nx) {  // fd.cpp:870-874
+    const size_t off = (size_t)(i + g.pml) * g.LDZ + (g.gz[i] + g.pml);
+    const float vt2 = coef(g.vel[off], g).vt2;
+    prev[off] = prev[off] - g.rec[(size_t)rec_k * g.nx + i] * vt2;
+  }
+  if (strip_k < 0 || i >= g.strip_len) return;
+  const float *src = g.strips + (size_t)strip_k * g.strip_len;
+  const int rowcells = 2 * LAYERS * g.nx;
+  int ix, iz;
+  if (i < rowcells) {
+    int l = i / g.nx, x = i - l * g.nx;
+    ix = x + g.pml;
+    iz = l < LAYERS ? g.pml + l : g.nz + g.pml - 1 - (l - LAYERS);
+  } else {
+    int j = i - rowcells;
+    int l = j / g.nz, z = j - l * g.nz;
+    iz = z + g.pml;
+    ix = l < LAYERS ? g.pml + l : g.nx + g.pml - 1 - (l - LAYERS);
+  }
+  cur[(size_t)ix * g.LDZ + iz] = src[i];  // SaveAtBoundary restore, fd.cpp:1206-1223
+}
+
 // Imaging of the reference RTM, one CTA per interior column (fd.cpp:668-669,
 // :681-684, FaQi :1272-1298):
 //   U = ((u2 + u0 - 2 u1)/dt^2) vel3,  img += U R,  img += 0.5 (U R - H[U] H[R])
 // with H the 61-tap Hilbert FIR along z over the whole padded column.
 constexpr int HILB_HALF = 30;
 __global__ void rtm_image_kernel(const ShotDev *__restrict__ shots, const int2 *__restrict__ cols,
-                                 int rot, int rot_b, const float *__restrict__ taps) {
+                                 int rot, int rot_b, const float *__restrict__ taps,
+                                 int faqi_only) {
   extern __shared__ float sh[];
   const int2 c = cols[blockIdx.x];
   const ShotDev &g = shots[c.x];
@@ -125,7 +161,7 @@ __global__ void rtm_image_kernel(const ShotDev *__restrict__ shots, const int2 *
     }
     float U = sU[iz], R = sR[iz];
     float *img = g.img + (size_t)c.y * g.nz + (iz - g.pml);
-    float acc = *img + U * R;
+    float acc = faqi_only ? *img : *img + U * R;  // adjointPlane images with FaQi alone
     acc = acc + 0.5f * (U * R - uh * rh);
     *img = acc;
   }
@@ -191,9 +227,17 @@ cudaError_t launch_rtm_restore(const ShotDev *d_shots, int nshots, int max_strip
 }
 
 cudaError_t launch_rtm_image(const ShotDev *d_shots, const int2 *d_cols, int ncols, int rot,
-                             int rot_b, int max_nz, const float *d_taps, cudaStream_t s) {
+                             int rot_b, int max_nz, const float *d_taps, cudaStream_t s,
+                             int faqi_only) {
   size_t smem = 2 * (size_t)max_nz * sizeof(float);
-  rtm_image_kernel<<<ncols, 256, smem, s>>>(d_shots, d_cols, rot, rot_b, d_taps);
+  rtm_image_kernel<<<ncols, 256, smem, s>>>(d_shots, d_cols, rot, rot_b, d_taps, faqi_only);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plane_rcv_prep(const ShotDev *d_shots, int nshots, int max_strip, int rot_b,
+                                  int strip_k, int rec_k, cudaStream_t s) {
+  dim3 grid((max_strip + 255) / 256, nshots);
+  plane_rcv_prep_kernel<<<grid, 256, 0, s>>>(d_shots, nshots, rot_b, strip_k, rec_k);
   return cudaGetLastError();
 }
 

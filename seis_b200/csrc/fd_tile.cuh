@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(NT_T, 2) tile_kernel(const ShotDev *__restrict
         if (PAD && !quad_model(cxj)) out_a[(size_t)cxj * g.LDZ + iz] = out;
         if (!BORN && record && iz == gzq[j])
           g.rec[(size_t)aa.rec_k * g.nx + (cxj - g.pml)] = out;
-        if (MODE == MODE_MODEL && aa.strip_k >= 0) save_strips(g, aa.strip_k, cxj, iz, out);
+        if (MODE != MODE_BORN && aa.strip_k >= 0) save_strips(g, aa.strip_k, cxj, iz, out);
         if (MODE == MODE_MODEL && aa.illum_on) {  // illum, fd.cpp:317-319
           float *ss = g.illum + (size_t)(cxj - g.pml) * g.nz + (iz - g.pml);
           *ss = *ss + out * out;

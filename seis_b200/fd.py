@@ -58,6 +58,20 @@ def forward_plane(dt, dx, dz, nt, ndel, nx, nz, pml, sz, gz, vel, sou, dv, ctx: 
     return rec
 
 
+def adjoint_plane(dt, dx, dz, nt, ndel, nx, nz, pml, sz, gz, vel, sou, rec, ctx: Context = None):
+    """Image ``img[nx][nz]`` of the areal source ``sou[nx][nt+ndel]`` and the gather
+    ``rec[nx][nt]`` at row gz (reference ``adjointPlane``, src/util/fd.cpp:787-921)."""
+    ctx = ctx or default_context()
+    s = _shot(dt, dx, dz, nt, ndel, nx, nz, pml, nx // 2, sz, np.full(nx, gz, np.int32))
+    sou = _f32(sou, (nx, s.NT))
+    vel = _f32(vel, (nx, nz))
+    rec = _f32(rec, (nx, nt))
+    img = np.zeros((nx, nz), np.float32)
+    d = s.to_c()
+    ctx.check(ctx.L.seis_fd_rtm_plane(ctx.h, d, ptr(sou), ptr(vel), ptr(rec), ptr(img)))
+    return img
+
+
 def illum(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, wav, vel, ctx: Context = None):
     """Source illumination ``ss[nx][nz]`` (reference ``illum``, src/util/fd.cpp:275-339)."""
     ctx = ctx or default_context()

@@ -80,3 +80,19 @@ def test_born_plane_restatement_matches_reference(g):
     gz = int(g.shot.gz[0])
     assert np.array_equal(O.born_plane(g.shot, sou, g.vel, g.dv, gz),
                           O.born_plane(g.shot, sou, g.vel, g.dv, gz, impl="ref"))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("g", CASES, ids=golden_ids())
+def test_rtm_plane_restatement_matches_reference(g):
+    """adjointPlane (src/util/fd.cpp:787-921): the C restatement bit for bit,
+    with the gather's last ndel + 2 samples zero (the reference reads them at
+    negative indices, fd.cpp:834, :873; the restatement skips those)."""
+    s = g.shot
+    rng = np.random.default_rng(3)
+    sou = np.outer(rng.standard_normal(s.nx), g.wav).astype(np.float32)
+    rec = rng.standard_normal((s.nx, s.nt)).astype(np.float32)
+    rec[:, s.nt - (s.ndel + 2):] = 0.0
+    gz = int(s.gz[0])
+    assert np.array_equal(O.rtm_plane(s, sou, g.vel, rec, gz),
+                          O.rtm_plane(s, sou, g.vel, rec, gz, impl="ref"))
