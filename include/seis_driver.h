@@ -85,6 +85,13 @@ int seis_driver_illum(seis_driver *d, float *h_ss);
  * PLANE_R_NEW<k>.dat ([nx][nt]).  Requires planeTag. */
 int seis_driver_plane_prepare(seis_driver *d);
 
+/* adjointPlane_MPI (inversion.cpp:1019-1103): for each wavenumber k < np,
+ * plane-wave RTM of PLANE_S_NEW<k>.dat with PLANE_R_NEW<k>.dat (born_data = 0)
+ * or BORN<k>.dat (1) over the whole v0file model, source row from shot 0's
+ * depth and receiver row from its first receiver's; each image (times the mask
+ * when mask = 1) written to wdir IMAGE<k>.dat and summed into h_img [nx][nz]. */
+int seis_driver_rtm_plane(seis_driver *d, int born_data, float *h_img);
+
 /* Least-squares RTM by CGLS over all shots: L = Born on each aperture
  * sub-grid, L^T its exact adjoint scattered back through the transpose of the
  * sub-grid extraction; observed data from precsg<is>.dat or BORN<is>.dat

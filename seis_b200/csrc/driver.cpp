@@ -687,6 +687,45 @@ int seis_driver_plane_prepare(seis_driver *d) {
   return SEIS_OK;
 }
 
+int seis_driver_rtm_plane(seis_driver *d, int born_data, float *h_img) {
+  if (!d || !h_img) return SEIS_ERR_ARG;
+  if (!d->ctx) return dfail(d, SEIS_ERR_STATE, "driver created without a device context");
+  const seis_params &p = d->p;
+  int rc = SEIS_OK;
+  const std::vector<float> v0 = load_model(d, p.v0file, &rc);
+  if (rc) return rc;
+  std::vector<float> mask;
+  if (p.mask) {
+    mask = load_model(d, p.maskfile, &rc);
+    if (rc) return rc;
+  }
+  const size_t nm = (size_t)p.nx * p.nz;
+  const int NT = p.nt + p.delaycal;
+  std::memset(h_img, 0, sizeof(float) * nm);
+  // source and receiver rows of every wavenumber (inversion.cpp:1062-1063)
+  const int sz = (int)((d->sc[1] - 0.0f) / p.dz + 0.0001f);
+  const int gz = (int)((d->gz(0)[0] - 0.0f) / p.dz + 0.0001f);
+  std::vector<int> gzs((size_t)p.nx, gz);
+  seis_shot_desc desc{p.nx, p.nz, p.npml, p.nt, p.delaycal, p.nx / 2, sz,
+                      p.dt, p.dx, p.dz, gzs.data()};
+  std::vector<float> sou((size_t)p.nx * NT), rec((size_t)p.nx * p.nt), img(nm);
+  for (int k = 0; k < p.np; k++) {
+    const std::string sn = std::string(p.wdir) + "PLANE_S_NEW" + std::to_string(k) + ".dat";
+    const std::string rn = born_data ? d->born_name(k)
+                                     : std::string(p.wdir) + "PLANE_R_NEW" + std::to_string(k) + ".dat";
+    if (!read_file(sn, sou.data(), sou.size())) return dfail(d, SEIS_ERR_ARG, "cannot read %s", sn.c_str());
+    if (!read_file(rn, rec.data(), rec.size())) return dfail(d, SEIS_ERR_ARG, "cannot read %s", rn.c_str());
+    int r = seis_fd_rtm_plane(d->ctx, &desc, sou.data(), v0.data(), rec.data(), img.data());
+    if (r) return dfail(d, r, "rtm_plane: %s", seis_fd_last_error(d->ctx));
+    if (p.mask)
+      for (size_t i = 0; i < nm; i++) img[i] = img[i] * mask[i];
+    const std::string in = std::string(p.wdir) + "IMAGE" + std::to_string(k) + ".dat";
+    if (!write_file(in, img.data(), nm)) return dfail(d, SEIS_ERR_ARG, "cannot write %s", in.c_str());
+    for (size_t i = 0; i < nm; i++) h_img[i] = img[i] + h_img[i];
+  }
+  return SEIS_OK;
+}
+
 int seis_driver_lsrtm(seis_driver *d, int born_data, int niter, const seis_lsrtm_opts *opts,
                       float *h_img, double *h_rr) {
   if (!d || !h_img || niter < 0) return SEIS_ERR_ARG;

@@ -8,7 +8,8 @@ same files with the same rules, and ``modeling``, ``born``, ``rtm`` follow
 the same file names and raw float32 layouts; ``lsrtm`` is the CG solver the
 reference declares (``cgsolver_MPI``) but does not define.
 
-    python -m seis_b200.driver PARAM_FILE {modeling|born|rtm|lsrtm|illum} [options]
+    python -m seis_b200.driver PARAM_FILE
+        {modeling|born|rtm|lsrtm|illum|plane_prepare|rtm_plane} [options]
 """
 from __future__ import annotations
 
@@ -58,6 +59,7 @@ def _setup():
     L.seis_driver_rtm.argtypes = [_P, _I, _P]
     L.seis_driver_illum.argtypes = [_P, _P]
     L.seis_driver_plane_prepare.argtypes = [_P]
+    L.seis_driver_rtm_plane.argtypes = [_P, _I, _P]
     L.seis_driver_lsrtm.argtypes = [_P, _I, _I, ctypes.POINTER(LsrtmOptsC), _P, _P]
     L._driver_ready = True
     return L
@@ -141,6 +143,13 @@ class Driver:
         self._run(self.L.seis_driver_rtm(self.h, 1 if born_data else 0, img.ctypes.data), "rtm")
         return img
 
+    def rtm_plane(self, born_data: bool = False) -> np.ndarray:
+        """Plane-wave RTM image [nx][nz] summed over the np wavenumbers (adjointPlane_MPI)."""
+        img = np.zeros((self.params.nx, self.params.nz), np.float32)
+        self._run(self.L.seis_driver_rtm_plane(self.h, 1 if born_data else 0, img.ctypes.data),
+                  "rtm_plane")
+        return img
+
     def illum(self) -> np.ndarray:
         """Source illumination [nx][nz] of all shots (illum_MPI)."""
         ss = np.zeros((self.params.nx, self.params.nz), np.float32)
@@ -178,7 +187,8 @@ class Driver:
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m seis_b200.driver", description=__doc__.split("\n")[0])
     ap.add_argument("param_file")
-    ap.add_argument("op", choices=["modeling", "born", "rtm", "lsrtm", "illum"])
+    ap.add_argument("op", choices=["modeling", "born", "rtm", "lsrtm", "illum", "plane_prepare",
+                                   "rtm_plane"])
     ap.add_argument("--dv", help="perturbation [nx][nz] float32 file (born)")
     ap.add_argument("--born-data", action="store_true", help="rtm/lsrtm from BORN<is>.dat")
     ap.add_argument("--niter", type=int, default=None, help="lsrtm iterations (default maxiter)")
@@ -186,6 +196,10 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=0, help="shots per device batch (0: all)")
     ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args(argv)
+    if a.op == "plane_prepare":
+        with Driver(None, a.param_file) as d:
+            d.plane_prepare()
+        return 0
     with Context(a.device) as ctx, Driver(ctx, a.param_file, a.batch) as d:
         p = d.params
         if a.op == "modeling":
@@ -197,6 +211,8 @@ def main(argv=None):
                 img = d.rtm(a.born_data)
             elif a.op == "illum":
                 img = d.illum()
+            elif a.op == "rtm_plane":
+                img = d.rtm_plane(a.born_data)
             else:
                 img, rr = d.lsrtm(a.niter if a.niter is not None else p.maxiter, a.born_data)
                 for i, r in enumerate(rr):

@@ -41,3 +41,30 @@ def test_rtm_plane_golden_bit_exact(ctx, g):
     want = O.rtm_plane(s, sou, g.vel, rec, gz)
     assert np.array_equal(got, want)
     assert np.abs(want).max() > 0
+
+
+def test_driver_plane_pipeline(ctx, tmp_path):
+    """planeWavePrepare then adjointPlane_MPI through the shot driver, against
+    the restatement on the files the preparation wrote."""
+    from seis_b200 import Shot
+    from seis_b200.driver import Driver
+    from test_plane_prepare import DELAYCAL, NT, NX, NZ, write_survey
+    param = write_survey(tmp_path, tmp_path / "W", np.random.default_rng(4))
+    v0 = np.broadcast_to(1800.0 + 20.0 * np.arange(NZ), (NX, NZ)).astype(np.float32)
+    v0.tofile(tmp_path / "v0.bin")
+    with Driver(ctx, str(param)) as d:
+        d.plane_prepare()
+        img = d.rtm_plane()
+        npw = d.params.np
+    shot = Shot(nx=NX, nz=NZ, pml=10, nt=NT, ndel=DELAYCAL, sx=NX // 2, sz=1, dt=1e-3, dx=10.0,
+                dz=10.0, gz=np.full(NX, 1, np.int32))
+    want = np.zeros((NX, NZ), np.float32)
+    for k in range(npw):
+        sou = np.fromfile(tmp_path / "W" / f"PLANE_S_NEW{k}.dat", np.float32).reshape(NX, NT + DELAYCAL)
+        rec = np.fromfile(tmp_path / "W" / f"PLANE_R_NEW{k}.dat", np.float32).reshape(NX, NT)
+        im = O.rtm_plane(shot, sou, v0, rec, 1)
+        got_k = np.fromfile(tmp_path / "W" / f"IMAGE{k}.dat", np.float32).reshape(NX, NZ)
+        assert np.array_equal(got_k, im), k
+        want = im + want
+    assert np.array_equal(img, want)
+    assert np.abs(img).max() > 0
