@@ -123,6 +123,12 @@ int seis_fd_illum_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots
 int seis_fd_born_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_sou,
                        const float *h_vel, const float *h_dv, float *h_rec);
 
+/* rtm_true (src/util/fd.cpp:924-1052): seis_fd_rtm with the receivers injected
+ * as vertical dipoles (-rec vt2/dz at row gz, +rec vt2/dz at row gz + 1) and
+ * the image FaQi(S vel3, R) of the reconstructed source field S itself. */
+int seis_fd_rtm_true(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
+                     const float *h_vel, const float *h_rec, float *h_img);
+
 /* adjointPlane (src/util/fd.cpp:787-921): RTM of the areal source
  * h_sou[nx][nt+ndel] at row shot->sz with the gather h_rec[nx][nt] at rows
  * shot->gz; the receiver field is back-propagated first keeping its boundary
@@ -151,6 +157,8 @@ int seis_fd_rtm_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float 
                                 (fd.cpp:178-274): source, velocity, dv -> gather */
 #define SEIS_OP_RTM_PLANE 6  /* adjointPlane, RTM of an areal source
                                 (fd.cpp:787-921): source, velocity, gather -> image */
+#define SEIS_OP_RTM_TRUE 7   /* rtm_true (fd.cpp:924-1052): the RTM with a dipole
+                                receiver injection and source-field imaging */
 
 #define SEIS_IN_VEL 0      /* [nx][nz] velocity of the shot's model         */
 #define SEIS_IN_DV 1       /* [nx][nz] velocity perturbation (SEIS_OP_BORN) */

@@ -165,6 +165,22 @@ def born_plane(shot, sou, vel, dv, gz, prec="f32", impl="oracle"):
     return rec
 
 
+def rtm_true(shot, wav, vel, rec, prec="f32", impl="oracle"):
+    """Image [nx][nz] of ``rtm_true`` (src/util/fd.cpp:924-1052)."""
+    dt, (gz, wav, vel, rec) = _prep(shot, prec, impl, wav, vel, rec)
+    img = np.zeros((shot.nx, shot.nz), dt)
+    if impl == "ref":
+        rc = ref_lib().ref_rtm_true(*_common_args(shot, None), _ptr(gz), _ptr(wav), _ptr(vel),
+                                    _ptr(rec), _ptr(img))
+    else:
+        rc = getattr(oracle_lib(), f"orc_rtm_true_{prec}")(*_common_args(shot, prec), _ptr(gz),
+                                                           _ptr(wav), _ptr(vel), _ptr(rec),
+                                                           _ptr(img))
+    if rc != 0:
+        raise RuntimeError(f"oracle rtm_true failed ({rc})")
+    return img
+
+
 def rtm_plane(shot, sou, vel, rec, gz, prec="f32", impl="oracle"):
     """Image [nx][nz] of ``adjointPlane`` (src/util/fd.cpp:787-921): areal source
     sou [nx][nt+ndel] at row shot.sz, receivers rec [nx][nt] at row gz."""

@@ -546,6 +546,60 @@ int F(orc_rtm)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int 
   return 0;
 }
 
+/* rtm_true, src/util/fd.cpp:924-1052: the RTM above with a vertical-dipole
+ * receiver injection (-rec vt2/dz at row gz, +rec vt2/dz at row gz + 1) and
+ * imaging FaQi(S vel3, R) of the source field itself. */
+int F(orc_rtm_true)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml, int sx,
+                    int sz, const int *gz, const REAL *wav, const REAL *vel, const REAL *rec,
+                    REAL *img)
+{
+  F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  F(coefs_t) c;
+  F(coefs_init)(g, vel, &c, 1);
+  size_t n = (size_t)g->NX * g->NZ, sl = F(strip_len)(g);
+  REAL *u0 = F(zalloc)(n), *u1 = F(zalloc)(n), *u2 = F(zalloc)(n);
+  REAL *b0 = F(zalloc)(n), *b1 = F(zalloc)(n), *b2 = F(zalloc)(n);
+  REAL *lap = F(zalloc)(n), *imgp = F(zalloc)(n);
+  REAL *store = F(zalloc)(sl * (size_t)nt);
+  REAL *h = F(zalloc)(61), *uh = F(zalloc)((size_t)g->NZ), *rh = F(zalloc)((size_t)g->NZ);
+  F(hilbert_taps)(30, h);
+  int sxp = sx + pml, szp = sz + pml, NT = nt + ndel;
+  for (int it = 0; it < NT; it++) {
+    F(twoway)(g, &c, u1, u0, u2);
+    if (it >= 1) AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+    F(absorb)(g, &c, u2, u1, u0);
+    if (it >= ndel) F(strips)(g, u2, store + sl * (size_t)(it - ndel), 1);
+    REAL *t = u0; u0 = u1; u1 = u2; u2 = t;
+  }
+  memset(u0, 0, n * sizeof(REAL)); memset(u1, 0, n * sizeof(REAL)); memset(u2, 0, n * sizeof(REAL));
+  for (int it = NT - 1; it >= ndel; it--) {
+    if (it - 1 > 0) AT(u2, sxp, szp) -= AT(c.vt2, sxp, szp) * wav[it - 1];
+    int itp = it - ndel;
+    F(strips)(g, u1, store + sl * (size_t)itp, 0);
+    F(twoway)(g, &c, u1, u2, u0);
+    F(absorb)(g, &c, u0, u1, u2);
+    F(twoway)(g, &c, b1, b2, b0);
+    for (int ix = 0; ix < nx; ix++) {  /* fd.cpp:1003-1008 */
+      int iz = gz[ix] + pml;
+      AT(b0, ix + pml, iz) -= rec[(size_t)ix * nt + itp] * AT(c.vt2, ix + pml, iz) / dz;
+      iz = iz + 1;
+      AT(b0, ix + pml, iz) += rec[(size_t)ix * nt + itp] * AT(c.vt2, ix + pml, iz) / dz;
+    }
+    F(absorb)(g, &c, b0, b1, b2);
+    for (size_t i = 0; i < n; i++) lap[i] = u0[i] * c.vel3[i];
+    F(faqi)(g, h, lap, b0, imgp, uh, rh);
+    REAL *t = u2; u2 = u1; u1 = u0; u0 = t;
+    t = b2; b2 = b1; b1 = b0; b0 = t;
+  }
+  for (int ix = 0; ix < nx; ix++)
+    for (int iz = 0; iz < nz; iz++) img[(size_t)ix * nz + iz] = AT(imgp, ix + pml, iz + pml);
+  free(u0); free(u1); free(u2); free(b0); free(b1); free(b2); free(lap); free(imgp);
+  free(store); free(h); free(uh); free(rh);
+  F(coefs_free)(&c);
+  return 0;
+}
+
 /* adjointPlane, src/util/fd.cpp:787-921: RTM of the areal source sou[nx][NT]
  * at row sz with receivers at row gz.  The receiver field is propagated back
  * first, keeping its boundary layers per step, then re-propagated forward in

@@ -155,6 +155,27 @@ int ref_rtm_plane(float dt, float dx, float dz, int nt, int ndel, int nx, int nz
   return 0;
 }
 
+/* rtm_true (src/util/fd.cpp:924-1052): rec [nx][nt], img_out [nx][nz] */
+int ref_rtm_true(float dt, float dx, float dz, int nt, int ndel, int nx, int nz, int pml, int sx,
+                 int sz, const int *gz, const float *wav, const float *vel, const float *rec,
+                 float *img_out) {
+  QuietCout q(g_verbose);
+  try {
+    float **v = to2d(vel, nz, nx);
+    float **r = to2d(rec, nt, nx);
+    float **img = rtm_true(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, const_cast<int *>(gz),
+                           const_cast<float *>(wav), v, r);
+    from2d(img_out, img, nz, nx);
+    MyAlloc<float>::free(img);
+    MyAlloc<float>::free(v);
+    MyAlloc<float>::free(r);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return -1;
+  }
+  return 0;
+}
+
 /* harmonic (src/util/InitInversion.cpp:141-150): phase rotation of a trace by
  * kx x through the 201-tap Hilbert filter */
 int ref_harmonic(const float *in, float *out, int nt, float kx, float x) {

@@ -52,7 +52,7 @@ namespace {
 
 enum Op {
   OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2, OP_BORN_ADJ = 3, OP_ILLUM = 4, OP_BORN_PLANE = 5,
-  OP_RTM_PLANE = 6
+  OP_RTM_PLANE = 6, OP_RTM_TRUE = 7
 };
 
 int fail(seis_fd_ctx *ctx, int code, const char *fmt, ...) {
@@ -387,7 +387,8 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (op == OP_BORN_PLANE || op == OP_RTM_PLANE)
       p->stage_elems = std::max(p->stage_elems, (size_t)d.nx * (d.nt + d.ndel));
     for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fa[k]);
-    if (op == OP_BORN || op == OP_RTM || op == OP_BORN_PLANE || op == OP_RTM_PLANE)
+    if (op == OP_BORN || op == OP_RTM || op == OP_BORN_PLANE || op == OP_RTM_PLANE ||
+        op == OP_RTM_TRUE)
       for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fb[k]);
     if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.u3s[0]);
     if (rc == SEIS_OK && (op == OP_BORN || op == OP_BORN_PLANE)) rc = alloc_field(*p, g, &g.u3s[1]);
@@ -403,10 +404,13 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (rc == SEIS_OK) rc = p->alloc(&wav, (size_t)g.NT);
     if (rc == SEIS_OK) rc = p->alloc(&rec, (size_t)d.nt * d.nx);
     if (rc == SEIS_OK) rc = p->alloc(&gzd, (size_t)d.nx);
-    if (rc == SEIS_OK && op == OP_RTM) rc = p->alloc(&g.strips, (size_t)d.nt * g.strip_len);
+    if (rc == SEIS_OK && (op == OP_RTM || op == OP_RTM_TRUE))
+      rc = p->alloc(&g.strips, (size_t)d.nt * g.strip_len);
+    g.rcv_dipole = op == OP_RTM_TRUE;
     if (rc == SEIS_OK && op == OP_RTM_PLANE)  // boundary layers of every step (fd.cpp:812-815)
       rc = p->alloc(&g.strips, (size_t)g.NT * g.strip_len);
-    if (rc == SEIS_OK && (op == OP_RTM || op == OP_BORN_ADJ || op == OP_ILLUM || op == OP_RTM_PLANE))
+    if (rc == SEIS_OK && (op == OP_RTM || op == OP_BORN_ADJ || op == OP_ILLUM || op == OP_RTM_PLANE ||
+                          op == OP_RTM_TRUE))
       rc = p->alloc(&g.img, (size_t)d.nx * d.nz);
     if (op == OP_ILLUM) g.illum = g.img;
     if (rc == SEIS_OK && op == OP_BORN_ADJ) rc = p->alloc(&g.grad, (size_t)d.nx * d.nz);
@@ -428,7 +432,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     for (const ShotDev &g : p->sd) {
       int64_t per = (op == OP_MODEL || op == OP_ILLUM) ? g.NT
                   : (op == OP_BORN || op == OP_BORN_PLANE) ? 2LL * g.NT
-                  : op == OP_RTM   ? g.NT + 2LL * g.nt
+                  : (op == OP_RTM || op == OP_RTM_TRUE) ? g.NT + 2LL * g.nt
                   : op == OP_RTM_PLANE ? g.NT + 2LL * (g.NT - 2)
                                    : 2LL * g.NT + 1;
       p->cell_updates += (int64_t)g.NX * g.NZ * per;
@@ -438,7 +442,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
   if (rc == SEIS_OK) rc = p->alloc(&p->d_tiles, p->tiles.size());
   if (rc == SEIS_OK) rc = p->alloc(&p->d_adj_tiles, p->adj_tiles.size());
   if (rc == SEIS_OK) rc = p->alloc(&p->d_chunks, p->chunks.size());
-  const bool imaging = op == OP_RTM || op == OP_RTM_PLANE;
+  const bool imaging = op == OP_RTM || op == OP_RTM_PLANE || op == OP_RTM_TRUE;
   if (rc == SEIS_OK && imaging) rc = p->alloc(&p->d_cols, p->cols.size());
   if (rc == SEIS_OK && imaging) rc = p->alloc(&p->d_taps, (size_t)61);
   if (rc == SEIS_OK) {
@@ -575,9 +579,10 @@ int run_forward(Plan &p, int mode) {
     a.rot_b = it;
     a.src_k = it >= 1 ? it - 1 : -1;
     int itp = it - p.ndel;
-    a.rec_k = (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_ILLUM && itp >= 0) ? itp : -1;
+    const bool rtm = p.op == OP_RTM || p.op == OP_RTM_TRUE;
+    a.rec_k = (!rtm && p.op != OP_BORN_ADJ && p.op != OP_ILLUM && itp >= 0) ? itp : -1;
     a.illum_on = p.op == OP_ILLUM && it > p.ndel;  // fd.cpp:318
-    a.strip_k = (p.op == OP_RTM && itp >= 0) ? itp : -1;
+    a.strip_k = (rtm && itp >= 0) ? itp : -1;
     a.snap_k = p.op == OP_BORN_ADJ ? snap_slot(it, p.NT - 1, p.snap_every) : -1;
     int rc = step(p, mode, a);
     if (rc) return rc;
@@ -611,7 +616,7 @@ int run_rtm_reverse(Plan &p) {
     rc = step(p, MODE_RCV, a);
     if (rc) return rc;
     CK(launch_rtm_image(p.d_sd, p.d_cols, (int)p.cols.size(), a.rot, a.rot_b, p.max_NZ,
-                        p.d_taps, ctx->stream));
+                        p.d_taps, ctx->stream, p.op == OP_RTM_TRUE ? 2 : 0));
     ctx->launches++;
   }
   return SEIS_OK;
@@ -731,6 +736,9 @@ int enqueue_operator(Plan &p) {
     case OP_ILLUM: return run_forward(p, MODE_MODEL);
     case OP_BORN_PLANE: return run_forward(p, MODE_BORN);
     case OP_RTM_PLANE: return run_rtm_plane(p);
+    case OP_RTM_TRUE:
+      rc = run_forward(p, MODE_MODEL);
+      return rc ? rc : run_rtm_reverse(p);
   }
   return fail(p.ctx, SEIS_ERR_NOTSUP, "unknown operator %d", p.op);
 }
@@ -906,7 +914,7 @@ int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_des
   if (rc) return rc;
   if (!out) return fail(ctx, SEIS_ERR_ARG, "out is null");
   *out = nullptr;
-  if (op < SEIS_OP_MODELING || op > SEIS_OP_RTM_PLANE) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
+  if (op < SEIS_OP_MODELING || op > SEIS_OP_RTM_TRUE) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
   Plan *p = nullptr;
   rc = plan_create(ctx, op, nshot, shots, &p);
   if (rc) return rc;
@@ -966,7 +974,7 @@ static int plan_input(seis_fd_plan *plan, int shot, int what, const float *src, 
       ctx->launches++;
       return SEIS_OK;
     case SEIS_IN_GATHER:
-      if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_RTM_PLANE)
+      if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_RTM_PLANE && p.op != OP_RTM_TRUE)
         return fail(ctx, SEIS_ERR_NOTSUP, "plan takes no gather input");
       CK(cudaMemcpyAsync(p.d_stage, src, sizeof(float) * d.nt * d.nx, kind, ctx->stream));
       CK(launch_transpose(p.d_stage, d.nx, d.nt, g.rec, ctx->stream));
@@ -999,11 +1007,13 @@ int seis_fd_plan_get(seis_fd_plan *plan, int shot, int what, float *h_dst) {
   if (shot < 0 || shot >= p.nshot) return fail(ctx, SEIS_ERR_ARG, "shot=%d of %d", shot, p.nshot);
   if (!h_dst) return fail(ctx, SEIS_ERR_ARG, "null destination");
   if (what == SEIS_OUT_GATHER) {
-    if (p.op == OP_RTM || p.op == OP_BORN_ADJ || p.op == OP_ILLUM || p.op == OP_RTM_PLANE)
+    if (p.op == OP_RTM || p.op == OP_BORN_ADJ || p.op == OP_ILLUM || p.op == OP_RTM_PLANE ||
+        p.op == OP_RTM_TRUE)
       return fail(ctx, SEIS_ERR_NOTSUP, "this plan outputs images");
     rc = download_gather(p, shot, h_dst);
   } else if (what == SEIS_OUT_IMAGE) {
-    if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_ILLUM && p.op != OP_RTM_PLANE)
+    if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_ILLUM && p.op != OP_RTM_PLANE &&
+        p.op != OP_RTM_TRUE)
       return fail(ctx, SEIS_ERR_NOTSUP, "plan outputs gathers");
     const seis_shot_desc &d = p.desc[shot];
     CK(cudaMemcpyAsync(h_dst, p.sd[shot].img, sizeof(float) * d.nx * d.nz,
@@ -1195,6 +1205,12 @@ int seis_fd_rtm_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float 
   d.sx = d.nx / 2;  // the areal source has no point position
   return run_batch(ctx, OP_RTM_PLANE, 1, &d, &h_sou, SEIS_IN_SOURCE, &h_vel, SEIS_IN_VEL,
                    &h_rec, SEIS_IN_GATHER, &h_img, SEIS_OUT_IMAGE);
+}
+
+int seis_fd_rtm_true(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
+                     const float *h_vel, const float *h_rec, float *h_img) {
+  return run_batch(ctx, OP_RTM_TRUE, 1, shot, &h_wav, SEIS_IN_WAVELET, &h_vel, SEIS_IN_VEL, &h_rec,
+                   SEIS_IN_GATHER, &h_img, SEIS_OUT_IMAGE);
 }
 
 int seis_fd_illum(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,

@@ -95,6 +95,8 @@ struct ShotDev {
   float *u3s[2];
   float *illum;          // source illumination [nx][nz] (illumination plans)
   const float *sou;      // areal source [NT][nx] at row szp (plane-wave plans), else null
+  int rcv_dipole;        // receiver injection as a vertical dipole (rtm_true)
+  int pad2_;
 };
 enum SnapType : int { SNAP_NONE = 0, SNAP_F32 = 1, SNAP_BF16 = 2, SNAP_F16 = 3 };
 static_assert(sizeof(ShotDev) % sizeof(int) == 0 && sizeof(ShotDev) <= 256 * sizeof(int),
@@ -190,7 +192,7 @@ cudaError_t launch_rtm_restore(const ShotDev *d_shots, int nshots, int max_strip
                                int it, cudaStream_t s);
 cudaError_t launch_rtm_image(const ShotDev *d_shots, const int2 *d_cols, int ncols, int rot,
                              int rot_b, int max_nz, const float *d_taps, cudaStream_t s,
-                             int faqi_only = 0);
+                             int mode = 0);
 cudaError_t launch_plane_rcv_prep(const ShotDev *d_shots, int nshots, int max_strip, int rot_b,
                                   int strip_k, int rec_k, cudaStream_t s);
 

@@ -127,9 +127,11 @@ __global__ void plane_rcv_prep_kernel(const ShotDev *__restrict__ shots, int nsh
 //   U = ((u2 + u0 - 2 u1)/dt^2) vel3,  img += U R,  img += 0.5 (U R - H[U] H[R])
 // with H the 61-tap Hilbert FIR along z over the whole padded column.
 constexpr int HILB_HALF = 30;
+// imaging of adjoint (lap vel3 R + FaQi), adjointPlane (FaQi of lap vel3),
+// rtm_true (FaQi of the source field times vel3)
+enum ImageMode { IMG_RTM = 0, IMG_PLANE = 1, IMG_TRUE = 2 };
 __global__ void rtm_image_kernel(const ShotDev *__restrict__ shots, const int2 *__restrict__ cols,
-                                 int rot, int rot_b, const float *__restrict__ taps,
-                                 int faqi_only) {
+                                 int rot, int rot_b, const float *__restrict__ taps, int mode) {
   extern __shared__ float sh[];
   const int2 c = cols[blockIdx.x];
   const ShotDev &g = shots[c.x];
@@ -142,10 +144,14 @@ __global__ void rtm_image_kernel(const ShotDev *__restrict__ shots, const int2 *
   const float *r0 = g.fb[(rot_b + 2) % 3];
   const size_t col = (size_t)ix * g.LDZ;
   for (int iz = threadIdx.x; iz < NZ; iz += blockDim.x) {
-    float lap = (u2[col + iz] + u0[col + iz] - 2.0f * u1[col + iz]) * g.idt2;
     float v = g.vel[col + iz];
     float vel3 = 2.0f / (v * v * v);
-    sU[iz] = lap * vel3;
+    if (mode == IMG_TRUE) {  // rtm_true images the source field itself, fd.cpp:1014
+      sU[iz] = u0[col + iz] * vel3;
+    } else {
+      float lap = (u2[col + iz] + u0[col + iz] - 2.0f * u1[col + iz]) * g.idt2;
+      sU[iz] = lap * vel3;
+    }
     sR[iz] = r0[col + iz];
   }
   __syncthreads();
@@ -161,7 +167,7 @@ __global__ void rtm_image_kernel(const ShotDev *__restrict__ shots, const int2 *
     }
     float U = sU[iz], R = sR[iz];
     float *img = g.img + (size_t)c.y * g.nz + (iz - g.pml);
-    float acc = faqi_only ? *img : *img + U * R;  // adjointPlane images with FaQi alone
+    float acc = mode == IMG_RTM ? *img + U * R : *img;  // the others image with FaQi alone
     acc = acc + 0.5f * (U * R - uh * rh);
     *img = acc;
   }
@@ -228,9 +234,9 @@ cudaError_t launch_rtm_restore(const ShotDev *d_shots, int nshots, int max_strip
 
 cudaError_t launch_rtm_image(const ShotDev *d_shots, const int2 *d_cols, int ncols, int rot,
                              int rot_b, int max_nz, const float *d_taps, cudaStream_t s,
-                             int faqi_only) {
+                             int mode) {
   size_t smem = 2 * (size_t)max_nz * sizeof(float);
-  rtm_image_kernel<<<ncols, 256, smem, s>>>(d_shots, d_cols, rot, rot_b, d_taps, faqi_only);
+  rtm_image_kernel<<<ncols, 256, smem, s>>>(d_shots, d_cols, rot, rot_b, d_taps, mode);
   return cudaGetLastError();
 }
 

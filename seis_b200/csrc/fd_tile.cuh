@@ -131,8 +131,15 @@ __device__ __forceinline__ float inject(const ShotDev &g, const StepArgs &a, int
         u3 = u3 + vt2 * g.wav[a.src_k];
       }
     }
-  } else if (a.rec_k >= 0 && iz == gzc) {
-    u3 = u3 + g.rec[(size_t)a.rec_k * g.nx + (ix - g.pml)] * vt2;
+  } else if (a.rec_k >= 0 && gzc >= 0) {
+    const float r = g.rec[(size_t)a.rec_k * g.nx + (ix - g.pml)];
+    if (!g.rcv_dipole) {
+      if (iz == gzc) u3 = u3 + r * vt2;
+    } else if (iz == gzc) {  // rtm_true, fd.cpp:1003-1008
+      u3 = u3 - r * vt2 / g.dz;
+    } else if (iz == gzc + 1) {
+      u3 = u3 + r * vt2 / g.dz;
+    }
   }
   return u3;
 }

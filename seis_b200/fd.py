@@ -58,6 +58,20 @@ def forward_plane(dt, dx, dz, nt, ndel, nx, nz, pml, sz, gz, vel, sou, dv, ctx: 
     return rec
 
 
+def rtm_true(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, rec, ctx: Context = None):
+    """Image ``img[nx][nz]`` of the reference ``rtm_true`` (src/util/fd.cpp:924-1052):
+    dipole receiver injection, FaQi imaging of the source field."""
+    ctx = ctx or default_context()
+    s = _shot(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz)
+    wav = _f32(wav, (s.NT,))
+    vel = _f32(vel, (nx, nz))
+    rec = _f32(rec, (nx, nt))
+    img = np.zeros((nx, nz), np.float32)
+    d = s.to_c()
+    ctx.check(ctx.L.seis_fd_rtm_true(ctx.h, d, ptr(wav), ptr(vel), ptr(rec), ptr(img)))
+    return img
+
+
 def adjoint_plane(dt, dx, dz, nt, ndel, nx, nz, pml, sz, gz, vel, sou, rec, ctx: Context = None):
     """Image ``img[nx][nz]`` of the areal source ``sou[nx][nt+ndel]`` and the gather
     ``rec[nx][nt]`` at row gz (reference ``adjointPlane``, src/util/fd.cpp:787-921)."""

@@ -96,3 +96,11 @@ def test_rtm_plane_restatement_matches_reference(g):
     gz = int(s.gz[0])
     assert np.array_equal(O.rtm_plane(s, sou, g.vel, rec, gz),
                           O.rtm_plane(s, sou, g.vel, rec, gz, impl="ref"))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("g", CASES, ids=golden_ids())
+def test_rtm_true_restatement_matches_reference(g):
+    """rtm_true (src/util/fd.cpp:924-1052): the C restatement bit for bit."""
+    assert np.array_equal(O.rtm_true(g.shot, g.wav, g.vel, g.rec),
+                          O.rtm_true(g.shot, g.wav, g.vel, g.rec, impl="ref"))
