@@ -129,6 +129,17 @@ int seis_fd_born_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float
 int seis_fd_rtm_true(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
                      const float *h_vel, const float *h_rec, float *h_img);
 
+/* adjointUpDown (src/util/fd.cpp:340-590): seis_fd_rtm with a second source
+ * field driven by h_wavh[nt+ndel] (the Hilbert transform of h_wav, see
+ * seis_fd_hilbert) and four imaging components summed over the reverse pass,
+ * H = the 61-tap Hilbert filter along depth:
+ *   h_comp[0] += S R, [1] += H[S] H[R], [2] += St H[R], [3] += H[St] R
+ * (S, St the two reconstructed source fields, R the receiver field);
+ * h_img = comp0 - comp1 + comp3 + comp2.  h_comp [4][nx][nz] may be NULL. */
+int seis_fd_rtm_updown(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
+                       const float *h_wavh, const float *h_vel, const float *h_rec, float *h_img,
+                       float *h_comp);
+
 /* adjointPlane (src/util/fd.cpp:787-921): RTM of the areal source
  * h_sou[nx][nt+ndel] at row shot->sz with the gather h_rec[nx][nt] at rows
  * shot->gz; the receiver field is back-propagated first keeping its boundary
@@ -159,14 +170,18 @@ int seis_fd_rtm_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float 
                                 (fd.cpp:787-921): source, velocity, gather -> image */
 #define SEIS_OP_RTM_TRUE 7   /* rtm_true (fd.cpp:924-1052): the RTM with a dipole
                                 receiver injection and source-field imaging */
+#define SEIS_OP_RTM_UPDOWN 8 /* adjointUpDown (fd.cpp:340-590): four-component
+                                RTM with a Hilbert-wavelet source field      */
 
 #define SEIS_IN_VEL 0      /* [nx][nz] velocity of the shot's model         */
 #define SEIS_IN_DV 1       /* [nx][nz] velocity perturbation (SEIS_OP_BORN) */
 #define SEIS_IN_WAVELET 2  /* [nt+ndel] source wavelet                      */
 #define SEIS_IN_GATHER 3   /* [nx][nt] receiver data (SEIS_OP_RTM)          */
 #define SEIS_IN_SOURCE 4   /* [nx][nt+ndel] areal source at row sz (plane-wave ops) */
+#define SEIS_IN_WAVELET_H 5 /* [nt+ndel] Hilbert-transformed wavelet (SEIS_OP_RTM_UPDOWN) */
 #define SEIS_OUT_GATHER 0  /* [nx][nt] recorded gather                      */
 #define SEIS_OUT_IMAGE 1   /* [nx][nz] image                                */
+#define SEIS_OUT_COMPONENTS 2 /* [4][nx][nz] imaging components (SEIS_OP_RTM_UPDOWN) */
 
 /* Storage of the source-term snapshots (background second time derivative)
  * that SEIS_OP_BORN_ADJOINT images with. */

@@ -181,6 +181,24 @@ def rtm_true(shot, wav, vel, rec, prec="f32", impl="oracle"):
     return img
 
 
+def rtm_updown(shot, wav, wavh, vel, rec, prec="f32", impl="oracle"):
+    """(image [nx][nz], components [4][nx][nz]) of ``adjointUpDown``
+    (src/util/fd.cpp:340-591); components in imagX order 00, zz, tz, zt."""
+    dt, (gz, wav, wavh, vel, rec) = _prep(shot, prec, impl, wav, wavh, vel, rec)
+    img = np.zeros((shot.nx, shot.nz), dt)
+    comp = np.zeros((4, shot.nx, shot.nz), dt)
+    if impl == "ref":
+        rc = ref_lib().ref_rtm_updown(*_common_args(shot, None), _ptr(gz), _ptr(wav), _ptr(wavh),
+                                      _ptr(vel), _ptr(rec), _ptr(img), _ptr(comp))
+    else:
+        rc = getattr(oracle_lib(), f"orc_rtm_updown_{prec}")(*_common_args(shot, prec), _ptr(gz),
+                                                             _ptr(wav), _ptr(wavh), _ptr(vel),
+                                                             _ptr(rec), _ptr(img), _ptr(comp))
+    if rc != 0:
+        raise RuntimeError(f"oracle rtm_updown failed ({rc})")
+    return img, comp
+
+
 def rtm_plane(shot, sou, vel, rec, gz, prec="f32", impl="oracle"):
     """Image [nx][nz] of ``adjointPlane`` (src/util/fd.cpp:787-921): areal source
     sou [nx][nt+ndel] at row shot.sz, receivers rec [nx][nt] at row gz."""

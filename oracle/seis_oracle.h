@@ -42,6 +42,10 @@ extern "C" {
   int orc_rtm_true_##S(R dt, R dx, R dz, int nt, int ndel, int nx, int nz,       \
                        int pml, int sx, int sz, const int *gz, const R *wav,     \
                        const R *vel, const R *rec, R *img);                      \
+  int orc_rtm_updown_##S(R dt, R dx, R dz, int nt, int ndel, int nx, int nz,     \
+                         int pml, int sx, int sz, const int *gz, const R *wav,   \
+                         const R *wavh, const R *vel, const R *rec, R *img,      \
+                         R *comp);                                               \
   int orc_illum_##S(R dt, R dx, R dz, int nt, int ndel, int nx, int nz, int pml, \
                     int sx, int sz, const R *wav, const R *vel, R *ss);         \
   int orc_born_adjoint_##S(R dt, R dx, R dz, int nt, int ndel, int nx, int nz,  \

@@ -600,6 +600,96 @@ int F(orc_rtm_true)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz,
   return 0;
 }
 
+/* adjointUpDown, src/util/fd.cpp:340-591: RTM with the source field S of wav
+ * and the source field St of its Hilbert transform wavh, both reconstructed
+ * from their boundary layers beside the receiver field R; every reverse step
+ * accumulates, with H the 61-tap z-Hilbert filter of each padded column,
+ *   c00 += S R,  czz += H[S] H[R],  czt += H[St] R,  ctz += St H[R]
+ * and img = c00 - czz + czt + ctz.  comp [4][nx][nz] = c00, czz, ctz, czt
+ * (the reference's imagX order, :392-395) on the model grid. */
+int F(orc_rtm_updown)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml,
+                      int sx, int sz, const int *gz, const REAL *wav, const REAL *wavh,
+                      const REAL *vel, const REAL *rec, REAL *img, REAL *comp)
+{
+  F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  F(coefs_t) c;
+  F(coefs_init)(g, vel, &c, 1);
+  size_t n = (size_t)g->NX * g->NZ, sl = F(strip_len)(g);
+  int NZ = g->NZ;
+  REAL *u[3], *t[3], *b[3];
+  for (int k = 0; k < 3; k++) { u[k] = F(zalloc)(n); t[k] = F(zalloc)(n); b[k] = F(zalloc)(n); }
+  REAL *store = F(zalloc)(sl * (size_t)nt), *store_t = F(zalloc)(sl * (size_t)nt);
+  REAL *c4[4];
+  for (int k = 0; k < 4; k++) c4[k] = F(zalloc)(n);
+  REAL *h = F(zalloc)(61), *sh = F(zalloc)((size_t)NZ), *rh = F(zalloc)((size_t)NZ),
+       *sth = F(zalloc)((size_t)NZ);
+  F(hilbert_taps)(30, h);
+  int sxp = sx + pml, szp = sz + pml, NT = nt + ndel;
+  /* forward passes of S and St with their layers (:402-438) */
+  for (int pass = 0; pass < 2; pass++) {
+    REAL **f = pass ? t : u;
+    const REAL *w = pass ? wavh : wav;
+    REAL *st = pass ? store_t : store;
+    REAL *f0 = f[0], *f1 = f[1], *f2 = f[2];
+    for (int it = 0; it < NT; it++) {
+      F(twoway)(g, &c, f1, f0, f2);
+      if (it >= 1) AT(f2, sxp, szp) += AT(c.vt2, sxp, szp) * w[it - 1];
+      F(absorb)(g, &c, f2, f1, f0);
+      if (it >= ndel) F(strips)(g, f2, st + sl * (size_t)(it - ndel), 1);
+      REAL *q = f0; f0 = f1; f1 = f2; f2 = q;
+    }
+    memset(f0, 0, n * sizeof(REAL)); memset(f1, 0, n * sizeof(REAL)); memset(f2, 0, n * sizeof(REAL));
+    f[0] = f0; f[1] = f1; f[2] = f2;
+  }
+  REAL *u0 = u[0], *u1 = u[1], *u2 = u[2], *t0 = t[0], *t1 = t[1], *t2 = t[2];
+  REAL *b0 = b[0], *b1 = b[1], *b2 = b[2];
+  for (int it = NT - 1; it >= ndel; it--) {
+    int itp = it - ndel;
+    if (it - 1 > 0) AT(u2, sxp, szp) -= AT(c.vt2, sxp, szp) * wav[it - 1];
+    F(strips)(g, u1, store + sl * (size_t)itp, 0);
+    F(twoway)(g, &c, u1, u2, u0);
+    F(absorb)(g, &c, u0, u1, u2);
+    if (it - 1 > 0) AT(t2, sxp, szp) -= AT(c.vt2, sxp, szp) * wavh[it - 1];
+    F(strips)(g, t1, store_t + sl * (size_t)itp, 0);
+    F(twoway)(g, &c, t1, t2, t0);
+    F(absorb)(g, &c, t0, t1, t2);
+    F(twoway)(g, &c, b1, b2, b0);
+    for (int ix = 0; ix < nx; ix++) {
+      int iz = gz[ix] + pml;
+      AT(b0, ix + pml, iz) += rec[(size_t)ix * nt + itp] * AT(c.vt2, ix + pml, iz);
+    }
+    F(absorb)(g, &c, b0, b1, b2);
+    for (int ix = pml; ix < g->NX - pml; ix++) {  /* :509-521 */
+      const REAL *S = u0 + (size_t)ix * NZ, *R = b0 + (size_t)ix * NZ, *St = t0 + (size_t)ix * NZ;
+      F(hilbert_apply)(h, 30, S, sh, NZ);
+      F(hilbert_apply)(h, 30, R, rh, NZ);
+      F(hilbert_apply)(h, 30, St, sth, NZ);
+      for (int iz = 0; iz < NZ; iz++) {
+        size_t i = (size_t)ix * NZ + iz;
+        c4[0][i] += S[iz] * R[iz];
+        c4[1][i] += sh[iz] * rh[iz];
+        c4[3][i] += sth[iz] * R[iz];
+        c4[2][i] += St[iz] * rh[iz];
+      }
+    }
+    REAL *q = u2; u2 = u1; u1 = u0; u0 = q;
+    q = b2; b2 = b1; b1 = b0; b0 = q;
+    q = t2; t2 = t1; t1 = t0; t0 = q;
+  }
+  for (int ix = 0; ix < nx; ix++)
+    for (int iz = 0; iz < nz; iz++) {
+      size_t i = (size_t)(ix + pml) * NZ + (iz + pml);
+      img[(size_t)ix * nz + iz] = c4[0][i] - c4[1][i] + c4[3][i] + c4[2][i];
+      for (int k = 0; k < 4; k++) comp[((size_t)k * nx + ix) * nz + iz] = c4[k][i];
+    }
+  free(u0); free(u1); free(u2); free(t0); free(t1); free(t2); free(b0); free(b1); free(b2);
+  free(store); free(store_t); free(h); free(sh); free(rh); free(sth);
+  for (int k = 0; k < 4; k++) free(c4[k]);
+  F(coefs_free)(&c);
+  return 0;
+}
+
 /* adjointPlane, src/util/fd.cpp:787-921: RTM of the areal source sou[nx][NT]
  * at row sz with receivers at row gz.  The receiver field is propagated back
  * first, keeping its boundary layers per step, then re-propagated forward in

@@ -176,6 +176,37 @@ int ref_rtm_true(float dt, float dx, float dz, int nt, int ndel, int nx, int nz,
   return 0;
 }
 
+/* adjointUpDown (src/util/fd.cpp:340-591): rec [nx][nt]; img_out [nx][nz];
+ * comp_out [4][nx][nz] = the model part of its four accumulators imagX (zero
+ * on entry, the caller's allocation in the reference). */
+int ref_rtm_updown(float dt, float dx, float dz, int nt, int ndel, int nx, int nz, int pml, int sx,
+                   int sz, const int *gz, const float *wav, const float *wavh, const float *vel,
+                   const float *rec, float *img_out, float *comp_out) {
+  QuietCout q(g_verbose);
+  try {
+    const int NX = nx + 2 * pml, NZ = nz + 2 * pml;
+    float **v = to2d(vel, nz, nx);
+    float **r = to2d(rec, nt, nx);
+    float ***imgX = MyAlloc<float>::alc(NZ, NX, 4);
+    float **img = adjointUpDown(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, const_cast<int *>(gz),
+                                const_cast<float *>(wav), const_cast<float *>(wavh), v, r, r,
+                                imgX);
+    from2d(img_out, img, nz, nx);
+    for (int k = 0; k < 4; k++)
+      for (int ix = 0; ix < nx; ix++)
+        for (int iz = 0; iz < nz; iz++)
+          comp_out[((size_t)k * nx + ix) * nz + iz] = imgX[k][ix + pml][iz + pml];
+    MyAlloc<float>::free(img);
+    MyAlloc<float>::free(imgX);
+    MyAlloc<float>::free(v);
+    MyAlloc<float>::free(r);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return -1;
+  }
+  return 0;
+}
+
 /* harmonic (src/util/InitInversion.cpp:141-150): phase rotation of a trace by
  * kx x through the 201-tap Hilbert filter */
 int ref_harmonic(const float *in, float *out, int nt, float kx, float x) {

@@ -52,7 +52,7 @@ namespace {
 
 enum Op {
   OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2, OP_BORN_ADJ = 3, OP_ILLUM = 4, OP_BORN_PLANE = 5,
-  OP_RTM_PLANE = 6, OP_RTM_TRUE = 7
+  OP_RTM_PLANE = 6, OP_RTM_TRUE = 7, OP_RTM_UPDOWN = 8
 };
 
 int fail(seis_fd_ctx *ctx, int code, const char *fmt, ...) {
@@ -123,6 +123,11 @@ struct Plan {
   std::vector<float *> field_bases;  // allocation starts of margin-padded fields
   std::vector<size_t> field_elems;
   CUtensorMap *d_maps = nullptr;
+  // adjointUpDown: the shot table of the Hilbert-wavelet source field (its own
+  // field A buffers, wavelet, boundary layers and tensor maps)
+  std::vector<ShotDev> sd_h;
+  ShotDev *d_sd_h = nullptr;
+  CUtensorMap *d_maps_h = nullptr;
   bool exact = true;
   std::vector<void *> allocs;
   ShotDev *d_sd = nullptr;
@@ -321,12 +326,12 @@ int encode_map(seis_fd_ctx *ctx, const ShotDev &g, const float *cell0, int width
   return SEIS_OK;
 }
 
-int encode_maps(Plan &p) {
+int encode_maps(Plan &p, std::vector<ShotDev> &sds, CUtensorMap **d_out) {
   std::vector<CUtensorMap> maps((size_t)p.nshot * NMAPS);
   std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
   const int wide = TX + 2 * HXC, narrow = TX + 2;
   for (int s = 0; s < p.nshot; s++) {
-    const ShotDev &g = p.sd[s];
+    const ShotDev &g = sds[s];
     CUtensorMap *m = maps.data() + (size_t)s * NMAPS;
     int rc = SEIS_OK;
     for (int k = 0; k < 3 && !rc; k++) {
@@ -340,12 +345,41 @@ int encode_maps(Plan &p) {
     if (!rc && g.dv) rc = encode_map(p.ctx, g, g.dv, narrow, &m[MAP_DV]);
     if (rc) return rc;
   }
-  int rc = p.alloc(&p.d_maps, maps.size());
+  int rc = p.alloc(d_out, maps.size());
   if (rc) return rc;
   seis_fd_ctx *ctx = p.ctx;
-  CK(cudaMemcpyAsync(p.d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
+  CK(cudaMemcpyAsync(*d_out, maps.data(), maps.size() * sizeof(CUtensorMap),
                      cudaMemcpyHostToDevice, ctx->stream));
-  for (int s = 0; s < p.nshot; s++) p.sd[s].maps = p.d_maps + (size_t)s * NMAPS;
+  for (int s = 0; s < p.nshot; s++) sds[s].maps = *d_out + (size_t)s * NMAPS;
+  return SEIS_OK;
+}
+
+// adjointUpDown: the shot table of the Hilbert-wavelet source field, a copy of
+// the main table with its own field A, wavelet and boundary layers
+int make_hilbert_table(Plan &p) {
+  p.sd_h = p.sd;
+  for (int s = 0; s < p.nshot; s++) {
+    ShotDev &h = p.sd_h[s];
+    const seis_shot_desc &d = p.desc[s];
+    for (int k = 0; k < 3; k++) {
+      int rc = alloc_field(p, h, &h.fa[k]);
+      if (rc) return rc;
+    }
+    float *wav = nullptr, *strips = nullptr;
+    int rc = p.alloc(&wav, (size_t)h.NT);
+    if (!rc) rc = p.alloc(&strips, (size_t)d.nt * h.strip_len);
+    if (rc) return rc;
+    h.wav = wav;
+    h.strips = strips;
+    h.img = nullptr;
+    h.comp = nullptr;
+  }
+  int rc = encode_maps(p, p.sd_h, &p.d_maps_h);
+  if (!rc) rc = p.alloc(&p.d_sd_h, (size_t)p.nshot);
+  if (rc) return rc;
+  seis_fd_ctx *ctx = p.ctx;
+  CK(cudaMemcpyAsync(p.d_sd_h, p.sd_h.data(), sizeof(ShotDev) * p.nshot, cudaMemcpyHostToDevice,
+                     ctx->stream));
   return SEIS_OK;
 }
 
@@ -357,7 +391,8 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (rc) return rc;
     // the reference keeps 4 boundary layers (fd.cpp:594, :1181-1203); they
     // must stay inside the padded grid
-    if (op == OP_RTM && descs[i].pml + std::min(descs[i].nx, descs[i].nz) < LAYERS)
+    if ((op == OP_RTM || op == OP_RTM_TRUE || op == OP_RTM_UPDOWN || op == OP_RTM_PLANE) &&
+        descs[i].pml + std::min(descs[i].nx, descs[i].nz) < LAYERS)
       return fail(ctx, SEIS_ERR_ARG, "shot %d: RTM needs pml + min(nx, nz) >= %d", i, LAYERS);
     if (descs[i].nt != descs[0].nt || descs[i].ndel != descs[0].ndel || descs[i].dt != descs[0].dt)
       return fail(ctx, SEIS_ERR_ARG, "shot %d: nt, ndel and dt must match across a batch", i);
@@ -388,7 +423,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
       p->stage_elems = std::max(p->stage_elems, (size_t)d.nx * (d.nt + d.ndel));
     for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fa[k]);
     if (op == OP_BORN || op == OP_RTM || op == OP_BORN_PLANE || op == OP_RTM_PLANE ||
-        op == OP_RTM_TRUE)
+        op == OP_RTM_TRUE || op == OP_RTM_UPDOWN)
       for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fb[k]);
     if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.u3s[0]);
     if (rc == SEIS_OK && (op == OP_BORN || op == OP_BORN_PLANE)) rc = alloc_field(*p, g, &g.u3s[1]);
@@ -404,13 +439,14 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (rc == SEIS_OK) rc = p->alloc(&wav, (size_t)g.NT);
     if (rc == SEIS_OK) rc = p->alloc(&rec, (size_t)d.nt * d.nx);
     if (rc == SEIS_OK) rc = p->alloc(&gzd, (size_t)d.nx);
-    if (rc == SEIS_OK && (op == OP_RTM || op == OP_RTM_TRUE))
+    if (rc == SEIS_OK && (op == OP_RTM || op == OP_RTM_TRUE || op == OP_RTM_UPDOWN))
       rc = p->alloc(&g.strips, (size_t)d.nt * g.strip_len);
+    if (rc == SEIS_OK && op == OP_RTM_UPDOWN) rc = p->alloc(&g.comp, 4 * (size_t)d.nx * d.nz);
     g.rcv_dipole = op == OP_RTM_TRUE;
     if (rc == SEIS_OK && op == OP_RTM_PLANE)  // boundary layers of every step (fd.cpp:812-815)
       rc = p->alloc(&g.strips, (size_t)g.NT * g.strip_len);
     if (rc == SEIS_OK && (op == OP_RTM || op == OP_BORN_ADJ || op == OP_ILLUM || op == OP_RTM_PLANE ||
-                          op == OP_RTM_TRUE))
+                          op == OP_RTM_TRUE || op == OP_RTM_UPDOWN))
       rc = p->alloc(&g.img, (size_t)d.nx * d.nz);
     if (op == OP_ILLUM) g.illum = g.img;
     if (rc == SEIS_OK && op == OP_BORN_ADJ) rc = p->alloc(&g.grad, (size_t)d.nx * d.nz);
@@ -423,7 +459,8 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     }
   }
   if (rc == SEIS_OK) rc = p->alloc(&p->d_stage, p->stage_elems);
-  if (rc == SEIS_OK) rc = encode_maps(*p);
+  if (rc == SEIS_OK) rc = encode_maps(*p, p->sd, &p->d_maps);
+  if (rc == SEIS_OK && op == OP_RTM_UPDOWN) rc = make_hilbert_table(*p);
   if (rc == SEIS_OK) {
     build_tiles(*p);
     build_adj_tiles(*p);
@@ -433,6 +470,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
       int64_t per = (op == OP_MODEL || op == OP_ILLUM) ? g.NT
                   : (op == OP_BORN || op == OP_BORN_PLANE) ? 2LL * g.NT
                   : (op == OP_RTM || op == OP_RTM_TRUE) ? g.NT + 2LL * g.nt
+                  : op == OP_RTM_UPDOWN ? 2LL * g.NT + 3LL * g.nt
                   : op == OP_RTM_PLANE ? g.NT + 2LL * (g.NT - 2)
                                    : 2LL * g.NT + 1;
       p->cell_updates += (int64_t)g.NX * g.NZ * per;
@@ -442,7 +480,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
   if (rc == SEIS_OK) rc = p->alloc(&p->d_tiles, p->tiles.size());
   if (rc == SEIS_OK) rc = p->alloc(&p->d_adj_tiles, p->adj_tiles.size());
   if (rc == SEIS_OK) rc = p->alloc(&p->d_chunks, p->chunks.size());
-  const bool imaging = op == OP_RTM || op == OP_RTM_PLANE || op == OP_RTM_TRUE;
+  const bool imaging = op == OP_RTM || op == OP_RTM_PLANE || op == OP_RTM_TRUE || op == OP_RTM_UPDOWN;
   if (rc == SEIS_OK && imaging) rc = p->alloc(&p->d_cols, p->cols.size());
   if (rc == SEIS_OK && imaging) rc = p->alloc(&p->d_taps, (size_t)61);
   if (rc == SEIS_OK) {
@@ -482,15 +520,15 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
 
 // One time step of every shot: the interior-tile kernel on the main stream and
 // the pad-tile kernel on the auxiliary stream, joined before the next step.
-int step(Plan &p, int mode, const StepArgs &a) {
+int step(Plan &p, int mode, const StepArgs &a, const ShotDev *shots = nullptr) {
   seis_fd_ctx *ctx = p.ctx;
   CK(cudaEventRecord(ctx->fork, ctx->stream));
   CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
   StepArgs b = a;
   b.chunks = p.d_chunks;
   b.nchunks = (int)p.chunks.size();
-  CK(launch_step(mode, p.exact, p.d_sd, p.d_tiles, p.n_int, p.n_pad, ctx->num_sms, b, ctx->d_err,
-                 ctx->stream, ctx->aux));
+  CK(launch_step(mode, p.exact, shots ? shots : p.d_sd, p.d_tiles, p.n_int, p.n_pad, ctx->num_sms, b,
+                 ctx->d_err, ctx->stream, ctx->aux));
   CK(cudaEventRecord(ctx->join, ctx->aux));
   CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
   ctx->launches += (p.n_int > 0) + (p.n_pad > 0) + (p.n_pad > 0 && b.nchunks > 0);
@@ -567,11 +605,17 @@ int clear_fields(Plan &p) {
     }
     if (g.img) CK(cudaMemsetAsync(g.img, 0, sizeof(float) * g.nx * g.nz, ctx->stream));
     if (g.grad) CK(cudaMemsetAsync(g.grad, 0, sizeof(double) * g.nx * g.nz, ctx->stream));
+    if (g.comp) CK(cudaMemsetAsync(g.comp, 0, sizeof(float) * 4 * g.nx * g.nz, ctx->stream));
+  }
+  for (const ShotDev &g : p.sd_h) {
+    FieldGeom fg = field_geom(g.NX, g.NZ);
+    for (int k = 0; k < 3; k++)
+      CK(cudaMemsetAsync(g.fa[k] - fg.origin, 0, sizeof(float) * fg.elems, ctx->stream));
   }
   return SEIS_OK;
 }
 
-int run_forward(Plan &p, int mode) {
+int run_forward(Plan &p, int mode, const ShotDev *shots = nullptr) {
   StepArgs a{};
   a.nshots = p.nshot;
   for (int it = 0; it < p.NT; it++) {
@@ -579,12 +623,12 @@ int run_forward(Plan &p, int mode) {
     a.rot_b = it;
     a.src_k = it >= 1 ? it - 1 : -1;
     int itp = it - p.ndel;
-    const bool rtm = p.op == OP_RTM || p.op == OP_RTM_TRUE;
+    const bool rtm = p.op == OP_RTM || p.op == OP_RTM_TRUE || p.op == OP_RTM_UPDOWN;
     a.rec_k = (!rtm && p.op != OP_BORN_ADJ && p.op != OP_ILLUM && itp >= 0) ? itp : -1;
     a.illum_on = p.op == OP_ILLUM && it > p.ndel;  // fd.cpp:318
     a.strip_k = (rtm && itp >= 0) ? itp : -1;
     a.snap_k = p.op == OP_BORN_ADJ ? snap_slot(it, p.NT - 1, p.snap_every) : -1;
-    int rc = step(p, mode, a);
+    int rc = step(p, mode, a, shots);
     if (rc) return rc;
   }
   return SEIS_OK;
@@ -680,6 +724,43 @@ int run_rtm_plane(Plan &p) {
   return SEIS_OK;
 }
 
+// Reverse pass of adjointUpDown (fd.cpp:449-537): the source fields of the
+// wavelet and of its Hilbert transform reconstructed from their layers, the
+// receiver field back-propagated, four-component imaging every step.
+int run_updown_reverse(Plan &p) {
+  seis_fd_ctx *ctx = p.ctx;
+  for (const std::vector<ShotDev> *v : {&p.sd, &p.sd_h})
+    for (const ShotDev &g : *v) {
+      FieldGeom fg = field_geom(g.NX, g.NZ);
+      for (int k = 0; k < 3; k++)
+        CK(cudaMemsetAsync(g.fa[k] - fg.origin, 0, sizeof(float) * fg.elems, ctx->stream));
+    }
+  int k = 0;
+  for (int it = p.NT - 1; it >= p.ndel; it--, k++) {
+    for (const ShotDev *tab : {p.d_sd, p.d_sd_h}) {
+      CK(launch_rtm_restore(tab, p.nshot, p.max_strip, k, it, ctx->stream));
+      ctx->launches++;
+      StepArgs a{};
+      a.nshots = p.nshot;
+      a.rot = k;
+      int rc = step(p, MODE_MODEL, a, tab);
+      if (rc) return rc;
+    }
+    StepArgs r{};
+    r.nshots = p.nshot;
+    r.rot_b = k;
+    r.rec_k = it - p.ndel;
+    int rc = step(p, MODE_RCV, r);
+    if (rc) return rc;
+    CK(launch_updown_image(p.d_sd, p.d_sd_h, p.d_cols, (int)p.cols.size(), k, k, p.max_NZ,
+                           p.d_taps, ctx->stream));
+    ctx->launches++;
+  }
+  CK(launch_updown_finalize(p.d_sd, p.nshot, ctx->stream));
+  ctx->launches++;
+  return SEIS_OK;
+}
+
 // Forward pass of the background field keeping the source-term snapshots
 // (adjoint plans); reused by every later run until the velocity or the
 // wavelet changes.
@@ -739,6 +820,10 @@ int enqueue_operator(Plan &p) {
     case OP_RTM_TRUE:
       rc = run_forward(p, MODE_MODEL);
       return rc ? rc : run_rtm_reverse(p);
+    case OP_RTM_UPDOWN:
+      rc = run_forward(p, MODE_MODEL);
+      if (!rc) rc = run_forward(p, MODE_MODEL, p.d_sd_h);
+      return rc ? rc : run_updown_reverse(p);
   }
   return fail(p.ctx, SEIS_ERR_NOTSUP, "unknown operator %d", p.op);
 }
@@ -914,7 +999,7 @@ int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_des
   if (rc) return rc;
   if (!out) return fail(ctx, SEIS_ERR_ARG, "out is null");
   *out = nullptr;
-  if (op < SEIS_OP_MODELING || op > SEIS_OP_RTM_TRUE) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
+  if (op < SEIS_OP_MODELING || op > SEIS_OP_RTM_UPDOWN) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
   Plan *p = nullptr;
   rc = plan_create(ctx, op, nshot, shots, &p);
   if (rc) return rc;
@@ -953,7 +1038,8 @@ static int plan_input(seis_fd_plan *plan, int shot, int what, const float *src, 
   const seis_shot_desc &d = p.desc[shot];
   ShotDev &g = p.sd[shot];
   cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  if (what == SEIS_IN_VEL || what == SEIS_IN_WAVELET) p.snaps_valid = false;
+  if (what == SEIS_IN_VEL || what == SEIS_IN_WAVELET || what == SEIS_IN_WAVELET_H)
+    p.snaps_valid = false;
   switch (what) {
     case SEIS_IN_VEL:
     case SEIS_IN_DV: {
@@ -967,6 +1053,11 @@ static int plan_input(seis_fd_plan *plan, int shot, int what, const float *src, 
     case SEIS_IN_WAVELET:
       CK(cudaMemcpyAsync(const_cast<float *>(g.wav), src, sizeof(float) * g.NT, kind, ctx->stream));
       return SEIS_OK;
+    case SEIS_IN_WAVELET_H:
+      if (p.sd_h.empty()) return fail(ctx, SEIS_ERR_NOTSUP, "plan takes no Hilbert wavelet");
+      CK(cudaMemcpyAsync(const_cast<float *>(p.sd_h[shot].wav), src, sizeof(float) * g.NT, kind,
+                         ctx->stream));
+      return SEIS_OK;
     case SEIS_IN_SOURCE:
       if (!g.sou) return fail(ctx, SEIS_ERR_NOTSUP, "plan takes no areal source");
       CK(cudaMemcpyAsync(p.d_stage, src, sizeof(float) * d.nx * g.NT, kind, ctx->stream));
@@ -974,7 +1065,8 @@ static int plan_input(seis_fd_plan *plan, int shot, int what, const float *src, 
       ctx->launches++;
       return SEIS_OK;
     case SEIS_IN_GATHER:
-      if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_RTM_PLANE && p.op != OP_RTM_TRUE)
+      if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_RTM_PLANE && p.op != OP_RTM_TRUE &&
+          p.op != OP_RTM_UPDOWN)
         return fail(ctx, SEIS_ERR_NOTSUP, "plan takes no gather input");
       CK(cudaMemcpyAsync(p.d_stage, src, sizeof(float) * d.nt * d.nx, kind, ctx->stream));
       CK(launch_transpose(p.d_stage, d.nx, d.nt, g.rec, ctx->stream));
@@ -1008,15 +1100,20 @@ int seis_fd_plan_get(seis_fd_plan *plan, int shot, int what, float *h_dst) {
   if (!h_dst) return fail(ctx, SEIS_ERR_ARG, "null destination");
   if (what == SEIS_OUT_GATHER) {
     if (p.op == OP_RTM || p.op == OP_BORN_ADJ || p.op == OP_ILLUM || p.op == OP_RTM_PLANE ||
-        p.op == OP_RTM_TRUE)
+        p.op == OP_RTM_TRUE || p.op == OP_RTM_UPDOWN)
       return fail(ctx, SEIS_ERR_NOTSUP, "this plan outputs images");
     rc = download_gather(p, shot, h_dst);
   } else if (what == SEIS_OUT_IMAGE) {
     if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_ILLUM && p.op != OP_RTM_PLANE &&
-        p.op != OP_RTM_TRUE)
+        p.op != OP_RTM_TRUE && p.op != OP_RTM_UPDOWN)
       return fail(ctx, SEIS_ERR_NOTSUP, "plan outputs gathers");
     const seis_shot_desc &d = p.desc[shot];
     CK(cudaMemcpyAsync(h_dst, p.sd[shot].img, sizeof(float) * d.nx * d.nz,
+                       cudaMemcpyDeviceToHost, ctx->stream));
+  } else if (what == SEIS_OUT_COMPONENTS) {
+    if (!p.sd[shot].comp) return fail(ctx, SEIS_ERR_NOTSUP, "plan has no imaging components");
+    const seis_shot_desc &d = p.desc[shot];
+    CK(cudaMemcpyAsync(h_dst, p.sd[shot].comp, sizeof(float) * 4 * d.nx * d.nz,
                        cudaMemcpyDeviceToHost, ctx->stream));
   } else {
     return fail(ctx, SEIS_ERR_ARG, "unknown output %d", what);
@@ -1205,6 +1302,29 @@ int seis_fd_rtm_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float 
   d.sx = d.nx / 2;  // the areal source has no point position
   return run_batch(ctx, OP_RTM_PLANE, 1, &d, &h_sou, SEIS_IN_SOURCE, &h_vel, SEIS_IN_VEL,
                    &h_rec, SEIS_IN_GATHER, &h_img, SEIS_OUT_IMAGE);
+}
+
+int seis_fd_rtm_updown(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,
+                       const float *h_wavh, const float *h_vel, const float *h_rec, float *h_img,
+                       float *h_comp) {
+  int rc = begin(ctx);
+  if (rc) return rc;
+  if (!h_wav || !h_wavh || !h_vel || !h_rec || !h_img) return fail(ctx, SEIS_ERR_ARG, "null array");
+  Plan *p = nullptr;
+  rc = plan_create(ctx, OP_RTM_UPDOWN, 1, shot, &p);
+  if (rc) return rc;
+  seis_fd_plan h{p};
+  rc = plan_input(&h, 0, SEIS_IN_WAVELET, h_wav, false);
+  if (!rc) rc = plan_input(&h, 0, SEIS_IN_WAVELET_H, h_wavh, false);
+  if (!rc) rc = plan_input(&h, 0, SEIS_IN_VEL, h_vel, false);
+  if (!rc) rc = plan_input(&h, 0, SEIS_IN_GATHER, h_rec, false);
+  if (!rc) rc = enqueue_operator(*p);
+  if (!rc) rc = seis_fd_plan_get(&h, 0, SEIS_OUT_IMAGE, h_img);
+  if (!rc && h_comp) rc = seis_fd_plan_get(&h, 0, SEIS_OUT_COMPONENTS, h_comp);
+  if (!rc) rc = sync(ctx);
+  cudaStreamSynchronize(ctx->stream);
+  delete p;
+  return rc;
 }
 
 int seis_fd_rtm_true(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,

@@ -95,6 +95,7 @@ struct ShotDev {
   float *u3s[2];
   float *illum;          // source illumination [nx][nz] (illumination plans)
   const float *sou;      // areal source [NT][nx] at row szp (plane-wave plans), else null
+  float *comp;           // four imaging accumulators [4][nx][nz] (adjointUpDown)
   int rcv_dipole;        // receiver injection as a vertical dipole (rtm_true)
   int pad2_;
 };
@@ -193,6 +194,10 @@ cudaError_t launch_rtm_restore(const ShotDev *d_shots, int nshots, int max_strip
 cudaError_t launch_rtm_image(const ShotDev *d_shots, const int2 *d_cols, int ncols, int rot,
                              int rot_b, int max_nz, const float *d_taps, cudaStream_t s,
                              int mode = 0);
+cudaError_t launch_updown_image(const ShotDev *d_shots, const ShotDev *d_shots_h,
+                                const int2 *d_cols, int ncols, int rot, int rot_b, int max_nz,
+                                const float *d_taps, cudaStream_t s);
+cudaError_t launch_updown_finalize(const ShotDev *d_shots, int nshots, cudaStream_t s);
 cudaError_t launch_plane_rcv_prep(const ShotDev *d_shots, int nshots, int max_strip, int rot_b,
                                   int strip_k, int rec_k, cudaStream_t s);
 

@@ -173,6 +173,60 @@ __global__ void rtm_image_kernel(const ShotDev *__restrict__ shots, const int2 *
   }
 }
 
+// adjointUpDown imaging (fd.cpp:501-521), one CTA per interior column: with
+// S the source field of the wavelet, St that of its Hilbert transform (the
+// shadow shot table) and R the receiver field, each with its 61-tap z-Hilbert
+// transform over the padded column,
+//   comp0 += S R, comp1 += H[S] H[R], comp2 += St H[R], comp3 += H[St] R.
+__global__ void updown_image_kernel(const ShotDev *__restrict__ shots,
+                                    const ShotDev *__restrict__ shots_h,
+                                    const int2 *__restrict__ cols, int rot, int rot_b,
+                                    const float *__restrict__ taps) {
+  extern __shared__ float sh[];
+  const int2 c = cols[blockIdx.x];
+  const ShotDev &g = shots[c.x];
+  const ShotDev &gh = shots_h[c.x];
+  const int ix = c.y + g.pml, NZ = g.NZ;
+  float *sS = sh, *sR = sh + NZ, *sT = sh + 2 * NZ;
+  __shared__ float h[2 * HILB_HALF + 1];
+  if (threadIdx.x < 2 * HILB_HALF + 1) h[threadIdx.x] = taps[threadIdx.x];
+  const size_t col = (size_t)ix * g.LDZ;
+  const float *S = g.fa[(rot + 2) % 3] + col, *T = gh.fa[(rot + 2) % 3] + col;
+  const float *R = g.fb[(rot_b + 2) % 3] + col;
+  for (int iz = threadIdx.x; iz < NZ; iz += blockDim.x) {
+    sS[iz] = S[iz];
+    sR[iz] = R[iz];
+    sT[iz] = T[iz];
+  }
+  __syncthreads();
+  const size_t plane = (size_t)g.nx * g.nz;
+  for (int iz = g.pml + threadIdx.x; iz < NZ - g.pml; iz += blockDim.x) {
+    const int i0 = max(iz - HILB_HALF, 0), i1 = min(iz + HILB_HALF, NZ - 1);
+    float hs = 0.0f, hr = 0.0f, ht = 0.0f;
+    const int start = i0 + (((iz - i0) & 1) ? 0 : 1);  // odd offsets: even taps are zero
+    for (int i = start; i <= i1; i += 2) {
+      const float hk = h[iz - i + HILB_HALF];
+      hs = hs + sS[i] * hk;
+      hr = hr + sR[i] * hk;
+      ht = ht + sT[i] * hk;
+    }
+    float *cp = g.comp + (size_t)c.y * g.nz + (iz - g.pml);
+    cp[0] = cp[0] + sS[iz] * sR[iz];
+    cp[plane] = cp[plane] + hs * hr;
+    cp[2 * plane] = cp[2 * plane] + sT[iz] * hr;
+    cp[3 * plane] = cp[3 * plane] + ht * sR[iz];
+  }
+}
+
+// img = comp0 - comp1 + comp3 + comp2 (fd.cpp:538-547)
+__global__ void updown_finalize_kernel(const ShotDev *__restrict__ shots) {
+  const ShotDev &g = shots[blockIdx.y];
+  const size_t n = (size_t)g.nx * g.nz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    g.img[i] = g.comp[i] - g.comp[n + i] + g.comp[3 * n + i] + g.comp[2 * n + i];
+}
+
 // Exact adjoint, last step: img = vt2 vel3 grad on the model interior (the
 // scattering source is vt2 lap vel3 dv, fd.cpp:138-139; dv is zero-padded).
 __global__ void finalize_image_kernel(const ShotDev *__restrict__ shots) {
@@ -236,7 +290,31 @@ cudaError_t launch_rtm_image(const ShotDev *d_shots, const int2 *d_cols, int nco
                              int rot_b, int max_nz, const float *d_taps, cudaStream_t s,
                              int mode) {
   size_t smem = 2 * (size_t)max_nz * sizeof(float);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(rtm_image_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
   rtm_image_kernel<<<ncols, 256, smem, s>>>(d_shots, d_cols, rot, rot_b, d_taps, mode);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_updown_image(const ShotDev *d_shots, const ShotDev *d_shots_h,
+                                const int2 *d_cols, int ncols, int rot, int rot_b, int max_nz,
+                                const float *d_taps, cudaStream_t s) {
+  size_t smem = 3 * (size_t)max_nz * sizeof(float);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(updown_image_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  updown_image_kernel<<<ncols, 256, smem, s>>>(d_shots, d_shots_h, d_cols, rot, rot_b, d_taps);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_updown_finalize(const ShotDev *d_shots, int nshots, cudaStream_t s) {
+  dim3 grid(64, nshots);
+  updown_finalize_kernel<<<grid, 256, 0, s>>>(d_shots);
   return cudaGetLastError();
 }
 

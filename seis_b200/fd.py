@@ -72,6 +72,28 @@ def rtm_true(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, rec, ctx: 
     return img
 
 
+def rtm_updown(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, wavh, vel, rec,
+               ctx: Context = None):
+    """Image ``img[nx][nz]`` and components ``comp[4][nx][nz]`` of the reference
+    ``adjointUpDown`` (src/util/fd.cpp:340-590).  ``wavh`` is the Hilbert transform
+    of ``wav`` (the reference's caller filters the first nt samples with 100
+    half-taps, src/lsrtm/lsrtm.cpp:97-99; see ``hilbert``); comp = (S R, H[S] H[R],
+    St H[R], H[St] R) summed over the reverse pass (the model cells of the
+    reference's padded imagX) and img = comp0 - comp1 + comp3 + comp2."""
+    ctx = ctx or default_context()
+    s = _shot(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz)
+    wav = _f32(wav, (s.NT,))
+    wavh = _f32(wavh, (s.NT,))
+    vel = _f32(vel, (nx, nz))
+    rec = _f32(rec, (nx, nt))
+    img = np.zeros((nx, nz), np.float32)
+    comp = np.zeros((4, nx, nz), np.float32)
+    d = s.to_c()
+    ctx.check(ctx.L.seis_fd_rtm_updown(ctx.h, d, ptr(wav), ptr(wavh), ptr(vel), ptr(rec),
+                                       ptr(img), ptr(comp)))
+    return img, comp
+
+
 def adjoint_plane(dt, dx, dz, nt, ndel, nx, nz, pml, sz, gz, vel, sou, rec, ctx: Context = None):
     """Image ``img[nx][nz]`` of the areal source ``sou[nx][nt+ndel]`` and the gather
     ``rec[nx][nt]`` at row gz (reference ``adjointPlane``, src/util/fd.cpp:787-921)."""

@@ -104,3 +104,16 @@ def test_rtm_true_restatement_matches_reference(g):
     """rtm_true (src/util/fd.cpp:924-1052): the C restatement bit for bit."""
     assert np.array_equal(O.rtm_true(g.shot, g.wav, g.vel, g.rec),
                           O.rtm_true(g.shot, g.wav, g.vel, g.rec, impl="ref"))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("g", CASES[:2], ids=golden_ids()[:2])
+def test_rtm_updown_restatement_matches_reference(g):
+    """adjointUpDown (src/util/fd.cpp:340-590): image and all four components
+    of the C restatement bit for bit."""
+    wavh = O.hilbert(g.wav, 30)
+    img, comp = O.rtm_updown(g.shot, g.wav, wavh, g.vel, g.rec)
+    rimg, rcomp = O.rtm_updown(g.shot, g.wav, wavh, g.vel, g.rec, impl="ref")
+    assert np.array_equal(img, rimg)
+    assert np.array_equal(comp, rcomp)
+    assert np.abs(comp).max(axis=(1, 2)).min() > 0
