@@ -98,6 +98,10 @@ struct ShotDev {
   float *comp;           // four imaging accumulators [4][nx][nz] (adjointUpDown)
   int rcv_dipole;        // receiver injection as a vertical dipole (rtm_true)
   int pad2_;
+  // exact adjoint, pad cells (NX x LDZ each): (1 - w) L of the ring cells of
+  // the current step; the ring terms of the next step; the prev-ring terms
+  // kept for the step after it
+  float *adj_rho, *adj_e, *adj_b;
 };
 enum SnapType : int { SNAP_NONE = 0, SNAP_F32 = 1, SNAP_BF16 = 2, SNAP_F16 = 3 };
 static_assert(sizeof(ShotDev) % sizeof(int) == 0 && sizeof(ShotDev) <= 256 * sizeof(int),
@@ -162,7 +166,8 @@ cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, i
                         int n_pad, int num_sms, const StepArgs &a, int *d_err, cudaStream_t s_int,
                         cudaStream_t s_pad);
 cudaError_t configure();
-// one reverse step of the exact Born adjoint over the adjoint tile list
+// one reverse step of the exact Born adjoint over the adjoint tile list; with
+// pad tiles, the ring kernel over the pad cells a.chunks follows on s_pad
 cudaError_t launch_adjoint(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
                            const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad);
 cudaError_t configure_adjoint();
