@@ -92,6 +92,12 @@ int seis_driver_plane_prepare(seis_driver *d);
  * when mask = 1) written to wdir IMAGE<k>.dat and summed into h_img [nx][nz]. */
 int seis_driver_rtm_plane(seis_driver *d, int born_data, float *h_img);
 
+/* illumPlane_MPI (inversion.cpp:291-345): for each wavenumber k < np, the
+ * illumination of PLANE_S_NEW<k>.dat over the whole v0file model (source row
+ * from shot 0's depth), written to wdir ILLUM_PLANE<k>.dat ([nx][nz]); h_ss
+ * (may be NULL) receives their sum. */
+int seis_driver_illum_plane(seis_driver *d, float *h_ss);
+
 /* Least-squares RTM by CGLS over all shots: L = Born on each aperture
  * sub-grid, L^T its exact adjoint scattered back through the transpose of the
  * sub-grid extraction; observed data from precsg<is>.dat or BORN<is>.dat

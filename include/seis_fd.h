@@ -123,6 +123,12 @@ int seis_fd_illum_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots
 int seis_fd_born_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_sou,
                        const float *h_vel, const float *h_dv, float *h_rec);
 
+/* illumPlane (src/util/fd.cpp:720-786): seis_fd_illum with the areal source
+ * h_sou[nx][nt+ndel] at row shot->sz of every model column (shot->sx and
+ * shot->gz are not used).  h_ss[nx][nz]. */
+int seis_fd_illum_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_sou,
+                        const float *h_vel, float *h_ss);
+
 /* rtm_true (src/util/fd.cpp:924-1052): seis_fd_rtm with the receivers injected
  * as vertical dipoles (-rec vt2/dz at row gz, +rec vt2/dz at row gz + 1) and
  * the image FaQi(S vel3, R) of the reconstructed source field S itself. */
@@ -172,6 +178,8 @@ int seis_fd_rtm_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float 
                                 receiver injection and source-field imaging */
 #define SEIS_OP_RTM_UPDOWN 8 /* adjointUpDown (fd.cpp:340-590): four-component
                                 RTM with a Hilbert-wavelet source field      */
+#define SEIS_OP_ILLUM_PLANE 9 /* illumPlane (fd.cpp:720-786): source, velocity
+                                 -> image [nx][nz]                           */
 
 #define SEIS_IN_VEL 0      /* [nx][nz] velocity of the shot's model         */
 #define SEIS_IN_DV 1       /* [nx][nz] velocity perturbation (SEIS_OP_BORN) */

@@ -232,6 +232,24 @@ def illum(shot, wav, vel, prec="f32", impl="oracle"):
     return ss
 
 
+def illum_plane(shot, sou, vel, prec="f32", impl="oracle"):
+    """Illumination [nx][nz] of ``illumPlane`` (src/util/fd.cpp:720-786): areal
+    source sou [nx][nt+ndel] at row shot.sz."""
+    dt, (_, sou, vel) = _prep(shot, prec, impl, sou, vel)
+    ss = np.zeros((shot.nx, shot.nz), dt)
+    R = _real(prec) if impl != "ref" else ctypes.c_float
+    s = shot
+    args = [R(s.dt), R(s.dx), R(s.dz), _I(s.nt), _I(s.ndel), _I(s.nx), _I(s.nz), _I(s.pml),
+            _I(s.sz)]
+    if impl == "ref":
+        rc = ref_lib().ref_illum_plane(*args, _ptr(sou), _ptr(vel), _ptr(ss))
+    else:
+        rc = getattr(oracle_lib(), f"orc_illum_plane_{prec}")(*args, _ptr(sou), _ptr(vel), _ptr(ss))
+    if rc != 0:
+        raise RuntimeError(f"oracle illum_plane failed ({rc})")
+    return ss
+
+
 def born(shot, wav, vel, dv, prec="f32", impl="oracle"):
     """Scattered gather [nx][nt] of ``forward`` (src/util/fd.cpp:81-177)."""
     dt, (gz, wav, vel, dv) = _prep(shot, prec, impl, wav, vel, dv)

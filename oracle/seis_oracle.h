@@ -48,6 +48,8 @@ extern "C" {
                          R *comp);                                               \
   int orc_illum_##S(R dt, R dx, R dz, int nt, int ndel, int nx, int nz, int pml, \
                     int sx, int sz, const R *wav, const R *vel, R *ss);         \
+  int orc_illum_plane_##S(R dt, R dx, R dz, int nt, int ndel, int nx, int nz,   \
+                          int pml, int sz, const R *sou, const R *vel, R *ss);  \
   int orc_born_adjoint_##S(R dt, R dx, R dz, int nt, int ndel, int nx, int nz,  \
                            int pml, int sx, int sz, const int *gz,              \
                            const R *wav, const R *vel, const R *rec, R *img);   \

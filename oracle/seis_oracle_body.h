@@ -353,8 +353,12 @@ int F(orc_modeling)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz,
 
 /* illum, src/util/fd.cpp:275-339: ss[nx][nz] = sum over it > ndel of the
  * blended source field squared, accumulated in REAL step by step. */
-int F(orc_illum)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml, int sx,
-                 int sz, const REAL *wav, const REAL *vel, REAL *ss)
+/* illum (point source wav at (sx, sz)) and illumPlane (sou != NULL: the areal
+ * source sou[ix][it] at every model column of row sz), src/util/fd.cpp:275-339,
+ * :720-786: the sum of the squared blended field over steps it > ndel. */
+static int F(illum_core)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml,
+                         int sx, int sz, const REAL *wav, const REAL *sou, const REAL *vel,
+                         REAL *ss)
 {
   F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
   const F(grid_t) *g = &gg;
@@ -366,9 +370,16 @@ int F(orc_illum)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, in
   for (size_t i = 0; i < (size_t)nx * nz; i++) ss[i] = KR(0);
   for (int it = 0; it < NT; it++) {
     F(twoway)(g, &c, u1, u0, u2);
-    if (it >= 1) AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+    if (it >= 1) {
+      if (sou) {  /* fd.cpp:754-757 */
+        for (int ix = 0; ix < nx; ix++)
+          AT(u2, ix + pml, szp) += AT(c.vt2, ix + pml, szp) * sou[(size_t)ix * NT + it - 1];
+      } else {
+        AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+      }
+    }
     F(absorb)(g, &c, u2, u1, u0);
-    if (it > ndel)  /* fd.cpp:318 */
+    if (it > ndel)  /* fd.cpp:318, :763 */
       for (int ix = 0; ix < nx; ix++)
         for (int iz = 0; iz < nz; iz++) {
           REAL u = AT(u2, ix + pml, iz + pml);
@@ -379,6 +390,18 @@ int F(orc_illum)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, in
   free(u0); free(u1); free(u2);
   F(coefs_free)(&c);
   return 0;
+}
+
+int F(orc_illum)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml, int sx,
+                 int sz, const REAL *wav, const REAL *vel, REAL *ss)
+{
+  return F(illum_core)(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, wav, NULL, vel, ss);
+}
+
+int F(orc_illum_plane)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml,
+                       int sz, const REAL *sou, const REAL *vel, REAL *ss)
+{
+  return F(illum_core)(dt, dx, dz, nt, ndel, nx, nz, pml, 0, sz, NULL, sou, vel, ss);
 }
 
 /* forward (Born), src/util/fd.cpp:81-177.  Scattering source

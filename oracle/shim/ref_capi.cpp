@@ -236,6 +236,26 @@ int ref_illum(float dt, float dx, float dz, int nt, int ndel, int nx, int nz, in
   return 0;
 }
 
+/* illumPlane (src/util/fd.cpp:720-786): sou [nx][nt+ndel] at row sz; gz is
+ * not used by the reference body.  ss_out [nx][nz] */
+int ref_illum_plane(float dt, float dx, float dz, int nt, int ndel, int nx, int nz, int pml,
+                    int sz, const float *sou, const float *vel, float *ss_out) {
+  QuietCout q(g_verbose);
+  try {
+    float **v = to2d(vel, nz, nx);
+    float **so = to2d(sou, nt + ndel, nx);
+    float **ss = illumPlane(dt, dx, dz, nt, ndel, nx, nz, pml, sz, 0, v, so);
+    from2d(ss_out, ss, nz, nx);
+    MyAlloc<float>::free(ss);
+    MyAlloc<float>::free(so);
+    MyAlloc<float>::free(v);
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return -1;
+  }
+  return 0;
+}
+
 /* forward, Born modeling (src/util/fd.cpp:81-177): rec_out [nx][nt] */
 int ref_born(float dt, float dx, float dz, int nt, int ndel, int nx, int nz,
              int pml, int sx, int sz, const int *gz, const float *wav,

@@ -123,6 +123,7 @@ def lib():
         L.seis_fd_rtm_plane.argtypes = [P, SD, P, P, P, P]
         L.seis_fd_rtm_true.argtypes = [P, SD, P, P, P, P]
         L.seis_fd_rtm_updown.argtypes = [P, SD, P, P, P, P, P, P]
+        L.seis_fd_illum_plane.argtypes = [P, SD, P, P, P]
         L.seis_fd_hilbert.argtypes = [P, P, I, I]
         L.seis_fd_illum_batch.argtypes = [P, I, SD, PP, PP, PP]
         L.seis_fd_vec_dot.argtypes = [P, P, P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)]
@@ -215,7 +216,7 @@ def validate_shot(shot: "Shot") -> str:
 
 
 (OP_MODELING, OP_BORN, OP_RTM, OP_BORN_ADJOINT, OP_ILLUM, OP_BORN_PLANE, OP_RTM_PLANE,
- OP_RTM_TRUE, OP_RTM_UPDOWN) = range(9)
+ OP_RTM_TRUE, OP_RTM_UPDOWN, OP_ILLUM_PLANE) = range(10)
 SNAP_F32, SNAP_BF16, SNAP_F16 = 1, 2, 3
 IN_VEL, IN_DV, IN_WAVELET, IN_GATHER, IN_SOURCE, IN_WAVELET_H = 0, 1, 2, 3, 4, 5
 OUT_GATHER, OUT_IMAGE, OUT_COMPONENTS = 0, 1, 2

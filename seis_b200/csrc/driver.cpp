@@ -726,6 +726,34 @@ int seis_driver_rtm_plane(seis_driver *d, int born_data, float *h_img) {
   return SEIS_OK;
 }
 
+int seis_driver_illum_plane(seis_driver *d, float *h_ss) {
+  if (!d) return SEIS_ERR_ARG;
+  if (!d->ctx) return dfail(d, SEIS_ERR_STATE, "driver created without a device context");
+  const seis_params &p = d->p;
+  int rc = SEIS_OK;
+  const std::vector<float> v0 = load_model(d, p.v0file, &rc);
+  if (rc) return rc;
+  const size_t nm = (size_t)p.nx * p.nz;
+  const int NT = p.nt + p.delaycal;
+  if (h_ss) std::memset(h_ss, 0, sizeof(float) * nm);
+  const int sz = (int)((d->sc[1] - 0.0f) / p.dz + 0.0001f);  // inversion.cpp:331
+  std::vector<int> gzs((size_t)p.nx, 0);
+  seis_shot_desc desc{p.nx, p.nz, p.npml, p.nt, p.delaycal, p.nx / 2, sz,
+                      p.dt, p.dx, p.dz, gzs.data()};
+  std::vector<float> sou((size_t)p.nx * NT), ss(nm);
+  for (int k = 0; k < p.np; k++) {
+    const std::string sn = std::string(p.wdir) + "PLANE_S_NEW" + std::to_string(k) + ".dat";
+    if (!read_file(sn, sou.data(), sou.size())) return dfail(d, SEIS_ERR_ARG, "cannot read %s", sn.c_str());
+    int r = seis_fd_illum_plane(d->ctx, &desc, sou.data(), v0.data(), ss.data());
+    if (r) return dfail(d, r, "illum_plane: %s", seis_fd_last_error(d->ctx));
+    const std::string on = std::string(p.wdir) + "ILLUM_PLANE" + std::to_string(k) + ".dat";
+    if (!write_file(on, ss.data(), nm)) return dfail(d, SEIS_ERR_ARG, "cannot write %s", on.c_str());
+    if (h_ss)
+      for (size_t i = 0; i < nm; i++) h_ss[i] = ss[i] + h_ss[i];
+  }
+  return SEIS_OK;
+}
+
 int seis_driver_lsrtm(seis_driver *d, int born_data, int niter, const seis_lsrtm_opts *opts,
                       float *h_img, double *h_rr) {
   if (!d || !h_img || niter < 0) return SEIS_ERR_ARG;

@@ -52,7 +52,7 @@ namespace {
 
 enum Op {
   OP_MODEL = 0, OP_BORN = 1, OP_RTM = 2, OP_BORN_ADJ = 3, OP_ILLUM = 4, OP_BORN_PLANE = 5,
-  OP_RTM_PLANE = 6, OP_RTM_TRUE = 7, OP_RTM_UPDOWN = 8
+  OP_RTM_PLANE = 6, OP_RTM_TRUE = 7, OP_RTM_UPDOWN = 8, OP_ILLUM_PLANE = 9
 };
 
 int fail(seis_fd_ctx *ctx, int code, const char *fmt, ...) {
@@ -445,7 +445,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     p->max_strip = std::max(p->max_strip, g.strip_len);
     p->max_NZ = std::max(p->max_NZ, g.NZ);
     p->stage_elems = std::max(p->stage_elems, std::max((size_t)d.nx * d.nz, (size_t)d.nx * d.nt));
-    if (op == OP_BORN_PLANE || op == OP_RTM_PLANE)
+    if (op == OP_BORN_PLANE || op == OP_RTM_PLANE || op == OP_ILLUM_PLANE)
       p->stage_elems = std::max(p->stage_elems, (size_t)d.nx * (d.nt + d.ndel));
     for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fa[k]);
     if (op == OP_BORN || op == OP_RTM || op == OP_BORN_PLANE || op == OP_RTM_PLANE ||
@@ -457,7 +457,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     int *gzd = nullptr;
     if (rc == SEIS_OK) rc = alloc_field(*p, g, &vel);
     if (rc == SEIS_OK && (op == OP_BORN || op == OP_BORN_PLANE)) rc = alloc_field(*p, g, &dv);
-    if (rc == SEIS_OK && (op == OP_BORN_PLANE || op == OP_RTM_PLANE)) {
+    if (rc == SEIS_OK && (op == OP_BORN_PLANE || op == OP_RTM_PLANE || op == OP_ILLUM_PLANE)) {
       float *sou = nullptr;
       rc = p->alloc(&sou, (size_t)g.NT * d.nx);
       g.sou = sou;
@@ -472,9 +472,9 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (rc == SEIS_OK && op == OP_RTM_PLANE)  // boundary layers of every step (fd.cpp:812-815)
       rc = p->alloc(&g.strips, (size_t)g.NT * g.strip_len);
     if (rc == SEIS_OK && (op == OP_RTM || op == OP_BORN_ADJ || op == OP_ILLUM || op == OP_RTM_PLANE ||
-                          op == OP_RTM_TRUE || op == OP_RTM_UPDOWN))
+                          op == OP_RTM_TRUE || op == OP_RTM_UPDOWN || op == OP_ILLUM_PLANE))
       rc = p->alloc(&g.img, (size_t)d.nx * d.nz);
-    if (op == OP_ILLUM) g.illum = g.img;
+    if (op == OP_ILLUM || op == OP_ILLUM_PLANE) g.illum = g.img;
     if (rc == SEIS_OK && op == OP_BORN_ADJ) rc = p->alloc(&g.grad, (size_t)d.nx * d.nz);
     if (op == OP_BORN_ADJ) {
       if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_rho);
@@ -498,7 +498,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     // padded cell-updates of one run: modeling NT, Born 2 NT, reference RTM
     // NT + 2 nt, exact adjoint NT (source pass) + NT + 1 (reverse pass)
     for (const ShotDev &g : p->sd) {
-      int64_t per = (op == OP_MODEL || op == OP_ILLUM) ? g.NT
+      int64_t per = (op == OP_MODEL || op == OP_ILLUM || op == OP_ILLUM_PLANE) ? g.NT
                   : (op == OP_BORN || op == OP_BORN_PLANE) ? 2LL * g.NT
                   : (op == OP_RTM || op == OP_RTM_TRUE) ? g.NT + 2LL * g.nt
                   : op == OP_RTM_UPDOWN ? 2LL * g.NT + 3LL * g.nt
@@ -662,8 +662,9 @@ int run_forward(Plan &p, int mode, const ShotDev *shots = nullptr) {
     a.src_k = it >= 1 ? it - 1 : -1;
     int itp = it - p.ndel;
     const bool rtm = p.op == OP_RTM || p.op == OP_RTM_TRUE || p.op == OP_RTM_UPDOWN;
-    a.rec_k = (!rtm && p.op != OP_BORN_ADJ && p.op != OP_ILLUM && itp >= 0) ? itp : -1;
-    a.illum_on = p.op == OP_ILLUM && it > p.ndel;  // fd.cpp:318
+    const bool ill = p.op == OP_ILLUM || p.op == OP_ILLUM_PLANE;
+    a.rec_k = (!rtm && p.op != OP_BORN_ADJ && !ill && itp >= 0) ? itp : -1;
+    a.illum_on = ill && it > p.ndel;  // fd.cpp:318, :763
     a.strip_k = (rtm && itp >= 0) ? itp : -1;
     a.snap_k = p.op == OP_BORN_ADJ ? snap_slot(it, p.NT - 1, p.snap_every) : -1;
     int rc = step(p, mode, a, shots);
@@ -854,7 +855,8 @@ int enqueue_operator(Plan &p) {
       rc = ensure_snapshots(p);
       if (!rc && !p.snaps_valid) rc = source_pass(p);
       return rc ? rc : run_adjoint(p);
-    case OP_ILLUM: return run_forward(p, MODE_MODEL);
+    case OP_ILLUM:
+    case OP_ILLUM_PLANE: return run_forward(p, MODE_MODEL);
     case OP_BORN_PLANE: return run_forward(p, MODE_BORN);
     case OP_RTM_PLANE: return run_rtm_plane(p);
     case OP_RTM_TRUE:
@@ -1039,7 +1041,7 @@ int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_des
   if (rc) return rc;
   if (!out) return fail(ctx, SEIS_ERR_ARG, "out is null");
   *out = nullptr;
-  if (op < SEIS_OP_MODELING || op > SEIS_OP_RTM_UPDOWN) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
+  if (op < SEIS_OP_MODELING || op > SEIS_OP_ILLUM_PLANE) return fail(ctx, SEIS_ERR_ARG, "op=%d", op);
   Plan *p = nullptr;
   rc = plan_create(ctx, op, nshot, shots, &p);
   if (rc) return rc;
@@ -1140,12 +1142,12 @@ int seis_fd_plan_get(seis_fd_plan *plan, int shot, int what, float *h_dst) {
   if (!h_dst) return fail(ctx, SEIS_ERR_ARG, "null destination");
   if (what == SEIS_OUT_GATHER) {
     if (p.op == OP_RTM || p.op == OP_BORN_ADJ || p.op == OP_ILLUM || p.op == OP_RTM_PLANE ||
-        p.op == OP_RTM_TRUE || p.op == OP_RTM_UPDOWN)
+        p.op == OP_RTM_TRUE || p.op == OP_RTM_UPDOWN || p.op == OP_ILLUM_PLANE)
       return fail(ctx, SEIS_ERR_NOTSUP, "this plan outputs images");
     rc = download_gather(p, shot, h_dst);
   } else if (what == SEIS_OUT_IMAGE) {
     if (p.op != OP_RTM && p.op != OP_BORN_ADJ && p.op != OP_ILLUM && p.op != OP_RTM_PLANE &&
-        p.op != OP_RTM_TRUE && p.op != OP_RTM_UPDOWN)
+        p.op != OP_RTM_TRUE && p.op != OP_RTM_UPDOWN && p.op != OP_ILLUM_PLANE)
       return fail(ctx, SEIS_ERR_NOTSUP, "plan outputs gathers");
     const seis_shot_desc &d = p.desc[shot];
     CK(cudaMemcpyAsync(h_dst, p.sd[shot].img, sizeof(float) * d.nx * d.nz,
@@ -1342,6 +1344,12 @@ int seis_fd_rtm_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float 
   d.sx = d.nx / 2;  // the areal source has no point position
   return run_batch(ctx, OP_RTM_PLANE, 1, &d, &h_sou, SEIS_IN_SOURCE, &h_vel, SEIS_IN_VEL,
                    &h_rec, SEIS_IN_GATHER, &h_img, SEIS_OUT_IMAGE);
+}
+
+int seis_fd_illum_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_sou,
+                        const float *h_vel, float *h_ss) {
+  return run_batch(ctx, OP_ILLUM_PLANE, 1, shot, &h_sou, SEIS_IN_SOURCE, &h_vel, SEIS_IN_VEL,
+                   nullptr, -1, &h_ss, SEIS_OUT_IMAGE);
 }
 
 int seis_fd_rtm_updown(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float *h_wav,

@@ -9,7 +9,7 @@ the same file names and raw float32 layouts; ``lsrtm`` is the CG solver the
 reference declares (``cgsolver_MPI``) but does not define.
 
     python -m seis_b200.driver PARAM_FILE
-        {modeling|born|rtm|lsrtm|illum|plane_prepare|rtm_plane} [options]
+        {modeling|born|rtm|lsrtm|illum|plane_prepare|rtm_plane|illum_plane} [options]
 """
 from __future__ import annotations
 
@@ -60,6 +60,7 @@ def _setup():
     L.seis_driver_illum.argtypes = [_P, _P]
     L.seis_driver_plane_prepare.argtypes = [_P]
     L.seis_driver_rtm_plane.argtypes = [_P, _I, _P]
+    L.seis_driver_illum_plane.argtypes = [_P, _P]
     L.seis_driver_lsrtm.argtypes = [_P, _I, _I, ctypes.POINTER(LsrtmOptsC), _P, _P]
     L._driver_ready = True
     return L
@@ -150,6 +151,13 @@ class Driver:
                   "rtm_plane")
         return img
 
+    def illum_plane(self) -> np.ndarray:
+        """Plane-wave illumination [nx][nz] summed over the np wavenumbers; each one
+        is also written to wdir ILLUM_PLANE<k>.dat (illumPlane_MPI)."""
+        ss = np.zeros((self.params.nx, self.params.nz), np.float32)
+        self._run(self.L.seis_driver_illum_plane(self.h, ss.ctypes.data), "illum_plane")
+        return ss
+
     def illum(self) -> np.ndarray:
         """Source illumination [nx][nz] of all shots (illum_MPI)."""
         ss = np.zeros((self.params.nx, self.params.nz), np.float32)
@@ -188,7 +196,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m seis_b200.driver", description=__doc__.split("\n")[0])
     ap.add_argument("param_file")
     ap.add_argument("op", choices=["modeling", "born", "rtm", "lsrtm", "illum", "plane_prepare",
-                                   "rtm_plane"])
+                                   "rtm_plane", "illum_plane"])
     ap.add_argument("--dv", help="perturbation [nx][nz] float32 file (born)")
     ap.add_argument("--born-data", action="store_true", help="rtm/lsrtm from BORN<is>.dat")
     ap.add_argument("--niter", type=int, default=None, help="lsrtm iterations (default maxiter)")
@@ -213,6 +221,8 @@ def main(argv=None):
                 img = d.illum()
             elif a.op == "rtm_plane":
                 img = d.rtm_plane(a.born_data)
+            elif a.op == "illum_plane":
+                img = d.illum_plane()
             else:
                 img, rr = d.lsrtm(a.niter if a.niter is not None else p.maxiter, a.born_data)
                 for i, r in enumerate(rr):

@@ -120,6 +120,19 @@ def illum(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, wav, vel, ctx: Context = No
     return ss
 
 
+def illum_plane(dt, dx, dz, nt, ndel, nx, nz, pml, sz, vel, sou, ctx: Context = None):
+    """Illumination ``ss[nx][nz]`` of the areal source ``sou[nx][nt+ndel]`` at row sz
+    (reference ``illumPlane``, src/util/fd.cpp:720-786)."""
+    ctx = ctx or default_context()
+    s = _shot(dt, dx, dz, nt, ndel, nx, nz, pml, nx // 2, sz, np.zeros(nx, np.int32))
+    sou = _f32(sou, (nx, s.NT))
+    vel = _f32(vel, (nx, nz))
+    ss = np.zeros((nx, nz), np.float32)
+    d = s.to_c()
+    ctx.check(ctx.L.seis_fd_illum_plane(ctx.h, d, ptr(sou), ptr(vel), ptr(ss)))
+    return ss
+
+
 def forward(dt, dx, dz, nt, ndel, nx, nz, pml, sx, sz, gz, wav, vel, dv, ctx: Context = None):
     """Born gather ``rec[nx][nt]`` (reference ``forward``, src/util/fd.cpp:81-177)."""
     ctx = ctx or default_context()

@@ -1,6 +1,7 @@
-"""Source illumination (reference illum, src/util/fd.cpp:275-339) on the GPU:
-bit for bit against the oracle restatement (pinned to the compiled reference
-by tests/test_oracle.py), single shots and a ragged batch."""
+"""Source illumination (reference illum, src/util/fd.cpp:275-339, and
+illumPlane, :720-786) on the GPU: bit for bit against the oracle restatement
+(pinned to the compiled reference by tests/test_oracle.py), single shots and a
+ragged batch."""
 import numpy as np
 import pytest
 
@@ -34,3 +35,15 @@ def test_illum_ragged_batch(ctx):
     outs = batch(ctx, OP_ILLUM, shots, wavs, vels)
     for s, w, v, o in zip(shots, wavs, vels, outs):
         assert np.array_equal(o, O.illum(s, w, v))
+
+
+@pytest.mark.parametrize("g", golden_cases(), ids=golden_ids())
+def test_illum_plane_golden_bit_exact(ctx, g):
+    s = g.shot
+    rng = np.random.default_rng(9)
+    sou = np.outer(rng.standard_normal(s.nx), g.wav).astype(np.float32)
+    got = fd.illum_plane(s.dt, s.dx, s.dz, s.nt, s.ndel, s.nx, s.nz, s.pml, s.sz, g.vel, sou,
+                         ctx=ctx)
+    want = O.illum_plane(s, sou, g.vel)
+    assert np.array_equal(got, want)
+    assert want.max() > 0

@@ -55,6 +55,7 @@ def test_driver_plane_pipeline(ctx, tmp_path):
     with Driver(ctx, str(param)) as d:
         d.plane_prepare()
         img = d.rtm_plane()
+        ss = d.illum_plane()
         npw = d.params.np
     shot = Shot(nx=NX, nz=NZ, pml=10, nt=NT, ndel=DELAYCAL, sx=NX // 2, sz=1, dt=1e-3, dx=10.0,
                 dz=10.0, gz=np.full(NX, 1, np.int32))
@@ -68,3 +69,13 @@ def test_driver_plane_pipeline(ctx, tmp_path):
         want = im + want
     assert np.array_equal(img, want)
     assert np.abs(img).max() > 0
+    # illumPlane_MPI: one ILLUM_PLANE<k>.dat per wavenumber
+    ss_want = np.zeros((NX, NZ), np.float32)
+    for k in range(npw):
+        sou = np.fromfile(tmp_path / "W" / f"PLANE_S_NEW{k}.dat", np.float32).reshape(NX, NT + DELAYCAL)
+        ill = O.illum_plane(shot, sou, v0)
+        got_k = np.fromfile(tmp_path / "W" / f"ILLUM_PLANE{k}.dat", np.float32).reshape(NX, NZ)
+        assert np.array_equal(got_k, ill), k
+        ss_want = ill + ss_want
+    assert np.array_equal(ss, ss_want)
+    assert ss.max() > 0

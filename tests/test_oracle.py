@@ -84,6 +84,17 @@ def test_born_plane_restatement_matches_reference(g):
 
 @pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
 @pytest.mark.parametrize("g", CASES, ids=golden_ids())
+def test_illum_plane_restatement_matches_reference(g):
+    """illumPlane (src/util/fd.cpp:720-786): the C restatement bit for bit."""
+    rng = np.random.default_rng(4)
+    sou = np.outer(rng.standard_normal(g.shot.nx), g.wav).astype(np.float32)
+    want = O.illum_plane(g.shot, sou, g.vel, impl="ref")
+    assert np.array_equal(O.illum_plane(g.shot, sou, g.vel), want)
+    assert want.max() > 0
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("g", CASES, ids=golden_ids())
 def test_rtm_plane_restatement_matches_reference(g):
     """adjointPlane (src/util/fd.cpp:787-921): the C restatement bit for bit,
     with the gather's last ndel + 2 samples zero (the reference reads them at
