@@ -41,7 +41,9 @@ struct TCfg {
   static constexpr int NCUR = BORN ? 2 : 1;   // arrays staged with the wide halo
   static constexpr int NOTH = BORN ? 4 : 2;   // prev, vel [, prev B, dv]
   static constexpr int BUF = (NCUR * CW_C + NOTH * CW_P) * SR;  // floats per buffer
-  static constexpr size_t bytes = sizeof(float) * (size_t)BUF + 16;
+  // pad tiles: two-way values of the cells within 3 of the grid edge, per field
+  static constexpr int EDGE = KIND == TILE_PAD ? NCUR * TX * TZ : 0;
+  static constexpr size_t bytes = sizeof(float) * (size_t)(BUF + EDGE) + 16;
 };
 
 // ---- PTX helpers: mbarrier + bulk asynchronous copy global -> shared
@@ -289,7 +291,8 @@ __global__ void __launch_bounds__(NT_T, 2) tile_kernel(const ShotDev *__restrict
   constexpr bool PAD = KIND == TILE_PAD;
   extern __shared__ __align__(128) unsigned char smraw[];
   float *bb = reinterpret_cast<float *>(smraw);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(bb + C::BUF);
+  float *sE = bb + C::BUF;  // pad tiles: frame / low-order two-way values
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sE + C::EDGE);
   __shared__ ShotDev sg;
   __shared__ float red[33];
   const int tid = threadIdx.x;
@@ -353,6 +356,39 @@ __global__ void __launch_bounds__(NT_T, 2) tile_kernel(const ShotDev *__restrict
   const bool record = MODE != MODE_RCV && aa.rec_k >= 0;
   const bool snap = MODE != MODE_RCV && aa.snap_k >= 0 && g.snap != nullptr;
 
+  // Cells within 3 of the grid edge (frame, fd.cpp:1057-1091; low-order rings,
+  // :1226-1241) take the general formula.  All threads form them over the
+  // tile's edge bands (a cell in two bands is formed twice, to the same
+  // value); every other cell takes the 8th-order vector path.  The band pass
+  // reads global memory: the frame's normal extrapolation reaches the
+  // velocity two columns inside the grid, past the staged one-column halo of
+  // a tile that holds only the last column.
+  const int xe = PAD ? min(x0 + TX, g.NX) : 0, ze = PAD ? min(z0 + TZ, g.NZ) : 0;
+  const bool edge = PAD && (x0 <= 3 || z0 <= 3 || xe - 1 >= g.NX - 4 || ze - 1 >= g.NZ - 4);
+  auto near_edge = [&](int cxj, int iz) {
+    return min(min(cxj, iz), min(g.NX - 1 - cxj, g.NZ - 1 - iz)) <= 3;
+  };
+  if (edge) {
+    const int ra = a.rot % 3, rb = a.rot_b % 3;
+    float *const *FA = MODE == MODE_RCV ? g.fb : g.fa;
+    const int rr = MODE == MODE_RCV ? rb : ra;
+    const GA GCa{FA[(rr + 1) % 3], g.LDZ}, GPa{FA[rr], g.LDZ}, GV{g.vel, g.LDZ};
+    const GA GCb{g.fb[(rb + 1) % 3], g.LDZ}, GPb{g.fb[rb], g.LDZ};
+#pragma unroll 1
+    for (int b = 0; b < 4; b++) {  // top, bottom, left, right band
+      const int bxa = b == 3 ? max(x0, g.NX - 4) : x0, bxb = b == 2 ? min(xe, 4) : xe;
+      const int bza = b == 1 ? max(z0, g.NZ - 4) : z0, bzb = b == 0 ? min(ze, 4) : ze;
+      const int nr = bzb - bza, nc = bxb - bxa;
+      if (nr <= 0 || nc <= 0) continue;
+      for (int i = tid; i < nr * nc; i += NT_T) {
+        const int cxj = bxa + i / nr, iz = bza + i % nr;
+        sE[(cxj - x0) * TZ + (iz - z0)] = twoway_cell(GCa, GPa, GV, g, cxj, iz);
+        if (BORN) sE[TX * TZ + (cxj - x0) * TZ + (iz - z0)] = twoway_cell(GCb, GPb, GV, g, cxj, iz);
+      }
+    }
+  }
+  if (PAD) __syncthreads();
+
   auto in_grid = [&](int cxj, int iz) { return !PAD || (cxj < g.NX && iz < g.NZ); };
   auto model = [&](int cxj, int iz) {
     return !PAD || (cxj >= g.pml && cxj < g.pml + g.nx && iz >= g.pml && iz < g.pml + g.nz);
@@ -366,45 +402,18 @@ __global__ void __launch_bounds__(NT_T, 2) tile_kernel(const ShotDev *__restrict
   // values of the model cells for the snapshot.
   auto quad = [&](int qx, int qz0, bool vec, float (&lv)[8], int (&lx)[8], int (&lz)[8],
                   unsigned &mask) {
-    auto twoway = [&](const SA &Cc, const SA &Pp, float4 o[2], float4 cen[2], float4 prv[2],
-                      float4 vel[2]) {
-      if (vec) {
-        pair_twoway(Cc, Pp, VV, g, qx, qz0, o, cen, prv, vel);
-        return;
-      }
-      // low-order ring cells (modeling2D_low, fd.cpp:1226-1241) from vector
-      // loads of the column and its x neighbours; frame cells and any
-      // 8th-order cell of a mixed micro-tile by the general formula
+    auto twoway = [&](const SA &Cc, const SA &Pp, int f, float4 o[2], float4 cen[2],
+                      float4 prv[2], float4 vel[2]) {
+      pair_twoway(Cc, Pp, VV, g, qx, qz0, o, cen, prv, vel);
+      if (!vec) {  // cells within 3 of the grid edge from the band pass
 #pragma unroll
-      for (int j = 0; j < 2; j++) {
-        o[j] = cen[j] = prv[j] = vel[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        const int cxj = qx + j;
-        if (PAD && cxj >= g.NX) continue;
-        const float4 c4 = Cc.quad(cxj, qz0), l4 = Cc.quad(cxj - 1, qz0), r4 = Cc.quad(cxj + 1, qz0);
-        const float cm = Cc(cxj, qz0 - 1), cp = Cc(cxj, qz0 + 4);
-        const float4 p4 = Pp.quad(cxj, qz0), v4 = VV.quad(cxj, qz0);
-        cen[j] = c4;
-        prv[j] = p4;
-        vel[j] = v4;
+        for (int j = 0; j < 2; j++)
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-          const int iz = qz0 + r;
-          if (!in_grid(cxj, iz)) continue;
-          const bool frame = cxj == 0 || cxj == g.NX - 1 || iz == 0 || iz == g.NZ - 1;
-          const bool high = cxj >= 4 && cxj <= g.NX - 5 && iz >= 4 && iz <= g.NZ - 5;
-          float u;
-          if (frame || high) {
-            u = twoway_cell(Cc, Pp, VV, g, cxj, iz);
-          } else {
-            const float c = comp(c4, r);
-            const float zm1 = r == 0 ? cm : comp(c4, r - 1), zp1 = r == 3 ? cp : comp(c4, r + 1);
-            Coef k = coef(comp(v4, r), g);
-            const float uzz = zm1 + zp1 - 2.0f * c;
-            const float uxx = comp(r4, r) + comp(l4, r) - 2.0f * c;
-            u = k.vz * uzz + k.vx * uxx + 2.0f * c - comp(p4, r);
+          for (int r = 0; r < 4; r++) {
+            const int cxj = qx + j, iz = qz0 + r;
+            if (in_grid(cxj, iz) && near_edge(cxj, iz))
+              set_comp(o[j], r, sE[f * TX * TZ + (cxj - x0) * TZ + (iz - z0)]);
           }
-          set_comp(o[j], r, u);
-        }
       }
     };
     // a column quad wholly in the grid (or wholly in the model) is stored as
@@ -420,7 +429,7 @@ __global__ void __launch_bounds__(NT_T, 2) tile_kernel(const ShotDev *__restrict
       gzq[j] = (x >= 0 && x < g.nx) ? g.gz[x] + g.pml : -1;
     }
     float4 o[2], cen[2], prv[2], vel[2];
-    twoway(CA, PA, o, cen, prv, vel);
+    twoway(CA, PA, 0, o, cen, prv, vel);
     float4 qs[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
 #pragma unroll
     for (int j = 0; j < 2; j++) {
@@ -465,7 +474,7 @@ __global__ void __launch_bounds__(NT_T, 2) tile_kernel(const ShotDev *__restrict
     }
     if (BORN) {
       float4 ob[2], cb4[2], pb4[2], vb4[2];
-      twoway(CB, PB, ob, cb4, pb4, vb4);
+      twoway(CB, PB, 1, ob, cb4, pb4, vb4);
 #pragma unroll
       for (int j = 0; j < 2; j++) {
         const int cxj = qx + j;
@@ -503,7 +512,7 @@ __global__ void __launch_bounds__(NT_T, 2) tile_kernel(const ShotDev *__restrict
     float (&l1)[8] = *reinterpret_cast<float(*)[8]>(lv);
     int (&x1)[8] = *reinterpret_cast<int(*)[8]>(lx);
     int (&z1)[8] = *reinterpret_cast<int(*)[8]>(lz);
-    const bool vecq = ix >= 4 && ix + 1 <= g.NX - 5 && iz0 >= 4 && iz0 + 3 <= g.NZ - 5;
+    const bool vecq = !edge || (ix >= 4 && ix + 1 <= g.NX - 5 && iz0 >= 4 && iz0 + 3 <= g.NZ - 5);
     if (ix < g.NX && iz0 < g.NZ) quad(ix, iz0, vecq, l1, x1, z1, mask);
     else
 #pragma unroll

@@ -49,3 +49,21 @@ def test_random_cases_against_restatement(ctx, seed):
     assert np.array_equal(fd.modeling(*fd_args(s), wav, vel, ctx=ctx), rec)
     assert np.array_equal(fd.forward(*fd_args(s), wav, vel, dv, ctx=ctx), O.born(s, wav, vel, dv))
     assert np.array_equal(fd.adjoint(*fd_args(s), wav, vel, rec, ctx=ctx), O.rtm(s, wav, vel, rec))
+
+
+@pytest.mark.parametrize("nx,nz,pml", [(95, 63, 1), (61, 30, 2), (33, 97, 16)])
+def test_tile_edge_sizes_against_restatement(ctx, nx, nz, pml):
+    """Grids whose last tile column holds one or two columns (NX = 97, 65 = 1
+    mod 32) or whose last tile row holds one row (NZ = 65, 129 = 1 mod 64):
+    the frame's normal extrapolation then reaches cells of the previous tile."""
+    from seis_b200 import Shot
+    rng = np.random.default_rng(nx * nz + pml)
+    s = Shot(nx=nx, nz=nz, pml=pml, nt=90, ndel=20, sx=nx // 3, sz=nz // 4, dt=1e-3, dx=10.0,
+             dz=12.0, gz=rng.integers(0, nz, nx))
+    vel = (1500 + 2500 * rng.random((nx, nz))).astype(np.float32)
+    dv = (rng.standard_normal((nx, nz)) * 50).astype(np.float32)
+    wav = O.ricker(s.dt, 25.0, s.ndel, s.NT)
+    rec = O.modeling(s, wav, vel)
+    assert np.array_equal(fd.modeling(*fd_args(s), wav, vel, ctx=ctx), rec)
+    assert np.array_equal(fd.forward(*fd_args(s), wav, vel, dv, ctx=ctx), O.born(s, wav, vel, dv))
+    assert np.array_equal(fd.adjoint(*fd_args(s), wav, vel, rec, ctx=ctx), O.rtm(s, wav, vel, rec))
