@@ -234,6 +234,15 @@ def observed_data(ctx, sv):
         return [p.get(i, OUT_GATHER) for i in range(len(sv.shots))]
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# each step path of this workload (all kernels of the path, 32 shots), from one
+# ncu capture each of `python -m seis_b200.probe {adjoint|born} --steps 3`:
+# adjoint pad tiles 225.6 MB + ring kernel 137.9 MB; adjoint interior tiles;
+# Born pad tiles 371.0 MB + absorbing kernel 229.6 MB; Born interior tiles.
+NCU_TRAFFIC = {"adjoint_pad": 363.5e6, "adjoint_interior": 196.4e6,
+               "born_pad": 600.6e6, "born_interior": 405.5e6}
+
+
 def kernel_roofline(ctx, sv, iter_ms):
     """Per-kernel CUDA-event durations of the Born and adjoint step kernels
     (separate plans over the same shots), their share of one iteration, and
@@ -422,7 +431,9 @@ def main():
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "cell_updates_per_step": e2e_cells},
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                     "frac": ach / hbm, "traffic": None, "kernel": top["kernel"],
+                     "frac": ach / hbm, "traffic": NCU_TRAFFIC.get(top["kernel"]),
+                     "traffic_unit": "bytes per launch (ncu capture of the same workload)",
+                     "kernel": top["kernel"],
                      "peak_source": src, "kernel_ms": top["ms"], "share": top["share"],
                      "kernels": rows},
         "plain_fp32": plain,

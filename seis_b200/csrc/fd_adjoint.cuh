@@ -61,7 +61,7 @@ __device__ __forceinline__ float snap_inv_scale(const ShotDev &g, int k, int x0,
 
 // ---------------------------------------------------------------- interior
 // L_k = Lz(vz L1) + Lx(vx L1) + 2 L1 - L2 + R^T d ; grad += w lap L1.
-__global__ void __launch_bounds__(A_NT_I, 2) adj_interior_kernel(const ShotDev *__restrict__ shots,
+__global__ void __launch_bounds__(A_NT_I, 3) adj_interior_kernel(const ShotDev *__restrict__ shots,
                                                                  const Tile *__restrict__ tiles,
                                                                  StepArgs a, int *__restrict__ err) {
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -219,7 +219,7 @@ __device__ float edge_terms(const ShotDev &g, const A &M, const A &V, int tx, in
 // L = S_cur^T M1 - M2 + E + R^T d on a tile with pad-ring cells, pad-ring
 // neighbours or consumers outside the 8th-order region; rho = (1 - w) L of
 // its ring cells; grad += w lap M1 on its model cells.
-__global__ void __launch_bounds__(A_NT_I, 2) adj_pad_kernel(const ShotDev *__restrict__ shots,
+__global__ void __launch_bounds__(A_NT_I, 3) adj_pad_kernel(const ShotDev *__restrict__ shots,
                                                             const Tile *__restrict__ tiles,
                                                             StepArgs a, int *__restrict__ err) {
   extern __shared__ __align__(128) unsigned char smraw[];

@@ -283,7 +283,7 @@ struct GA {
 };
 
 template <int MODE, int KIND>
-__global__ void __launch_bounds__(NT_T, 2) tile_kernel(const ShotDev *__restrict__ shots,
+__global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict__ shots,
                                                        const Tile *__restrict__ tiles, StepArgs a,
                                                        int *__restrict__ err) {
   using C = TCfg<MODE, KIND>;

@@ -44,7 +44,7 @@ def test_rtm_plane_golden_bit_exact(ctx, g):
 
 
 def test_driver_plane_pipeline(ctx, tmp_path):
-    """planeWavePrepare then adjointPlane_MPI through the shot driver, against
+    """planeWavePrepare, then adjointPlane_MPI and illumPlane_MPI through the shot driver, against
     the restatement on the files the preparation wrote."""
     from seis_b200 import Shot
     from seis_b200.driver import Driver
