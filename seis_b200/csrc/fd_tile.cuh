@@ -41,9 +41,7 @@ struct TCfg {
   static constexpr int NCUR = BORN ? 2 : 1;   // arrays staged with the wide halo
   static constexpr int NOTH = BORN ? 4 : 2;   // prev, vel [, prev B, dv]
   static constexpr int BUF = (NCUR * CW_C + NOTH * CW_P) * SR;  // floats per buffer
-  // pad tiles: two-way values of the cells within 3 of the grid edge, per field
-  static constexpr int EDGE = KIND == TILE_PAD ? NCUR * TX * TZ : 0;
-  static constexpr size_t bytes = sizeof(float) * (size_t)(BUF + EDGE) + 16;
+  static constexpr size_t bytes = sizeof(float) * (size_t)BUF + 16;
 };
 
 // ---- PTX helpers: mbarrier + bulk asynchronous copy global -> shared
@@ -291,8 +289,7 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
   constexpr bool PAD = KIND == TILE_PAD;
   extern __shared__ __align__(128) unsigned char smraw[];
   float *bb = reinterpret_cast<float *>(smraw);
-  float *sE = bb + C::BUF;  // pad tiles: frame / low-order two-way values
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sE + C::EDGE);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(bb + C::BUF);
   __shared__ ShotDev sg;
   __shared__ float red[33];
   const int tid = threadIdx.x;
@@ -359,7 +356,9 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
   // Cells within 3 of the grid edge (frame, fd.cpp:1057-1091; low-order rings,
   // :1226-1241) take the general formula.  All threads form them over the
   // tile's edge bands (a cell in two bands is formed twice, to the same
-  // value); every other cell takes the 8th-order vector path.  The band pass
+  // value) into the tile's cells of the two-way scratch field, which the
+  // cell's own thread reads back after the barrier and then overwrites with
+  // the injected value; every other cell takes the 8th-order vector path.  The band pass
   // reads global memory: the frame's normal extrapolation reaches the
   // velocity two columns inside the grid, past the staged one-column halo of
   // a tile that holds only the last column.
@@ -382,8 +381,9 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
       if (nr <= 0 || nc <= 0) continue;
       for (int i = tid; i < nr * nc; i += NT_T) {
         const int cxj = bxa + i / nr, iz = bza + i % nr;
-        sE[(cxj - x0) * TZ + (iz - z0)] = twoway_cell(GCa, GPa, GV, g, cxj, iz);
-        if (BORN) sE[TX * TZ + (cxj - x0) * TZ + (iz - z0)] = twoway_cell(GCb, GPb, GV, g, cxj, iz);
+        const size_t at = (size_t)cxj * g.LDZ + iz;
+        g.u3s[0][at] = twoway_cell(GCa, GPa, GV, g, cxj, iz);
+        if (BORN) g.u3s[1][at] = twoway_cell(GCb, GPb, GV, g, cxj, iz);
       }
     }
   }
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
           for (int r = 0; r < 4; r++) {
             const int cxj = qx + j, iz = qz0 + r;
             if (in_grid(cxj, iz) && near_edge(cxj, iz))
-              set_comp(o[j], r, sE[f * TX * TZ + (cxj - x0) * TZ + (iz - z0)]);
+              set_comp(o[j], r, g.u3s[f][(size_t)cxj * g.LDZ + iz]);
           }
       }
     };
