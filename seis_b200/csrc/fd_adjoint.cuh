@@ -60,7 +60,9 @@ __device__ __forceinline__ float snap_inv_scale(const ShotDev &g, int k, int x0,
 }
 
 // ---------------------------------------------------------------- interior
-// L_k = Lz(vz L1) + Lx(vx L1) + 2 L1 - L2 + R^T d ; grad += w lap L1.
+// L_k = Lz(vz M1) + Lx(vx M1) + 2 M1 - M2 + R^T d ; grad += w lap M1.  On these
+// tiles M = L (no ring cell within one cell), so the staged arrays (named L1,
+// L2 below) hold M_{k+1}, M_{k+2} and the output is L_k = M_k.
 __global__ void __launch_bounds__(A_NT_I, 3) adj_interior_kernel(const ShotDev *__restrict__ shots,
                                                                  const Tile *__restrict__ tiles,
                                                                  StepArgs a, int *__restrict__ err) {
