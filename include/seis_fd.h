@@ -223,6 +223,17 @@ int64_t seis_fd_plan_launches_per_run(const seis_fd_plan *plan);
  * memory (the imaging term of a stored step is weighted by `every`).  Default:
  * every = 1, SEIS_SNAP_F32.  Call before the first run. */
 int seis_fd_plan_set_snapshots(seis_fd_plan *plan, int every, int dtype);
+/* Source-field checkpoints of SEIS_OP_BORN_ADJOINT plans, for surveys whose
+ * snapshots do not fit in device memory (the largest configuration, 4000 x
+ * 1000 cells and 8000 steps, needs about 16 GB of BF16 snapshots per shot).
+ * every = 0 (default) keeps every snapshot of the run.  every = C > 0, a
+ * multiple of the snapshot interval: the source pass keeps only the two time
+ * levels before every C-th step, and each run recomputes the snapshots of one
+ * C-step segment at a time, just before the reverse steps that image with
+ * them, into storage for C / every + 1 snapshots.  The image is bit-identical
+ * to every = 0; a run advances one more field per step.  No counterpart in
+ * the reference, which keeps no snapshots.  Call before the first run. */
+int seis_fd_plan_set_checkpoints(seis_fd_plan *plan, int every);
 /* Bytes of device memory the plan holds (fields, models, gathers, images,
  * snapshots once allocated). */
 int64_t seis_fd_plan_device_bytes(const seis_fd_plan *plan);
@@ -302,6 +313,8 @@ typedef struct {
   int snap_every;  /* source-term snapshot interval (default 1)            */
   int snap_dtype;  /* SEIS_SNAP_* (default SEIS_SNAP_BF16)                 */
   int exact;       /* Born kernels round like the reference (default 0)    */
+  int checkpoint_every; /* source-field checkpoint interval (default 0 = keep
+                           every snapshot; see seis_fd_plan_set_checkpoints) */
 } seis_lsrtm_opts;
 
 int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot,

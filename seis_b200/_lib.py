@@ -67,7 +67,7 @@ class Shot:
 
 class LsrtmOptsC(ctypes.Structure):
     _fields_ = [("snap_every", ctypes.c_int), ("snap_dtype", ctypes.c_int),
-                ("exact", ctypes.c_int)]
+                ("exact", ctypes.c_int), ("checkpoint_every", ctypes.c_int)]
 
 
 _lib = None
@@ -107,6 +107,7 @@ def lib():
         L.seis_fd_plan_launches_per_run.restype = ctypes.c_int64
         L.seis_fd_plan_set_exact.argtypes = [P, I]
         L.seis_fd_plan_set_snapshots.argtypes = [P, I, I]
+        L.seis_fd_plan_set_checkpoints.argtypes = [P, I]
         L.seis_fd_plan_device_bytes.argtypes = [P]
         L.seis_fd_plan_device_bytes.restype = ctypes.c_int64
         L.seis_fd_born_adjoint.argtypes = [P, SD, P, P, P, P]
@@ -268,6 +269,11 @@ class Plan:
     def set_snapshots(self, every: int = 1, dtype: int = 1):
         self.ctx.check(self.ctx.L.seis_fd_plan_set_snapshots(self.h, every, dtype))
 
+    def set_checkpoints(self, every: int):
+        """Keep source-field checkpoints every `every` steps instead of every
+        snapshot (seis_fd_plan_set_checkpoints); 0 = keep every snapshot."""
+        self.ctx.check(self.ctx.L.seis_fd_plan_set_checkpoints(self.h, every))
+
     @property
     def device_bytes(self) -> int:
         return int(self.ctx.L.seis_fd_plan_device_bytes(self.h))
@@ -344,13 +350,15 @@ class Lsrtm:
     """
 
     def __init__(self, ctx: Context, nx: int, nz: int, shots, x0=None, snap_every: int = 1,
-                 snap_dtype: int = None, exact: bool = False, colmaps=None):
+                 snap_dtype: int = None, exact: bool = False, colmaps=None,
+                 checkpoint_every: int = 0):
         """Shot k covers columns x0[k] .. x0[k] + nx_k - 1, or the model columns
-        colmaps[k] (one per sub-grid column, non-decreasing)."""
+        colmaps[k] (one per sub-grid column, non-decreasing).  checkpoint_every > 0
+        keeps source-field checkpoints instead of every snapshot."""
         self.ctx, self.nx, self.nz, self.shots = ctx, nx, nz, list(shots)
         self._descs = shot_array(self.shots)
         o = LsrtmOptsC(snap_every, SNAP_BF16 if snap_dtype is None else snap_dtype,
-                       1 if exact else 0)
+                       1 if exact else 0, checkpoint_every)
         h = ctypes.c_void_p()
         if colmaps is None:
             self._x0 = (ctypes.c_int * len(self.shots))(*[int(v) for v in x0])

@@ -118,6 +118,15 @@ struct Plan {
   std::vector<PadChunk> adj_chunks;  // pad cells + model edge cells (adjoint ring kernel)
   PadChunk *d_adj_chunks = nullptr;
   int snap_every = 1, snap_dtype = SNAP_F32;
+  // source-field checkpoints (adjoint plans, 0 = keep every snapshot): the
+  // two time levels before every ck_every-th step; the reverse pass
+  // recomputes each segment's snapshots into a buffer of one segment, on the
+  // shot table sd_c (its own field A buffers)
+  int ck_every = 0;
+  std::vector<std::vector<float *>> ck;  // per shot: 2 fields per checkpoint j >= 1
+  std::vector<ShotDev> sd_c;
+  ShotDev *d_sd_c = nullptr;
+  CUtensorMap *d_maps_c = nullptr;
   bool snaps_ready = false;  // storage allocated
   bool snaps_valid = false;  // storage holds the source terms of the current inputs
   int64_t device_bytes = 0;
@@ -592,6 +601,46 @@ float snap_weight(int k, int K, int m) {
   return 0.5f * (float)(next - prev + (k == 0) + (k == K));
 }
 
+// Snapshot slots held at once: every slot of the run, or with checkpoints
+// those of one segment (ck_every / snap_every, and the last step's).
+int snap_slots(const Plan &p, int NT) {
+  return p.ck_every > 0 ? p.ck_every / p.snap_every + 1 : snap_count(NT - 1, p.snap_every);
+}
+
+// First snapshot slot of the segment that starts at step s0 (ck_every is a
+// multiple of snap_every, so s0 is a stored step).
+int seg_slot0(const Plan &p, int s0) { return p.ck_every > 0 ? s0 / p.snap_every : 0; }
+
+// Checkpoint storage and the recompute shot table (after the snapshots).
+int ensure_checkpoints(Plan &p) {
+  seis_fd_ctx *ctx = p.ctx;
+  p.sd_c = p.sd;
+  p.ck.assign(p.nshot, {});
+  const int nck = (p.NT - 1) / p.ck_every;  // checkpoints j = 1 .. nck
+  for (int s = 0; s < p.nshot; s++) {
+    ShotDev &c = p.sd_c[s];
+    for (int k = 0; k < 3; k++) {
+      int rc = alloc_field(p, c, &c.fa[k]);
+      if (rc) return rc;
+    }
+    for (int j = 0; j < 2 * nck; j++) {
+      float *f = nullptr;
+      int rc = alloc_field(p, c, &f);
+      if (rc) return rc;
+      p.ck[s].push_back(f);
+    }
+    c.img = nullptr;
+    c.grad = nullptr;
+    c.illum = nullptr;
+  }
+  int rc = encode_maps(p, p.sd_c, &p.d_maps_c);
+  if (!rc) rc = p.alloc(&p.d_sd_c, (size_t)p.nshot);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(p.d_sd_c, p.sd_c.data(), sizeof(ShotDev) * p.nshot, cudaMemcpyHostToDevice,
+                     ctx->stream));
+  return SEIS_OK;
+}
+
 // Snapshot storage of every shot (first run of an adjoint plan), then the
 // shot table is uploaded again with the new pointers.
 int ensure_snapshots(Plan &p) {
@@ -600,7 +649,7 @@ int ensure_snapshots(Plan &p) {
   const size_t esize = p.snap_dtype == SNAP_F32 ? 4 : 2;
   for (int s = 0; s < p.nshot; s++) {
     ShotDev &g = p.sd[s];
-    int nsnap = snap_count(g.NT - 1, p.snap_every);
+    int nsnap = snap_slots(p, g.NT);
     int ntx = (g.NX + TX - 1) / TX;
     unsigned char *snap = nullptr;
     int rc = p.alloc(&snap, (size_t)nsnap * g.nx * g.nz * esize);
@@ -612,6 +661,10 @@ int ensure_snapshots(Plan &p) {
   }
   CK(cudaMemcpyAsync(p.d_sd, p.sd.data(), sizeof(ShotDev) * p.nshot, cudaMemcpyHostToDevice,
                      ctx->stream));
+  if (p.ck_every > 0) {
+    int rc = ensure_checkpoints(p);
+    if (rc) return rc;
+  }
   p.snaps_ready = true;
   return SEIS_OK;
 }
@@ -804,9 +857,71 @@ int run_updown_reverse(Plan &p) {
 // (adjoint plans); reused by every later run until the velocity or the
 // wavelet changes.
 int source_pass(Plan &p) {
-  int rc = run_forward(p, MODE_MODEL);
+  int rc = SEIS_OK;
+  if (p.ck_every == 0) {
+    rc = run_forward(p, MODE_MODEL);
+  } else {
+    // the whole forward pass on the recompute table, keeping the two time
+    // levels before every ck_every-th step instead of the snapshots
+    seis_fd_ctx *ctx = p.ctx;
+    for (const ShotDev &c : p.sd_c) {
+      FieldGeom fg = field_geom(c.NX, c.NZ);
+      for (int k = 0; k < 3; k++)
+        CK(cudaMemsetAsync(c.fa[k] - fg.origin, 0, sizeof(float) * fg.elems, ctx->stream));
+    }
+    StepArgs a{};
+    a.nshots = p.nshot;
+    for (int it = 0; it < p.NT && !rc; it++) {
+      if (it > 0 && it % p.ck_every == 0) {
+        const int j = it / p.ck_every;
+        for (int s = 0; s < p.nshot; s++) {
+          const ShotDev &c = p.sd_c[s];
+          FieldGeom fg = field_geom(c.NX, c.NZ);
+          for (int l = 0; l < 2; l++)  // prev = fa[it % 3], cur = fa[(it + 1) % 3]
+            CK(cudaMemcpyAsync(p.ck[s][2 * (j - 1) + l] - fg.origin, c.fa[(it + l) % 3] - fg.origin,
+                               sizeof(float) * fg.elems, cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+      }
+      a.rot = it;
+      a.rot_b = it;
+      a.src_k = it >= 1 ? it - 1 : -1;
+      rc = step(p, MODE_MODEL, a, p.d_sd_c);
+    }
+  }
   if (!rc) p.snaps_valid = true;
   return rc;
+}
+
+// Recompute the snapshots of forward steps s0 .. s1-1 (one checkpoint
+// segment) into the segment buffer, from checkpoint s0 / ck_every.
+int recompute_segment(Plan &p, int s0, int s1) {
+  seis_fd_ctx *ctx = p.ctx;
+  const int j = s0 / p.ck_every;
+  for (int s = 0; s < p.nshot; s++) {
+    const ShotDev &c = p.sd_c[s];
+    FieldGeom fg = field_geom(c.NX, c.NZ);
+    for (int l = 0; l < 2; l++) {
+      float *dst = c.fa[(s0 + l) % 3] - fg.origin;
+      if (j == 0)
+        CK(cudaMemsetAsync(dst, 0, sizeof(float) * fg.elems, ctx->stream));
+      else
+        CK(cudaMemcpyAsync(dst, p.ck[s][2 * (j - 1) + l] - fg.origin, sizeof(float) * fg.elems,
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+  }
+  StepArgs a{};
+  a.nshots = p.nshot;
+  const int slot0 = seg_slot0(p, s0);
+  for (int it = s0; it < s1; it++) {
+    a.rot = it;
+    a.rot_b = it;
+    a.src_k = it >= 1 ? it - 1 : -1;
+    const int sl = snap_slot(it, p.NT - 1, p.snap_every);
+    a.snap_k = sl >= 0 ? sl - slot0 : -1;
+    int rc = step(p, MODE_MODEL, a, p.d_sd_c);
+    if (rc) return rc;
+  }
+  return SEIS_OK;
 }
 
 // Reverse pass of the exact adjoint: L_k for k = NT .. 0 from L_{k+1}, L_{k+2};
@@ -825,13 +940,24 @@ int run_adjoint(Plan &p) {
   a.src_k = -1;
   a.strip_k = -1;
   int r = 0;
+  // with checkpoints, before the reverse steps of each segment [s0, s1) its
+  // snapshots are recomputed (k = NT images nothing)
+  const int C = p.ck_every > 0 ? p.ck_every : p.NT + 1;
+  int slot0 = 0;
   for (int k = p.NT; k >= 0; k--, r++) {
+    if (p.ck_every > 0 && k < p.NT && (k == p.NT - 1 || (k + 1) % C == 0)) {
+      const int s0 = (k / C) * C;
+      int rc = recompute_segment(p, s0, k + 1);
+      if (rc) return rc;
+      slot0 = seg_slot0(p, s0);
+    }
     a.rot = r;
     a.rot_b = r;
     int kd = k - 1 - p.ndel;
     a.rec_k = (kd >= 0 && kd < p.nt) ? kd : -1;
-    a.snap_k = snap_slot(k, p.NT - 1, p.snap_every);
-    a.img_w = a.snap_k >= 0 ? snap_weight(k, p.NT - 1, p.snap_every) : 0.0f;
+    const int sl = snap_slot(k, p.NT - 1, p.snap_every);
+    a.snap_k = sl >= 0 ? sl - slot0 : -1;
+    a.img_w = sl >= 0 ? snap_weight(k, p.NT - 1, p.snap_every) : 0.0f;
     int rc = adj_step(p, a);
     if (rc) return rc;
   }
@@ -1251,8 +1377,26 @@ int seis_fd_plan_set_snapshots(seis_fd_plan *plan, int every, int dtype) {
   if (every < 1 || dtype < SEIS_SNAP_F32 || dtype > SEIS_SNAP_F16)
     return fail(p.ctx, SEIS_ERR_ARG, "snapshots every=%d dtype=%d", every, dtype);
   if (p.snaps_ready) return fail(p.ctx, SEIS_ERR_STATE, "snapshots already allocated");
+  if (p.ck_every > 0 && p.ck_every % every != 0)
+    return fail(p.ctx, SEIS_ERR_ARG, "snapshot interval %d does not divide the checkpoint interval %d",
+                every, p.ck_every);
   p.snap_every = every;
   p.snap_dtype = dtype;
+  return SEIS_OK;
+}
+
+int seis_fd_plan_set_checkpoints(seis_fd_plan *plan, int every) {
+  if (!plan || !plan->p) return SEIS_ERR_ARG;
+  Plan &p = *plan->p;
+  if (p.op != OP_BORN_ADJ) return fail(p.ctx, SEIS_ERR_NOTSUP, "plan keeps no snapshots");
+  if (every < 0 || (every > 0 && every % p.snap_every != 0))
+    return fail(p.ctx, SEIS_ERR_ARG, "checkpoints every=%d: a multiple of the snapshot interval %d",
+                every, p.snap_every);
+  if (p.snaps_ready) return fail(p.ctx, SEIS_ERR_STATE, "snapshots already allocated");
+  // the segment recomputation adds one forward field per step to a run
+  for (const ShotDev &g : p.sd)
+    p.cell_updates += (int64_t)g.NX * g.NZ * g.NT * ((every > 0) - (p.ck_every > 0));
+  p.ck_every = every;
   return SEIS_OK;
 }
 
@@ -1575,7 +1719,7 @@ int seis_fd_lsrtm_create_mapped(seis_fd_ctx *ctx, int nx, int nz, int nshot,
     }
     off += shots[k].nx;
   }
-  seis_lsrtm_opts o{1, SEIS_SNAP_BF16, 0};
+  seis_lsrtm_opts o{1, SEIS_SNAP_BF16, 0, 0};
   if (opts) o = *opts;
   seis_fd_lsrtm *L = new (std::nothrow) seis_fd_lsrtm();
   if (!L) return fail(ctx, SEIS_ERR_NOMEM, "host allocation failed");
@@ -1611,6 +1755,7 @@ int seis_fd_lsrtm_create_mapped(seis_fd_ctx *ctx, int nx, int nz, int nshot,
     pa->exact = o.exact != 0;
     seis_fd_plan h{pa};
     rc = seis_fd_plan_set_snapshots(&h, o.snap_every, o.snap_dtype);
+    if (!rc && o.checkpoint_every > 0) rc = seis_fd_plan_set_checkpoints(&h, o.checkpoint_every);
   }
   size_t nm = (size_t)nx * nz;
   if (!rc) rc = L->alloc(&L->m, nm);

@@ -7,7 +7,7 @@ import oracle as O
 from helpers import fd_args, rel_l2
 from seis_b200 import Shot, fd
 from seis_b200._lib import (IN_GATHER, IN_VEL, IN_WAVELET, OP_BORN_ADJOINT, OUT_IMAGE, SNAP_BF16,
-                            SNAP_F16, SNAP_F32, Plan)
+                            SNAP_F16, SNAP_F32, Plan, SeisError)
 
 pytestmark = pytest.mark.gpu
 
@@ -84,3 +84,55 @@ def test_mixed_snapshot_image_error(ctx, every, dtype, tol):
           f"(vs thinned FP64 {err_thin:.3e}; thinning alone {inherent:.3e})")
     assert err < tol
     assert err_thin < tol
+
+
+def _adjoint_images(ctx, shots, vels, wav, gathers, every, dtype, ck, runs=2):
+    """Images of a batch of shots from one adjoint plan, run `runs` times (the
+    first run captures the graph, later runs replay it) with new gathers."""
+    out = []
+    with Plan(ctx, OP_BORN_ADJOINT, shots) as p:
+        p.set_snapshots(every, dtype)
+        if ck:
+            p.set_checkpoints(ck)
+        for i, v in enumerate(vels):
+            p.set(i, IN_VEL, v)
+            p.set(i, IN_WAVELET, wav)
+        for r in range(runs):
+            for i, d in enumerate(gathers):
+                p.set(i, IN_GATHER, d * (1.0 + r))
+            p.run()
+            out.append([p.get(i, OUT_IMAGE) for i in range(len(shots))])
+    return out
+
+
+@pytest.mark.parametrize("every,dtype,ck", [(1, SNAP_F32, 7), (2, SNAP_BF16, 6),
+                                            (4, SNAP_F16, 8), (4, SNAP_BF16, 64)])
+def test_checkpointed_adjoint_is_bit_identical(ctx, every, dtype, ck):
+    """Source-field checkpoints (the two time levels before every ck-th step,
+    each segment's snapshots recomputed before the reverse steps that use them)
+    give the same images, bit for bit, as keeping every snapshot: a ragged batch
+    whose step count is not a multiple of ck, run twice through the graph."""
+    rng = np.random.default_rng(31)
+    shots, vels, gathers = [], [], []
+    for nx, nz, pml in ((70, 44, 10), (41, 63, 3)):
+        s = Shot(nx=nx, nz=nz, pml=pml, nt=181, ndel=25, sx=nx // 2, sz=2, dt=1e-3, dx=10.0,
+                 dz=10.0, gz=rng.integers(0, nz, nx))
+        shots.append(s)
+        vels.append((1800 + 1500 * rng.random((nx, nz))).astype(np.float32))
+        gathers.append(rng.standard_normal((nx, s.nt)).astype(np.float32))
+    wav = O.ricker(1e-3, 25.0, 25, shots[0].NT)
+    keep = _adjoint_images(ctx, shots, vels, wav, gathers, every, dtype, 0)
+    ckpt = _adjoint_images(ctx, shots, vels, wav, gathers, every, dtype, ck)
+    for r in range(2):
+        for a, b in zip(keep[r], ckpt[r]):
+            assert np.abs(a).max() > 0
+            assert np.array_equal(a, b), (r, rel_l2(b, a))
+
+
+def test_checkpoint_interval_must_hold_whole_snapshot_intervals(ctx):
+    s, vel, wav, m, d = make(40, 30, 8, 10.0, 12.5)
+    with Plan(ctx, OP_BORN_ADJOINT, [s]) as p:
+        p.set_snapshots(4, SNAP_BF16)
+        with pytest.raises(SeisError):
+            p.set_checkpoints(6)
+        p.set_checkpoints(8)
