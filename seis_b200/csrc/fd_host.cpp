@@ -1982,7 +1982,11 @@ int seis_fd_lsrtm_model(seis_fd_lsrtm *L, float *h_m) {
 int64_t seis_fd_lsrtm_cell_updates(const seis_fd_lsrtm *L) {
   if (!L) return 0;
   int64_t c = 0;
-  for (const ShotDev &g : L->born.p->sd) c += (int64_t)g.NX * g.NZ * (2LL * g.NT + g.NT + 1);
+  // Born (two fields), the adjoint's reverse pass, and with checkpoints the
+  // recomputed source field
+  const int64_t ck = L->adj.p->ck_every > 0 ? 1 : 0;
+  for (const ShotDev &g : L->born.p->sd)
+    c += (int64_t)g.NX * g.NZ * (2LL * g.NT + g.NT + 1 + ck * g.NT);
   return c;
 }
 

@@ -9,6 +9,7 @@ import pytest
 
 import oracle as O
 from helpers import golden_cases, golden_ids, rel_l2
+from seis_b200 import Shot
 
 CASES = golden_cases()
 
@@ -128,3 +129,22 @@ def test_rtm_updown_restatement_matches_reference(g):
     assert np.array_equal(img, rimg)
     assert np.array_equal(comp, rcomp)
     assert np.abs(comp).max(axis=(1, 2)).min() > 0
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+def test_reference_scheme_unstable_above_courant_053():
+    """The reference's own modeling (fd.cpp:15-80) grows without bound at a
+    Courant number v dt / dx of 0.55 -- below the 0.5546 limit of its interior
+    8th-order update, so the growth comes from its boundary treatment -- and
+    decays at 0.45; the restatement follows it bit for bit in both regimes."""
+    amp = {}
+    for v in (5500.0, 4500.0):
+        s = Shot(nx=60, nz=50, pml=20, nt=3000, ndel=60, sx=30, sz=1, dt=5e-4, dx=5.0, dz=5.0,
+                 gz=np.full(60, 1, np.int32))
+        vel = np.full((s.nx, s.nz), v, np.float32)
+        wav = O.ricker(s.dt, 25.0, s.ndel, s.NT)
+        ref = O.modeling(s, wav, vel, impl="ref")
+        assert np.array_equal(O.modeling(s, wav, vel), ref)
+        amp[v] = np.abs(ref[:, -500:]).max() / np.abs(ref[:, :1000]).max()
+    assert amp[5500.0] > 1e3
+    assert amp[4500.0] < 1e-3
