@@ -315,6 +315,11 @@ typedef struct {
   int exact;       /* Born kernels round like the reference (default 0)    */
   int checkpoint_every; /* source-field checkpoint interval (default 0 = keep
                            every snapshot; see seis_fd_plan_set_checkpoints) */
+  int group_shots; /* 0 (default): the plans of all shots stay on the device.
+                      n > 0: each operator application builds the plans of n
+                      shots at a time and frees them (for surveys whose plans
+                      do not fit at once); the source pass then runs in every
+                      application, and the results are identical */
 } seis_lsrtm_opts;
 
 int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot,

@@ -67,7 +67,8 @@ class Shot:
 
 class LsrtmOptsC(ctypes.Structure):
     _fields_ = [("snap_every", ctypes.c_int), ("snap_dtype", ctypes.c_int),
-                ("exact", ctypes.c_int), ("checkpoint_every", ctypes.c_int)]
+                ("exact", ctypes.c_int), ("checkpoint_every", ctypes.c_int),
+                ("group_shots", ctypes.c_int)]
 
 
 _lib = None
@@ -351,14 +352,16 @@ class Lsrtm:
 
     def __init__(self, ctx: Context, nx: int, nz: int, shots, x0=None, snap_every: int = 1,
                  snap_dtype: int = None, exact: bool = False, colmaps=None,
-                 checkpoint_every: int = 0):
+                 checkpoint_every: int = 0, group_shots: int = 0):
         """Shot k covers columns x0[k] .. x0[k] + nx_k - 1, or the model columns
         colmaps[k] (one per sub-grid column, non-decreasing).  checkpoint_every > 0
-        keeps source-field checkpoints instead of every snapshot."""
+        keeps source-field checkpoints instead of every snapshot; group_shots > 0
+        builds the plans of that many shots at a time in every operator
+        application instead of keeping all of them."""
         self.ctx, self.nx, self.nz, self.shots = ctx, nx, nz, list(shots)
         self._descs = shot_array(self.shots)
         o = LsrtmOptsC(snap_every, SNAP_BF16 if snap_dtype is None else snap_dtype,
-                       1 if exact else 0, checkpoint_every)
+                       1 if exact else 0, checkpoint_every, group_shots)
         h = ctypes.c_void_p()
         if colmaps is None:
             self._x0 = (ctypes.c_int * len(self.shots))(*[int(v) for v in x0])

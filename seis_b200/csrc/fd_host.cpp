@@ -1624,6 +1624,13 @@ struct seis_fd_lsrtm {
   double *sc = nullptr;  // FP64 scalars: 0 gamma, 1 |q|^2, 2 alpha, 3 gamma_new, 4 beta
   double *rr = nullptr;  // |r|^2 per iteration
   int rr_cap = 0;
+  // shot groups (group > 0): the plans of `group` shots at a time are built
+  // for each operator application and freed after it; the background and
+  // wavelet stay on the device, q = L p in its own data-space buffer
+  int group = 0;
+  seis_lsrtm_opts opts{};
+  float *d_v0 = nullptr, *d_wav = nullptr, *q = nullptr, *stage = nullptr;
+  int64_t group_bytes = 0;  // largest device memory of one group's plan
   bool ready = false;    // reset done
   int64_t device_bytes = 0;
   ~seis_fd_lsrtm() {
@@ -1652,42 +1659,137 @@ namespace {
 
 // s = L^T r: adjoint plan over the residuals, per-shot images scattered into
 // the global grid.
+// The plan of shots k0 .. k1-1 of a grouped solver: velocity sub-grids and
+// wavelet from the device copies; an adjoint plan reads the residual.
+int lsrtm_group_plan(seis_fd_lsrtm &L, int op, int k0, int k1, Plan **out) {
+  seis_fd_ctx *ctx = L.ctx;
+  Plan *p = nullptr;
+  int rc = plan_create(ctx, op, k1 - k0, L.shots.data() + k0, &p);
+  if (rc) return rc;
+  p->exact = L.opts.exact != 0;
+  seis_fd_plan h{p};
+  if (op == OP_BORN_ADJ) {
+    rc = seis_fd_plan_set_snapshots(&h, L.opts.snap_every, L.opts.snap_dtype);
+    if (!rc && L.opts.checkpoint_every > 0)
+      rc = seis_fd_plan_set_checkpoints(&h, L.opts.checkpoint_every);
+  }
+  for (int j = 0; j < k1 - k0 && !rc; j++) {
+    const int k = k0 + j;
+    ShotDev &g = p->sd[j];
+    cudaError_t e = launch_gather_cols(L.d_v0, L.nz, L.d_cmap + L.cmap_off[k], g.nx, p->d_stage,
+                                       ctx->stream);
+    if (e == cudaSuccess)
+      e = launch_pad(p->d_stage, g.nx, g.nz, g.pml, g.LDZ, true, const_cast<float *>(g.vel),
+                     ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(const_cast<float *>(g.wav), L.d_wav, sizeof(float) * g.NT,
+                          cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e != cudaSuccess) rc = fail(ctx, SEIS_ERR_CUDA, "group plan: %s", cudaGetErrorString(e));
+    ctx->launches += 2;
+    if (op == OP_BORN_ADJ) g.rec = L.r + L.doff[k];
+  }
+  if (!rc && op == OP_BORN_ADJ) {
+    cudaError_t e = cudaMemcpyAsync(p->d_sd, p->sd.data(), sizeof(ShotDev) * p->nshot,
+                                    cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) rc = fail(ctx, SEIS_ERR_CUDA, "group plan: %s", cudaGetErrorString(e));
+  }
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return SEIS_OK;
+}
+
+// Free a group's plan once the stream has finished with it.
+int lsrtm_group_done(seis_fd_lsrtm &L, Plan *p) {
+  cudaError_t e = cudaStreamSynchronize(L.ctx->stream);
+  L.group_bytes = std::max(L.group_bytes, p->device_bytes);
+  delete p;
+  return e == cudaSuccess ? SEIS_OK : fail(L.ctx, SEIS_ERR_CUDA, "%s", cudaGetErrorString(e));
+}
+
+// s = L^T r: the adjoint plan's images scattered into the global grid, shot
+// after shot.
 int lsrtm_adjoint(seis_fd_lsrtm &L) {
   seis_fd_ctx *ctx = L.ctx;
   size_t nm = (size_t)L.nx * L.nz;
-  int rc = plan_run(*L.adj.p);
-  if (rc) return rc;
+  if (L.group == 0) {
+    int rc = plan_run(*L.adj.p);
+    if (rc) return rc;
+  }
   CK(cudaMemsetAsync(L.s, 0, sizeof(float) * nm, ctx->stream));
-  for (int k = 0; k < L.nshot; k++) {
-    const ShotDev &g = L.adj.p->sd[k];
-    CK(launch_scatter_cols(L.s, L.nz, L.d_ranges + L.range_off[k], L.g0[k], L.gcount[k], g.img,
-                           ctx->stream));
-    ctx->launches++;
+  const int G = L.group > 0 ? L.group : L.nshot;
+  for (int k0 = 0; k0 < L.nshot; k0 += G) {
+    const int k1 = std::min(k0 + G, L.nshot);
+    Plan *pa = L.adj.p;
+    if (L.group > 0) {
+      int rc = lsrtm_group_plan(L, OP_BORN_ADJ, k0, k1, &pa);
+      if (!rc) rc = enqueue_operator(*pa);
+      if (rc) {
+        if (pa) lsrtm_group_done(L, pa);
+        return rc;
+      }
+    }
+    for (int k = k0; k < k1; k++) {
+      const ShotDev &g = pa->sd[k - (L.group > 0 ? k0 : 0)];
+      CK(launch_scatter_cols(L.s, L.nz, L.d_ranges + L.range_off[k], L.g0[k], L.gcount[k], g.img,
+                             ctx->stream));
+      ctx->launches++;
+    }
+    if (L.group > 0) {
+      int rc = lsrtm_group_done(L, pa);
+      if (rc) return rc;
+    }
   }
   return SEIS_OK;
 }
 
-// q = L p into the Born plan's gathers: each shot's perturbation is its
-// sub-grid of p (column map), padded into the plan.
+// q = L p into the Born plan's gathers (grouped: into L.q): each shot's
+// perturbation is its sub-grid of p (column map), padded into the plan.
 int lsrtm_forward(seis_fd_lsrtm &L) {
   seis_fd_ctx *ctx = L.ctx;
-  Plan &pb = *L.born.p;
-  for (int k = 0; k < L.nshot; k++) {
-    const ShotDev &g = pb.sd[k];
-    CK(launch_gather_cols(L.p, L.nz, L.d_cmap + L.cmap_off[k], g.nx, pb.d_stage, ctx->stream));
-    CK(launch_pad(pb.d_stage, g.nx, g.nz, g.pml, g.LDZ, false, const_cast<float *>(g.dv),
-                  ctx->stream));
-    ctx->launches += 2;
+  const int G = L.group > 0 ? L.group : L.nshot;
+  for (int k0 = 0; k0 < L.nshot; k0 += G) {
+    const int k1 = std::min(k0 + G, L.nshot);
+    Plan *pb = L.born.p;
+    if (L.group > 0) {
+      int rc = lsrtm_group_plan(L, OP_BORN, k0, k1, &pb);
+      if (rc) return rc;
+    }
+    for (int k = k0; k < k1; k++) {
+      const ShotDev &g = pb->sd[k - (L.group > 0 ? k0 : 0)];
+      CK(launch_gather_cols(L.p, L.nz, L.d_cmap + L.cmap_off[k], g.nx, pb->d_stage, ctx->stream));
+      CK(launch_pad(pb->d_stage, g.nx, g.nz, g.pml, g.LDZ, false, const_cast<float *>(g.dv),
+                    ctx->stream));
+      ctx->launches += 2;
+    }
+    if (L.group == 0) return plan_run(*pb);
+    int rc = enqueue_operator(*pb);
+    for (int k = k0; k < k1 && !rc; k++) {
+      const size_t n = (size_t)L.shots[k].nx * L.nt;
+      cudaError_t e = cudaMemcpyAsync(L.q + L.doff[k], pb->sd[k - k0].rec, sizeof(float) * n,
+                                      cudaMemcpyDeviceToDevice, ctx->stream);
+      if (e != cudaSuccess) rc = fail(ctx, SEIS_ERR_CUDA, "%s", cudaGetErrorString(e));
+    }
+    int rc2 = lsrtm_group_done(L, pb);
+    if (rc) return rc;
+    if (rc2) return rc2;
   }
-  return plan_run(pb);
+  return SEIS_OK;
 }
 
-// out = sum over shots of <a_s, b_s> in data space; a from the Born plan's
-// gathers when `from_q`, else the residual.
+// q = L p of shot k in data space ([nt][nx_s])
+const float *lsrtm_q(const seis_fd_lsrtm &L, int k) {
+  return L.group > 0 ? L.q + L.doff[k] : L.born.p->sd[k].rec;
+}
+
+// out = sum over shots of <a_s, b_s> in data space; a from q = L p when
+// `q_left`, else the residual; b likewise.
 int data_dot(seis_fd_lsrtm &L, bool q_left, bool q_right, double *out) {
   seis_fd_ctx *ctx = L.ctx;
   for (int k = 0; k < L.nshot; k++) {
-    const float *q = L.born.p->sd[k].rec, *r = L.r + L.doff[k];
+    const float *q = lsrtm_q(L, k), *r = L.r + L.doff[k];
     size_t n = (size_t)L.shots[k].nx * L.nt;
     CK(launch_dot(q_left ? q : r, q_right ? q : r, n, ctx->d_partial, out, k > 0, ctx->stream));
     ctx->launches += 2;
@@ -1719,13 +1821,18 @@ int seis_fd_lsrtm_create_mapped(seis_fd_ctx *ctx, int nx, int nz, int nshot,
     }
     off += shots[k].nx;
   }
-  seis_lsrtm_opts o{1, SEIS_SNAP_BF16, 0, 0};
+  seis_lsrtm_opts o{1, SEIS_SNAP_BF16, 0, 0, 0};
   if (opts) o = *opts;
   seis_fd_lsrtm *L = new (std::nothrow) seis_fd_lsrtm();
   if (!L) return fail(ctx, SEIS_ERR_NOMEM, "host allocation failed");
   L->ctx = ctx;
   L->nx = nx; L->nz = nz; L->nshot = nshot; L->nt = shots[0].nt;
   L->shots.assign(shots, shots + nshot);
+  L->gz.resize(nshot);
+  for (int k = 0; k < nshot; k++) {  // group plans are built after this call returns
+    L->gz[k].assign(shots[k].gz, shots[k].gz + shots[k].nx);
+    L->shots[k].gz = L->gz[k].data();
+  }
   std::vector<int2> ranges;
   off = 0;
   for (int k = 0; k < nshot; k++) {
@@ -1746,11 +1853,18 @@ int seis_fd_lsrtm_create_mapped(seis_fd_ctx *ctx, int nx, int nz, int nshot,
     }
   }
   Plan *pb = nullptr, *pa = nullptr;
-  rc = plan_create(ctx, OP_BORN, nshot, shots, &pb);
-  if (!rc) rc = plan_create(ctx, OP_BORN_ADJ, nshot, shots, &pa);
-  L->born.p = pb;
-  L->adj.p = pa;
-  if (!rc) {
+  L->opts = o;
+  L->group = (o.group_shots > 0 && o.group_shots < nshot) ? o.group_shots : 0;
+  if (o.snap_every < 1 || (o.checkpoint_every > 0 && o.checkpoint_every % o.snap_every != 0))
+    rc = fail(ctx, SEIS_ERR_ARG, "lsrtm: snapshot interval %d, checkpoint interval %d",
+              o.snap_every, o.checkpoint_every);
+  if (!rc && L->group == 0) {
+    rc = plan_create(ctx, OP_BORN, nshot, shots, &pb);
+    if (!rc) rc = plan_create(ctx, OP_BORN_ADJ, nshot, shots, &pa);
+    L->born.p = pb;
+    L->adj.p = pa;
+  }
+  if (!rc && L->group == 0) {
     pb->exact = o.exact != 0;
     pa->exact = o.exact != 0;
     seis_fd_plan h{pa};
@@ -1774,11 +1888,22 @@ int seis_fd_lsrtm_create_mapped(seis_fd_ctx *ctx, int nx, int nz, int nshot,
   }
   if (!rc) rc = L->alloc(&L->d_cmap, off);
   if (!rc) rc = L->alloc(&L->d_ranges, ranges.size());
+  if (!rc && L->group > 0) {
+    size_t st = 0;
+    for (int k = 0; k < nshot; k++) st = std::max(st, (size_t)shots[k].nx * L->nt);
+    rc = L->alloc(&L->d_v0, nm);
+    if (!rc) rc = L->alloc(&L->d_wav, (size_t)(L->nt + shots[0].ndel));
+    if (!rc) rc = L->alloc(&L->q, L->ndata);
+    if (!rc) rc = L->alloc(&L->stage, st);
+  }
   if (!rc) {
     // the adjoint plan reads its receiver data straight from the residual
-    for (int k = 0; k < nshot; k++) pa->sd[k].rec = L->r + L->doff[k];
-    cudaError_t e = cudaMemcpyAsync(pa->d_sd, pa->sd.data(), sizeof(ShotDev) * nshot,
-                                    cudaMemcpyHostToDevice, ctx->stream);
+    cudaError_t e = cudaSuccess;
+    if (pa) {
+      for (int k = 0; k < nshot; k++) pa->sd[k].rec = L->r + L->doff[k];
+      e = cudaMemcpyAsync(pa->d_sd, pa->sd.data(), sizeof(ShotDev) * nshot,
+                          cudaMemcpyHostToDevice, ctx->stream);
+    }
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(L->d_cmap, colmap, sizeof(int) * off, cudaMemcpyHostToDevice,
                           ctx->stream);
@@ -1825,6 +1950,16 @@ int seis_fd_lsrtm_set_background(seis_fd_lsrtm *L, const float *h_v0, const floa
   int rc = begin(L->ctx);
   if (rc) return rc;
   if (!h_v0 || !h_wav) return fail(L->ctx, SEIS_ERR_ARG, "null array");
+  if (L->group > 0) {  // group plans take their sub-grids from the device copy
+    seis_fd_ctx *ctx = L->ctx;
+    const int NT = L->nt + L->shots[0].ndel;
+    CK(cudaMemcpyAsync(L->d_v0, h_v0, sizeof(float) * L->nx * L->nz, cudaMemcpyHostToDevice,
+                       L->ctx->stream));
+    CK(cudaMemcpyAsync(L->d_wav, h_wav, sizeof(float) * NT, cudaMemcpyHostToDevice,
+                       L->ctx->stream));
+    L->ready = false;
+    return sync(L->ctx);
+  }
   std::vector<float> sub;
   for (int k = 0; k < L->nshot && !rc; k++) {
     const std::vector<int> &m = L->cmap[k];
@@ -1848,10 +1983,10 @@ int seis_fd_lsrtm_set_data(seis_fd_lsrtm *L, int shot, const float *h_d) {
   if (rc) return rc;
   if (shot < 0 || shot >= L->nshot || !h_d) return fail(ctx, SEIS_ERR_ARG, "shot %d", shot);
   const int nxs = L->shots[shot].nx;
-  Plan &pb = *L->born.p;
-  CK(cudaMemcpyAsync(pb.d_stage, h_d, sizeof(float) * nxs * L->nt, cudaMemcpyHostToDevice,
+  float *stage = L->group > 0 ? L->stage : L->born.p->d_stage;
+  CK(cudaMemcpyAsync(stage, h_d, sizeof(float) * nxs * L->nt, cudaMemcpyHostToDevice,
                      ctx->stream));
-  CK(launch_transpose(pb.d_stage, nxs, L->nt, L->dobs + L->doff[shot], ctx->stream));
+  CK(launch_transpose(stage, nxs, L->nt, L->dobs + L->doff[shot], ctx->stream));
   ctx->launches++;
   L->ready = false;
   return sync(ctx);
@@ -1902,7 +2037,7 @@ int seis_fd_lsrtm_phase_update(seis_fd_lsrtm *L, const double *d_qq, float *d_s,
   CK(launch_ratio(gamma, d_qq, alpha, ctx->stream));
   CK(launch_axpby_dev(L->m, L->p, alpha, 1.0, nullptr, 1.0, nm, ctx->stream));
   for (int k = 0; k < L->nshot; k++)
-    CK(launch_axpby_dev(L->r + L->doff[k], L->born.p->sd[k].rec, alpha, -1.0, nullptr, 1.0,
+    CK(launch_axpby_dev(L->r + L->doff[k], lsrtm_q(*L, k), alpha, -1.0, nullptr, 1.0,
                         (size_t)L->shots[k].nx * L->nt, ctx->stream));
   ctx->launches += 2 + L->nshot;
   rc = data_dot(*L, false, false, d_rr);
@@ -1982,16 +2117,20 @@ int seis_fd_lsrtm_model(seis_fd_lsrtm *L, float *h_m) {
 int64_t seis_fd_lsrtm_cell_updates(const seis_fd_lsrtm *L) {
   if (!L) return 0;
   int64_t c = 0;
-  // Born (two fields), the adjoint's reverse pass, and with checkpoints the
-  // recomputed source field
-  const int64_t ck = L->adj.p->ck_every > 0 ? 1 : 0;
-  for (const ShotDev &g : L->born.p->sd)
-    c += (int64_t)g.NX * g.NZ * (2LL * g.NT + g.NT + 1 + ck * g.NT);
+  // Born (two fields), the adjoint's reverse pass, with checkpoints the
+  // recomputed source field, with shot groups the source pass of every run
+  const int64_t ck = L->opts.checkpoint_every > 0 ? 1 : 0, gr = L->group > 0 ? 1 : 0;
+  for (const seis_shot_desc &d : L->shots) {
+    const int64_t NX = d.nx + 2 * d.pml, NZ = d.nz + 2 * d.pml, NT = d.nt + d.ndel;
+    c += NX * NZ * (2 * NT + NT + 1 + ck * NT + gr * NT);
+  }
   return c;
 }
 
 int64_t seis_fd_lsrtm_device_bytes(const seis_fd_lsrtm *L) {
-  return L ? L->device_bytes + L->born.p->device_bytes + L->adj.p->device_bytes : 0;
+  if (!L) return 0;
+  if (L->group > 0) return L->device_bytes + L->group_bytes;  // one group's plan at a time
+  return L->device_bytes + L->born.p->device_bytes + L->adj.p->device_bytes;
 }
 
 }  // extern "C"

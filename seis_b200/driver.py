@@ -165,12 +165,14 @@ class Driver:
         return ss
 
     def lsrtm(self, niter: int, born_data: bool = False, snap_every: int = 1,
-              snap_dtype: int = SNAP_BF16, exact: bool = False, checkpoint_every: int = 0):
+              snap_dtype: int = SNAP_BF16, exact: bool = False, checkpoint_every: int = 0,
+              group_shots: int = 0):
         """(model [nx][nz], [|d|^2, |r|^2 per iteration]) of CGLS over all shots;
-        checkpoint_every > 0 keeps source-field checkpoints instead of every snapshot."""
+        checkpoint_every > 0 keeps source-field checkpoints instead of every snapshot,
+        group_shots > 0 builds the plans of that many shots at a time."""
         img = np.zeros((self.params.nx, self.params.nz), np.float32)
         rr = np.zeros(niter + 1, np.float64)
-        o = LsrtmOptsC(snap_every, snap_dtype, 1 if exact else 0, checkpoint_every)
+        o = LsrtmOptsC(snap_every, snap_dtype, 1 if exact else 0, checkpoint_every, group_shots)
         self._run(self.L.seis_driver_lsrtm(self.h, 1 if born_data else 0, niter, ctypes.byref(o),
                                            img.ctypes.data, rr.ctypes.data), "lsrtm")
         return img, rr
@@ -205,6 +207,8 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=0, help="shots per device batch (0: all)")
     ap.add_argument("--checkpoint-every", type=int, default=0,
                     help="lsrtm: source-field checkpoint interval (0: keep every snapshot)")
+    ap.add_argument("--group-shots", type=int, default=0,
+                    help="lsrtm: shots whose plans are built at a time (0: all)")
     ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args(argv)
     if a.op == "plane_prepare":
@@ -228,7 +232,8 @@ def main(argv=None):
                 img = d.illum_plane()
             else:
                 img, rr = d.lsrtm(a.niter if a.niter is not None else p.maxiter, a.born_data,
-                                  checkpoint_every=a.checkpoint_every)
+                                  checkpoint_every=a.checkpoint_every,
+                                  group_shots=a.group_shots)
                 for i, r in enumerate(rr):
                     print(f"iteration {i}: |r|^2 = {r:.6e}")
             if a.out:

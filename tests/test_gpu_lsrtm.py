@@ -127,3 +127,17 @@ def test_lsrtm_with_checkpoints_is_bit_identical(ctx):
     assert rr0 == rr1
     assert np.array_equal(h0, h1)
     assert np.array_equal(m0, m1)
+
+
+@pytest.mark.parametrize("group,ck", [(1, 0), (2, 20)])
+def test_lsrtm_in_shot_groups_is_bit_identical(ctx, group, ck):
+    """CGLS that builds the plans of `group` shots at a time in every operator
+    application (for surveys whose plans do not fit on the device at once),
+    with or without checkpoints, reproduces the solver that keeps every plan,
+    model and residual history bit for bit."""
+    sv = survey()
+    m0, rr0, h0 = run_gpu(ctx, sv, 3, snap_every=4)
+    m1, rr1, h1 = run_gpu(ctx, sv, 3, snap_every=4, checkpoint_every=ck, group_shots=group)
+    assert rr0 == rr1
+    assert np.array_equal(h0, h1)
+    assert np.array_equal(m0, m1)
