@@ -213,7 +213,11 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": "Gcell-updates/s", "value": v, "unit": "Gcell/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": args.workload},
+            "data": "synthetic (layered + faulted 1200x400 model; observed data = Born of the true "
+                    "perturbation)",
+            "config": {"workload": args.workload, "shots_per_gpu": len(sv.shots),
+                       "grid": "1200x400 at 10 m, pml 40", "nt": sv.shots[0].nt,
+                       "ndel": sv.shots[0].ndel},
             "cpu_baseline": {"value": v, "unit": "Gcell/s", "cores": r["cores"], "kind": r["kind"],
                              "sample": r["sample"]},
             "e2e": {"value": v, "unit": "Gcell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
