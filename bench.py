@@ -385,7 +385,6 @@ def main():
     h_m = torch.empty((sv.nx, sv.nz), dtype=torch.float32).pin_memory()
     h_rr = torch.empty(2, dtype=torch.float64)
     L = ctx.L
-    import ctypes
 
     def e2e_step():
         ctx.check(L.seis_fd_lsrtm_set_background(ls.h, h_v0.data_ptr(), h_wav.data_ptr()))

@@ -1,7 +1,6 @@
 """The shot driver's file readers against the reference's own: the parameter
 file (Inversion::readParamFile with ParserFromFile rules) and the coordinate
 file (Coords).  Host-only."""
-import os
 
 import numpy as np
 import pytest

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from helpers import fd_args, golden_cases, golden_ids
+from helpers import golden_cases, golden_ids
 from seis_b200 import Shot, fd
 from seis_b200._lib import OP_ILLUM, batch
 
