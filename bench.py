@@ -32,6 +32,12 @@ iteration time.
   oracle/_ref) on shot 0 with the time loop cut short, all host threads,
   expressed as this iteration's cell-updates per second.
 
+* ``largest_config_sample``: 4 shots of the largest configuration (4000 x
+  1000 cells, 8120 steps, velocities capped at 3000 m/s where the reference's
+  scheme is stable), one batched BF16 LSRTM iteration (snapshots kept whole
+  and checkpointed) against the plain FP32 path, and the image error between
+  the two storage choices (``python -m seis_b200.probe large``).
+
 Under torchrun (N > 1) every rank runs its own 32-shot survey (weak scaling).
 """
 from __future__ import annotations
@@ -322,6 +328,8 @@ def main():
     ap.add_argument("--workload", default="lsrtm_iter")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-large-sample", action="store_true",
+                    help="skip the 4-shot sample of the largest configuration")
     ap.add_argument("--nt", type=int, default=5000,
                     help="recorded time samples (a shorter loop of the same launches, for profiling)")
     args = ap.parse_args()
@@ -448,6 +456,15 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sv)
     ctx.close()
+    if world == 1 and not args.no_large_sample and args.nt == 5000:
+        # the largest configuration (4000 x 1000, 8120 steps) on 4 of its shots:
+        # batched BF16 LSRTM iteration against the plain FP32 path, image error
+        # between their storage choices (seis_b200.probe large)
+        try:
+            from seis_b200 import probe
+            line["largest_config_sample"] = probe.large(4)
+        except Exception as e:  # reported, not fatal: the headline line stands
+            line["largest_config_sample"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     barrier(world)
