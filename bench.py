@@ -150,11 +150,34 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
+def load_synth():
+    """seis_b200/synth.py loaded as a module of its own (numpy and scipy only),
+    so that the reference arm builds the same inputs without importing this
+    package or loading its CUDA library."""
+    import importlib.util
+    path = os.path.join(ROOT, "seis_b200", "synth.py")
+    spec = importlib.util.spec_from_file_location("seis_bench_synth", path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def workload(name: str, rank: int, nt: int = 5000):
-    from seis_b200 import synth
+    synth = load_synth()
     if name == "lsrtm_iter":
         return synth.lsrtm(nt=nt)
     raise SystemExit(f"unknown workload {name}")
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 SNAP_EVERY = 4
@@ -179,13 +202,13 @@ def cpu_baseline(sv, steps_cap: int = 150):
     time, i.e. the reference's speed on the same job."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    from seis_b200 import Shot
+    import dataclasses
     s0 = sv.shots[0]
-    s = Shot(nx=s0.nx, nz=s0.nz, pml=s0.pml, nt=steps_cap, ndel=s0.ndel, sx=s0.sx, sz=s0.sz,
-             dt=s0.dt, dx=s0.dx, dz=s0.dz, gz=s0.gz)
-    wav = sv.wavelet()[:s.NT]
-    vel, dv = sv.sub(sv.vel0, 0), sv.sub(sv.dv, 0)
+    s = dataclasses.replace(s0, nt=steps_cap)
     kind = "reference" if O.ref_available() else "port"
+    make = lambda dt, fr, d, n: O.ricker(dt, fr, d, n, impl="ref" if kind == "reference" else "oracle")
+    wav = sv.wavelet(make)[:s.NT]
+    vel, dv = sv.sub(sv.vel0, 0), sv.sub(sv.dv, 0)
     cores = len(os.sched_getaffinity(0))
     impl = "ref" if kind == "reference" else "oracle"
     if kind == "reference":
@@ -201,6 +224,7 @@ def cpu_baseline(sv, steps_cap: int = 150):
     dt = t_born + t_adj
     cells = iteration_cells([s])
     return {"value": cells / dt / 1e9, "unit": "Gcell/s", "cores": cores, "kind": kind,
+            "cpu": cpu_model(),
             "sample": f"forward (Born) {t_born:.2f} s + adjoint (RTM) {t_adj:.2f} s of shot 0 "
                       f"({s.nx}x{s.nz}, pml {s.pml}), {s.NT} of {s0.NT} steps; the reference has "
                       f"no CG, so one iteration = these two calls per shot"}

@@ -286,11 +286,17 @@ int seis_fd_vec_dot(seis_fd_ctx *ctx, const float *d_a, const float *d_b, size_t
  * null = legacy default stream) of the current device; the call returns once
  * the work is enqueued.  Its scratch, 16384 partial sums (128 KiB) in a fixed
  * array inside the library, limits n to SEIS_DOT_NOALLOC_MAX_N elements;
- * larger n returns SEIS_ERR_ARG.  The first call on a device looks up that
- * array's device address; make it before any stream capture.  All calls on a
- * device share the array: calls whose GPU work overlaps (e.g. on two streams
- * without ordering between them) race and give wrong sums.  A message for
- * any error goes to err (err_len bytes, may be null). */
+ * larger n returns SEIS_ERR_ARG.  Every GPU that loads the library holds the
+ * array until the process exits.  The array's device address belongs to the
+ * current CUDA context (each context, e.g. one made by cuCtxCreate or the
+ * primary context made again after cudaDeviceReset, has its own copy): a call
+ * outside stream capture looks it up in the current context; a call whose
+ * stream is capturing uses the address recorded by an earlier call in the
+ * same context and returns SEIS_ERR_STATE if there was none, so make one call
+ * in each context before capturing.  All calls in a context share the array:
+ * calls whose GPU work overlaps (e.g. on two streams without ordering between
+ * them) race and give wrong sums.  A message for any error goes to err
+ * (err_len bytes, may be null). */
 #define SEIS_DOT_NOALLOC_MAX_N ((size_t)16384 * 4096)
 int seis_fd_vec_dot_noalloc(const float *d_a, const float *d_b, size_t n, double *d_out,
                             void *stream, char *err, size_t err_len);

@@ -58,11 +58,18 @@ class Shot:
         return self.nt + self.ndel
 
     def to_c(self) -> ShotDescC:
-        d = ShotDescC(self.nx, self.nz, self.pml, self.nt, self.ndel, self.sx, self.sz,
-                      self.dt, self.dx, self.dz,
-                      self.gz.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
-        d._keep = self.gz  # keep the receiver array alive with the struct
-        return d
+        return shot_desc(self)
+
+
+def shot_desc(s) -> ShotDescC:
+    """``seis_shot_desc`` of any record with the fields of ``Shot`` (this
+    class, or the survey records of ``seis_b200.synth``)."""
+    gz = np.ascontiguousarray(s.gz, np.int32)
+    d = ShotDescC(int(s.nx), int(s.nz), int(s.pml), int(s.nt), int(s.ndel), int(s.sx), int(s.sz),
+                  float(s.dt), float(s.dx), float(s.dz),
+                  gz.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    d._keep = gz  # keep the receiver array alive with the struct
+    return d
 
 
 class LsrtmOptsC(ctypes.Structure):
@@ -213,7 +220,7 @@ def ricker(dt: float, fr: float, delay: int, n: int) -> np.ndarray:
 def validate_shot(shot: "Shot") -> str:
     """Host-only argument check of one shot; returns '' if valid, else the reason."""
     buf = ctypes.create_string_buffer(512)
-    rc = lib().seis_fd_validate_shot(shot.to_c(), buf, 512)
+    rc = lib().seis_fd_validate_shot(shot_desc(shot), buf, 512)
     return "" if rc == SEIS_OK else (buf.value.decode() or f"error {rc}")
 
 
@@ -228,7 +235,7 @@ def shot_array(shots):
     arr = (ShotDescC * len(shots))()
     keep = []
     for i, s in enumerate(shots):
-        c = s.to_c()
+        c = shot_desc(s)
         keep.append(c._keep)
         arr[i] = c
     arr._keep = keep

@@ -13,6 +13,7 @@
 // (src/util/arraymath.h:230-299): each product is formed in FP32 and the sum
 // is carried in FP64.  The reduction is deterministic but chunked differently
 // from seis_fd_vec_dot, so the two agree to FP64 rounding, not bit for bit.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -77,9 +78,36 @@ __global__ void __launch_bounds__(NA_VT) na_dot_final_kernel(const double *__res
   if (threadIdx.x == 0) *out = acc;
 }
 
-constexpr int NA_MAX_DEVICES = 64;
+// The array's device address belongs to a CUDA context: each context that
+// loads the library (the device's primary context, a context the host
+// application made with cuCtxCreate, or the primary context made again after
+// cudaDeviceReset) holds its own copy at its own address.  A call outside
+// stream capture looks the address up in the current context every time and
+// records it here under that context's handle; a call made while its stream
+// is capturing (where the lookup, which may load the module, must not run)
+// takes the recorded address of the current context, and fails if there is
+// none.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    return cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess
+               ? reinterpret_cast<CtxGetCurrentFn>(p)
+               : nullptr;
+  }();
+  return fn;
+}
+
+constexpr int NA_MAX_CONTEXTS = 64;
+struct ScratchSlot {
+  CUcontext ctx;
+  double *ptr;
+};
 std::mutex g_setup_mu;
-double *g_scratch_ptr[NA_MAX_DEVICES] = {};  // device address of the scratch, per device
+ScratchSlot g_slots[NA_MAX_CONTEXTS] = {};
+int g_next_slot = 0;
 
 int na_error(char *err, size_t err_len, int rc, const char *fmt, ...) {
   if (err && err_len > 0) {
@@ -106,29 +134,45 @@ extern "C" int seis_fd_vec_dot_noalloc(const float *d_a, const float *d_b, size_
                     "seis_fd_vec_dot_noalloc: n = %zu exceeds the maximum of %zu elements "
                     "(the fixed scratch holds %d partial sums of %d elements each)",
                     n, (size_t)SEIS_DOT_NOALLOC_MAX_N, NA_MAX_PARTS, NA_CHUNK);
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cap);
   if (e != cudaSuccess)
-    return na_error(err, err_len, SEIS_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= NA_MAX_DEVICES)
-    return na_error(err, err_len, SEIS_ERR_ARG, "device %d beyond the %d supported", dev,
-                    NA_MAX_DEVICES);
+    return na_error(err, err_len, SEIS_ERR_CUDA, "cudaStreamIsCapturing: %s",
+                    cudaGetErrorString(e));
+  void *found = nullptr;
+  if (cap == cudaStreamCaptureStatusNone) {
+    // the host-side name of the array is not a device address: look the
+    // address up in the current context (this also makes the device's
+    // primary context current on a thread that has none yet)
+    e = cudaGetSymbolAddress(&found, g_dot_scratch);
+    if (e != cudaSuccess)
+      return na_error(err, err_len, SEIS_ERR_CUDA, "cudaGetSymbolAddress: %s",
+                      cudaGetErrorString(e));
+  }
+  CtxGetCurrentFn get = ctx_get_current();
+  CUcontext cur = nullptr;
+  if (!get || get(&cur) != CUDA_SUCCESS || !cur)
+    return na_error(err, err_len, SEIS_ERR_CUDA, "no current CUDA context");
   double *scratch = nullptr;
   {
-    // set-up, once per device, with that device current: the host-side name
-    // of the array is not a device address, so look the address up
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_ptr[dev]) {
-      void *p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_dot_scratch);
-      if (e != cudaSuccess)
-        return na_error(err, err_len, SEIS_ERR_CUDA, "cudaGetSymbolAddress: %s",
-                        cudaGetErrorString(e));
-      g_scratch_ptr[dev] = static_cast<double *>(p);
+    int slot = -1;
+    for (int i = 0; i < NA_MAX_CONTEXTS; i++)
+      if (g_slots[i].ctx == cur) slot = i;
+    if (found) {
+      if (slot < 0) {
+        slot = g_next_slot;
+        g_next_slot = (g_next_slot + 1) % NA_MAX_CONTEXTS;
+      }
+      g_slots[slot] = ScratchSlot{cur, static_cast<double *>(found)};
+    } else if (slot < 0) {
+      return na_error(err, err_len, SEIS_ERR_STATE,
+                      "seis_fd_vec_dot_noalloc: first call in this CUDA context made during "
+                      "stream capture; make one call outside capture first");
     }
-    scratch = g_scratch_ptr[dev];
+    scratch = g_slots[slot].ptr;
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int nparts = (int)((n + NA_CHUNK - 1) / NA_CHUNK);
   if (nparts > 0) na_dot_chunk_kernel<<<nparts, NA_VT, 0, s>>>(d_a, d_b, n, scratch);
   na_dot_final_kernel<<<1, NA_VT, 0, s>>>(scratch, nparts, d_out);

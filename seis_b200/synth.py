@@ -17,18 +17,46 @@ Workloads (pml = 40 everywhere):
   nt 5000, dt 0.8 ms.
 * ``large_sweep``      4000x1000 at 5 m, layers + anomalies 1500-5500 m/s, 256
   shots of aperture 1000-4000, nt 8000, dt 0.5 ms, 25 Hz.
+
+The module imports numpy and scipy only (no part of this package), so that a
+CPU-only measurement of the reference can build the same inputs without
+loading the CUDA library; its shot records carry the fields of the C ABI's
+``seis_shot_desc`` and are accepted wherever a ``seis_b200.Shot`` is.
 """
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 from typing import List
 
 import numpy as np
 
-from ._lib import Shot
-
 PML = 40
+
+
+@dataclass
+class ShotGeom:
+    """One shot's scalars (src/util/fd.h:3-5) and receiver depths ``gz[nx]``."""
+    nx: int
+    nz: int
+    pml: int
+    nt: int
+    ndel: int
+    sx: int
+    sz: int
+    dt: float
+    dx: float
+    dz: float
+    gz: np.ndarray = field(default=None)
+
+    def __post_init__(self):
+        if self.gz is None:
+            self.gz = np.zeros(self.nx, np.int32)
+        self.gz = np.ascontiguousarray(self.gz, np.int32)
+
+    @property
+    def NT(self) -> int:
+        return self.nt + self.ndel
 
 
 def ndel_for(fr: float, dt: float) -> int:
@@ -37,7 +65,7 @@ def ndel_for(fr: float, dt: float) -> int:
 
 def ricker(dt: float, fr: float, delay: int, n: int) -> np.ndarray:
     """Reference Ricker wavelet (src/util/wavelet.cpp:7-18), via the library."""
-    from ._lib import ricker as _ricker
+    from seis_b200._lib import ricker as _ricker
     return _ricker(dt, fr, delay, n)
 
 
@@ -55,7 +83,7 @@ class Survey:
     fr: float
     vel: np.ndarray          # true velocity [nx][nz]
     vel0: np.ndarray         # smooth background [nx][nz]
-    shots: List[Shot]        # per-shot aperture descriptors
+    shots: List[ShotGeom]    # per-shot aperture descriptors
     x0: List[int]            # first global column of each aperture
 
     @property
@@ -66,8 +94,10 @@ class Survey:
     def dv(self) -> np.ndarray:
         return (self.vel - self.vel0).astype(np.float32)
 
-    def wavelet(self) -> np.ndarray:
-        return ricker(self.dt, self.fr, self.ndel, self.nt + self.ndel)
+    def wavelet(self, make=None) -> np.ndarray:
+        """The survey's wavelet; ``make(dt, fr, delay, n)`` defaults to the
+        library's ``seis_fd_ricker``."""
+        return (make or ricker)(self.dt, self.fr, self.ndel, self.nt + self.ndel)
 
     def sub(self, a: np.ndarray, s: int) -> np.ndarray:
         """Aperture sub-model of shot s (columns x0 .. x0+nx)."""
@@ -113,8 +143,8 @@ def _anomalies(v, n, rng, amp=300.0, rmin=5, rmax=20):
     return v
 
 
-def _shot(nx_sub, nz, sx, sz, gz, dt, dx, dz, nt, fr, pml=PML) -> Shot:
-    return Shot(nx=nx_sub, nz=nz, pml=pml, nt=nt, ndel=ndel_for(fr, dt), sx=sx, sz=sz,
+def _shot(nx_sub, nz, sx, sz, gz, dt, dx, dz, nt, fr, pml=PML) -> ShotGeom:
+    return ShotGeom(nx=nx_sub, nz=nz, pml=pml, nt=nt, ndel=ndel_for(fr, dt), sx=sx, sz=sz,
                 dt=dt, dx=dx, dz=dz, gz=np.full(nx_sub, gz, np.int32))
 
 

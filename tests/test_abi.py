@@ -69,3 +69,20 @@ def test_validate_rejects_receiver_on_frame():
     s = base_shot()
     s.gz[3] = -5
     assert "gz[3]" in validate_shot(s)
+
+
+def test_noalloc_dot_rejects_null_pointers_without_a_device():
+    """seis_fd_vec_dot_noalloc checks its pointers before any CUDA call: null
+    operands give SEIS_ERR_ARG with a message, and a null message buffer is
+    accepted."""
+    f = seis_b200.lib().seis_fd_vec_dot_noalloc
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                  ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    f.restype = ctypes.c_int
+    err = ctypes.create_string_buffer(128)
+    fake = ctypes.c_void_p(0x1000)  # never dereferenced: the call fails first
+    assert f(None, fake, 8, fake, None, err, len(err)) == -1
+    assert b"null pointer" in err.value
+    assert f(fake, fake, 8, None, None, err, len(err)) == -1
+    assert b"null pointer" in err.value
+    assert f(fake, None, 8, fake, None, None, 0) == -1
