@@ -1,0 +1,121 @@
+"""The CUDA path at the full sizes of the two single-shot benchmark
+configurations, against the reference's own outputs (tests/golden/configs.npz,
+made by tests/golden/make_config_golden.py from the compiled reference).
+
+* modeling, 201 x 201, nt 2000 + 100 (src/util/fd.cpp:15-80);
+* Born modeling, 737 x 240, nt 4000 + 75 (fd.cpp:81-177), and the reference
+  RTM of that Born gather (fd.cpp:592-719);
+* the dot-product test of the Born operator the solver runs (fast build) and
+  its exact adjoint on the 737 x 240 shot with the seeded N(0, 1) vectors.
+
+Bar: the exact build equals the reference bit for bit (SHA-256 of the float32
+output, and the stored subsample element by element); the fast build is within
+1e-5 relative L2 of it."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, fd_args, rel_l2
+from seis_b200 import fd, synth
+from seis_b200._lib import IN_DV, IN_VEL, IN_WAVELET, OP_BORN, OP_MODELING, OUT_GATHER, Plan
+
+pytestmark = pytest.mark.gpu
+FAST_TOL = 1e-5
+STEP_C1, STEP_BORN, STEP_IMG = 16, 48, 8  # subsamples of the fixture
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return dict(np.load(os.path.join(GOLDEN, "configs.npz")))
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()
+
+
+def run_fast(ctx, op, s, wav, vel, dv=None):
+    with Plan(ctx, op, [s]) as p:
+        p.set_exact(False)
+        p.set(0, IN_VEL, vel)
+        p.set(0, IN_WAVELET, wav)
+        if dv is not None:
+            p.set(0, IN_DV, dv)
+        p.run()
+        return p.get(0, OUT_GATHER)
+
+
+def test_config1_modeling_201x201(ctx, gold):
+    c = synth.single_modeling()
+    s = c.shots[0]
+    assert sha(c.vel) == str(gold["c1_vel_sha"]), "model generation changed"
+    wav = c.wavelet()
+    assert sha(wav) == str(gold["c1_wav_sha"])
+    rec = fd.modeling(*fd_args(s), wav, c.vel, ctx=ctx)
+    assert rec.shape == (201, 2000)
+    assert np.array_equal(rec[::STEP_C1], gold["c1_rec_sub"])
+    assert sha(rec) == str(gold["c1_rec_sha"])
+    fast = run_fast(ctx, OP_MODELING, s, wav, c.vel)
+    err = rel_l2(fast, rec)
+    print(f"config 1 fast vs reference: rel L2 {err:.2e}")
+    assert err <= FAST_TOL
+
+
+@pytest.fixture(scope="module")
+def config2(ctx, gold):
+    c = synth.born_rtm_pair()
+    assert sha(c.vel) == str(gold["c2_vel_sha"]) and sha(c.vel0) == str(gold["c2_vel0_sha"]), \
+        "model generation changed"
+    wav = c.wavelet()
+    assert sha(wav) == str(gold["c2_wav_sha"])
+    born = fd.forward(*fd_args(c.shots[0]), wav, c.vel0, c.dv, ctx=ctx)
+    return c, wav, born
+
+
+def test_config2_born_737x240(ctx, gold, config2):
+    c, wav, born = config2
+    assert born.shape == (737, 4000)
+    assert np.array_equal(born[::STEP_BORN], gold["c2_born_sub"])
+    assert sha(born) == str(gold["c2_born_sha"])
+    fast = run_fast(ctx, OP_BORN, c.shots[0], wav, c.vel0, c.dv)
+    err = rel_l2(fast, born)
+    print(f"config 2 Born fast vs reference: rel L2 {err:.2e}")
+    assert err <= FAST_TOL
+
+
+def test_config2_rtm_737x240(ctx, gold, config2):
+    c, wav, born = config2
+    # the input gather is the reference's own (the exact build equals it bit
+    # for bit: previous test)
+    img = fd.adjoint(*fd_args(c.shots[0]), wav, c.vel0, born, ctx=ctx)
+    assert img.shape == (737, 240)
+    assert np.array_equal(img[::STEP_IMG], gold["c2_img_sub"])
+    assert sha(img) == str(gold["c2_img_sha"])
+
+
+def test_config2_dot_product(ctx, gold, config2):
+    """<L m, d> against <m, L^T d> in FP32 over 4075 steps.  For N(0, 1)
+    vectors the inner product itself cancels down to about |Lm||d|/sqrt(N)
+    (N = 2.9e6 samples), so the plain relative mismatch is the operators'
+    FP32 rounding (~1e-7 of |Lm||d|) amplified about 1700 times; the transpose
+    itself is exact: the FP64 pair of the same operators (the restatement's
+    double build, stored with the fixture) agrees to 1.5e-15 of |Lm||d| and,
+    through the same cancellation, to 2.1e-12 plainly."""
+    c, wav, _ = config2
+    s = c.shots[0]
+    rng = np.random.default_rng(22)
+    m = rng.standard_normal((s.nx, s.nz)).astype(np.float32)
+    d = rng.standard_normal((s.nx, s.nt)).astype(np.float32)
+    Lm = run_fast(ctx, OP_BORN, s, wav, c.vel0, m).astype(np.float64)
+    Ltd = fd.born_adjoint(*fd_args(s), wav, c.vel0, d, ctx=ctx).astype(np.float64)
+    a, b = float(np.sum(Lm * d)), float(np.sum(m * Ltd))
+    rel = abs(a - b) / max(abs(a), abs(b))
+    rel_norm = abs(a - b) / (np.linalg.norm(Lm) * np.linalg.norm(d))
+    a64, b64, nlm64, nd64 = (float(v) for v in gold["c2_dot_fp64"])
+    rel64 = abs(a64 - b64) / max(abs(a64), abs(b64))
+    print(f"config 2 dot test FP32: {a:.9e} {b:.9e} rel {rel:.3e} rel/(|Lm||d|) {rel_norm:.3e}; "
+          f"FP64 pair rel {rel64:.3e}; <Lm,d> FP32 vs FP64 {abs(a - a64) / abs(a64):.2e}")
+    assert rel64 <= 1e-11 and abs(a64 - b64) / (nlm64 * nd64) <= 1e-14
+    assert rel_norm <= 1e-6, (a, b)
+    assert rel <= 2e-3, (a, b)
