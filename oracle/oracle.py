@@ -294,6 +294,18 @@ def born_adjoint(shot, wav, vel, rec, prec="f64", every=1):
     return img
 
 
+def born_adjoint_ck(shot, wav, vel, rec, ck, prec="f64"):
+    """born_adjoint with every = 1 in bounded memory: the source terms are
+    recomputed per ck-step segment from checkpoints (the same image)."""
+    dt, (gz, wav, vel, rec) = _prep(shot, prec, "oracle", wav, vel, rec)
+    img = np.zeros((shot.nx, shot.nz), dt)
+    rc = getattr(oracle_lib(), f"orc_born_adjoint_ck_{prec}")(
+        *_common_args(shot, prec), _ptr(gz), _ptr(wav), _ptr(vel), _ptr(rec), _I(ck), _ptr(img))
+    if rc != 0:
+        raise RuntimeError(f"oracle born_adjoint_ck failed ({rc})")
+    return img
+
+
 def lsrtm_cgls(nx, nz, shots, x0, wav, v0, dobs, niter, prec="f64", cols=None):
     """CGLS on the global model (the solver the reference declares as
     Inversion::conope_MPI / cgsolver_MPI, src/lsrtm/inversion.h:81,87, without

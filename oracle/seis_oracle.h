@@ -56,7 +56,11 @@ extern "C" {
   int orc_born_adjoint_thin_##S(R dt, R dx, R dz, int nt, int ndel, int nx,     \
                                 int nz, int pml, int sx, int sz, const int *gz, \
                                 const R *wav, const R *vel, const R *rec,       \
-                                int every, R *img);
+                                int every, R *img);                            \
+  int orc_born_adjoint_ck_##S(R dt, R dx, R dz, int nt, int ndel, int nx,       \
+                              int nz, int pml, int sx, int sz, const int *gz,   \
+                              const R *wav, const R *vel, const R *rec, int ck, \
+                              R *img);
 
 SEIS_ORACLE_DECL(float, f32)
 SEIS_ORACLE_DECL(double, f64)

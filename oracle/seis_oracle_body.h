@@ -1040,6 +1040,76 @@ int F(orc_born_adjoint_thin)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx
   return 0;
 }
 
+/* The same operator as orc_born_adjoint_thin with every = 1, for grids whose
+ * source terms of all steps do not fit in host memory: the background pass
+ * keeps its two time levels before every ck-th step, and the reverse sweep
+ * recomputes the source terms of one ck-step segment at a time from them.
+ * The recomputed terms are the stored ones, so the image is the same bit for
+ * bit. */
+int F(orc_born_adjoint_ck)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz,
+                           int pml, int sx, int sz, const int *gz, const REAL *wav,
+                           const REAL *vel, const REAL *rec, int ck, REAL *img)
+{
+  if (ck < 1) return -2;
+  F(grid_t) gg = F(mkgrid)(dt, dx, dz, nx, nz, pml);
+  const F(grid_t) *g = &gg;
+  F(coefs_t) c;
+  F(coefs_init)(g, vel, &c, 1);
+  size_t n = (size_t)g->NX * g->NZ;
+  int sxp = sx + pml, szp = sz + pml, NT = nt + ndel;
+  int nseg = (NT + ck - 1) / ck;
+  REAL idt2 = KR(1.0) / dt / dt;
+  REAL *states = F(zalloc)(2 * n * (size_t)nseg);  /* (u0, u1) before step s*ck */
+  REAL *laps = F(zalloc)(n * (size_t)ck);
+  REAL *u0 = F(zalloc)(n), *u1 = F(zalloc)(n), *u2 = F(zalloc)(n);
+  if (!states || !laps || !u0 || !u1 || !u2) return -1;
+  for (int it = 0; it < NT; it++) {
+    if (it % ck == 0) {
+      memcpy(states + 2 * n * (size_t)(it / ck), u0, n * sizeof(REAL));
+      memcpy(states + 2 * n * (size_t)(it / ck) + n, u1, n * sizeof(REAL));
+    }
+    F(twoway)(g, &c, u1, u0, u2);
+    if (it >= 1) AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+    F(absorb)(g, &c, u2, u1, u0);
+    REAL *t = u0; u0 = u1; u1 = u2; u2 = t;
+  }
+  REAL *A = F(zalloc)(n), *B = F(zalloc)(n), *C = F(zalloc)(n);
+  REAL *u3b = F(zalloc)(n), *u31b = F(zalloc)(n), *gp = F(zalloc)(n);
+  int seg = -1;
+  for (int k = NT - 1; k >= 0; k--) {
+    if (k / ck != seg) {  /* recompute the source terms of steps s0 .. k */
+      seg = k / ck;
+      int s0 = seg * ck;
+      memcpy(u0, states + 2 * n * (size_t)seg, n * sizeof(REAL));
+      memcpy(u1, states + 2 * n * (size_t)seg + n, n * sizeof(REAL));
+      for (int it = s0; it <= k; it++) {
+        F(twoway)(g, &c, u1, u0, u2);
+        if (it >= 1) AT(u2, sxp, szp) += AT(c.vt2, sxp, szp) * wav[it - 1];
+        F(absorb)(g, &c, u2, u1, u0);
+        for (size_t i = 0; i < n; i++)
+          laps[(size_t)(it - s0) * n + i] = (u2[i] + u0[i] - KR(2) * u1[i]) * idt2;
+        REAL *t = u0; u0 = u1; u1 = u2; u2 = t;
+      }
+    }
+    if (k >= ndel)
+      for (int ix = 0; ix < nx; ix++) AT(A, ix + pml, gz[ix] + pml) += rec[(size_t)ix * nt + (k - ndel)];
+    F(step_T)(g, &c, A, B, C, u3b, u31b);
+    const REAL *lap = laps + (size_t)(k - seg * ck) * n;
+    for (size_t i = 0; i < n; i++) gp[i] += KR(1) * lap[i] * u3b[i];
+    REAL *t = A; A = B; B = C; C = t;
+    memset(C, 0, n * sizeof(REAL));
+  }
+  for (int ix = 0; ix < nx; ix++)
+    for (int iz = 0; iz < nz; iz++) {
+      int jx = ix + pml, jz = iz + pml;
+      img[(size_t)ix * nz + iz] = AT(c.vt2, jx, jz) * AT(c.vel3, jx, jz) * AT(gp, jx, jz);
+    }
+  free(states); free(laps); free(u0); free(u1); free(u2);
+  free(A); free(B); free(C); free(u3b); free(u31b); free(gp);
+  F(coefs_free)(&c);
+  return 0;
+}
+
 int F(orc_born_adjoint)(REAL dt, REAL dx, REAL dz, int nt, int ndel, int nx, int nz, int pml,
                         int sx, int sz, const int *gz, const REAL *wav, const REAL *vel,
                         const REAL *rec, REAL *img)
