@@ -144,8 +144,6 @@ struct Plan {
   ShotDev *d_sd = nullptr;
   Tile *d_tiles = nullptr;
   int2 *d_cols = nullptr;
-  std::vector<PadChunk> chunks;  // pad cells of the batch (absorbing kernel)
-  PadChunk *d_chunks = nullptr;
   float *d_taps = nullptr;
   float *d_stage = nullptr;  // staging for unpadded uploads / transposes
   size_t stage_elems = 0;
@@ -213,11 +211,10 @@ void fill_scalars(ShotDev &g, const seis_shot_desc &s) {
   g.idt2 = 1.0f / dt / dt;
 }
 
-// Tiles of every shot's padded grid; interior tiles (every cell inside the
-// model and 8th order) take the kernel's fast path.  All interior tiles come
-// first, then all pad tiles, each group interleaved across shots: the
-// persistent CTAs then run one code path at a time (instruction-cache
-// locality) and shots are spread evenly over the SMs.
+// Tiles of every shot's padded grid; interior tiles (every cell a model cell
+// in the 8th-order region) take the kernel without boundary logic.  All
+// interior tiles come first, then all pad tiles, each group interleaved
+// across shots, so that shots are spread evenly over the SMs.
 void build_tiles(Plan &p) {
   p.tiles.clear();
   p.cols.clear();
@@ -225,11 +222,8 @@ void build_tiles(Plan &p) {
   size_t most = 0;
   for (int s = 0; s < p.nshot; s++) {
     const ShotDev &g = p.sd[s];
-    // interior tiles keep one cell off the model edge: the one-way update of
-    // the first pad ring reads the two-way values of the edge cells, which
-    // only pad tiles keep
-    int lox = std::max(g.pml + 1, 4), hix = std::min(g.pml + g.nx - 1, g.NX - 4);
-    int loz = std::max(g.pml + 1, 4), hiz = std::min(g.pml + g.nz - 1, g.NZ - 4);
+    const int lox = std::max(g.pml, 4), hix = std::min(g.pml + g.nx, g.NX - 4);
+    const int loz = std::max(g.pml, 4), hiz = std::min(g.pml + g.nz, g.NZ - 4);
     for (int x0 = 0; x0 < g.NX; x0 += TX)
       for (int z0 = 0; z0 < g.NZ; z0 += TZ) {
         bool in = x0 >= lox && x0 + TX <= hix && z0 >= loz && z0 + TZ <= hiz;
@@ -245,27 +239,6 @@ void build_tiles(Plan &p) {
   p.n_int = 0;
   for (const Tile &t : p.tiles) p.n_int += t.kind == TILE_INTERIOR;
   p.n_pad = (int)p.tiles.size() - p.n_int;
-  // pad cells: left and right blocks over the full height, top and bottom
-  // blocks over the model columns, cut into rectangles of at most
-  // ABS_NT * ABS_CPT cells (z fastest)
-  p.chunks.clear();
-  constexpr int CH = ABS_NT * ABS_CPT;
-  auto block = [&](int s, int xa, int xb, int za, int zb) {
-    const int R = zb - za, Cn = xb - xa;
-    if (R <= 0 || Cn <= 0) return;
-    const int k = (R + CH - 1) / CH, nrows = (R + k - 1) / k;
-    const int ncols = std::max(1, CH / nrows);
-    for (int x = xa; x < xb; x += ncols)
-      for (int z = za; z < zb; z += nrows)
-        p.chunks.push_back(PadChunk{s, x, z, std::min(ncols, xb - x), std::min(nrows, zb - z)});
-  };
-  for (int s = 0; s < p.nshot; s++) {
-    const ShotDev &g = p.sd[s];
-    block(s, 0, g.pml, 0, g.NZ);
-    block(s, g.pml + g.nx, g.NX, 0, g.NZ);
-    block(s, g.pml, g.pml + g.nx, 0, g.pml);
-    block(s, g.pml, g.pml + g.nx, g.pml + g.nz, g.NZ);
-  }
 }
 
 // Tiles for the exact adjoint: an interior tile holds no pad cell and no
@@ -460,8 +433,6 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (op == OP_BORN || op == OP_RTM || op == OP_BORN_PLANE || op == OP_RTM_PLANE ||
         op == OP_RTM_TRUE || op == OP_RTM_UPDOWN)
       for (int k = 0; k < 3 && rc == SEIS_OK; k++) rc = alloc_field(*p, g, &g.fb[k]);
-    if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.u3s[0]);
-    if (rc == SEIS_OK && (op == OP_BORN || op == OP_BORN_PLANE)) rc = alloc_field(*p, g, &g.u3s[1]);
     float *vel = nullptr, *dv = nullptr, *wav = nullptr, *rec = nullptr;
     int *gzd = nullptr;
     if (rc == SEIS_OK) rc = alloc_field(*p, g, &vel);
@@ -519,7 +490,6 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
   }
   if (rc == SEIS_OK) rc = p->alloc(&p->d_tiles, p->tiles.size());
   if (rc == SEIS_OK) rc = p->alloc(&p->d_adj_tiles, p->adj_tiles.size());
-  if (rc == SEIS_OK) rc = p->alloc(&p->d_chunks, p->chunks.size());
   if (rc == SEIS_OK) rc = p->alloc(&p->d_adj_chunks, p->adj_chunks.size());
   const bool imaging = op == OP_RTM || op == OP_RTM_PLANE || op == OP_RTM_TRUE || op == OP_RTM_UPDOWN;
   if (rc == SEIS_OK && imaging) rc = p->alloc(&p->d_cols, p->cols.size());
@@ -533,9 +503,6 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
                           cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(p->d_adj_tiles, p->adj_tiles.data(), sizeof(Tile) * p->adj_tiles.size(),
-                          cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && !p->chunks.empty())
-      e = cudaMemcpyAsync(p->d_chunks, p->chunks.data(), sizeof(PadChunk) * p->chunks.size(),
                           cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && !p->adj_chunks.empty())
       e = cudaMemcpyAsync(p->d_adj_chunks, p->adj_chunks.data(),
@@ -568,14 +535,11 @@ int step(Plan &p, int mode, const StepArgs &a, const ShotDev *shots = nullptr) {
   seis_fd_ctx *ctx = p.ctx;
   CK(cudaEventRecord(ctx->fork, ctx->stream));
   CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
-  StepArgs b = a;
-  b.chunks = p.d_chunks;
-  b.nchunks = (int)p.chunks.size();
-  CK(launch_step(mode, p.exact, shots ? shots : p.d_sd, p.d_tiles, p.n_int, p.n_pad, ctx->num_sms, b,
+  CK(launch_step(mode, p.exact, shots ? shots : p.d_sd, p.d_tiles, p.n_int, p.n_pad, ctx->num_sms, a,
                  ctx->d_err, ctx->stream, ctx->aux));
   CK(cudaEventRecord(ctx->join, ctx->aux));
   CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
-  ctx->launches += (p.n_int > 0) + (p.n_pad > 0) + (p.n_pad > 0 && b.nchunks > 0);
+  ctx->launches += (p.n_int > 0) + (p.n_pad > 0);
   return SEIS_OK;
 }
 
@@ -1328,8 +1292,10 @@ int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double 
   StepArgs a{};
   a.nshots = p.nshot;
   a.strip_k = -1;
-  a.chunks = adj ? p.d_adj_chunks : p.d_chunks;
-  a.nchunks = (int)(adj ? p.adj_chunks.size() : p.chunks.size());
+  if (adj) {
+    a.chunks = p.d_adj_chunks;
+    a.nchunks = (int)p.adj_chunks.size();
+  }
   double t_int = 0, t_pad = 0, t_step = 0;
   for (int k = 0; k < steps; k++) {
     a.rot = k; a.rot_b = k;

@@ -29,11 +29,8 @@ struct Tile {
   int shot, x0, z0, kind;
 };
 
-// A rectangle of pad cells (one shot, ncols x nrows cells, z fastest) given to
-// one CTA of the absorbing-boundary kernel (ABS_NT threads, ABS_CPT cells
-// each); ncols * nrows <= ABS_NT * ABS_CPT.
-constexpr int ABS_NT = 256;
-constexpr int ABS_CPT = 4;
+// A rectangle of ring cells (one shot, ncols x nrows cells, z fastest) given
+// to one CTA of the adjoint's ring kernel.
 struct PadChunk {
   int shot, x0, z0, ncols, nrows;
 };
@@ -89,10 +86,6 @@ struct ShotDev {
   int snap_every;
   int ntz;               // tiles along z of this shot (scale indexing)
   int pad_;
-  // two-way values of the cells of pad tiles before the absorbing blend
-  // (field A or the receiver field; Born: [1] = scattered field), read by the
-  // absorbing-boundary kernel
-  float *u3s[2];
   float *illum;          // source illumination [nx][nz] (illumination plans)
   const float *sou;      // areal source [NT][nx] at row szp (plane-wave plans), else null
   float *comp;           // four imaging accumulators [4][nx][nz] (adjointUpDown)
@@ -118,7 +111,7 @@ struct StepArgs {
   int snap_k = -1;   // snapshot index written (forward) or imaged (adjoint)
   float img_w = 0.f; // adjoint: weight of the imaging term (snapshot interval)
   int illum_on = 0;  // add the square of every model cell's new value to g.illum
-  const PadChunk *chunks = nullptr;  // pad cells of the batch (absorbing kernel)
+  const PadChunk *chunks = nullptr;  // ring cells of the batch (adjoint ring kernel)
   int nchunks = 0;
 };
 
@@ -150,7 +143,7 @@ enum StepMode : int {
 
 // One time step over every tile of a batch: the first n_int tiles are
 // interior tiles (one CTA each, stream s_int), the next n_pad pad tiles
-// (persistent CTAs, stream s_pad).  `exact` selects the build that rounds like
+// (one CTA each, stream s_pad; the absorbing boundary fused in).  `exact` selects the build that rounds like
 // the reference; otherwise the contracted build.
 cudaError_t launch_step(int mode, bool exact, const ShotDev *d_shots, const Tile *d_tiles,
                         int n_int, int n_pad, int num_sms, const StepArgs &a, int *d_err,

@@ -7,37 +7,35 @@ namespace seis {
 namespace SEIS_NS {
 
 namespace {
-template <int MODE, int KIND>
+template <int MODE>
 cudaError_t setup() {
-  return cudaFuncSetAttribute(tile_kernel<MODE, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)TCfg<MODE, KIND>::bytes);
+  cudaError_t e = cudaFuncSetAttribute(tile_kernel<MODE, TILE_INTERIOR>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)TCfg<MODE, TILE_INTERIOR>::bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(pad_tile_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)PCfg<MODE>::bytes);
+  return e;
 }
 
-// Interior tiles on s_int; pad tiles and then the absorbing kernel on s_pad
-// (it reads the pad tiles' two-way values).
+// Interior tiles on s_int, pad tiles on s_pad (concurrently).
 template <int MODE>
 cudaError_t launch_t(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
                      const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad) {
   if (n_int > 0)
     tile_kernel<MODE, TILE_INTERIOR><<<n_int, NT_T, TCfg<MODE, TILE_INTERIOR>::bytes, s_int>>>(
         d_shots, d_tiles, a, d_err);
-  if (n_pad > 0) {
-    tile_kernel<MODE, TILE_PAD><<<n_pad, NT_T, TCfg<MODE, TILE_PAD>::bytes, s_pad>>>(
-        d_shots, d_tiles + n_int, a, d_err);
-    if (a.nchunks > 0)
-      absorb_kernel<MODE><<<a.nchunks, ABS_NT, 0, s_pad>>>(d_shots, a.chunks, a);
-  }
+  if (n_pad > 0)
+    pad_tile_kernel<MODE><<<n_pad, NT_T, PCfg<MODE>::bytes, s_pad>>>(d_shots, d_tiles + n_int, a,
+                                                                     d_err);
   return cudaGetLastError();
 }
 }  // namespace
 
 cudaError_t configure() {
-  cudaError_t e = setup<MODE_MODEL, TILE_INTERIOR>();
-  if (e == cudaSuccess) e = setup<MODE_MODEL, TILE_PAD>();
-  if (e == cudaSuccess) e = setup<MODE_RCV, TILE_INTERIOR>();
-  if (e == cudaSuccess) e = setup<MODE_RCV, TILE_PAD>();
-  if (e == cudaSuccess) e = setup<MODE_BORN, TILE_INTERIOR>();
-  if (e == cudaSuccess) e = setup<MODE_BORN, TILE_PAD>();
+  cudaError_t e = setup<MODE_MODEL>();
+  if (e == cudaSuccess) e = setup<MODE_RCV>();
+  if (e == cudaSuccess) e = setup<MODE_BORN>();
   return e;
 }
 

@@ -1,22 +1,18 @@
 // Time-step kernels of the 2-D acoustic FD engine (sm_100a).
 //
-// One step of a batch is two launches over the tile list plus one over the
-// pad cells:
+// One step of a batch is two launches over the tile list, on two streams:
 //  * tile_kernel<MODE, TILE_INTERIOR>: tiles whose every cell is a model cell
 //    in the 8th-order region; the absorbing blend is the identity there
 //    (w = 1, u31 = 0; src/util/fd.cpp:55-56);
-//  * tile_kernel<MODE, TILE_PAD>: tiles touching the pad, the frame, the
-//    low-order rings or the model edge: the same two-way update (the frame
-//    and low-order cells by the per-cell formula), model cells finished as in
-//    the interior, and the two-way value u3 of every cell kept in the shot's
-//    scratch field;
-//  * absorb_kernel<MODE>: every pad cell, the one-way update from u3 and the
-//    blend (processBoundary, fd.cpp:1092-1179), elementwise from global
-//    memory (no halo exchange, no barrier).
-// Tile kernels: one 32 x 64 tile per CTA, 2-D TMA tensor copies of the
-// current field (5-column / 8-row halo), the previous field, the velocity and,
-// for Born, the perturbation (1-column / 8-row halo) into shared memory (one
-// mbarrier, no multicast); each thread owns a 4-row x 2-column micro-tile.
+//  * pad_tile_kernel<MODE>: every other tile, in one pass: the two-way update
+//    (frame and low-order cells by the per-cell formula), injection, the
+//    two-way values of the tile and a one-cell halo kept in shared memory,
+//    then the one-way update and blend of the pad cells (processBoundary,
+//    fd.cpp:1092-1179).
+// Both: one 32 x 64 tile per CTA, 2-D TMA tensor copies of the current field
+// (5-column / 8-row halo), the previous field, the velocity and, for Born, the
+// perturbation (1-column / 8-row halo) into shared memory (one mbarrier, no
+// multicast); each thread owns a 4-row x 2-column micro-tile.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -280,13 +276,83 @@ struct GA {
   }
 };
 
+// Two-way values of a pad tile and its one-cell halo in shared memory:
+// columns x0-1 .. x0+TX, rows z0-4 .. z0+TZ+3 (the tile's row quads stay
+// 16-byte aligned; only rows z0-1 .. z0+TZ are used).
+constexpr int U3C = TX + 2;
+constexpr int U3R = TZ + 8;
+constexpr int U3N = U3C * U3R;
+constexpr int NHALO = 2 * (TX + 2) + 2 * TZ;  // halo ring cells of a tile
+struct UA {
+  float *s;
+  int x0, z0;
+  __device__ __forceinline__ float &ref(int ix, int iz) const {
+    return s[(ix - x0 + 1) * U3R + (iz - z0 + 4)];
+  }
+  __device__ __forceinline__ float operator()(int ix, int iz) const { return ref(ix, iz); }
+};
+// Halo cell i of the tile at (x0, z0): the rows above and below the tile
+// (TX + 2 cells each, corners included), then the columns left and right.
+__device__ __forceinline__ void halo_cell(int i, int x0, int z0, int &hx, int &hz) {
+  if (i < 2 * (TX + 2)) {
+    hx = x0 - 1 + i % (TX + 2);
+    hz = i < TX + 2 ? z0 - 1 : z0 + TZ;
+  } else {
+    const int j = i - 2 * (TX + 2);
+    hx = j < TZ ? x0 - 1 : x0 + TX;
+    hz = z0 + j % TZ;
+  }
+}
+
+template <int MODE>
+struct PCfg {
+  static constexpr int NF = MODE == MODE_BORN ? 2 : 1;  // fields with two-way arrays
+  static constexpr int BUF = TCfg<MODE, TILE_PAD>::BUF;
+  static constexpr size_t bytes = sizeof(float) * ((size_t)BUF + (size_t)NF * U3N) + 16;
+  static constexpr int MIN_CTAS = MODE == MODE_BORN ? 2 : 3;
+};
+
+// Stage the arrays of one tile with 2-D tensor copies: rows [z0 - ZM, z0 +
+// TZ + ZM) of columns [x0 - halo, x0 + TX + halo), addressed from the
+// allocation start (row + ZM, column + XM), so coordinates are never negative
+// and the row coordinate is a multiple of TZ (16-byte aligned).  Thread 0
+// issues the copies; every thread then waits on the mbarrier.
+template <int MODE, int KIND>
+__device__ __forceinline__ bool stage_tile(const ShotDev &g, const StepArgs &a, int x0, int z0,
+                                           float *bb, uint64_t *bar) {
+  using C = TCfg<MODE, KIND>;
+  if (threadIdx.x == 0) {
+    fence_proxy_async();
+    mbar_expect_tx(bar, (uint32_t)(C::BUF * sizeof(float)));
+    const int ra = a.rot % 3, rca = (a.rot + 1) % 3, rb = a.rot_b % 3, rcb = (a.rot_b + 1) % 3;
+    int maps[6];
+    if (MODE == MODE_RCV) {
+      maps[0] = MAP_FB_WIDE + rcb; maps[1] = MAP_FB_NARROW + rb; maps[2] = MAP_VEL;
+    } else if (!C::BORN) {
+      maps[0] = MAP_FA_WIDE + rca; maps[1] = MAP_FA_NARROW + ra; maps[2] = MAP_VEL;
+    } else {
+      maps[0] = MAP_FA_WIDE + rca; maps[1] = MAP_FB_WIDE + rcb; maps[2] = MAP_FA_NARROW + ra;
+      maps[3] = MAP_VEL; maps[4] = MAP_FB_NARROW + rb; maps[5] = MAP_DV;
+    }
+#pragma unroll
+    for (int arr = 0; arr < C::NCUR + C::NOTH; arr++) {
+      const int col = x0 + XM - (arr < C::NCUR ? HXC : 1);
+      const int off = arr < C::NCUR ? arr * CW_C * SR : C::NCUR * CW_C * SR + (arr - C::NCUR) * CW_P * SR;
+      tma_load_2d(bb + off, g.maps + maps[arr], z0, col, bar);
+    }
+  }
+  return mbar_wait(bar, 0);
+}
+
+// Interior tiles: every cell a model cell in the 8th-order region, where the
+// absorbing blend is the identity (w = 1, u31 = 0; src/util/fd.cpp:55-56).
 template <int MODE, int KIND>
 __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict__ shots,
                                                        const Tile *__restrict__ tiles, StepArgs a,
                                                        int *__restrict__ err) {
+  static_assert(KIND == TILE_INTERIOR, "pad tiles run pad_tile_kernel");
   using C = TCfg<MODE, KIND>;
   constexpr bool BORN = C::BORN;
-  constexpr bool PAD = KIND == TILE_PAD;
   extern __shared__ __align__(128) unsigned char smraw[];
   float *bb = reinterpret_cast<float *>(smraw);
   uint64_t *bar = reinterpret_cast<uint64_t *>(bb + C::BUF);
@@ -302,39 +368,13 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
   }
   __syncthreads();
   const ShotDev &g = sg;
-
-  // staged arrays: cur A [, cur B] (wide halo), then prev A, vel [, prev B, dv]
-  auto arr_off = [](int arr) -> int {
-    return arr < C::NCUR ? arr * CW_C * SR : C::NCUR * CW_C * SR + (arr - C::NCUR) * CW_P * SR;
-  };
-  // One 2-D tensor copy per staged array: rows [z0 - ZM, z0 + TZ + ZM) of
-  // columns [x0 - halo, x0 + TX + halo), addressed from the allocation start
-  // (row + ZM, column + XM), so coordinates are never negative and the row
-  // coordinate is a multiple of TZ (16-byte aligned).
-  if (tid == 0) {
-    fence_proxy_async();
-    mbar_expect_tx(bar, (uint32_t)(C::BUF * sizeof(float)));
-    const int ra = a.rot % 3, rca = (a.rot + 1) % 3, rb = a.rot_b % 3, rcb = (a.rot_b + 1) % 3;
-    int maps[6];
-    if (MODE == MODE_RCV) {
-      maps[0] = MAP_FB_WIDE + rcb; maps[1] = MAP_FB_NARROW + rb; maps[2] = MAP_VEL;
-    } else if (!BORN) {
-      maps[0] = MAP_FA_WIDE + rca; maps[1] = MAP_FA_NARROW + ra; maps[2] = MAP_VEL;
-    } else {
-      maps[0] = MAP_FA_WIDE + rca; maps[1] = MAP_FB_WIDE + rcb; maps[2] = MAP_FA_NARROW + ra;
-      maps[3] = MAP_VEL; maps[4] = MAP_FB_NARROW + rb; maps[5] = MAP_DV;
-    }
-#pragma unroll
-    for (int arr = 0; arr < C::NCUR + C::NOTH; arr++) {
-      const int col = t.x0 + XM - (arr < C::NCUR ? HXC : 1);
-      tma_load_2d(bb + arr_off(arr), g.maps + maps[arr], t.z0, col, bar);
-    }
-  }
-  if (!mbar_wait(bar, 0)) {
+  if (!stage_tile<MODE, KIND>(g, a, t.x0, t.z0, bb, bar)) {
     if (tid == 0) atomicExch(err, 1);
     return;
   }
-
+  auto arr_off = [](int arr) -> int {
+    return arr < C::NCUR ? arr * CW_C * SR : C::NCUR * CW_C * SR + (arr - C::NCUR) * CW_P * SR;
+  };
   StepArgs aa = a;
   if (MODE != MODE_RCV && aa.rec_k >= g.nt) aa.rec_k = -1;
   float *na = g.fa[(a.rot + 2) % 3];
@@ -353,20 +393,144 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
   const bool record = MODE != MODE_RCV && aa.rec_k >= 0;
   const bool snap = MODE != MODE_RCV && aa.snap_k >= 0 && g.snap != nullptr;
 
-  // Cells within 3 of the grid edge (frame, fd.cpp:1057-1091; low-order rings,
-  // :1226-1241) take the general formula.  All threads form them over the
-  // tile's edge bands (a cell in two bands is formed twice, to the same
-  // value) into the tile's cells of the two-way scratch field, which the
-  // cell's own thread reads back after the barrier and then overwrites with
-  // the injected value; every other cell takes the 8th-order vector path.  The band pass
-  // reads global memory: the frame's normal extrapolation reaches the
-  // velocity two columns inside the grid, past the staged one-column halo of
-  // a tile that holds only the last column.
-  const int xe = PAD ? min(x0 + TX, g.NX) : 0, ze = PAD ? min(z0 + TZ, g.NZ) : 0;
-  const bool edge = PAD && (x0 <= 3 || z0 <= 3 || xe - 1 >= g.NX - 4 || ze - 1 >= g.NZ - 4);
-  auto near_edge = [&](int cxj, int iz) {
-    return min(min(cxj, iz), min(g.NX - 1 - cxj, g.NZ - 1 - iz)) <= 3;
+  int gzq[2];
+#pragma unroll
+  for (int j = 0; j < 2; j++) gzq[j] = g.gz[ix + j - g.pml] + g.pml;
+  float lv[8];
+  int lx[8], lz[8];
+  unsigned mask = 0;
+  float4 o[2], cen[2], prv[2], vel[2];
+  pair_twoway(CA, PA, VV, g, ix, iz0, o, cen, prv, vel);
+  float4 qs[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int cxj = ix + j;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int iz = iz0 + r;
+      lx[4 * j + r] = cxj;
+      lz[4 * j + r] = iz;
+      Coef kk = coef(comp(vel[j], r), g);
+      const float out = inject<MODE>(g, aa, cxj, iz, gzq[j], comp(o[j], r), kk.vt2) + 0.0f;
+      set_comp(o[j], r, out);
+      if (!BORN && record && iz == gzq[j]) g.rec[(size_t)aa.rec_k * g.nx + (cxj - g.pml)] = out;
+      if (MODE != MODE_BORN && aa.strip_k >= 0) save_strips(g, aa.strip_k, cxj, iz, out);
+      if (MODE == MODE_MODEL && aa.illum_on) {  // illum, fd.cpp:317-319
+        float *ss = g.illum + (size_t)(cxj - g.pml) * g.nz + (iz - g.pml);
+        *ss = *ss + out * out;
+      }
+      lv[4 * j + r] = 0.0f;
+      if (BORN || snap) {  // scattering source vt2 lap vel3 dv, fd.cpp:134-139
+        float lap = (out + comp(prv[j], r) - 2.0f * comp(cen[j], r)) * g.idt2;
+        lv[4 * j + r] = lap;
+        mask |= 1u << (4 * j + r);
+        if (BORN) {
+          float vv = comp(vel[j], r);
+          float vel3 = 2.0f / (vv * vv * vv);
+          set_comp(qs[j], r, kk.vt2 * lap * vel3 * DV(cxj, iz));
+        }
+      }
+    }
+    *reinterpret_cast<float4 *>(out_a + (size_t)cxj * g.LDZ + iz0) = o[j];
+  }
+  if (BORN) {
+    float4 ob[2], cb4[2], pb4[2], vb4[2];
+    pair_twoway(CB, PB, VV, g, ix, iz0, ob, cb4, pb4, vb4);
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const int cxj = ix + j;
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const int iz = iz0 + r;
+        const float out = comp(ob[j], r) + comp(qs[j], r) + 0.0f;
+        set_comp(ob[j], r, out);
+        if (record && iz == gzq[j]) g.rec[(size_t)aa.rec_k * g.nx + (cxj - g.pml)] = out;
+      }
+      *reinterpret_cast<float4 *>(nb_ + (size_t)cxj * g.LDZ + iz0) = ob[j];
+    }
+  }
+  if (snap) snap_write<NT_T, 8>(g, aa.snap_k, x0, z0, lv, lx, lz, mask, red);
+}
+
+// Pad tiles: tiles with a pad cell, a cell within 3 of the grid edge (frame,
+// src/util/fd.cpp:1057-1091; low-order rings, :1226-1241) or a model cell the
+// interior tiles do not take.  One pass per step:
+//  1. the two-way values (before injection) of the tile's and its halo's
+//     cells within 3 of the grid edge, by the per-cell formula over global
+//     memory (the frame's normal extrapolation reaches two cells inside),
+//     into shared memory;
+//  2. the tile's cells: the 8th-order two-way value from shared memory (or
+//     the value of step 1), injection (fd.cpp:49-51) and, for Born, the
+//     scattering source; model cells are final (w = 1) and stored, every
+//     two-way value is kept in shared memory;
+//  3. the same for the halo ring (one cell around the tile), which the
+//     one-way update of the tile's edge cells reads;
+//  4. every pad cell: the one-way update from the two-way values and the
+//     blend (processBoundary fd.cpp:1092-1179, :55-56), stored.
+// A halo cell's two-way value is formed by the same per-cell arithmetic as
+// in the tile that owns it.
+template <int MODE>
+__global__ void __launch_bounds__(NT_T, PCfg<MODE>::MIN_CTAS) pad_tile_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
+    int *__restrict__ err) {
+  using C = TCfg<MODE, TILE_PAD>;
+  constexpr bool BORN = C::BORN;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float *bb = reinterpret_cast<float *>(smraw);
+  float *u3m = bb + C::BUF;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(u3m + PCfg<MODE>::NF * U3N);
+  __shared__ ShotDev sg;
+  __shared__ float red[33];
+  const int tid = threadIdx.x;
+  const Tile t = tiles[blockIdx.x];
+  if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+    reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const ShotDev &g = sg;
+  const int x0 = t.x0, z0 = t.z0, NX = g.NX, NZ = g.NZ;
+  if (!stage_tile<MODE, TILE_PAD>(g, a, x0, z0, bb, bar)) {
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  auto arr_off = [](int arr) -> int {
+    return arr < C::NCUR ? arr * CW_C * SR : C::NCUR * CW_C * SR + (arr - C::NCUR) * CW_P * SR;
   };
+  StepArgs aa = a;
+  if (MODE != MODE_RCV && aa.rec_k >= g.nt) aa.rec_k = -1;
+  float *na = g.fa[(a.rot + 2) % 3];
+  float *nb_ = g.fb[(a.rot_b + 2) % 3];
+  float *out_a = MODE == MODE_RCV ? nb_ : na;
+  const int zm = z0 - ZM;
+  const SA CA{bb + arr_off(0), x0 - HXC, zm};
+  const SA CB{bb + arr_off(BORN ? 1 : 0), x0 - HXC, zm};
+  const SA PA{bb + arr_off(C::NCUR), x0 - 1, zm};
+  const SA VV{bb + arr_off(C::NCUR + 1), x0 - 1, zm};
+  const SA PB{bb + arr_off(BORN ? C::NCUR + 2 : C::NCUR), x0 - 1, zm};
+  const SA DV{bb + arr_off(BORN ? C::NCUR + 3 : C::NCUR + 1), x0 - 1, zm};
+  const UA UA_{u3m, x0, z0};
+  const UA UB_{u3m + (BORN ? U3N : 0), x0, z0};
+  const bool record = MODE != MODE_RCV && aa.rec_k >= 0;
+  const bool snap = MODE != MODE_RCV && aa.snap_k >= 0 && g.snap != nullptr;
+  auto near_edge = [&](int cx, int cz) {
+    return min(min(cx, cz), min(NX - 1 - cx, NZ - 1 - cz)) <= 3;
+  };
+  auto model = [&](int cx, int cz) {
+    return cx >= g.pml && cx < g.pml + g.nx && cz >= g.pml && cz < g.pml + g.nz;
+  };
+  auto rcv_row = [&](int cx) {
+    const int x = cx - g.pml;
+    return (x >= 0 && x < g.nx) ? g.gz[x] + g.pml : -1;
+  };
+
+  // 1. cells of the tile and its halo within 3 of the grid edge (a cell in two
+  // bands is formed twice, to the same value)
+  const int xa = max(x0 - 1, 0), xb = min(x0 + TX + 1, NX);
+  const int za = max(z0 - 1, 0), zb = min(z0 + TZ + 1, NZ);
+  const bool edge = xa <= 3 || za <= 3 || xb - 1 >= NX - 4 || zb - 1 >= NZ - 4;
   if (edge) {
     const int ra = a.rot % 3, rb = a.rot_b % 3;
     float *const *FA = MODE == MODE_RCV ? g.fb : g.fa;
@@ -375,81 +539,64 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
     const GA GCb{g.fb[(rb + 1) % 3], g.LDZ}, GPb{g.fb[rb], g.LDZ};
 #pragma unroll 1
     for (int b = 0; b < 4; b++) {  // top, bottom, left, right band
-      const int bxa = b == 3 ? max(x0, g.NX - 4) : x0, bxb = b == 2 ? min(xe, 4) : xe;
-      const int bza = b == 1 ? max(z0, g.NZ - 4) : z0, bzb = b == 0 ? min(ze, 4) : ze;
+      const int bxa = b == 3 ? max(xa, NX - 4) : xa, bxb = b == 2 ? min(xb, 4) : xb;
+      const int bza = b == 1 ? max(za, NZ - 4) : za, bzb = b == 0 ? min(zb, 4) : zb;
       const int nr = bzb - bza, nc = bxb - bxa;
       if (nr <= 0 || nc <= 0) continue;
       for (int i = tid; i < nr * nc; i += NT_T) {
-        const int cxj = bxa + i / nr, iz = bza + i % nr;
-        const size_t at = (size_t)cxj * g.LDZ + iz;
-        g.u3s[0][at] = twoway_cell(GCa, GPa, GV, g, cxj, iz);
-        if (BORN) g.u3s[1][at] = twoway_cell(GCb, GPb, GV, g, cxj, iz);
+        const int cx = bxa + i / nr, cz = bza + i % nr;
+        UA_.ref(cx, cz) = twoway_cell(GCa, GPa, GV, g, cx, cz);
+        if (BORN) UB_.ref(cx, cz) = twoway_cell(GCb, GPb, GV, g, cx, cz);
       }
     }
+    __syncthreads();
   }
-  if (PAD) __syncthreads();
 
-  auto in_grid = [&](int cxj, int iz) { return !PAD || (cxj < g.NX && iz < g.NZ); };
-  auto model = [&](int cxj, int iz) {
-    return !PAD || (cxj >= g.pml && cxj < g.pml + g.nx && iz >= g.pml && iz < g.pml + g.nz);
-  };
-
-  // One micro-tile (columns qx, qx+1, rows qz0 .. qz0+3): two-way values,
-  // injection, model cells finished (w = 1), every u3 of a pad tile kept.
-  // `vec`: all eight cells in the 8th-order region (vector path from shared
-  // memory); otherwise cell by cell with the general formula (frame,
-  // low-order rings, cells past the grid skipped).  lv/mask: source-term
-  // values of the model cells for the snapshot.
-  auto quad = [&](int qx, int qz0, bool vec, float (&lv)[8], int (&lx)[8], int (&lz)[8],
-                  unsigned &mask) {
-    auto twoway = [&](const SA &Cc, const SA &Pp, int f, float4 o[2], float4 cen[2],
-                      float4 prv[2], float4 vel[2]) {
-      pair_twoway(Cc, Pp, VV, g, qx, qz0, o, cen, prv, vel);
-      if (!vec) {  // cells within 3 of the grid edge from the band pass
+  // 2. the tile's cells, one 4-row x 2-column micro-tile per thread
+  const int qz = tid % QZ, cxp = tid / QZ;
+  const int ix = x0 + 2 * cxp, iz0 = z0 + 4 * qz;
+  float lv[8];
+  int lx[8], lz[8];
+  unsigned mask = 0;
 #pragma unroll
-        for (int j = 0; j < 2; j++)
-#pragma unroll
-          for (int r = 0; r < 4; r++) {
-            const int cxj = qx + j, iz = qz0 + r;
-            if (in_grid(cxj, iz) && near_edge(cxj, iz))
-              set_comp(o[j], r, g.u3s[f][(size_t)cxj * g.LDZ + iz]);
-          }
-      }
+  for (int k = 0; k < 8; k++) {
+    lv[k] = 0.0f;
+    lx[k] = ix + k / 4;
+    lz[k] = iz0 + k % 4;
+  }
+  const bool vecq = !edge || (ix >= 4 && ix + 1 <= NX - 5 && iz0 >= 4 && iz0 + 3 <= NZ - 5);
+  if (ix < NX && iz0 < NZ) {
+    auto quad_in = [&](int cx) { return cx < NX && iz0 + 3 < NZ; };
+    auto quad_model = [&](int cx) {
+      return cx >= g.pml && cx < g.pml + g.nx && iz0 >= g.pml && iz0 + 3 < g.pml + g.nz;
     };
-    // a column quad wholly in the grid (or wholly in the model) is stored as
-    // one vector; the other cells of a pad tile one by one
-    auto quad_in = [&](int cxj) { return !PAD || (cxj < g.NX && qz0 + 3 < g.NZ); };
-    auto quad_model = [&](int cxj) {
-      return !PAD || (cxj >= g.pml && cxj < g.pml + g.nx && qz0 >= g.pml && qz0 + 3 < g.pml + g.nz);
-    };
-    int gzq[2];
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-      int x = qx + j - g.pml;
-      gzq[j] = (x >= 0 && x < g.nx) ? g.gz[x] + g.pml : -1;
-    }
+    int gzq[2] = {rcv_row(ix), rcv_row(ix + 1)};
     float4 o[2], cen[2], prv[2], vel[2];
-    twoway(CA, PA, 0, o, cen, prv, vel);
+    pair_twoway(CA, PA, VV, g, ix, iz0, o, cen, prv, vel);
+    if (!vecq)
+#pragma unroll
+      for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+          if (ix + j < NX && iz0 + r < NZ && near_edge(ix + j, iz0 + r))
+            set_comp(o[j], r, UA_(ix + j, iz0 + r));
     float4 qs[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
 #pragma unroll
     for (int j = 0; j < 2; j++) {
-      const int cxj = qx + j;
+      const int cxj = ix + j;
       float4 u4 = o[j];
 #pragma unroll
       for (int r = 0; r < 4; r++) {
-        const int iz = qz0 + r;
-        lv[4 * j + r] = 0.0f;
-        lx[4 * j + r] = cxj;
-        lz[4 * j + r] = iz;
-        if (!in_grid(cxj, iz)) continue;
+        const int iz = iz0 + r;
+        if (cxj >= NX || iz >= NZ) continue;
         Coef kk = coef(comp(vel[j], r), g);
         const float u = inject<MODE>(g, aa, cxj, iz, gzq[j], comp(o[j], r), kk.vt2);
         set_comp(u4, r, u);
-        if (PAD && !quad_in(cxj)) g.u3s[0][(size_t)cxj * g.LDZ + iz] = u;
-        if (!model(cxj, iz)) continue;  // pad cell: finished by absorb_kernel
+        if (!quad_in(cxj)) UA_.ref(cxj, iz) = u;
+        if (!model(cxj, iz)) continue;  // pad cell: finished in part 4
         const float out = u + 0.0f;
         set_comp(o[j], r, out);
-        if (PAD && !quad_model(cxj)) out_a[(size_t)cxj * g.LDZ + iz] = out;
+        if (!quad_model(cxj)) out_a[(size_t)cxj * g.LDZ + iz] = out;
         if (!BORN && record && iz == gzq[j])
           g.rec[(size_t)aa.rec_k * g.nx + (cxj - g.pml)] = out;
         if (MODE != MODE_BORN && aa.strip_k >= 0) save_strips(g, aa.strip_k, cxj, iz, out);
@@ -468,103 +615,90 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
           }
         }
       }
-      if (PAD && quad_in(cxj))
-        *reinterpret_cast<float4 *>(g.u3s[0] + (size_t)cxj * g.LDZ + qz0) = u4;
-      if (quad_model(cxj)) *reinterpret_cast<float4 *>(out_a + (size_t)cxj * g.LDZ + qz0) = o[j];
+      if (quad_in(cxj)) *reinterpret_cast<float4 *>(&UA_.ref(cxj, iz0)) = u4;
+      if (quad_model(cxj)) *reinterpret_cast<float4 *>(out_a + (size_t)cxj * g.LDZ + iz0) = o[j];
     }
     if (BORN) {
       float4 ob[2], cb4[2], pb4[2], vb4[2];
-      twoway(CB, PB, 1, ob, cb4, pb4, vb4);
+      pair_twoway(CB, PB, VV, g, ix, iz0, ob, cb4, pb4, vb4);
+      if (!vecq)
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+          for (int r = 0; r < 4; r++)
+            if (ix + j < NX && iz0 + r < NZ && near_edge(ix + j, iz0 + r))
+              set_comp(ob[j], r, UB_(ix + j, iz0 + r));
 #pragma unroll
       for (int j = 0; j < 2; j++) {
-        const int cxj = qx + j;
+        const int cxj = ix + j;
         float4 u4 = ob[j];
 #pragma unroll
         for (int r = 0; r < 4; r++) {
-          const int iz = qz0 + r;
-          if (!in_grid(cxj, iz)) continue;
+          const int iz = iz0 + r;
+          if (cxj >= NX || iz >= NZ) continue;
           const float u = comp(ob[j], r) + comp(qs[j], r);
           set_comp(u4, r, u);
-          if (PAD && !quad_in(cxj)) g.u3s[1][(size_t)cxj * g.LDZ + iz] = u;
+          if (!quad_in(cxj)) UB_.ref(cxj, iz) = u;
           if (!model(cxj, iz)) continue;
           const float out = u + 0.0f;
           set_comp(ob[j], r, out);
-          if (PAD && !quad_model(cxj)) nb_[(size_t)cxj * g.LDZ + iz] = out;
+          if (!quad_model(cxj)) nb_[(size_t)cxj * g.LDZ + iz] = out;
           if (record && iz == gzq[j]) g.rec[(size_t)aa.rec_k * g.nx + (cxj - g.pml)] = out;
         }
-        if (PAD && quad_in(cxj))
-          *reinterpret_cast<float4 *>(g.u3s[1] + (size_t)cxj * g.LDZ + qz0) = u4;
-        if (quad_model(cxj)) *reinterpret_cast<float4 *>(nb_ + (size_t)cxj * g.LDZ + qz0) = ob[j];
+        if (quad_in(cxj)) *reinterpret_cast<float4 *>(&UB_.ref(cxj, iz0)) = u4;
+        if (quad_model(cxj)) *reinterpret_cast<float4 *>(nb_ + (size_t)cxj * g.LDZ + iz0) = ob[j];
       }
     }
-  };
+  }
 
-  float lv[8];
-  int lx[8], lz[8];
-  unsigned mask = 0;
-  if (!PAD) {
-    float (&l0)[8] = *reinterpret_cast<float(*)[8]>(lv);
-    int (&x0_)[8] = *reinterpret_cast<int(*)[8]>(lx);
-    int (&z0_)[8] = *reinterpret_cast<int(*)[8]>(lz);
-    quad(ix, iz0, true, l0, x0_, z0_, mask);
-    if (snap) snap_write<NT_T, 8>(g, aa.snap_k, x0, z0, l0, x0_, z0_, mask, red);
-  } else {
-    float (&l1)[8] = *reinterpret_cast<float(*)[8]>(lv);
-    int (&x1)[8] = *reinterpret_cast<int(*)[8]>(lx);
-    int (&z1)[8] = *reinterpret_cast<int(*)[8]>(lz);
-    const bool vecq = !edge || (ix >= 4 && ix + 1 <= g.NX - 5 && iz0 >= 4 && iz0 + 3 <= g.NZ - 5);
-    if (ix < g.NX && iz0 < g.NZ) quad(ix, iz0, vecq, l1, x1, z1, mask);
-    else
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        lv[k] = 0.0f;
-        lx[k] = ix;
-        lz[k] = iz0;
+  // 3. the halo ring: the same two-way values, injection and scattering
+  // source (zero outside the grid, where nothing reads them)
+  for (int i = tid; i < NHALO; i += NT_T) {
+    int hx, hz;
+    halo_cell(i, x0, z0, hx, hz);
+    if (hx < 0 || hz < 0 || hx >= NX || hz >= NZ) {
+      UA_.ref(hx, hz) = 0.0f;
+      if (BORN) UB_.ref(hx, hz) = 0.0f;
+      continue;
+    }
+    const bool ne = near_edge(hx, hz);
+    const float va = VV(hx, hz);
+    float ua = ne ? UA_(hx, hz) : twoway_cell(CA, PA, VV, g, hx, hz);
+    const Coef kk = coef(va, g);
+    ua = inject<MODE>(g, aa, hx, hz, rcv_row(hx), ua, kk.vt2);
+    UA_.ref(hx, hz) = ua;
+    if (BORN) {
+      float ub = ne ? UB_(hx, hz) : twoway_cell(CB, PB, VV, g, hx, hz);
+      float q = 0.0f;
+      if (model(hx, hz)) {
+        const float out = ua + 0.0f;
+        const float lap = (out + PA(hx, hz) - 2.0f * CA(hx, hz)) * g.idt2;
+        const float vel3 = 2.0f / (va * va * va);
+        q = kk.vt2 * lap * vel3 * DV(hx, hz);
       }
-    if (snap) snap_write<NT_T, 8>(g, aa.snap_k, x0, z0, l1, x1, z1, mask, red);
+      UB_.ref(hx, hz) = ub + q;
+    }
   }
-}
+  // snapshot of the model cells' source terms (holds block barriers), then
+  // every two-way value of the tile and halo is in shared memory
+  if (snap) snap_write<NT_T, 8>(g, aa.snap_k, x0, z0, lv, lx, lz, mask, red);
+  __syncthreads();
 
-// Absorbing boundary of the pad cells: one-way update from the two-way values
-// kept by the pad tiles, and the blend (fd.cpp:1092-1179, :55-56).  Each
-// thread takes ABS_CPT cells of its chunk (z fastest, stride ABS_NT) and
-// forms all of them before storing any, so their loads overlap; every input
-// is read-only during the launch.
-template <int MODE>
-__global__ void __launch_bounds__(ABS_NT) absorb_kernel(const ShotDev *__restrict__ shots,
-                                                        const PadChunk *__restrict__ chunks,
-                                                        StepArgs a) {
-  const PadChunk c = chunks[blockIdx.x];
-  const ShotDev &g = shots[c.shot];
-  const int ldz = g.LDZ;
-  const GA V{g.vel, ldz};
-  const int ra = MODE == MODE_RCV ? a.rot_b : a.rot;
-  float *const *FA = MODE == MODE_RCV ? g.fb : g.fa;
-  const GA UA{g.u3s[0], ldz}, CA{FA[(ra + 1) % 3], ldz}, PA{FA[ra % 3], ldz};
-  float *outa = FA[(ra + 2) % 3];
-  const int rb = a.rot_b;
-  const GA UB{g.u3s[1], ldz}, CB{g.fb[(rb + 1) % 3], ldz}, PB{g.fb[rb % 3], ldz};
-  float *outb = g.fb[(rb + 2) % 3];
-  float va[ABS_CPT], vb[ABS_CPT];
-  size_t off[ABS_CPT];
-  bool act[ABS_CPT];
+  // 4. pad cells: one-way update and blend
+  if (ix < NX && iz0 < NZ) {
 #pragma unroll
-  for (int k = 0; k < ABS_CPT; k++) {
-    const int flat = threadIdx.x + k * ABS_NT;
-    const int col = flat / c.nrows, row = flat - col * c.nrows;
-    act[k] = col < c.ncols;
-    const int ix = c.x0 + (act[k] ? col : 0), iz = c.z0 + (act[k] ? row : 0);
-    off[k] = (size_t)ix * ldz + iz;
-    va[k] = vb[k] = 0.0f;
-    if (!act[k]) continue;
-    va[k] = absorb_cell(UA(ix, iz), UA, CA, PA, V, g, ix, iz);
-    if (MODE == MODE_BORN) vb[k] = absorb_cell(UB(ix, iz), UB, CB, PB, V, g, ix, iz);
-  }
+    for (int j = 0; j < 2; j++) {
+      const int cxj = ix + j;
+      if (cxj >= NX) continue;
 #pragma unroll
-  for (int k = 0; k < ABS_CPT; k++) {
-    if (!act[k]) continue;
-    outa[off[k]] = va[k];
-    if (MODE == MODE_BORN) outb[off[k]] = vb[k];
+      for (int r = 0; r < 4; r++) {
+        const int iz = iz0 + r;
+        if (iz >= NZ || model(cxj, iz)) continue;
+        const size_t at = (size_t)cxj * g.LDZ + iz;
+        out_a[at] = absorb_cell(UA_(cxj, iz), UA_, CA, PA, VV, g, cxj, iz);
+        if (BORN) nb_[at] = absorb_cell(UB_(cxj, iz), UB_, CB, PB, VV, g, cxj, iz);
+      }
+    }
   }
 }
 
