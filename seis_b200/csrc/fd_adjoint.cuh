@@ -19,17 +19,20 @@
 //   L_k = S_cur^T M_{k+1} - M_{k+2} + E_k + R^T d,
 //   E_k = P_cur^T rho_{k+1} + P_prev^T rho_{k+2},
 // and every term is a gather over a fixed neighbourhood summed in a fixed
-// order, so the adjoint is bit-for-bit repeatable without atomics.  Three
-// launches per step:
+// order, so the adjoint is bit-for-bit repeatable without atomics.  Two
+// launches per step, on two streams:
 //  * adj_interior_kernel: tiles with no pad-ring neighbour and every consumer
 //    8th order: L = Lz(vz M1) + Lx(vx M1) + 2 M1 - M2 + R^T d;
-//  * adj_pad_kernel: the other tiles; the same gather over the 8th-order
-//    consumers, the low-order and frame consumers (outer 4 cells of the grid)
-//    by a per-cell transpose of the two-way formulas, plus E; writes L and
-//    rho of its ring cells;
-//  * adj_ring_kernel: the pad cells and the model edge cells: M = w L +
-//    P_u3^T rho, and E of the next step (the cur terms of this step's rho
-//    plus the prev terms kept from the last one).
+//  * adj_pad_kernel: the other tiles, in one pass: L of the tile and of its
+//    one-cell halo by the same gather over the 8th-order consumers, the
+//    low-order and frame consumers (outer 4 cells of the grid) by a per-cell
+//    transpose of the two-way formulas, plus E; rho of the ring cells with
+//    their one-way coefficients in shared memory; then for the pad and model
+//    edge cells M = w L + P_u3^T rho, E of the next step (the cur terms of
+//    this step's rho plus the prev terms kept from the last one) and the
+//    prev terms kept for the step after.  E alternates between two buffers
+//    by step (a tile reads this step's E on its halo while its neighbour
+//    writes the next step's).
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -218,10 +221,82 @@ __device__ float edge_terms(const ShotDev &g, const A &M, const A &V, int tx, in
 }
 
 // ---------------------------------------------------------------- pad tiles
+// The one-way update of a strip cell (fd.cpp:1098-1104) is
+//   u31 = al (u3_i + p) + be (u3_i+t + u3_i-t + p_+t + p_-t) + ga (c + c_i) - p_i
+// with al = (a1 - a2 - 2 a3)/d, be = a3/d, ga = 2 a2/d, d = a1 + a2 (c, p =
+// cur, prev at the cell; _i at the inner neighbour, +-t along the strip), and
+// of a corner cell (fd.cpp:1146-1178) u31 = cz u3_z + cx u3_x + bK c.  Every
+// ring cell of a tile and its halo stores rho times its coefficients and a
+// 3-bit role for each of the 9 offsets of the cells it feeds; each pad or
+// model edge cell then gathers from its 3 x 3 neighbours in a fixed order.
+enum RingRole : int {
+  ROLE_NONE = 0,
+  ROLE_SELF = 1,    // strip cell itself: cur ga, prev al
+  ROLE_INNER = 2,   // its inner neighbour: u3 al, cur ga, prev -1
+  ROLE_TANG = 3,    // along the strip: prev be
+  ROLE_DIAG = 4,    // inner +- along: u3 be
+  ROLE_CZ = 5,      // corner: u3 at the z-inner neighbour
+  ROLE_CX = 6,      // corner: u3 at the x-inner neighbour
+  ROLE_CSELF = 7,   // corner cell itself: cur bK
+};
+__device__ __forceinline__ int role_slot(int ox, int oz) { return 3 * ((ox + 1) * 3 + (oz + 1)); }
+
+// rho-weighted one-way coefficients and roles of one ring cell
+__device__ __forceinline__ int ring_coefs(const ShotDev &g, const PadPos &pp, float v, float rho,
+                                          float &p0, float &p1, float &p2, float &p3) {
+  const int nx_ = pp.dl > 0 ? 1 : (pp.distx > 0 ? -1 : 0);
+  const int nz_ = pp.du > 0 ? 1 : (pp.distz > 0 ? -1 : 0);
+  if (pp.distx == pp.ring && pp.distz == pp.ring) {
+    const float ax3 = g.sqrt2f / v / g.dt;
+    const float re = 1.0f / (g.ax1 + g.ax2 + ax3);
+    p0 = g.ax1 * re * rho;
+    p1 = g.ax2 * re * rho;
+    p2 = ax3 * re * rho;
+    p3 = 0.0f;
+    return ROLE_CSELF << role_slot(0, 0) | ROLE_CZ << role_slot(0, nz_) |
+           ROLE_CX << role_slot(nx_, 0);
+  }
+  const bool zs = pp.distz == pp.ring;  // top / bottom strip: inner along z
+  const int ix_ = zs ? 0 : nx_, iz_ = zs ? nz_ : 0, tx_ = zs, tz_ = !zs;
+  const float a1 = zs ? g.a1z : g.a1x;
+  const float a2 = g.hdt2 * (1.0f / v);
+  const float a3 = v * 0.25f * (zs ? g.invdx2 : g.invdz2);
+  const float rd = 1.0f / (a1 + a2);
+  p0 = (a1 - a2 - 2.0f * a3) * rd * rho;
+  p1 = a3 * rd * rho;
+  p2 = 2.0f * a2 * rd * rho;
+  p3 = rho;
+  return ROLE_SELF << role_slot(0, 0) | ROLE_INNER << role_slot(ix_, iz_) |
+         ROLE_TANG << role_slot(tx_, tz_) | ROLE_TANG << role_slot(-tx_, -tz_) |
+         ROLE_DIAG << role_slot(ix_ + tx_, iz_ + tz_) |
+         ROLE_DIAG << role_slot(ix_ - tx_, iz_ - tz_);
+}
+
+// Cells of a tile and its one-cell halo: columns x0-1 .. x0+TX, rows z0-1 ..
+// z0+TZ.
+constexpr int RW = TZ + 2;
+constexpr int RN = (TX + 2) * RW;
+constexpr int ADJ_NHALO = 2 * (TX + 2) + 2 * TZ;
+static_assert(ADJ_NHALO <= A_NT_I, "one halo cell per thread");
+static_assert(5 * RN <= NARROW + 2 * WIDE + RN, "ring arrays fit over the dead buffers");
+constexpr int ADJ_PAD_FLOATS = 4 * WIDE + NARROW + RN;
+
+__device__ __forceinline__ void adj_halo_cell(int i, int x0, int z0, int &hx, int &hz) {
+  if (i < 2 * (TX + 2)) {
+    hx = x0 - 1 + i % (TX + 2);
+    hz = i < TX + 2 ? z0 - 1 : z0 + TZ;
+  } else {
+    const int j = i - 2 * (TX + 2);
+    hx = j < TZ ? x0 - 1 : x0 + TX;
+    hz = z0 + j % TZ;
+  }
+}
+
 // L = S_cur^T M1 - M2 + E + R^T d on a tile with pad-ring cells, pad-ring
-// neighbours or consumers outside the 8th-order region; rho = (1 - w) L of
-// its ring cells; grad += w lap M1 on its model cells.
-__global__ void __launch_bounds__(A_NT_I, 3) adj_pad_kernel(const ShotDev *__restrict__ shots,
+// neighbours or consumers outside the 8th-order region; grad += w lap M1 on
+// its model cells; then M, E (next step) and B of its pad and model edge
+// cells, L = M elsewhere.
+__global__ void __launch_bounds__(A_NT_I, 2) adj_pad_kernel(const ShotDev *__restrict__ shots,
                                                             const Tile *__restrict__ tiles,
                                                             StepArgs a, int *__restrict__ err) {
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -230,8 +305,11 @@ __global__ void __launch_bounds__(A_NT_I, 3) adj_pad_kernel(const ShotDev *__res
   float *sL2 = sV + WIDE;                          // narrow
   float *sWZ = sL2 + NARROW;                       // wide
   float *sWX = sWZ + WIDE;                         // wide
-  float *sCOR = sWX + WIDE;                        // tile: frame / low-order terms
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sCOR + TX * TZ);
+  float *sCOR = sWX + WIDE;                        // tile + halo: frame / low-order terms
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sCOR + RN);
+  // ring arrays of tile + halo, over sL2 .. sCOR once L is formed
+  float *rp0 = sL2, *rp1 = rp0 + RN, *rp2 = rp1 + RN, *rp3 = rp2 + RN;
+  int *rmask = reinterpret_cast<int *>(rp3 + RN);
   const int tid = threadIdx.x;
   const Tile t = tiles[blockIdx.x];
   __shared__ ShotDev sg;
@@ -271,68 +349,167 @@ __global__ void __launch_bounds__(A_NT_I, 3) adj_pad_kernel(const ShotDev *__res
   const SA L1{sL1, x0 - HXC, zm}, V{sV, x0 - HXC, zm}, WZ{sWZ, x0 - HXC, zm},
       WX{sWX, x0 - HXC, zm};
   const SA L2{sL2, x0 - 1, zm};
-  // cells within 4 of the grid edge have low-order or frame consumers: their
-  // terms are formed by all threads over the edge bands of the tile (a cell in
-  // two bands is formed twice, to the same value)
-  const int xe = min(x0 + TX, NX), ze = min(z0 + TZ, NZ);
-  const bool edge = x0 <= 4 || z0 <= 4 || xe - 1 >= NX - 5 || ze - 1 >= NZ - 5;
+  auto ridx = [&](int cx, int cz) { return (cx - x0 + 1) * RW + (cz - z0 + 1); };
+  auto near4 = [&](int cx, int cz) {
+    return min(min(cx, cz), min(NX - 1 - cx, NZ - 1 - cz)) <= 4;
+  };
+  // cells of the tile and halo within 4 of the grid edge have low-order or
+  // frame consumers: their terms are formed by all threads over the edge
+  // bands (a cell in two bands is formed twice, to the same value)
+  const int xa = max(x0 - 1, 0), xb = min(x0 + TX + 1, NX);
+  const int za = max(z0 - 1, 0), zb = min(z0 + TZ + 1, NZ);
+  const bool edge = xa <= 4 || za <= 4 || xb - 1 >= NX - 5 || zb - 1 >= NZ - 5;
   if (edge) {
 #pragma unroll 1
     for (int b = 0; b < 4; b++) {  // top, bottom, left, right band
-      const int bxa = b == 3 ? max(x0, NX - 5) : x0, bxb = b == 2 ? min(xe, 5) : xe;
-      const int bza = b == 1 ? max(z0, NZ - 5) : z0, bzb = b == 0 ? min(ze, 5) : ze;
+      const int bxa = b == 3 ? max(xa, NX - 5) : xa, bxb = b == 2 ? min(xb, 5) : xb;
+      const int bza = b == 1 ? max(za, NZ - 5) : za, bzb = b == 0 ? min(zb, 5) : zb;
       const int nr = bzb - bza, nc = bxb - bxa;
       if (nr <= 0 || nc <= 0) continue;
       for (int i = tid; i < nr * nc; i += A_NT_I) {
         const int cx = bxa + i / nr, cz = bza + i % nr;
-        sCOR[(cx - x0) * TZ + (cz - z0)] = edge_terms(g, L1, V, cx, cz);
+        sCOR[ridx(cx, cz)] = edge_terms(g, L1, V, cx, cz);
       }
     }
   }
   __syncthreads();
+  const float *Ecur = g.adj_e[a.rot & 1];
+  float *Enext = g.adj_e[(a.rot + 1) & 1];
+
+  // L of the tile's cells (kept in registers), imaging on its model cells
   const int qz = tid % QZ, cxp = tid / QZ;
   const int ix = x0 + 2 * cxp, iz0 = z0 + 4 * qz;
-  float *out = g.fa[(a.rot + 2) % 3];
   const bool img = a.snap_k >= 0 && g.snap != nullptr;
-  const float inv_scale = img ? snap_inv_scale(g, a.snap_k, x0, z0) : 0.0f;
-  float4 xm[10];
+  float Lt[8];
+  {
+    const float inv_scale = img ? snap_inv_scale(g, a.snap_k, x0, z0) : 0.0f;
+    float4 xm[10];
 #pragma unroll
-  for (int m = 0; m < 10; m++) xm[m] = WX.quad(ix - 4 + m, iz0);
+    for (int m = 0; m < 10; m++) xm[m] = WX.quad(ix - 4 + m, iz0);
 #pragma unroll
-  for (int j = 0; j < 2; j++) {
-    const int cx = ix + j;
-    if (cx >= NX || iz0 >= NZ) continue;
-    const float4 za = WZ.quad(cx, iz0 - 4), zb = WZ.quad(cx, iz0), zc = WZ.quad(cx, iz0 + 4);
-    const float zz[12] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w, zc.x, zc.y, zc.z, zc.w};
-    const float4 l1 = L1.quad(cx, iz0), l2 = L2.quad(cx, iz0);
-    const size_t col = (size_t)cx * g.LDZ;
-    const float4 e4 = *reinterpret_cast<const float4 *>(g.adj_e + col + iz0);
-    const int x = cx - g.pml;
-    const int gzr = (x >= 0 && x < g.nx) ? g.gz[x] + g.pml : -1;
-    float4 o;
+    for (int j = 0; j < 2; j++) {
+      const int cx = ix + j;
+      const float4 za4 = WZ.quad(cx, iz0 - 4), zb4 = WZ.quad(cx, iz0), zc4 = WZ.quad(cx, iz0 + 4);
+      const float zz[12] = {za4.x, za4.y, za4.z, za4.w, zb4.x, zb4.y,
+                            zb4.z, zb4.w, zc4.x, zc4.y, zc4.z, zc4.w};
+      const float4 l1 = L1.quad(cx, iz0), l2 = L2.quad(cx, iz0);
+      float4 e4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (cx < NX && iz0 < NZ)
+        e4 = *reinterpret_cast<const float4 *>(Ecur + (size_t)cx * g.LDZ + iz0);
+      const int x = cx - g.pml;
+      const int gzr = (x >= 0 && x < g.nx && cx < NX) ? g.gz[x] + g.pml : -1;
 #pragma unroll
-    for (int r = 0; r < 4; r++) {
-      const int cz = iz0 + r;
-      const float sz_ = lap8(zz[r], zz[r + 1], zz[r + 2], zz[r + 3], zz[r + 4], zz[r + 5],
-                             zz[r + 6], zz[r + 7], zz[r + 8]);
-      const float sx_ = lap8(comp(xm[j], r), comp(xm[j + 1], r), comp(xm[j + 2], r),
-                             comp(xm[j + 3], r), comp(xm[j + 4], r), comp(xm[j + 5], r),
-                             comp(xm[j + 6], r), comp(xm[j + 7], r), comp(xm[j + 8], r));
-      float v = sz_ + sx_ + 2.0f * comp(l1, r);
-      if (edge && cz < NZ && min(min(cx, cz), min(NX - 1 - cx, NZ - 1 - cz)) <= 4)
-        v = v + sCOR[(cx - x0) * TZ + (cz - z0)];
-      v = v - comp(l2, r) + comp(e4, r);
-      if (a.rec_k >= 0 && cz == gzr) v += g.rec[(size_t)a.rec_k * g.nx + x];
-      set_comp(o, r, v);
-      if (cz < NZ) {
-        const PadPos pp = pad_pos(g, cx, cz);
-        if (pp.ring > 0) g.adj_rho[col + cz] = (1.0f - pad_weight(g, pp)) * v;
+      for (int r = 0; r < 4; r++) {
+        const int cz = iz0 + r;
+        const float sz_ = lap8(zz[r], zz[r + 1], zz[r + 2], zz[r + 3], zz[r + 4], zz[r + 5],
+                               zz[r + 6], zz[r + 7], zz[r + 8]);
+        const float sx_ = lap8(comp(xm[j], r), comp(xm[j + 1], r), comp(xm[j + 2], r),
+                               comp(xm[j + 3], r), comp(xm[j + 4], r), comp(xm[j + 5], r),
+                               comp(xm[j + 6], r), comp(xm[j + 7], r), comp(xm[j + 8], r));
+        float v = sz_ + sx_ + 2.0f * comp(l1, r);
+        if (edge && cx < NX && cz < NZ && near4(cx, cz)) v = v + sCOR[ridx(cx, cz)];
+        v = v - comp(l2, r) + comp(e4, r);
+        if (a.rec_k >= 0 && cz == gzr) v += g.rec[(size_t)a.rec_k * g.nx + x];
+        Lt[4 * j + r] = v;
         const int z = cz - g.pml;
-        if (img && x >= 0 && x < g.nx && z >= 0 && z < g.nz) {
+        if (img && cx < NX && x >= 0 && x < g.nx && z >= 0 && z < g.nz) {
           const float lap = snap_load(g, a.snap_k, x, z) * inv_scale;
           g.grad[(size_t)x * g.nz + z] += (double)(a.img_w * lap * comp(l1, r));
         }
       }
+    }
+  }
+  // L of the halo's pad cells (the only halo cells whose rho is read)
+  int hx = -1, hz = -1;
+  float Lh = 0.0f;
+  PadPos hp{};
+  bool hring = false;
+  if (tid < ADJ_NHALO) {
+    adj_halo_cell(tid, x0, z0, hx, hz);
+    if (hx >= 0 && hz >= 0 && hx < NX && hz < NZ) {
+      hp = pad_pos(g, hx, hz);
+      hring = hp.ring > 0;
+    }
+    if (hring) {
+      const float sz_ = lap8(WZ(hx, hz - 4), WZ(hx, hz - 3), WZ(hx, hz - 2), WZ(hx, hz - 1),
+                             WZ(hx, hz), WZ(hx, hz + 1), WZ(hx, hz + 2), WZ(hx, hz + 3),
+                             WZ(hx, hz + 4));
+      const float sx_ = lap8(WX(hx - 4, hz), WX(hx - 3, hz), WX(hx - 2, hz), WX(hx - 1, hz),
+                             WX(hx, hz), WX(hx + 1, hz), WX(hx + 2, hz), WX(hx + 3, hz),
+                             WX(hx + 4, hz));
+      float v = sz_ + sx_ + 2.0f * L1(hx, hz);
+      if (edge && near4(hx, hz)) v = v + sCOR[ridx(hx, hz)];
+      v = v - L2(hx, hz) + Ecur[(size_t)hx * g.LDZ + hz];
+      const int x = hx - g.pml;
+      if (a.rec_k >= 0 && x >= 0 && x < g.nx && hz == g.gz[x] + g.pml)
+        v += g.rec[(size_t)a.rec_k * g.nx + x];
+      Lh = v;
+    }
+  }
+  __syncthreads();  // sL2, sWZ, sWX and sCOR are dead: the ring arrays go there
+  // rho = (1 - w) L of the ring cells, times their one-way coefficients
+  auto put_ring = [&](int cx, int cz, const PadPos &pp, bool ring, float L) {
+    const int i = ridx(cx, cz);
+    int mask = 0;
+    float p0 = 0.0f, p1 = 0.0f, p2 = 0.0f, p3 = 0.0f;
+    if (ring) mask = ring_coefs(g, pp, V(cx, cz), (1.0f - pad_weight(g, pp)) * L, p0, p1, p2, p3);
+    rmask[i] = mask;
+    rp0[i] = p0;
+    rp1[i] = p1;
+    rp2[i] = p2;
+    rp3[i] = p3;
+  };
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const int cx = ix + k / 4, cz = iz0 + k % 4;
+    const bool in = cx < NX && cz < NZ;
+    const PadPos pp = pad_pos(g, cx, cz);
+    put_ring(cx, cz, pp, in && pp.ring > 0, Lt[k]);
+  }
+  if (tid < ADJ_NHALO) put_ring(hx, hz, hp, hring, Lh);
+  __syncthreads();
+
+  // M = w L + P_u3^T rho on the pad and model edge cells (L elsewhere), E of
+  // the next step and the kept prev terms
+  float *out = g.fa[(a.rot + 2) % 3];
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int cx = ix + j;
+    if (cx >= NX || iz0 >= NZ) continue;
+    const size_t col = (size_t)cx * g.LDZ;
+    float4 o;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int cz = iz0 + r;
+      float L = Lt[4 * j + r];
+      const PadPos pt = pad_pos(g, cx, cz);
+      const bool edge_cell = cx == g.pml || cx == g.pml + g.nx - 1 || cz == g.pml ||
+                             cz == g.pml + g.nz - 1;
+      if (cz < NZ && (pt.ring > 0 || edge_cell)) {
+        float m = 0.0f, e = 0.0f, b = 0.0f;
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++)
+#pragma unroll
+          for (int dz = -1; dz <= 1; dz++) {
+            const int i = ridx(cx + dx, cz + dz);
+            // this cell sits at offset (-dx, -dz) from the ring cell
+            switch ((rmask[i] >> role_slot(-dx, -dz)) & 7) {
+              case ROLE_SELF: e += rp2[i]; b += rp0[i]; break;
+              case ROLE_INNER: m += rp0[i]; e += rp2[i]; b -= rp3[i]; break;
+              case ROLE_TANG: b += rp1[i]; break;
+              case ROLE_DIAG: m += rp1[i]; break;
+              case ROLE_CZ: m += rp0[i]; break;
+              case ROLE_CX: m += rp1[i]; break;
+              case ROLE_CSELF: e += rp2[i]; break;
+              default: break;
+            }
+          }
+        const float w = pt.ring == 0 ? 1.0f : pad_weight(g, pt);
+        L = w * L + m;
+        Enext[col + cz] = e + g.adj_b[col + cz];
+        g.adj_b[col + cz] = b;
+      }
+      set_comp(o, r, L);
     }
     if (iz0 + 3 < NZ) {
       *reinterpret_cast<float4 *>(out + col + iz0) = o;
@@ -342,115 +519,6 @@ __global__ void __launch_bounds__(A_NT_I, 3) adj_pad_kernel(const ShotDev *__res
         if (iz0 + r < NZ) out[col + iz0 + r] = comp(o, r);
     }
   }
-}
-
-// ---------------------------------------------------------------- ring cells
-// Over the pad cells and the model edge cells (chunks of at most R_NT cells):
-//   M = w L + P_u3^T rho            (in place over L)
-//   E = P_cur^T rho + B,  B = P_prev^T rho
-// The one-way update of a strip cell (fd.cpp:1098-1104) is
-//   u31 = al (u3_i + p) + be (u3_i+t + u3_i-t + p_+t + p_-t) + ga (c + c_i) - p_i
-// with al = (a1 - a2 - 2 a3)/d, be = a3/d, ga = 2 a2/d, d = a1 + a2 (c, p =
-// cur, prev at the cell; _i at the inner neighbour, +-t along the strip), and
-// of a corner cell (fd.cpp:1146-1178) u31 = cz u3_z + cx u3_x + bK c.  Every
-// ring cell of the chunk + 1 stages rho times its coefficients and a 3-bit
-// role for each of the 9 offsets of the cells it feeds; each cell then gathers
-// from its 3 x 3 neighbours in a fixed order.
-constexpr int R_NT = 256;
-constexpr int R_MAXW = 774;  // (ncols + 2) (nrows + 2) for ncols nrows <= R_NT
-enum RingRole : int {
-  ROLE_NONE = 0,
-  ROLE_SELF = 1,    // strip cell itself: cur ga, prev al
-  ROLE_INNER = 2,   // its inner neighbour: u3 al, cur ga, prev -1
-  ROLE_TANG = 3,    // along the strip: prev be
-  ROLE_DIAG = 4,    // inner +- along: u3 be
-  ROLE_CZ = 5,      // corner: u3 at the z-inner neighbour
-  ROLE_CX = 6,      // corner: u3 at the x-inner neighbour
-  ROLE_CSELF = 7,   // corner cell itself: cur bK
-};
-__device__ __forceinline__ int role_slot(int ox, int oz) { return 3 * ((ox + 1) * 3 + (oz + 1)); }
-
-__global__ void __launch_bounds__(R_NT) adj_ring_kernel(const ShotDev *__restrict__ shots,
-                                                        StepArgs a) {
-  __shared__ int smask[R_MAXW];
-  __shared__ float sp[4][R_MAXW];
-  const PadChunk ch = a.chunks[blockIdx.x];
-  const ShotDev &g = shots[ch.shot];
-  const int NX = g.NX, NZ = g.NZ, LDZ = g.LDZ;
-  const int wr = ch.nrows + 2, nw = (ch.ncols + 2) * wr;
-  for (int i = threadIdx.x; i < nw; i += R_NT) {
-    const int rx = ch.x0 - 1 + i / wr, rz = ch.z0 - 1 + i % wr;
-    int mask = 0;
-    float p0 = 0.0f, p1 = 0.0f, p2 = 0.0f, p3 = 0.0f;
-    if (rx >= 0 && rx < NX && rz >= 0 && rz < NZ) {
-      const PadPos pp = pad_pos(g, rx, rz);
-      if (pp.ring > 0) {
-        const size_t idx = (size_t)rx * LDZ + rz;
-        const float rho = g.adj_rho[idx];
-        const float v = g.vel[idx];
-        const int nx_ = pp.dl > 0 ? 1 : (pp.distx > 0 ? -1 : 0);
-        const int nz_ = pp.du > 0 ? 1 : (pp.distz > 0 ? -1 : 0);
-        if (pp.distx == pp.ring && pp.distz == pp.ring) {
-          const float ax3 = g.sqrt2f / v / g.dt;
-          const float re = 1.0f / (g.ax1 + g.ax2 + ax3);
-          p0 = g.ax1 * re * rho;
-          p1 = g.ax2 * re * rho;
-          p2 = ax3 * re * rho;
-          mask = ROLE_CSELF << role_slot(0, 0) | ROLE_CZ << role_slot(0, nz_) |
-                 ROLE_CX << role_slot(nx_, 0);
-        } else {
-          const bool zs = pp.distz == pp.ring;  // top / bottom strip: inner along z
-          const int ix_ = zs ? 0 : nx_, iz_ = zs ? nz_ : 0, tx_ = zs, tz_ = !zs;
-          const float a1 = zs ? g.a1z : g.a1x;
-          const float a2 = g.hdt2 * (1.0f / v);
-          const float a3 = v * 0.25f * (zs ? g.invdx2 : g.invdz2);
-          const float rd = 1.0f / (a1 + a2);
-          p0 = (a1 - a2 - 2.0f * a3) * rd * rho;
-          p1 = a3 * rd * rho;
-          p2 = 2.0f * a2 * rd * rho;
-          p3 = rho;
-          mask = ROLE_SELF << role_slot(0, 0) | ROLE_INNER << role_slot(ix_, iz_) |
-                 ROLE_TANG << role_slot(tx_, tz_) | ROLE_TANG << role_slot(-tx_, -tz_) |
-                 ROLE_DIAG << role_slot(ix_ + tx_, iz_ + tz_) |
-                 ROLE_DIAG << role_slot(ix_ - tx_, iz_ - tz_);
-        }
-      }
-    }
-    smask[i] = mask;
-    sp[0][i] = p0;
-    sp[1][i] = p1;
-    sp[2][i] = p2;
-    sp[3][i] = p3;
-  }
-  __syncthreads();
-  if ((int)threadIdx.x >= ch.ncols * ch.nrows) return;
-  const int lx = threadIdx.x / ch.nrows, lz = threadIdx.x % ch.nrows;
-  const int tx = ch.x0 + lx, tz = ch.z0 + lz;
-  float m = 0.0f, e = 0.0f, b = 0.0f;
-#pragma unroll
-  for (int dx = -1; dx <= 1; dx++)
-#pragma unroll
-    for (int dz = -1; dz <= 1; dz++) {
-      const int i = (lx + 1 + dx) * wr + (lz + 1 + dz);
-      // this cell sits at offset (-dx, -dz) from the ring cell
-      switch ((smask[i] >> role_slot(-dx, -dz)) & 7) {
-        case ROLE_SELF: e += sp[2][i]; b += sp[0][i]; break;
-        case ROLE_INNER: m += sp[0][i]; e += sp[2][i]; b -= sp[3][i]; break;
-        case ROLE_TANG: b += sp[1][i]; break;
-        case ROLE_DIAG: m += sp[1][i]; break;
-        case ROLE_CZ: m += sp[0][i]; break;
-        case ROLE_CX: m += sp[1][i]; break;
-        case ROLE_CSELF: e += sp[2][i]; break;
-        default: break;
-      }
-    }
-  const size_t idx = (size_t)tx * LDZ + tz;
-  const PadPos pt = pad_pos(g, tx, tz);
-  const float w = pt.ring == 0 ? 1.0f : pad_weight(g, pt);
-  float *L = g.fa[(a.rot + 2) % 3];
-  L[idx] = w * L[idx] + m;
-  g.adj_e[idx] = e + g.adj_b[idx];
-  g.adj_b[idx] = b;
 }
 
 }  // namespace SEIS_NS

@@ -9,7 +9,7 @@ namespace seis {
 namespace fast {
 
 constexpr size_t ADJ_TILE_SMEM = sizeof(float) * (size_t)(4 * WIDE + NARROW) + 16;
-constexpr size_t ADJ_PAD_SMEM = ADJ_TILE_SMEM + sizeof(float) * (size_t)(TX * TZ);
+constexpr size_t ADJ_PAD_SMEM = sizeof(float) * (size_t)ADJ_PAD_FLOATS + 16;
 
 cudaError_t configure_adjoint() {
   cudaError_t e = cudaFuncSetAttribute(adj_interior_kernel,
@@ -25,10 +25,8 @@ cudaError_t launch_adjoint(const ShotDev *d_shots, const Tile *d_tiles, int n_in
                            const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad) {
   if (n_int > 0)
     adj_interior_kernel<<<n_int, A_NT_I, ADJ_TILE_SMEM, s_int>>>(d_shots, d_tiles, a, d_err);
-  if (n_pad > 0) {
+  if (n_pad > 0)
     adj_pad_kernel<<<n_pad, A_NT_I, ADJ_PAD_SMEM, s_pad>>>(d_shots, d_tiles + n_int, a, d_err);
-    if (a.nchunks > 0) adj_ring_kernel<<<a.nchunks, R_NT, 0, s_pad>>>(d_shots, a);
-  }
   return cudaGetLastError();
 }
 

@@ -115,8 +115,6 @@ struct Plan {
   std::vector<Tile> adj_tiles;  // adjoint classification (stricter interior)
   int n_int_adj = 0, n_pad_adj = 0;
   Tile *d_adj_tiles = nullptr;
-  std::vector<PadChunk> adj_chunks;  // pad cells + model edge cells (adjoint ring kernel)
-  PadChunk *d_adj_chunks = nullptr;
   int snap_every = 1, snap_dtype = SNAP_F32;
   // source-field checkpoints (adjoint plans, 0 = keep every snapshot): the
   // two time levels before every ck_every-th step; the reverse pass
@@ -242,34 +240,11 @@ void build_tiles(Plan &p) {
 }
 
 // Tiles for the exact adjoint: an interior tile holds no pad cell and no
-// model edge cell (the cells whose adjoint the ring kernel completes), and
-// every consumer of its cells is 8th order (cells 8 or more from the grid
-// edge), so that the adjoint there is the symmetric gather.  The ring kernel
-// covers the pad cells and the model edge cells in chunks of at most
-// R_NT cells: left and right blocks over the full height, top and bottom
-// blocks between them.
+// model edge cell (the cells whose adjoint carries the absorbing ring terms),
+// and every consumer of its cells is 8th order (cells 8 or more from the grid
+// edge), so that the adjoint there is the symmetric gather.
 void build_adj_tiles(Plan &p) {
   std::vector<Tile> in_t, pad_t;
-  p.adj_chunks.clear();
-  constexpr int RCH = 256;
-  auto block = [&](int s, int xa, int xb, int za, int zb) {
-    const int R = zb - za, Cn = xb - xa;
-    if (R <= 0 || Cn <= 0) return;
-    const int nrows = std::min(R, 64), ncols = std::min(Cn, std::max(1, RCH / nrows));
-    for (int x = xa; x < xb; x += ncols)
-      for (int z = za; z < zb; z += nrows)
-        p.adj_chunks.push_back(
-            PadChunk{s, x, z, std::min(ncols, xb - x), std::min(nrows, zb - z)});
-  };
-  for (int s = 0; s < p.nshot; s++) {
-    const ShotDev &g = p.sd[s];
-    const int xl = std::min(g.pml + 1, g.NX), xr = std::max(g.pml + g.nx - 1, xl);
-    const int zt = std::min(g.pml + 1, g.NZ), zb = std::max(g.pml + g.nz - 1, zt);
-    block(s, 0, xl, 0, g.NZ);
-    block(s, xr, g.NX, 0, g.NZ);
-    block(s, xl, xr, 0, zt);
-    block(s, xl, xr, zb, g.NZ);
-  }
   for (int s = 0; s < p.nshot; s++) {
     const ShotDev &g = p.sd[s];
     int lox = g.pml + 1, hix = g.pml + g.nx - 2;  // inclusive bounds of tile cells
@@ -457,8 +432,8 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (op == OP_ILLUM || op == OP_ILLUM_PLANE) g.illum = g.img;
     if (rc == SEIS_OK && op == OP_BORN_ADJ) rc = p->alloc(&g.grad, (size_t)d.nx * d.nz);
     if (op == OP_BORN_ADJ) {
-      if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_rho);
-      if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_e);
+      if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_e[0]);
+      if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_e[1]);
       if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_b);
     }
     g.ntz = (g.NZ + TZ - 1) / TZ;
@@ -490,7 +465,6 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
   }
   if (rc == SEIS_OK) rc = p->alloc(&p->d_tiles, p->tiles.size());
   if (rc == SEIS_OK) rc = p->alloc(&p->d_adj_tiles, p->adj_tiles.size());
-  if (rc == SEIS_OK) rc = p->alloc(&p->d_adj_chunks, p->adj_chunks.size());
   const bool imaging = op == OP_RTM || op == OP_RTM_PLANE || op == OP_RTM_TRUE || op == OP_RTM_UPDOWN;
   if (rc == SEIS_OK && imaging) rc = p->alloc(&p->d_cols, p->cols.size());
   if (rc == SEIS_OK && imaging) rc = p->alloc(&p->d_taps, (size_t)61);
@@ -504,9 +478,6 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(p->d_adj_tiles, p->adj_tiles.data(), sizeof(Tile) * p->adj_tiles.size(),
                           cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && !p->adj_chunks.empty())
-      e = cudaMemcpyAsync(p->d_adj_chunks, p->adj_chunks.data(),
-                          sizeof(PadChunk) * p->adj_chunks.size(), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && imaging) {
       e = cudaMemcpyAsync(p->d_cols, p->cols.data(), sizeof(int2) * p->cols.size(),
                           cudaMemcpyHostToDevice, st);
@@ -638,14 +609,11 @@ int adj_step(Plan &p, const StepArgs &a) {
   seis_fd_ctx *ctx = p.ctx;
   CK(cudaEventRecord(ctx->fork, ctx->stream));
   CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
-  StepArgs b = a;
-  b.chunks = p.d_adj_chunks;
-  b.nchunks = (int)p.adj_chunks.size();
-  CK(fast::launch_adjoint(p.d_sd, p.d_adj_tiles, p.n_int_adj, p.n_pad_adj, b, ctx->d_err,
+  CK(fast::launch_adjoint(p.d_sd, p.d_adj_tiles, p.n_int_adj, p.n_pad_adj, a, ctx->d_err,
                           ctx->stream, ctx->aux));
   CK(cudaEventRecord(ctx->join, ctx->aux));
   CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
-  ctx->launches += (p.n_int_adj > 0) + (p.n_pad_adj > 0) + (p.n_pad_adj > 0 && b.nchunks > 0);
+  ctx->launches += (p.n_int_adj > 0) + (p.n_pad_adj > 0);
   return SEIS_OK;
 }
 
@@ -896,7 +864,7 @@ int run_adjoint(Plan &p) {
     FieldGeom fg = field_geom(g.NX, g.NZ);
     for (int k = 0; k < 3; k++)
       CK(cudaMemsetAsync(g.fa[k] - fg.origin, 0, sizeof(float) * fg.elems, ctx->stream));
-    for (float *f : {g.adj_rho, g.adj_e, g.adj_b})
+    for (float *f : {g.adj_e[0], g.adj_e[1], g.adj_b})
       CK(cudaMemsetAsync(f - fg.origin, 0, sizeof(float) * fg.elems, ctx->stream));
   }
   StepArgs a{};
@@ -1292,10 +1260,6 @@ int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double 
   StepArgs a{};
   a.nshots = p.nshot;
   a.strip_k = -1;
-  if (adj) {
-    a.chunks = p.d_adj_chunks;
-    a.nchunks = (int)p.adj_chunks.size();
-  }
   double t_int = 0, t_pad = 0, t_step = 0;
   for (int k = 0; k < steps; k++) {
     a.rot = k; a.rot_b = k;
@@ -1327,7 +1291,7 @@ int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double 
     CK(cudaEventElapsedTime(&a2, ev[2], ev[3]));
     CK(cudaEventElapsedTime(&a3, ev[0], ev[4]));
     t_int += a1; t_pad += a2; t_step += a3;
-    ctx->launches += 2 + (n_pad > 0 && a.nchunks > 0);
+    ctx->launches += 2;
   }
   for (auto &e : ev) cudaEventDestroy(e);
   ms[0] = t_int / steps; ms[1] = t_pad / steps; ms[2] = t_step / steps;

@@ -29,12 +29,6 @@ struct Tile {
   int shot, x0, z0, kind;
 };
 
-// A rectangle of ring cells (one shot, ncols x nrows cells, z fastest) given
-// to one CTA of the adjoint's ring kernel.
-struct PadChunk {
-  int shot, x0, z0, ncols, nrows;
-};
-
 // 2-D TMA tensor maps of one shot (each describes one margin-padded field
 // allocation, LDZ rows x ncols columns; box = staged rows x staged columns).
 // Wide boxes (TX + 2*HXC columns) stage a field read as "current"; narrow boxes
@@ -91,10 +85,10 @@ struct ShotDev {
   float *comp;           // four imaging accumulators [4][nx][nz] (adjointUpDown)
   int rcv_dipole;        // receiver injection as a vertical dipole (rtm_true)
   int pad2_;
-  // exact adjoint, pad cells (NX x LDZ each): (1 - w) L of the ring cells of
-  // the current step; the ring terms of the next step; the prev-ring terms
-  // kept for the step after it
-  float *adj_rho, *adj_e, *adj_b;
+  // exact adjoint, pad and model edge cells (NX x LDZ each): the ring terms
+  // of a step, in two buffers used by alternate steps (this step's read, the
+  // next step's written); the prev-ring terms kept for the step after next
+  float *adj_e[2], *adj_b;
 };
 enum SnapType : int { SNAP_NONE = 0, SNAP_F32 = 1, SNAP_BF16 = 2, SNAP_F16 = 3 };
 static_assert(sizeof(ShotDev) % sizeof(int) == 0 && sizeof(ShotDev) <= 256 * sizeof(int),
@@ -111,8 +105,6 @@ struct StepArgs {
   int snap_k = -1;   // snapshot index written (forward) or imaged (adjoint)
   float img_w = 0.f; // adjoint: weight of the imaging term (snapshot interval)
   int illum_on = 0;  // add the square of every model cell's new value to g.illum
-  const PadChunk *chunks = nullptr;  // ring cells of the batch (adjoint ring kernel)
-  int nchunks = 0;
 };
 
 // Allocation geometry of one field of a shot: LDZ floats per column, and the
@@ -159,8 +151,8 @@ cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, i
                         int n_pad, int num_sms, const StepArgs &a, int *d_err, cudaStream_t s_int,
                         cudaStream_t s_pad);
 cudaError_t configure();
-// one reverse step of the exact Born adjoint over the adjoint tile list; with
-// pad tiles, the ring kernel over the pad cells a.chunks follows on s_pad
+// one reverse step of the exact Born adjoint over the adjoint tile list
+// (interior tiles on s_int, pad tiles on s_pad)
 cudaError_t launch_adjoint(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
                            const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad);
 cudaError_t configure_adjoint();
