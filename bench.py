@@ -1,44 +1,56 @@
 """Benchmark of the B200 FD engine -- one JSON line on stdout (rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--nt NT]
+                    [--workload lsrtm_large|lsrtm_1200x400]
 
-Workload ``lsrtm_iter`` (default): one least-squares RTM CG iteration (CGLS)
-on the 32-shot survey of the 1200x400 model (10 m grid, pml 40, nt 5000 + 94
-delay steps, dt 0.8 ms, 20 Hz Ricker, full-aperture receivers at gz=1):
-Born modeling of all 32 shots (two fields per step), the exact adjoint of all
-32 shots (one field per step, imaging from BF16 source snapshots kept every 4
-steps) and the FP64 CG vector algebra.  The background velocity is fixed, so
-the source snapshots are computed once when the solver is reset and reused by
-every iteration.  One step = one CG iteration.  Metric: padded grid
-cell-updates per second (Gcell/s), whole job; ``ms_per_step`` is the LSRTM
+Workload ``lsrtm_large`` (default): least-squares RTM by CG (CGLS) on the
+largest survey -- 4000 x 1000 cells at 5 m, pml 40, nt 8000 + 120 delay steps,
+dt 0.5 ms, 25 Hz Ricker, 256 shots with apertures of 1000-4000 columns drawn
+from a seed, layered model with velocity anomalies.  Velocities are capped at
+3000 m/s: at this survey's 5500 m/s (Courant number 0.55) the reference's
+scheme -- its absorbing boundary, which this library reproduces bit for bit --
+grows without bound over 8120 steps from a Courant number of about 0.33 up.
+One GPU runs a sample of 8 of the 256 shots (shots 0, 32, ..., 224; under
+torchrun rank r takes shots r, 32 + r, ...: weak scaling, no collective on
+the data path), with the solver as the full survey needs it on a GPU: BF16
+source-term snapshots every 4 steps with one power-of-two scale per tile,
+source-field checkpoints every 256 steps, FP64 CG scalars.  One step = one CG
+iteration over the sample: Born modeling of its 8 shots (two fields per step),
+their exact adjoint (reverse pass plus the recomputed source field of each
+checkpoint segment) and the FP64 vector algebra.  Metric: padded grid
+cell-updates per second (Gcell/s), whole job; ``ms_per_step`` is the
 iteration time.
 
 * ``value``: device-resident solver state, CUDA-event timed iterations.
 * ``e2e``: the public LSRTM API with host buffers, every step: background and
-  wavelet upload, observed data of every shot uploaded from pinned memory,
-  reset (source pass + first adjoint), one iteration, model download; its
-  Gcell/s counts every cell-update of that work.
-* ``plain_fp32``: the same iteration on the plain path -- one shot per plan
-  and launch sequence, FP32 source snapshots at every step recomputed for
-  every shot (32 shots' snapshots do not fit in HBM), timed on a sample of
-  shots and scaled to 32.
-* ``roofline``: the kernel with the largest share of the iteration,
+  wavelet upload, the observed data of every shot from pinned memory, reset
+  (checkpoint pass + first adjoint), one iteration, model download.
+* ``plain_fp32``: the same Born + adjoint work on the plain path -- one shot
+  per plan and launch sequence, FP32 source snapshots at every step (with the
+  same checkpoints: kept whole they take ~40 GB per wide shot), the source
+  pass made per shot -- timed on every shot of the sample.
+  ``mixed_regrouped``: the batched mixed solver rebuilding its plans in every
+  operator application (shot-group mode, as on one GPU for all 256 shots),
+  which also redoes the checkpoint pass: it separates batching and mixed
+  storage from the reuse of the source field across iterations.
+* ``image_error``: the first CG gradient image L^T d of one shot (shot 64)
+  from the mixed-storage and the plain FP32 adjoints, against the FP64 image
+  of the same shot and data (the restatement's double build, computed offline
+  by tests/golden/make_large_fp64.py; compared on its stored subsample), and
+  mixed against plain over all 8 shots.
+* ``roofline``: the step kernel with the largest share of the iteration,
   algorithmic bytes per launch (16 B per field cell-update: read prev, cur,
-  velocity, write next; Born's dv read is inside its 2 x 16 B) over its mean
-  CUDA-event duration, against the measured HBM copy bandwidth.
-* ``cpu_baseline``: the reference's own ``forward`` and ``adjoint``
-  (src/util/fd.cpp:81-177, :592-719, compiled from its sources into
-  oracle/_ref) on shot 0 with the time loop cut short, all host threads,
-  expressed as this iteration's cell-updates per second.
+  velocity, write next) over its mean CUDA-event duration, against the
+  measured HBM copy bandwidth.
+* ``cpu_baseline``: the reference's own ``forward`` (Born) and ``adjoint``
+  (RTM) (src/util/fd.cpp:81-177, :592-719, compiled from its sources into
+  oracle/_ref) on the sample's narrowest shot with the recorded samples cut
+  to 24 (the 120 delay steps all run), all host threads, as cell-updates per
+  second of the same work.
 
-* ``largest_config_sample``: 4 shots of the largest configuration (4000 x
-  1000 cells, 8120 steps, velocities capped at 3000 m/s where the reference's
-  scheme is stable), one batched BF16 LSRTM iteration (snapshots kept whole
-  and checkpointed) against the plain FP32 path, and the image error between
-  the two storage choices (``python -m seis_b200.probe large``).
-
-Under torchrun (N > 1) every rank runs its own 32-shot survey (weak scaling).
+Workload ``lsrtm_1200x400``: one CG iteration of the 32-shot 1200 x 400 survey
+(10 m, nt 5000 + 94, dt 0.8 ms, 20 Hz, BF16 snapshots every 4 steps kept
+whole, no checkpoints).
 """
 from __future__ import annotations
 
@@ -56,6 +68,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 L2_BYTES = 126 * 2 ** 20
+SNAP_EVERY = 4
+CK_EVERY = 256      # lsrtm_large: source-field checkpoint interval
+SAMPLE = 8          # lsrtm_large: shots per GPU
+STRIDE = 32         # lsrtm_large: shot index stride of a GPU's sample
+FP64_SHOT = 64      # lsrtm_large: the shot with an FP64 image fixture
 
 
 def peaks():
@@ -163,11 +180,38 @@ def load_synth():
     return mod
 
 
-def workload(name: str, rank: int, nt: int = 5000):
+def workload(name: str, rank: int, world: int):
+    """(whole survey, this rank's shot indices, solver options)."""
     synth = load_synth()
-    if name == "lsrtm_iter":
-        return synth.lsrtm(nt=nt)
+    if name == "lsrtm_large":
+        full = synth.large_sweep(vmax=3000.0)
+        mine = [k * STRIDE + rank for k in range(SAMPLE)]
+        return full, mine, {"checkpoint_every": CK_EVERY}
+    if name == "lsrtm_1200x400":
+        full = synth.lsrtm(nshots=32 * world)
+        mine = list(range(32 * rank, 32 * rank + 32))
+        return full, mine, {"checkpoint_every": 0}
     raise SystemExit(f"unknown workload {name}")
+
+
+def config_of(name: str, full, sv, world: int) -> dict:
+    """The workload's `config`, the same for both arms."""
+    s0 = sv.shots[0]
+    c = {"workload": name, "shots_per_gpu": len(sv.shots), "shots_total_survey": len(full.shots),
+         "shots_timed_total": len(sv.shots) * world, "apertures_rank0": [s.nx for s in sv.shots],
+         "grid": f"{full.nx}x{full.nz} at {full.dx:g} m, pml {s0.pml}",
+         "nt": s0.nt, "ndel": s0.ndel, "dt_s": s0.dt, "ricker_hz": full.fr,
+         "snapshots": f"BF16 every {SNAP_EVERY} steps, per-tile power-of-two scale",
+         "step": "one CG iteration over the GPU's shots: Born of every shot, its exact "
+                 "adjoint, FP64 CG algebra",
+         "exchange": "per CG iteration: NCCL all-reduce of the image and 2 FP64 sums"
+                     if world > 1 else "none"}
+    if name == "lsrtm_large":
+        c.update({"velocity_cap_m_s": 3000.0, "checkpoint_every": CK_EVERY,
+                  "shot_indices_rank0": [k * STRIDE for k in range(SAMPLE)],
+                  "sample": f"{SAMPLE} of the survey's {len(full.shots)} shots per GPU "
+                            f"(every {STRIDE}th)"})
+    return c
 
 
 def cpu_model() -> str:
@@ -180,37 +224,25 @@ def cpu_model() -> str:
     return "unknown"
 
 
-SNAP_EVERY = 4
-
-
-def iteration_cells(shots) -> int:
-    """Cell-updates of one CG iteration: Born (2 fields x NT steps) and the
-    exact adjoint's reverse pass (1 field x NT+1 steps) of every shot."""
-    return sum((s.nx + 2 * s.pml) * (s.nz + 2 * s.pml) * (3 * s.NT + 1) for s in shots)
-
-
-def reset_cells(shots) -> int:
-    """Cell-updates of a solver reset: source pass (NT) + one adjoint (NT+1)."""
-    return sum((s.nx + 2 * s.pml) * (s.nz + 2 * s.pml) * (2 * s.NT + 1) for s in shots)
-
-
-def cpu_baseline(sv, steps_cap: int = 150):
+def cpu_baseline(sv, steps_cap: int):
     """The reference's `forward` (Born) and `adjoint` (RTM), compiled from its
-    own sources, on shot 0 with the recorded time samples cut to `steps_cap`;
-    rate = this library's cell-updates of one CG iteration for that shot and
-    step count (3 NT + 1 per padded cell) over the reference's Born + adjoint
-    time, i.e. the reference's speed on the same job."""
+    own sources, on the sample's narrowest shot with the recorded time samples
+    cut to `steps_cap` (the delay steps all run); rate = the cell-updates of
+    one CG iteration of that shot and step count (3 NT + 1 per padded cell:
+    Born two fields, adjoint one) over the reference's Born + adjoint time,
+    i.e. the reference's speed on the same job."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
     import dataclasses
-    s0 = sv.shots[0]
+
+    import oracle as O
+    k = min(range(len(sv.shots)), key=lambda i: sv.shots[i].nx)
+    s0 = sv.shots[k]
     s = dataclasses.replace(s0, nt=steps_cap)
     kind = "reference" if O.ref_available() else "port"
-    make = lambda dt, fr, d, n: O.ricker(dt, fr, d, n, impl="ref" if kind == "reference" else "oracle")
-    wav = sv.wavelet(make)[:s.NT]
-    vel, dv = sv.sub(sv.vel0, 0), sv.sub(sv.dv, 0)
-    cores = len(os.sched_getaffinity(0))
     impl = "ref" if kind == "reference" else "oracle"
+    wav = sv.wavelet(lambda dt, fr, d, n: O.ricker(dt, fr, d, n, impl=impl))[:s.NT]
+    vel, dv = sv.sub(sv.vel0, k), sv.sub(sv.dv, k)
+    cores = len(os.sched_getaffinity(0))
     if kind == "reference":
         O.ref_set_threads(cores)
     else:
@@ -222,125 +254,170 @@ def cpu_baseline(sv, steps_cap: int = 150):
     O.rtm(s, wav, vel, rec, impl=impl)
     t_adj = time.perf_counter() - t
     dt = t_born + t_adj
-    cells = iteration_cells([s])
+    cells = (s.nx + 2 * s.pml) * (s.nz + 2 * s.pml) * (3 * s.NT + 1)
     return {"value": cells / dt / 1e9, "unit": "Gcell/s", "cores": cores, "kind": kind,
             "cpu": cpu_model(),
-            "sample": f"forward (Born) {t_born:.2f} s + adjoint (RTM) {t_adj:.2f} s of shot 0 "
+            "sample": f"forward (Born) {t_born:.2f} s + adjoint (RTM) {t_adj:.2f} s of one shot "
                       f"({s.nx}x{s.nz}, pml {s.pml}), {s.NT} of {s0.NT} steps; the reference has "
                       f"no CG, so one iteration = these two calls per shot"}
 
 
+def synth_data_note(name: str) -> str:
+    if name == "lsrtm_large":
+        return ("synthetic (seeded 4000x1000 layered model with Gaussian anomalies, capped at "
+                "3000 m/s; observed data = Born modeling of the true perturbation)")
+    return ("synthetic (seeded layered + faulted 1200x400 model; observed data = Born modeling "
+            "of the true perturbation)")
+
+
 def run_reference(args, rank, world):
+    """The reference's CPU path on this workload (bounded sample per step)."""
     if rank != 0:
         return
-    sv = workload(args.workload, rank, args.nt)
-    vals = []
+    full, mine, _ = workload(args.workload, rank, world)
+    sv = full.subset(mine)
+    cap = 24 if args.workload == "lsrtm_large" else 150
+    vals, last = [], None
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(sv, steps_cap=40 if i < args.warmup else 150)
+        last = cpu_baseline(sv, steps_cap=cap)
         if i >= args.warmup:
-            vals.append(r["value"])
+            vals.append(last["value"])
     v = statistics.median(vals)
     line = {"impl": "reference", "metric": "Gcell-updates/s", "value": v, "unit": "Gcell/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (layered + faulted 1200x400 model; observed data = Born of the true "
-                    "perturbation)",
-            "config": {"workload": args.workload, "shots_per_gpu": len(sv.shots),
-                       "grid": "1200x400 at 10 m, pml 40", "nt": sv.shots[0].nt,
-                       "ndel": sv.shots[0].ndel},
-            "cpu_baseline": {"value": v, "unit": "Gcell/s", "cores": r["cores"], "kind": r["kind"],
-                             "sample": r["sample"]},
+            "data": synth_data_note(args.workload),
+            "config": config_of(args.workload, full, sv, world),
+            "cpu_baseline": {"value": v, "unit": "Gcell/s", "cores": last["cores"],
+                             "kind": last["kind"], "cpu": last["cpu"], "sample": last["sample"]},
             "e2e": {"value": v, "unit": "Gcell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def observed_data(ctx, sv):
     """Synthetic observed data: Born gathers of the true perturbation over the
-    background, exact-rounding kernels."""
+    background, exact-rounding kernels (equal to the reference's own Born)."""
     from seis_b200._lib import IN_DV, IN_VEL, IN_WAVELET, OP_BORN, OUT_GATHER, Plan
     wav = sv.wavelet()
-    with Plan(ctx, OP_BORN, sv.shots) as p:
-        for i in range(len(sv.shots)):
-            p.set(i, IN_VEL, sv.sub(sv.vel0, i))
-            p.set(i, IN_DV, sv.sub(sv.dv, i))
-            p.set(i, IN_WAVELET, wav)
-        p.run()
-        return [p.get(i, OUT_GATHER) for i in range(len(sv.shots))]
+    out = []
+    for i in range(len(sv.shots)):  # one at a time: the widest gathers are 130 MB
+        with Plan(ctx, OP_BORN, [sv.shots[i]]) as p:
+            p.set(0, IN_VEL, sv.sub(sv.vel0, i))
+            p.set(0, IN_DV, sv.sub(sv.dv, i))
+            p.set(0, IN_WAVELET, wav)
+            p.run()
+            out.append(p.get(0, OUT_GATHER))
+    return out
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
-# each step path of this workload (all kernels of the path, 32 shots), from one
-# ncu capture each of `python -m seis_b200.probe {adjoint|born} --steps 3`:
-# adjoint pad tiles 225.6 MB + ring kernel 137.9 MB; adjoint interior tiles;
-# Born pad tiles 371.0 MB + absorbing kernel 229.6 MB; Born interior tiles.
-NCU_TRAFFIC = {"adjoint_pad": 363.5e6, "adjoint_interior": 196.4e6,
-               "born_pad": 600.6e6, "born_interior": 405.5e6}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of one
+# launch of each step kernel, from ncu captures (profiles/); a launch's
+# traffic is this times the cells it updates.
+NCU_TRAFFIC_PER_CELL = {}
 
 
-def kernel_roofline(ctx, sv, iter_ms):
+def kernel_roofline(ctx, sv, iter_ms, launches_per_iter):
     """Per-kernel CUDA-event durations of the Born and adjoint step kernels
-    (separate plans over the same shots), their share of one iteration, and
-    the roofline of the kernel with the largest share."""
+    (separate plans over the same shots, the two kernels of a step concurrent
+    as in a run), their share of one iteration, and the roofline of the
+    kernel with the largest share."""
     from seis_b200._lib import IN_VEL, IN_WAVELET, OP_BORN, OP_BORN_ADJOINT, Plan
     wav = sv.wavelet()
-    NT = sv.shots[0].NT
     rows = []
-    for op, name, launches in ((OP_BORN, "born", NT), (OP_BORN_ADJOINT, "adjoint", NT + 1)):
+    for op, name in ((OP_BORN, "born"), (OP_BORN_ADJOINT, "adjoint")):
         with Plan(ctx, op, sv.shots) as p:
             if op == OP_BORN:
                 p.set_exact(False)  # the solver's Born operator runs the fast build
             for i in range(len(sv.shots)):
                 p.set(i, IN_VEL, sv.sub(sv.vel0, i))
                 p.set(i, IN_WAVELET, wav)
-            p.time_kernels(20)
-            ms, by = p.time_kernels(200)
+            p.time_kernels(10)
+            ms, by = p.time_kernels(100)
+        n = launches_per_iter[name]
+        per_cell = 32.0 if op == OP_BORN else 16.0
         for k, kname in ((0, "interior"), (1, "pad")):
-            rows.append({"kernel": f"{name}_{kname}", "ms": ms[k], "bytes": by[k],
-                         "launches_per_iter": launches,
-                         "share": ms[k] * launches / iter_ms})
-        rows.append({"kernel": f"{name}_step", "ms": ms[2], "launches_per_iter": launches,
-                     "share": ms[2] * launches / iter_ms})
-    kern = [r for r in rows if "bytes" in r]
+            kern = f"{name}_{kname}"
+            tr = NCU_TRAFFIC_PER_CELL.get(kern)
+            rows.append({"kernel": kern, "ms": ms[k], "bytes": by[k], "launches_per_iter": n,
+                         "share": ms[k] * n / iter_ms, "GB_s": by[k] / (ms[k] * 1e6),
+                         "traffic": tr * by[k] / per_cell if tr else None})
+        rows.append({"kernel": f"{name}_step", "ms": ms[2], "bytes": by[0] + by[1],
+                     "launches_per_iter": n, "share": ms[2] * n / iter_ms,
+                     "GB_s": (by[0] + by[1]) / (ms[2] * 1e6)})
+    kern = [r for r in rows if not r["kernel"].endswith("_step")]
     top = max(kern, key=lambda r: r["ms"] * r["launches_per_iter"])
     return top, rows
 
 
-def plain_fp32(ctx, sv, dobs, nsample: int = 2):
-    """One CG iteration on the plain path, timed on `nsample` shots and scaled
-    to the survey: per shot, one single-shot Born plan run and one single-shot
-    adjoint plan run with FP32 snapshots at every step (recomputed per shot)."""
+def adjoint_images(ctx, sv, dobs, every, dtype, ck):
+    """Per-shot exact-adjoint images L_s^T d_s (one batched plan)."""
+    from seis_b200._lib import IN_GATHER, IN_VEL, IN_WAVELET, OP_BORN_ADJOINT, OUT_IMAGE, Plan
+    wav = sv.wavelet()
+    with Plan(ctx, OP_BORN_ADJOINT, sv.shots) as p:
+        p.set_snapshots(every, dtype)
+        if ck:
+            p.set_checkpoints(ck)
+        for i in range(len(sv.shots)):
+            p.set(i, IN_VEL, sv.sub(sv.vel0, i))
+            p.set(i, IN_WAVELET, wav)
+            p.set(i, IN_GATHER, dobs[i])
+        p.run()
+        return [p.get(i, OUT_IMAGE) for i in range(len(sv.shots))]
+
+
+def plain_fp32(ctx, sv, dobs, ck):
+    """The Born + adjoint work of one CG iteration on the plain path, every
+    shot of the sample: per shot one single-shot Born plan (FP32, fast build)
+    and one single-shot adjoint plan with FP32 snapshots at every step (and
+    the solver's checkpoints), source pass per shot, plans built per shot.
+    Returns (seconds, per-shot images of the adjoint)."""
     import torch
     from seis_b200._lib import (IN_DV, IN_GATHER, IN_VEL, IN_WAVELET, OP_BORN, OP_BORN_ADJOINT,
-                                SNAP_F32, Plan)
+                                OUT_IMAGE, SNAP_F32, Plan)
     wav = sv.wavelet()
-    p0 = np.zeros((sv.nx, sv.nz), np.float32) + 1.0
-    with Plan(ctx, OP_BORN, [sv.shots[0]]) as pb, Plan(ctx, OP_BORN_ADJOINT, [sv.shots[0]]) as pa:
-        pa.set_snapshots(1, SNAP_F32)
-        stream = torch.cuda.ExternalStream(ctx.stream_ptr)
-
-        def shot(i):
+    p0 = np.ones((sv.nx, sv.nz), np.float32)
+    imgs = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i, s in enumerate(sv.shots):
+        with Plan(ctx, OP_BORN, [s]) as pb, Plan(ctx, OP_BORN_ADJOINT, [s]) as pa:
+            pb.set_exact(False)
             pb.set(0, IN_VEL, sv.sub(sv.vel0, i))
             pb.set(0, IN_WAVELET, wav)
             pb.set(0, IN_DV, sv.sub(p0, i))
             pb.run()
+            pa.set_snapshots(1, SNAP_F32)
+            if ck:
+                pa.set_checkpoints(ck)
             pa.set(0, IN_VEL, sv.sub(sv.vel0, i))
             pa.set(0, IN_WAVELET, wav)
             pa.set(0, IN_GATHER, dobs[i])
             pa.run()
             pa.sync()
+            imgs.append(pa.get(0, OUT_IMAGE))
+    return time.perf_counter() - t0, imgs
 
-        shot(0)
-        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        start.record(stream)
-        for i in range(1, 1 + nsample):
-            shot(i)
-        stop.record(stream)
-        stop.synchronize()
-        per_shot = start.elapsed_time(stop) / nsample
-    return {"iter_ms": per_shot * len(sv.shots), "per_shot_ms": per_shot, "sampled_shots": nsample,
-            "how": "one shot per plan and graph; Born run, then adjoint with FP32 snapshots at "
-                   "every step, source pass recomputed per shot; sample scaled to all shots"}
+
+def image_errors(mine, img_mixed, img_plain):
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out = {"mixed_vs_plain_all_shots": rel(np.concatenate([x.ravel() for x in img_mixed]),
+                                            np.concatenate([x.ravel() for x in img_plain]))}
+    path = os.path.join(ROOT, "tests", "golden", "large_fp64.npz")
+    if FP64_SHOT in mine and os.path.exists(path):
+        g = np.load(path)
+        k = mine.index(FP64_SHOT)
+        st = int(g["step"])
+        ref = g["img_sub"].astype(np.float64)
+        out.update({
+            "fp64_shot": FP64_SHOT,
+            "fp64_reference": "exact Born adjoint in FP64 (the restatement's double build) of the "
+                              "same shot and data, computed offline (tests/golden/"
+                              f"make_large_fp64.py); compared on every {st}th column and row",
+            "mixed_vs_fp64": rel(img_mixed[k][::st, ::st], ref),
+            "plain_fp32_vs_fp64": rel(img_plain[k][::st, ::st], ref)})
+    return out
 
 
 def main():
@@ -349,13 +426,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lsrtm_iter")
+    ap.add_argument("--workload", default="lsrtm_large", choices=["lsrtm_large", "lsrtm_1200x400"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--no-large-sample", action="store_true",
-                    help="skip the 4-shot sample of the largest configuration")
-    ap.add_argument("--nt", type=int, default=5000,
-                    help="recorded time samples (a shorter loop of the same launches, for profiling)")
     args = ap.parse_args()
     rank, world, local = dist_init()
     if args.impl == "reference":
@@ -368,25 +441,23 @@ def main():
     from seis_b200._lib import SNAP_BF16, Lsrtm
 
     torch.cuda.set_device(local)
-    from seis_b200.shards import DeviceEngine, ShardedCGLS, nccl_reduce, shard_shots
-    # N ranks: a survey of 32 N shots, 32 per rank, image and CG sums all-reduced
-    full = workload(args.workload, rank, args.nt) if world == 1 else \
-        __import__("seis_b200.synth", fromlist=["lsrtm"]).lsrtm(nshots=32 * world, nt=args.nt)
-    mine = shard_shots([full.cell_updates_of(i) for i in range(len(full.shots))], world)[rank]
+    from seis_b200.shards import DeviceEngine, ShardedCGLS, nccl_reduce
+    full, mine, opts = workload(args.workload, rank, world)
     sv = full.subset(mine)
     shots = sv.shots
+    ck = opts["checkpoint_every"]
     ctx = Context(local)
     wav = sv.wavelet()
     dobs = observed_data(ctx, sv)
-    ls = Lsrtm(ctx, sv.nx, sv.nz, shots, sv.x0, snap_every=SNAP_EVERY, snap_dtype=SNAP_BF16)
+    ls = Lsrtm(ctx, sv.nx, sv.nz, shots, sv.x0, snap_every=SNAP_EVERY, snap_dtype=SNAP_BF16,
+               checkpoint_every=ck)
     ls.set_background(sv.vel0, wav)
     for i, d in enumerate(dobs):
         ls.set_data(i, d)
     eng = DeviceEngine(ls)
     cg = ShardedCGLS(eng, nccl_reduce(eng))
     rr0 = cg.reset()
-    cells = iteration_cells(shots)
-    assert cells == ls.cell_updates, (cells, ls.cell_updates)
+    cells = ls.cell_updates
 
     # ---- device-resident: CG iterations timed with CUDA events on the
     # library's stream
@@ -426,69 +497,93 @@ def main():
         h_rr[1] = cg.iterate(1)[0]
         ctx.check(L.seis_fd_lsrtm_model(ls.h, h_m.data_ptr()))
 
-    e2e_steps = max(1, args.steps // 2)
+    e2e_steps = max(1, args.steps // 4)
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         e2e_step()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
     e2e_ms = max_over_ranks(e2e_ms, world)
-    e2e_cells = (cells + reset_cells(shots)) * world
+    # reset = checkpoint (or snapshot) pass + one adjoint application (with
+    # checkpoints: reverse pass + recomputed source field)
+    reset_cells = sum((s.nx + 2 * s.pml) * (s.nz + 2 * s.pml) *
+                      (s.NT + (s.NT + 1) + (s.NT if ck else 0)) for s in shots)
+    e2e_cells = (cells + reset_cells) * world
     h2d = sv.vel0.nbytes + wav.nbytes + sum(d.nbytes for d in dobs)
     d2h = h_m.numel() * 4 + 16
     dev_bytes = ls.device_bytes
     ls.close()
 
-    # ---- roofline of the kernel with the largest share, plain FP32 path
-    top, rows = kernel_roofline(ctx, sv, ms_per_step)
+    # ---- the same iteration with the plans rebuilt in every application
+    regroup = None
+    if world == 1 and not args.no_plain and args.workload == "lsrtm_large":
+        with Lsrtm(ctx, sv.nx, sv.nz, shots, sv.x0, snap_every=SNAP_EVERY, snap_dtype=SNAP_BF16,
+                   checkpoint_every=ck, group_shots=len(shots)) as lg:
+            lg.set_background(sv.vel0, wav)
+            for i, d in enumerate(dobs):
+                lg.set_data(i, d)
+            lg.reset()
+            lg.iterate(1)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            lg.iterate(1)
+            torch.cuda.synchronize()
+            regroup = {"iter_ms": (time.perf_counter() - t) * 1e3,
+                       "how": "the batched mixed solver in shot-group mode: the plans of the "
+                              "group built in every operator application, checkpoint pass redone"}
+
+    # ---- plain FP32 path and image errors
+    plain = errors = None
+    if world == 1 and not args.no_plain:
+        t_plain, img_plain = plain_fp32(ctx, sv, dobs, ck)
+        img_mixed = adjoint_images(ctx, sv, dobs, SNAP_EVERY, SNAP_BF16, ck)
+        plain = {"iter_ms": t_plain * 1e3, "shots": len(shots),
+                 "how": "one shot per plan and graph; Born run, then the exact adjoint with FP32 "
+                        "snapshots at every step" + (f" (checkpoints every {ck} steps)" if ck else "")
+                        + ", source pass per shot; every shot of the sample timed"}
+        errors = image_errors(mine, img_mixed, img_plain)
+
+    # ---- roofline of the kernel with the largest share
+    per_iter_launches = {"born": shots[0].NT, "adjoint": shots[0].NT + 1}
+    top, rows = kernel_roofline(ctx, sv, ms_per_step, per_iter_launches)
     hbm, src = peaks()
     ach = top["bytes"] / (top["ms"] * 1e-3) / 1e9
-    plain = None if (args.no_plain or world > 1) else plain_fp32(ctx, sv, dobs)
     line = {
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (layered + faulted 1200x400 model; observed data = Born of the true "
-                "perturbation)",
-        "config": {"workload": args.workload, "shots_per_gpu": len(shots),
-                   "shots_total": len(full.shots),
-                   "exchange": "per CG iteration: NCCL all-reduce of the image and 2 FP64 sums"
-                               if world > 1 else "none",
-                   "grid": "1200x400 at 10 m, pml 40", "nt": shots[0].nt, "ndel": shots[0].ndel,
-                   "snapshots": f"BF16 every {SNAP_EVERY} steps, per-tile scale",
-                   "cell_updates_per_step": cells, "lsrtm_iter_ms": ms_per_step,
-                   "device_bytes": dev_bytes,
-                   "l2": "inputs larger than L2: fields, snapshots and data of 32 shots "
-                         f"({dev_bytes / 2**30:.1f} GiB resident)",
-                   "residual": {"rr0": rr0, "after_warmup": list(map(float, rr_warm)),
-                                "timed": rr}},
+        "data": synth_data_note(args.workload),
+        "config": config_of(args.workload, full, sv, world),
         "e2e": {"value": e2e_cells / (e2e_ms / 1e3) / 1e9, "unit": "Gcell/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "cell_updates_per_step": e2e_cells},
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                     "frac": ach / hbm, "traffic": NCU_TRAFFIC.get(top["kernel"]),
-                     "traffic_unit": "bytes per launch (ncu capture of the same workload)",
-                     "kernel": top["kernel"],
-                     "peak_source": src, "kernel_ms": top["ms"], "share": top["share"],
-                     "kernels": rows},
-        "plain_fp32": plain,
+                     "frac": ach / hbm, "traffic": top.get("traffic"),
+                     "traffic_unit": "bytes per launch (ncu dram read + write, scaled by cells)",
+                     "kernel": top["kernel"], "peak_source": src, "kernel_ms": top["ms"],
+                     "share": top["share"], "kernels": rows},
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    cfg = line["config"]
+    cfg.update({"cell_updates_per_step": cells, "lsrtm_iter_ms": ms_per_step,
+                "device_bytes": dev_bytes,
+                "l2": "inputs larger than L2: fields, checkpoints, snapshots and data of the "
+                      f"shots ({dev_bytes / 2**30:.1f} GiB resident)",
+                "residual": {"rr0": rr0, "after_warmup": list(map(float, rr_warm)),
+                             "timed": rr}})
     if plain:
-        line["config"]["speedup_vs_plain_fp32"] = plain["iter_ms"] / ms_per_step
+        line["plain_fp32"] = plain
+        cfg["speedup_vs_plain_fp32"] = plain["iter_ms"] / ms_per_step
+    if regroup:
+        line["mixed_regrouped"] = regroup
+        if plain:
+            cfg["speedup_regrouped_vs_plain_fp32"] = plain["iter_ms"] / regroup["iter_ms"]
+    if errors:
+        line["image_error"] = errors
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(sv)
+        line["cpu_baseline"] = cpu_baseline(sv, 24 if args.workload == "lsrtm_large" else 150)
     ctx.close()
-    if world == 1 and not args.no_large_sample and args.nt == 5000:
-        # the largest configuration (4000 x 1000, 8120 steps) on 4 of its shots:
-        # batched BF16 LSRTM iteration against the plain FP32 path, image error
-        # between their storage choices (seis_b200.probe large)
-        try:
-            from seis_b200 import probe
-            line["largest_config_sample"] = probe.large(4)
-        except Exception as e:  # reported, not fatal: the headline line stands
-            line["largest_config_sample"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     barrier(world)

@@ -102,3 +102,21 @@ def nccl_reduce(engine: DeviceEngine, group=None) -> Callable:
             with torch.cuda.stream(engine.stream):
                 dist.all_reduce(buf, group=group)
     return reduce
+
+
+def host_reduce(engine: DeviceEngine, group=None) -> Callable:
+    """In-place sum over the ranks through host memory, for process groups
+    whose backend reduces host tensors only (gloo): the buffer is copied to
+    the host once the engine's stream has produced it, summed, and copied
+    back on the engine's stream."""
+    import torch
+    import torch.distributed as dist
+
+    def reduce(buf):
+        if dist.is_initialized() and dist.get_world_size(group) > 1:
+            with torch.cuda.stream(engine.stream):
+                h = buf.cpu()  # waits for the engine's stream
+            dist.all_reduce(h, group=group)
+            with torch.cuda.stream(engine.stream):
+                buf.copy_(h)
+    return reduce
