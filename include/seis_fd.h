@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define SEIS_FD_ABI_VERSION 1
+#define SEIS_FD_ABI_VERSION 2
 
 /* status codes */
 #define SEIS_OK 0
@@ -254,6 +254,30 @@ int seis_fd_plan_set_exact(seis_fd_plan *plan, int exact);
  * fields are clobbered; the next run starts from its cleared state. */
 int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double *bytes);
 
+/* Tile shapes of the step kernels (columns x rows of one CTA's tile; no
+ * counterpart in the reference, whose OpenMP loops split x only,
+ * src/util/fd.cpp:1242-1271).  Every shape gives the same results bit for bit;
+ * they differ in halo overhead, threads per CTA and CTAs per SM. */
+#define SEIS_TILE_32x64 0   /* 256 threads (default) */
+#define SEIS_TILE_64x32 1   /* 256 threads */
+#define SEIS_TILE_16x128 2  /* 256 threads */
+#define SEIS_TILE_64x64 3   /* 512 threads */
+#define SEIS_TILE_32x32 4   /* 128 threads */
+#define SEIS_TILE_SHAPES 5
+/* Set the plan's tile shape.  SEIS_ERR_STATE once an adjoint plan's snapshots
+ * are allocated (their scales are tiled like the kernels). */
+int seis_fd_plan_set_tile_shape(seis_fd_plan *plan, int shape);
+/* The plan's tile shape, or SEIS_ERR_ARG. */
+int seis_fd_plan_tile_shape(const seis_fd_plan *plan);
+/* Autotuner: time `steps` steps of the plan's own kernels (as
+ * seis_fd_plan_time_kernels, on its current inputs) in every tile shape and
+ * keep the fastest.  The choice is cached in the process per plan signature
+ * (operator, build flavour, every shot's padded grid) and reused by later
+ * plans of the same signature unless `force` is set.  h_ms[SEIS_TILE_SHAPES]
+ * (may be null) receives each shape's mean step time (0 where not timed),
+ * *h_best (may be null) the shape kept.  The plan's fields are clobbered. */
+int seis_fd_plan_autotune(seis_fd_plan *plan, int steps, int force, double *h_ms, int *h_best);
+
 /* Batched forms of the single-shot calls: h_*[i] are the arrays of shot i. */
 int seis_fd_modeling_batch(seis_fd_ctx *ctx, int nshot, const seis_shot_desc *shots,
                            const float *const *h_wav, const float *const *h_vel,
@@ -326,6 +350,10 @@ typedef struct {
                       shots at a time and frees them (for surveys whose plans
                       do not fit at once); the source pass then runs in every
                       application, and the results are identical */
+  int tile_shape;  /* 0 (default): the tile shape of each Born and adjoint plan
+                      is picked by seis_fd_plan_autotune once its background
+                      is set (cached per plan signature); k > 0: shape k - 1
+                      (SEIS_TILE_*) */
 } seis_lsrtm_opts;
 
 int seis_fd_lsrtm_create(seis_fd_ctx *ctx, int nx, int nz, int nshot,

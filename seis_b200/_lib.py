@@ -75,7 +75,7 @@ def shot_desc(s) -> ShotDescC:
 class LsrtmOptsC(ctypes.Structure):
     _fields_ = [("snap_every", ctypes.c_int), ("snap_dtype", ctypes.c_int),
                 ("exact", ctypes.c_int), ("checkpoint_every", ctypes.c_int),
-                ("group_shots", ctypes.c_int)]
+                ("group_shots", ctypes.c_int), ("tile_shape", ctypes.c_int)]
 
 
 _lib = None
@@ -121,6 +121,10 @@ def lib():
         L.seis_fd_born_adjoint.argtypes = [P, SD, P, P, P, P]
         L.seis_fd_plan_time_kernels.argtypes = [P, I, ctypes.POINTER(ctypes.c_double),
                                                 ctypes.POINTER(ctypes.c_double)]
+        L.seis_fd_plan_set_tile_shape.argtypes = [P, I]
+        L.seis_fd_plan_tile_shape.argtypes = [P]
+        L.seis_fd_plan_autotune.argtypes = [P, I, I, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_int)]
         PP = ctypes.POINTER(P)
         L.seis_fd_modeling_batch.argtypes = [P, I, SD, PP, PP, PP]
         L.seis_fd_born_batch.argtypes = [P, I, SD, PP, PP, PP, PP]
@@ -227,6 +231,10 @@ def validate_shot(shot: "Shot") -> str:
 (OP_MODELING, OP_BORN, OP_RTM, OP_BORN_ADJOINT, OP_ILLUM, OP_BORN_PLANE, OP_RTM_PLANE,
  OP_RTM_TRUE, OP_RTM_UPDOWN, OP_ILLUM_PLANE) = range(10)
 SNAP_F32, SNAP_BF16, SNAP_F16 = 1, 2, 3
+# tile shapes of the step kernels (include/seis_fd.h SEIS_TILE_*)
+TILE_32x64, TILE_64x32, TILE_16x128, TILE_64x64, TILE_32x32 = range(5)
+TILE_SHAPES = {TILE_32x64: (32, 64), TILE_64x32: (64, 32), TILE_16x128: (16, 128),
+               TILE_64x64: (64, 64), TILE_32x32: (32, 32)}
 IN_VEL, IN_DV, IN_WAVELET, IN_GATHER, IN_SOURCE, IN_WAVELET_H = 0, 1, 2, 3, 4, 5
 OUT_GATHER, OUT_IMAGE, OUT_COMPONENTS = 0, 1, 2
 
@@ -288,6 +296,21 @@ class Plan:
 
     def set_exact(self, exact: bool):
         self.ctx.check(self.ctx.L.seis_fd_plan_set_exact(self.h, 1 if exact else 0))
+
+    def set_tile_shape(self, shape: int):
+        self.ctx.check(self.ctx.L.seis_fd_plan_set_tile_shape(self.h, shape))
+
+    @property
+    def tile_shape(self) -> int:
+        return int(self.ctx.L.seis_fd_plan_tile_shape(self.h))
+
+    def autotune(self, steps: int = 10, force: bool = False):
+        """(chosen shape, mean step ms of every shape; 0 where not timed)."""
+        ms = (ctypes.c_double * len(TILE_SHAPES))()
+        best = ctypes.c_int()
+        self.ctx.check(self.ctx.L.seis_fd_plan_autotune(self.h, steps, 1 if force else 0, ms,
+                                                        ctypes.byref(best)))
+        return best.value, list(ms)
 
     def time_kernels(self, steps: int):
         ms = (ctypes.c_double * 3)()
@@ -359,16 +382,18 @@ class Lsrtm:
 
     def __init__(self, ctx: Context, nx: int, nz: int, shots, x0=None, snap_every: int = 1,
                  snap_dtype: int = None, exact: bool = False, colmaps=None,
-                 checkpoint_every: int = 0, group_shots: int = 0):
+                 checkpoint_every: int = 0, group_shots: int = 0, tile_shape: int = None):
         """Shot k covers columns x0[k] .. x0[k] + nx_k - 1, or the model columns
         colmaps[k] (one per sub-grid column, non-decreasing).  checkpoint_every > 0
         keeps source-field checkpoints instead of every snapshot; group_shots > 0
         builds the plans of that many shots at a time in every operator
-        application instead of keeping all of them."""
+        application instead of keeping all of them.  tile_shape: None (default)
+        lets the autotuner pick each plan's tile shape; else a TILE_* shape."""
         self.ctx, self.nx, self.nz, self.shots = ctx, nx, nz, list(shots)
         self._descs = shot_array(self.shots)
         o = LsrtmOptsC(snap_every, SNAP_BF16 if snap_dtype is None else snap_dtype,
-                       1 if exact else 0, checkpoint_every, group_shots)
+                       1 if exact else 0, checkpoint_every, group_shots,
+                       0 if tile_shape is None else tile_shape + 1)
         h = ctypes.c_void_p()
         if colmaps is None:
             self._x0 = (ctypes.c_int * len(self.shots))(*[int(v) for v in x0])

@@ -43,8 +43,28 @@
 namespace seis {
 namespace SEIS_NS {
 
-constexpr int A_NT_I = 256;  // interior adjoint kernel threads
-constexpr int WIDE = CW_C * SR, NARROW = CW_P * SR;
+// Adjoint geometry of tile shape S: staged window sizes, the tile + halo
+// ring arrays of the pad kernel, halo cells per thread.
+template <int S>
+struct AGeo {
+  using G = Geo<S>;
+  static constexpr int WIDE = G::CW_C * G::SR, NARROW = G::CW_P * G::SR;
+  static constexpr int RW = G::TZ + 2;
+  static constexpr int RN = (G::TX + 2) * RW;
+  static constexpr int NHALO = 2 * (G::TX + 2) + 2 * G::TZ;
+  static constexpr int HPT = (NHALO + G::NT - 1) / G::NT;  // halo cells per thread
+  static constexpr int PAD_FLOATS = 4 * WIDE + NARROW + RN;
+  static_assert(5 * RN <= 3 * WIDE + NARROW + RN, "ring arrays fit over the dead buffers");
+  static constexpr size_t TILE_SMEM = sizeof(float) * (size_t)(4 * WIDE + NARROW) + 16;
+  static constexpr size_t PAD_SMEM = sizeof(float) * (size_t)PAD_FLOATS + 16;
+  static constexpr int MIN_I = ctas_fit(TILE_SMEM, 768 / G::NT) > 0 ? ctas_fit(TILE_SMEM, 768 / G::NT) : 1;
+  static constexpr int MIN_P = ctas_fit(PAD_SMEM, 512 / G::NT) > 0 ? ctas_fit(PAD_SMEM, 512 / G::NT) : 1;
+};
+#define SEIS_AGEO(S)                                                        \
+  SEIS_GEO(S);                                                              \
+  using AG_ = AGeo<S>;                                                      \
+  constexpr int WIDE = AG_::WIDE, NARROW = AG_::NARROW, A_NT_I = G_::NT;    \
+  (void)WIDE; (void)NARROW; (void)A_NT_I
 
 __device__ __forceinline__ float snap_load(const ShotDev &g, int k, int x, int z) {
   size_t i = (size_t)k * g.nx * g.nz + (size_t)x * g.nz + z;
@@ -56,6 +76,7 @@ __device__ __forceinline__ float snap_load(const ShotDev &g, int k, int x, int z
   }
 }
 
+template <int TX, int TZ>
 __device__ __forceinline__ float snap_inv_scale(const ShotDev &g, int k, int x0, int z0) {
   if (g.snap_dtype == SNAP_F32) return 1.0f;
   const int ntx = (g.NX + TX - 1) / TX;
@@ -66,9 +87,12 @@ __device__ __forceinline__ float snap_inv_scale(const ShotDev &g, int k, int x0,
 // L_k = Lz(vz M1) + Lx(vx M1) + 2 M1 - M2 + R^T d ; grad += w lap M1.  On these
 // tiles M = L (no ring cell within one cell), so the staged arrays (named L1,
 // L2 below) hold M_{k+1}, M_{k+2} and the output is L_k = M_k.
-__global__ void __launch_bounds__(A_NT_I, 3) adj_interior_kernel(const ShotDev *__restrict__ shots,
-                                                                 const Tile *__restrict__ tiles,
-                                                                 StepArgs a, int *__restrict__ err) {
+template <int S>
+__global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_I) adj_interior_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
+    int *__restrict__ err) {
+  SEIS_AGEO(S);
+  using SA = SAT<SR>;
   extern __shared__ __align__(128) unsigned char smraw[];
   float *sL1 = reinterpret_cast<float *>(smraw);  // wide
   float *sV = sL1 + WIDE;                          // wide
@@ -117,7 +141,7 @@ __global__ void __launch_bounds__(A_NT_I, 3) adj_interior_kernel(const ShotDev *
 #pragma unroll
   for (int m = 0; m < 10; m++) xm[m] = WX.quad(ix - 4 + m, iz0);
   const bool img = a.snap_k >= 0 && g.snap != nullptr;
-  float inv_scale = img ? snap_inv_scale(g, a.snap_k, x0, z0) : 0.0f;
+  float inv_scale = img ? snap_inv_scale<TX, TZ>(g, a.snap_k, x0, z0) : 0.0f;
 #pragma unroll
   for (int j = 0; j < 2; j++) {
     const float4 za = WZ.quad(ix + j, iz0 - 4), zb = WZ.quad(ix + j, iz0), zc = WZ.quad(ix + j, iz0 + 4);
@@ -272,15 +296,9 @@ __device__ __forceinline__ int ring_coefs(const ShotDev &g, const PadPos &pp, fl
          ROLE_DIAG << role_slot(ix_ - tx_, iz_ - tz_);
 }
 
-// Cells of a tile and its one-cell halo: columns x0-1 .. x0+TX, rows z0-1 ..
-// z0+TZ.
-constexpr int RW = TZ + 2;
-constexpr int RN = (TX + 2) * RW;
-constexpr int ADJ_NHALO = 2 * (TX + 2) + 2 * TZ;
-static_assert(ADJ_NHALO <= A_NT_I, "one halo cell per thread");
-static_assert(5 * RN <= NARROW + 2 * WIDE + RN, "ring arrays fit over the dead buffers");
-constexpr int ADJ_PAD_FLOATS = 4 * WIDE + NARROW + RN;
-
+// Halo cell i of the tile at (x0, z0) (columns x0-1 .. x0+TX, rows z0-1 ..
+// z0+TZ): the rows above and below, then the columns left and right.
+template <int TX, int TZ>
 __device__ __forceinline__ void adj_halo_cell(int i, int x0, int z0, int &hx, int &hz) {
   if (i < 2 * (TX + 2)) {
     hx = x0 - 1 + i % (TX + 2);
@@ -296,19 +314,23 @@ __device__ __forceinline__ void adj_halo_cell(int i, int x0, int z0, int &hx, in
 // neighbours or consumers outside the 8th-order region; grad += w lap M1 on
 // its model cells; then M, E (next step) and B of its pad and model edge
 // cells, L = M elsewhere.
-__global__ void __launch_bounds__(A_NT_I, 2) adj_pad_kernel(const ShotDev *__restrict__ shots,
-                                                            const Tile *__restrict__ tiles,
-                                                            StepArgs a, int *__restrict__ err) {
+template <int S>
+__global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
+    int *__restrict__ err) {
+  SEIS_AGEO(S);
+  using SA = SAT<SR>;
+  constexpr int RW = AG_::RW, RN = AG_::RN, ADJ_NHALO = AG_::NHALO, HPT = AG_::HPT;
   extern __shared__ __align__(128) unsigned char smraw[];
-  float *sL1 = reinterpret_cast<float *>(smraw);  // wide
-  float *sV = sL1 + WIDE;                          // wide
-  float *sL2 = sV + WIDE;                          // narrow
+  float *sV = reinterpret_cast<float *>(smraw);   // wide
+  float *sL1 = sV + WIDE;                          // wide
+  float *sL2 = sL1 + WIDE;                         // narrow
   float *sWZ = sL2 + NARROW;                       // wide
   float *sWX = sWZ + WIDE;                         // wide
   float *sCOR = sWX + WIDE;                        // tile + halo: frame / low-order terms
   uint64_t *bar = reinterpret_cast<uint64_t *>(sCOR + RN);
-  // ring arrays of tile + halo, over sL2 .. sCOR once L is formed
-  float *rp0 = sL2, *rp1 = rp0 + RN, *rp2 = rp1 + RN, *rp3 = rp2 + RN;
+  // ring arrays of tile + halo, over sL1 .. sCOR once L is formed
+  float *rp0 = sL1, *rp1 = rp0 + RN, *rp2 = rp1 + RN, *rp3 = rp2 + RN;
   int *rmask = reinterpret_cast<int *>(rp3 + RN);
   const int tid = threadIdx.x;
   const Tile t = tiles[blockIdx.x];
@@ -382,7 +404,7 @@ __global__ void __launch_bounds__(A_NT_I, 2) adj_pad_kernel(const ShotDev *__res
   const bool img = a.snap_k >= 0 && g.snap != nullptr;
   float Lt[8];
   {
-    const float inv_scale = img ? snap_inv_scale(g, a.snap_k, x0, z0) : 0.0f;
+    const float inv_scale = img ? snap_inv_scale<TX, TZ>(g, a.snap_k, x0, z0) : 0.0f;
     float4 xm[10];
 #pragma unroll
     for (int m = 0; m < 10; m++) xm[m] = WX.quad(ix - 4 + m, iz0);
@@ -419,34 +441,43 @@ __global__ void __launch_bounds__(A_NT_I, 2) adj_pad_kernel(const ShotDev *__res
       }
     }
   }
-  // L of the halo's pad cells (the only halo cells whose rho is read)
-  int hx = -1, hz = -1;
-  float Lh = 0.0f;
-  PadPos hp{};
-  bool hring = false;
-  if (tid < ADJ_NHALO) {
-    adj_halo_cell(tid, x0, z0, hx, hz);
-    if (hx >= 0 && hz >= 0 && hx < NX && hz < NZ) {
-      hp = pad_pos(g, hx, hz);
-      hring = hp.ring > 0;
+  // L of the halo's pad cells (the only halo cells whose rho is read); halo
+  // cell tid + h * A_NT_I of thread tid
+  int hx[HPT], hz[HPT];
+  float Lh[HPT];
+  PadPos hp[HPT];
+  bool hring[HPT];
+#pragma unroll
+  for (int h = 0; h < HPT; h++) {
+    const int i = tid + h * A_NT_I;
+    hx[h] = hz[h] = -1;
+    Lh[h] = 0.0f;
+    hp[h] = PadPos{};
+    hring[h] = false;
+    if (i >= ADJ_NHALO) continue;
+    adj_halo_cell<TX, TZ>(i, x0, z0, hx[h], hz[h]);
+    const int cx = hx[h], cz = hz[h];
+    if (cx >= 0 && cz >= 0 && cx < NX && cz < NZ) {
+      hp[h] = pad_pos(g, cx, cz);
+      hring[h] = hp[h].ring > 0;
     }
-    if (hring) {
-      const float sz_ = lap8(WZ(hx, hz - 4), WZ(hx, hz - 3), WZ(hx, hz - 2), WZ(hx, hz - 1),
-                             WZ(hx, hz), WZ(hx, hz + 1), WZ(hx, hz + 2), WZ(hx, hz + 3),
-                             WZ(hx, hz + 4));
-      const float sx_ = lap8(WX(hx - 4, hz), WX(hx - 3, hz), WX(hx - 2, hz), WX(hx - 1, hz),
-                             WX(hx, hz), WX(hx + 1, hz), WX(hx + 2, hz), WX(hx + 3, hz),
-                             WX(hx + 4, hz));
-      float v = sz_ + sx_ + 2.0f * L1(hx, hz);
-      if (edge && near4(hx, hz)) v = v + sCOR[ridx(hx, hz)];
-      v = v - L2(hx, hz) + Ecur[(size_t)hx * g.LDZ + hz];
-      const int x = hx - g.pml;
-      if (a.rec_k >= 0 && x >= 0 && x < g.nx && hz == g.gz[x] + g.pml)
+    if (hring[h]) {
+      const float sz_ = lap8(WZ(cx, cz - 4), WZ(cx, cz - 3), WZ(cx, cz - 2), WZ(cx, cz - 1),
+                             WZ(cx, cz), WZ(cx, cz + 1), WZ(cx, cz + 2), WZ(cx, cz + 3),
+                             WZ(cx, cz + 4));
+      const float sx_ = lap8(WX(cx - 4, cz), WX(cx - 3, cz), WX(cx - 2, cz), WX(cx - 1, cz),
+                             WX(cx, cz), WX(cx + 1, cz), WX(cx + 2, cz), WX(cx + 3, cz),
+                             WX(cx + 4, cz));
+      float v = sz_ + sx_ + 2.0f * L1(cx, cz);
+      if (edge && near4(cx, cz)) v = v + sCOR[ridx(cx, cz)];
+      v = v - L2(cx, cz) + Ecur[(size_t)cx * g.LDZ + cz];
+      const int x = cx - g.pml;
+      if (a.rec_k >= 0 && x >= 0 && x < g.nx && cz == g.gz[x] + g.pml)
         v += g.rec[(size_t)a.rec_k * g.nx + x];
-      Lh = v;
+      Lh[h] = v;
     }
   }
-  __syncthreads();  // sL2, sWZ, sWX and sCOR are dead: the ring arrays go there
+  __syncthreads();  // sL1, sL2, sWZ, sWX and sCOR are dead: the ring arrays go there
   // rho = (1 - w) L of the ring cells, times their one-way coefficients
   auto put_ring = [&](int cx, int cz, const PadPos &pp, bool ring, float L) {
     const int i = ridx(cx, cz);
@@ -466,7 +497,9 @@ __global__ void __launch_bounds__(A_NT_I, 2) adj_pad_kernel(const ShotDev *__res
     const PadPos pp = pad_pos(g, cx, cz);
     put_ring(cx, cz, pp, in && pp.ring > 0, Lt[k]);
   }
-  if (tid < ADJ_NHALO) put_ring(hx, hz, hp, hring, Lh);
+#pragma unroll
+  for (int h = 0; h < HPT; h++)
+    if (tid + h * A_NT_I < ADJ_NHALO) put_ring(hx[h], hz[h], hp[h], hring[h], Lh[h]);
   __syncthreads();
 
   // M = w L + P_u3^T rho on the pad and model edge cells (L elsewhere), E of

@@ -8,26 +8,57 @@
 namespace seis {
 namespace fast {
 
-constexpr size_t ADJ_TILE_SMEM = sizeof(float) * (size_t)(4 * WIDE + NARROW) + 16;
-constexpr size_t ADJ_PAD_SMEM = sizeof(float) * (size_t)ADJ_PAD_FLOATS + 16;
-
-cudaError_t configure_adjoint() {
-  cudaError_t e = cudaFuncSetAttribute(adj_interior_kernel,
+namespace {
+template <int S>
+cudaError_t setup_adjoint() {
+  cudaError_t e = cudaFuncSetAttribute(adj_interior_kernel<S>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)ADJ_TILE_SMEM);
+                                       (int)AGeo<S>::TILE_SMEM);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(adj_pad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)ADJ_PAD_SMEM);
+    e = cudaFuncSetAttribute(adj_pad_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)AGeo<S>::PAD_SMEM);
   return e;
 }
 
-cudaError_t launch_adjoint(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
-                           const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad) {
+template <int S>
+cudaError_t launch_adj(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
+                       const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad) {
+  constexpr int NT = Geo<S>::NT;
   if (n_int > 0)
-    adj_interior_kernel<<<n_int, A_NT_I, ADJ_TILE_SMEM, s_int>>>(d_shots, d_tiles, a, d_err);
+    adj_interior_kernel<S><<<n_int, NT, AGeo<S>::TILE_SMEM, s_int>>>(d_shots, d_tiles, a, d_err);
   if (n_pad > 0)
-    adj_pad_kernel<<<n_pad, A_NT_I, ADJ_PAD_SMEM, s_pad>>>(d_shots, d_tiles + n_int, a, d_err);
+    adj_pad_kernel<S><<<n_pad, NT, AGeo<S>::PAD_SMEM, s_pad>>>(d_shots, d_tiles + n_int, a,
+                                                                d_err);
   return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t configure_adjoint() {
+  cudaError_t e = setup_adjoint<SHAPE_32x64>();
+  if (e == cudaSuccess) e = setup_adjoint<SHAPE_64x32>();
+  if (e == cudaSuccess) e = setup_adjoint<SHAPE_16x128>();
+  if (e == cudaSuccess) e = setup_adjoint<SHAPE_64x64>();
+  if (e == cudaSuccess) e = setup_adjoint<SHAPE_32x32>();
+  return e;
+}
+
+cudaError_t launch_adjoint(int shape, const ShotDev *d_shots, const Tile *d_tiles, int n_int,
+                           int n_pad, const StepArgs &a, int *d_err, cudaStream_t s_int,
+                           cudaStream_t s_pad) {
+  switch (shape) {
+    case SHAPE_32x64:
+      return launch_adj<SHAPE_32x64>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    case SHAPE_64x32:
+      return launch_adj<SHAPE_64x32>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    case SHAPE_16x128:
+      return launch_adj<SHAPE_16x128>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    case SHAPE_64x64:
+      return launch_adj<SHAPE_64x64>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    case SHAPE_32x32:
+      return launch_adj<SHAPE_32x32>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    default:
+      return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace fast

@@ -20,6 +20,9 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "../../include/seis_fd.h"
@@ -138,7 +141,9 @@ struct Plan {
   ShotDev *d_sd_h = nullptr;
   CUtensorMap *d_maps_h = nullptr;
   bool exact = true;
+  int shape = SHAPE_32x64;   // tile shape of every kernel of the plan (TileShapeId)
   std::vector<void *> allocs;
+  std::vector<size_t> alloc_bytes;
   ShotDev *d_sd = nullptr;
   Tile *d_tiles = nullptr;
   int2 *d_cols = nullptr;
@@ -156,6 +161,17 @@ struct Plan {
     if (graph) cudaGraphDestroy(graph);
     for (void *p : allocs) cudaFree(p);
   }
+  // free one allocation made by alloc() (null: nothing)
+  void release(void *q) {
+    for (size_t i = 0; q && i < allocs.size(); i++)
+      if (allocs[i] == q) {
+        cudaFree(q);
+        device_bytes -= (int64_t)alloc_bytes[i];
+        allocs.erase(allocs.begin() + i);
+        alloc_bytes.erase(alloc_bytes.begin() + i);
+        return;
+      }
+  }
   template <class T>
   int alloc(T **p, size_t n) {
     void *q = nullptr;
@@ -166,6 +182,7 @@ struct Plan {
                   "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
     }
     allocs.push_back(q);
+    alloc_bytes.push_back(std::max<size_t>(n, 1) * sizeof(T));
     device_bytes += (int64_t)(std::max<size_t>(n, 1) * sizeof(T));
     *p = static_cast<T *>(q);
     e = cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), ctx->stream);
@@ -214,6 +231,7 @@ void fill_scalars(ShotDev &g, const seis_shot_desc &s) {
 // interior tiles come first, then all pad tiles, each group interleaved
 // across shots, so that shots are spread evenly over the SMs.
 void build_tiles(Plan &p) {
+  const int TX = shape_tx(p.shape), TZ = shape_tz(p.shape);
   p.tiles.clear();
   p.cols.clear();
   std::vector<std::vector<Tile>> per(p.nshot);
@@ -244,6 +262,7 @@ void build_tiles(Plan &p) {
 // and every consumer of its cells is 8th order (cells 8 or more from the grid
 // edge), so that the adjoint there is the symmetric gather.
 void build_adj_tiles(Plan &p) {
+  const int TX = shape_tx(p.shape), TZ = shape_tz(p.shape);
   std::vector<Tile> in_t, pad_t;
   for (int s = 0; s < p.nshot; s++) {
     const ShotDev &g = p.sd[s];
@@ -291,16 +310,17 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// Tensor map of one field (cell (0,0) at `cell0`) with a box of the staged
+// Tensor map of one field (cell (0,0) at `cell0`) with a box of `rows` staged
 // rows by `width` columns.
-int encode_map(seis_fd_ctx *ctx, const ShotDev &g, const float *cell0, int width, CUtensorMap *m) {
+int encode_map(seis_fd_ctx *ctx, const ShotDev &g, const float *cell0, int rows, int width,
+               CUtensorMap *m) {
   auto fn = encode_fn();
   if (!fn) return fail(ctx, SEIS_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   FieldGeom fg = field_geom(g.NX, g.NZ);
   void *base = const_cast<float *>(cell0 - fg.origin);
   cuuint64_t dims[2] = {(cuuint64_t)fg.LDZ, (cuuint64_t)fg.ncols};
   cuuint64_t strides[1] = {(cuuint64_t)fg.LDZ * sizeof(float)};
-  cuuint32_t box[2] = {(cuuint32_t)(TZ + 2 * ZM), (cuuint32_t)width};
+  cuuint32_t box[2] = {(cuuint32_t)rows, (cuuint32_t)width};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -312,20 +332,21 @@ int encode_map(seis_fd_ctx *ctx, const ShotDev &g, const float *cell0, int width
 int encode_maps(Plan &p, std::vector<ShotDev> &sds, CUtensorMap **d_out) {
   std::vector<CUtensorMap> maps((size_t)p.nshot * NMAPS);
   std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
-  const int wide = TX + 2 * HXC, narrow = TX + 2;
+  const int wide = shape_tx(p.shape) + 2 * HXC, narrow = shape_tx(p.shape) + 2;
+  const int rows = shape_tz(p.shape) + 2 * ZM;
   for (int s = 0; s < p.nshot; s++) {
     const ShotDev &g = sds[s];
     CUtensorMap *m = maps.data() + (size_t)s * NMAPS;
     int rc = SEIS_OK;
     for (int k = 0; k < 3 && !rc; k++) {
-      rc = encode_map(p.ctx, g, g.fa[k], wide, &m[MAP_FA_WIDE + k]);
-      if (!rc) rc = encode_map(p.ctx, g, g.fa[k], narrow, &m[MAP_FA_NARROW + k]);
-      if (!rc && g.fb[k]) rc = encode_map(p.ctx, g, g.fb[k], wide, &m[MAP_FB_WIDE + k]);
-      if (!rc && g.fb[k]) rc = encode_map(p.ctx, g, g.fb[k], narrow, &m[MAP_FB_NARROW + k]);
+      rc = encode_map(p.ctx, g, g.fa[k], rows, wide, &m[MAP_FA_WIDE + k]);
+      if (!rc) rc = encode_map(p.ctx, g, g.fa[k], rows, narrow, &m[MAP_FA_NARROW + k]);
+      if (!rc && g.fb[k]) rc = encode_map(p.ctx, g, g.fb[k], rows, wide, &m[MAP_FB_WIDE + k]);
+      if (!rc && g.fb[k]) rc = encode_map(p.ctx, g, g.fb[k], rows, narrow, &m[MAP_FB_NARROW + k]);
     }
-    if (!rc) rc = encode_map(p.ctx, g, g.vel, narrow, &m[MAP_VEL]);
-    if (!rc) rc = encode_map(p.ctx, g, g.vel, wide, &m[MAP_VEL_WIDE]);
-    if (!rc && g.dv) rc = encode_map(p.ctx, g, g.dv, narrow, &m[MAP_DV]);
+    if (!rc) rc = encode_map(p.ctx, g, g.vel, rows, narrow, &m[MAP_VEL]);
+    if (!rc) rc = encode_map(p.ctx, g, g.vel, rows, wide, &m[MAP_VEL_WIDE]);
+    if (!rc && g.dv) rc = encode_map(p.ctx, g, g.dv, rows, narrow, &m[MAP_DV]);
     if (rc) return rc;
   }
   int rc = p.alloc(d_out, maps.size());
@@ -436,7 +457,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
       if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_e[1]);
       if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_b);
     }
-    g.ntz = (g.NZ + TZ - 1) / TZ;
+    g.ntz = (g.NZ + shape_tz(p->shape) - 1) / shape_tz(p->shape);
     if (rc == SEIS_OK) {
       g.vel = vel; g.dv = dv; g.wav = wav; g.rec = rec; g.gz = gzd;
       cudaError_t e = cudaMemcpyAsync(gzd, d.gz, sizeof(int) * d.nx, cudaMemcpyHostToDevice,
@@ -506,7 +527,7 @@ int step(Plan &p, int mode, const StepArgs &a, const ShotDev *shots = nullptr) {
   seis_fd_ctx *ctx = p.ctx;
   CK(cudaEventRecord(ctx->fork, ctx->stream));
   CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
-  CK(launch_step(mode, p.exact, shots ? shots : p.d_sd, p.d_tiles, p.n_int, p.n_pad, ctx->num_sms, a,
+  CK(launch_step(mode, p.exact, shots ? shots : p.d_sd, p.d_tiles, p.n_int, p.n_pad, p.shape, a,
                  ctx->d_err, ctx->stream, ctx->aux));
   CK(cudaEventRecord(ctx->join, ctx->aux));
   CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
@@ -585,7 +606,7 @@ int ensure_snapshots(Plan &p) {
   for (int s = 0; s < p.nshot; s++) {
     ShotDev &g = p.sd[s];
     int nsnap = snap_slots(p, g.NT);
-    int ntx = (g.NX + TX - 1) / TX;
+    int ntx = (g.NX + shape_tx(p.shape) - 1) / shape_tx(p.shape);
     unsigned char *snap = nullptr;
     int rc = p.alloc(&snap, (size_t)nsnap * g.nx * g.nz * esize);
     if (!rc) rc = p.alloc(&g.snap_scale, (size_t)nsnap * ntx * g.ntz);
@@ -609,8 +630,8 @@ int adj_step(Plan &p, const StepArgs &a) {
   seis_fd_ctx *ctx = p.ctx;
   CK(cudaEventRecord(ctx->fork, ctx->stream));
   CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
-  CK(fast::launch_adjoint(p.d_sd, p.d_adj_tiles, p.n_int_adj, p.n_pad_adj, a, ctx->d_err,
-                          ctx->stream, ctx->aux));
+  CK(fast::launch_adjoint(p.shape, p.d_sd, p.d_adj_tiles, p.n_int_adj, p.n_pad_adj, a,
+                          ctx->d_err, ctx->stream, ctx->aux));
   CK(cudaEventRecord(ctx->join, ctx->aux));
   CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
   ctx->launches += (p.n_int_adj > 0) + (p.n_pad_adj > 0);
@@ -1235,17 +1256,20 @@ int64_t seis_fd_plan_launches_per_run(const seis_fd_plan *plan) {
   return plan && plan->p ? plan->p->launches_per_run : 0;
 }
 
-int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double *bytes) {
-  if (!plan || !plan->p || !ms || !bytes || steps < 1) return SEIS_ERR_ARG;
-  Plan &p = *plan->p;
+namespace {
+// `steps` time steps of the plan's step kernels (forward plans: the operator's
+// step; adjoint plans: the reverse step without imaging), the interior kernel
+// on the main stream and the pad kernel on the auxiliary one, concurrently,
+// each bracketed by CUDA events on its own stream.  ms = mean interior, pad
+// and whole-step milliseconds; bytes = algorithmic bytes of the interior and
+// pad tiles (16 per field cell-update).  The fields are cleared afterwards.
+int time_steps(Plan &p, int steps, double *ms, double *bytes) {
   seis_fd_ctx *ctx = p.ctx;
-  int rc = begin(ctx);
-  if (rc) return rc;
+  const int TX = shape_tx(p.shape), TZ = shape_tz(p.shape);
   int mode = p.op == OP_BORN ? MODE_BORN : MODE_MODEL;
   int fields = p.op == OP_BORN ? 2 : 1;
   cudaEvent_t ev[5];
   for (auto &e : ev) CK(cudaEventCreate(&e));
-  // adjoint plans time the reverse-step kernels (no imaging term)
   const bool adj = p.op == OP_BORN_ADJ;
   const std::vector<Tile> &tl = adj ? p.adj_tiles : p.tiles;
   const int n_int = adj ? p.n_int_adj : p.n_int, n_pad = adj ? p.n_pad_adj : p.n_pad;
@@ -1266,20 +1290,19 @@ int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double 
     int it = k % p.NT;
     a.src_k = it >= 1 ? it - 1 : -1;
     a.rec_k = it - p.ndel >= 0 && p.op != OP_RTM && !adj ? it - p.ndel : -1;
-    // interior kernel on the main stream, pad kernel on the auxiliary one,
-    // concurrently, each bracketed by events on its own stream
     CK(cudaEventRecord(ev[0], ctx->stream));
     CK(cudaStreamWaitEvent(ctx->aux, ev[0], 0));
     CK(cudaEventRecord(ev[2], ctx->aux));
     if (adj) {
-      CK(fast::launch_adjoint(p.d_sd, d_tl, n_int, 0, a, ctx->d_err, ctx->stream, ctx->aux));
-      CK(fast::launch_adjoint(p.d_sd, d_tl + n_int, 0, n_pad, a, ctx->d_err, ctx->stream,
+      CK(fast::launch_adjoint(p.shape, p.d_sd, d_tl, n_int, 0, a, ctx->d_err, ctx->stream,
                               ctx->aux));
+      CK(fast::launch_adjoint(p.shape, p.d_sd, d_tl + n_int, 0, n_pad, a, ctx->d_err,
+                              ctx->stream, ctx->aux));
     } else {
-      CK(launch_step(mode, p.exact, p.d_sd, d_tl, n_int, 0, ctx->num_sms, a, ctx->d_err,
+      CK(launch_step(mode, p.exact, p.d_sd, d_tl, n_int, 0, p.shape, a, ctx->d_err, ctx->stream,
+                     ctx->aux));
+      CK(launch_step(mode, p.exact, p.d_sd, d_tl + n_int, 0, n_pad, p.shape, a, ctx->d_err,
                      ctx->stream, ctx->aux));
-      CK(launch_step(mode, p.exact, p.d_sd, d_tl + n_int, 0, n_pad, ctx->num_sms, a,
-                     ctx->d_err, ctx->stream, ctx->aux));
     }
     CK(cudaEventRecord(ev[1], ctx->stream));
     CK(cudaEventRecord(ev[3], ctx->aux));
@@ -1295,9 +1318,129 @@ int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double 
   }
   for (auto &e : ev) cudaEventDestroy(e);
   ms[0] = t_int / steps; ms[1] = t_pad / steps; ms[2] = t_step / steps;
-  bytes[0] = 16.0 * fields * (double)cells_int;
-  bytes[1] = 16.0 * fields * (double)cells_pad;
+  if (bytes) {
+    bytes[0] = 16.0 * fields * (double)cells_int;
+    bytes[1] = 16.0 * fields * (double)cells_pad;
+  }
   return clear_fields(p) ? SEIS_ERR_CUDA : sync(ctx);
+}
+
+// Switch a plan to tile shape s: tile lists, tensor-map boxes and
+// snapshot-scale tiling of every shot table, and a new graph at the next run.
+// The snapshot scales are tiled like the kernels, so the shape is fixed once
+// the snapshots exist.
+int apply_shape(Plan &p, int s) {
+  seis_fd_ctx *ctx = p.ctx;
+  if (s < 0 || s >= NSHAPES) return fail(ctx, SEIS_ERR_ARG, "tile shape %d", s);
+  if (s == p.shape) return SEIS_OK;
+  if (p.snaps_ready)
+    return fail(ctx, SEIS_ERR_STATE, "the tile shape is fixed once snapshots are allocated");
+  CK(cudaStreamSynchronize(ctx->stream));
+  p.shape = s;
+  const int TZ = shape_tz(s);
+  for (std::vector<ShotDev> *v : {&p.sd, &p.sd_c, &p.sd_h})
+    for (ShotDev &g : *v) g.ntz = (g.NZ + TZ - 1) / TZ;
+  build_tiles(p);
+  build_adj_tiles(p);
+  p.release(p.d_tiles);
+  p.release(p.d_adj_tiles);
+  p.d_tiles = p.d_adj_tiles = nullptr;
+  int rc = p.alloc(&p.d_tiles, p.tiles.size());
+  if (!rc) rc = p.alloc(&p.d_adj_tiles, p.adj_tiles.size());
+  struct Table { std::vector<ShotDev> *sd; ShotDev **d; CUtensorMap **maps; };
+  for (Table t : {Table{&p.sd, &p.d_sd, &p.d_maps}, Table{&p.sd_c, &p.d_sd_c, &p.d_maps_c},
+                  Table{&p.sd_h, &p.d_sd_h, &p.d_maps_h}}) {
+    if (rc || t.sd->empty() || !*t.d) continue;
+    p.release(*t.maps);
+    *t.maps = nullptr;
+    rc = encode_maps(p, *t.sd, t.maps);
+    if (!rc) {
+      cudaError_t e = cudaMemcpyAsync(*t.d, t.sd->data(), sizeof(ShotDev) * p.nshot,
+                                      cudaMemcpyHostToDevice, ctx->stream);
+      if (e != cudaSuccess) rc = fail(ctx, SEIS_ERR_CUDA, "shot table: %s", cudaGetErrorString(e));
+    }
+  }
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(p.d_tiles, p.tiles.data(), sizeof(Tile) * p.tiles.size(),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(p.d_adj_tiles, p.adj_tiles.data(), sizeof(Tile) * p.adj_tiles.size(),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  if (p.exec) cudaGraphExecDestroy(p.exec);
+  if (p.graph) cudaGraphDestroy(p.graph);
+  p.exec = nullptr;
+  p.graph = nullptr;
+  return sync(ctx);
+}
+
+// Tile shape chosen for a plan signature (operator, build flavour and every
+// shot's padded grid), shared by the plans of the process.
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune_cache;
+
+std::string tune_key(const Plan &p) {
+  std::string k = std::to_string(p.op) + (p.exact ? "e" : "f");
+  for (const ShotDev &g : p.sd) k += ":" + std::to_string(g.NX) + "x" + std::to_string(g.NZ);
+  return k;
+}
+
+// Time `steps` steps of the plan in every tile shape and keep the fastest
+// (the cached choice for this plan's signature unless `force`).  ms: the
+// mean step time of every shape (0 where not timed), may be null.
+int autotune(Plan &p, int steps, bool force, double *ms, int *best) {
+  const std::string key = tune_key(p);
+  if (ms)
+    for (int s = 0; s < NSHAPES; s++) ms[s] = 0.0;
+  if (!force) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      if (best) *best = it->second;
+      return apply_shape(p, it->second);
+    }
+  }
+  int pick = p.shape;
+  double t_best = 0.0;
+  for (int s = 0; s < NSHAPES; s++) {
+    int rc = apply_shape(p, s);
+    double t[3];
+    if (!rc) rc = time_steps(p, 3, t, nullptr);  // warm-up
+    if (!rc) rc = time_steps(p, steps, t, nullptr);
+    if (rc) return rc;
+    if (ms) ms[s] = t[2];
+    if (s == 0 || t[2] < t_best) {
+      t_best = t[2];
+      pick = s;
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = pick;
+  }
+  if (best) *best = pick;
+  return apply_shape(p, pick);
+}
+}  // namespace
+
+int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double *bytes) {
+  if (!plan || !plan->p || !ms || !bytes || steps < 1) return SEIS_ERR_ARG;
+  int rc = begin(plan->p->ctx);
+  return rc ? rc : time_steps(*plan->p, steps, ms, bytes);
+}
+
+int seis_fd_plan_set_tile_shape(seis_fd_plan *plan, int shape) {
+  if (!plan || !plan->p) return SEIS_ERR_ARG;
+  int rc = begin(plan->p->ctx);
+  return rc ? rc : apply_shape(*plan->p, shape);
+}
+
+int seis_fd_plan_tile_shape(const seis_fd_plan *plan) {
+  return plan && plan->p ? plan->p->shape : SEIS_ERR_ARG;
+}
+
+int seis_fd_plan_autotune(seis_fd_plan *plan, int steps, int force, double *h_ms, int *h_best) {
+  if (!plan || !plan->p || steps < 1) return SEIS_ERR_ARG;
+  int rc = begin(plan->p->ctx);
+  return rc ? rc : autotune(*plan->p, steps, force != 0, h_ms, h_best);
 }
 
 int seis_fd_plan_set_snapshots(seis_fd_plan *plan, int every, int dtype) {
@@ -1587,6 +1730,13 @@ struct seis_fd_lsrtm {
 
 namespace {
 
+// The tile shape of a solver plan whose velocity and wavelet are loaded: the
+// fixed shape of the options, or the autotuner's (10 timed steps per shape).
+int lsrtm_shape(seis_fd_lsrtm &L, Plan &p) {
+  if (L.opts.tile_shape > 0) return apply_shape(p, L.opts.tile_shape - 1);
+  return autotune(p, 10, false, nullptr, nullptr);
+}
+
 // s = L^T r: adjoint plan over the residuals, per-shot images scattered into
 // the global grid.
 // The plan of shots k0 .. k1-1 of a grouped solver: velocity sub-grids and
@@ -1618,6 +1768,7 @@ int lsrtm_group_plan(seis_fd_lsrtm &L, int op, int k0, int k1, Plan **out) {
     ctx->launches += 2;
     if (op == OP_BORN_ADJ) g.rec = L.r + L.doff[k];
   }
+  if (!rc) rc = lsrtm_shape(L, *p);
   if (!rc && op == OP_BORN_ADJ) {
     cudaError_t e = cudaMemcpyAsync(p->d_sd, p->sd.data(), sizeof(ShotDev) * p->nshot,
                                     cudaMemcpyHostToDevice, ctx->stream);
@@ -1751,7 +1902,7 @@ int seis_fd_lsrtm_create_mapped(seis_fd_ctx *ctx, int nx, int nz, int nshot,
     }
     off += shots[k].nx;
   }
-  seis_lsrtm_opts o{1, SEIS_SNAP_BF16, 0, 0, 0};
+  seis_lsrtm_opts o{1, SEIS_SNAP_BF16, 0, 0, 0, 0};
   if (opts) o = *opts;
   seis_fd_lsrtm *L = new (std::nothrow) seis_fd_lsrtm();
   if (!L) return fail(ctx, SEIS_ERR_NOMEM, "host allocation failed");
@@ -1785,6 +1936,8 @@ int seis_fd_lsrtm_create_mapped(seis_fd_ctx *ctx, int nx, int nz, int nshot,
   Plan *pb = nullptr, *pa = nullptr;
   L->opts = o;
   L->group = (o.group_shots > 0 && o.group_shots < nshot) ? o.group_shots : 0;
+  if (o.tile_shape < 0 || o.tile_shape > NSHAPES)
+    rc = fail(ctx, SEIS_ERR_ARG, "lsrtm: tile shape %d", o.tile_shape);
   if (o.snap_every < 1 || (o.checkpoint_every > 0 && o.checkpoint_every % o.snap_every != 0))
     rc = fail(ctx, SEIS_ERR_ARG, "lsrtm: snapshot interval %d, checkpoint interval %d",
               o.snap_every, o.checkpoint_every);
@@ -1902,6 +2055,8 @@ int seis_fd_lsrtm_set_background(seis_fd_lsrtm *L, const float *h_v0, const floa
     if (!rc) rc = plan_input(&L->adj, k, SEIS_IN_WAVELET, h_wav, false);
     if (!rc) rc = sync(L->ctx);  // the host sub-grid is reused by the next shot
   }
+  if (!rc && !L->adj.p->snaps_ready) rc = lsrtm_shape(*L, *L->born.p);
+  if (!rc && !L->adj.p->snaps_ready) rc = lsrtm_shape(*L, *L->adj.p);
   L->ready = false;
   return rc ? rc : sync(L->ctx);
 }

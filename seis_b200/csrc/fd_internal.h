@@ -7,13 +7,27 @@
 
 namespace seis {
 
-// Tiling.  The padded grid of every shot is cut into TX x TZ tiles (TZ rows
-// along the contiguous z axis).  Field arrays carry zero margins (ZM rows above
-// and below, XM columns on either side) so that every staged column segment
-// [z0 - ZM, z0 + TZ + ZM) of every tile, with an HXC-column halo, lies inside
-// the allocation.
-constexpr int TX = 32;
-constexpr int TZ = 64;
+// Tiling.  The padded grid of every shot is cut into tiles of TX columns x TZ
+// rows (z contiguous), one tile per CTA, each thread a 4-row x 2-column
+// micro-tile (TX * TZ / 8 threads).  A plan uses one of the shapes below,
+// fixed when it is built or picked by timing its own steps
+// (seis_fd_plan_autotune).  Field arrays carry zero margins (ZM rows above and
+// below, XM columns on either side) and are rounded up to the largest tile in
+// each direction, so that every staged column segment [z0 - ZM, z0 + TZ + ZM)
+// of every tile of every shape, with an HXC-column halo, lies inside the
+// allocation.
+enum TileShapeId : int {
+  SHAPE_32x64 = 0,   // 256 threads
+  SHAPE_64x32 = 1,   // 256 threads
+  SHAPE_16x128 = 2,  // 256 threads
+  SHAPE_64x64 = 3,   // 512 threads
+  SHAPE_32x32 = 4,   // 128 threads
+  NSHAPES = 5,
+};
+constexpr int shape_tx(int s) { return s == 1 || s == 3 ? 64 : s == 2 ? 16 : 32; }
+constexpr int shape_tz(int s) { return s == 2 ? 128 : s == 0 || s == 3 ? 64 : 32; }
+constexpr int TX_MAX = 64;
+constexpr int TZ_MAX = 128;
 constexpr int HXC = 5;      // column halo of the current field (stencil radius 4 + 1)
 constexpr int ZM = 8;
 constexpr int XM = 16;
@@ -117,9 +131,9 @@ struct FieldGeom {
 };
 inline FieldGeom field_geom(int NX, int NZ) {
   FieldGeom f;
-  int nstrip = (NZ + TZ - 1) / TZ;
-  f.LDZ = ((ZM + nstrip * TZ + ZM) + 31) / 32 * 32;
-  int right = ((NX + TX - 1) / TX) * TX - NX + XM;
+  int nstrip = (NZ + TZ_MAX - 1) / TZ_MAX;
+  f.LDZ = ((ZM + nstrip * TZ_MAX + ZM) + 31) / 32 * 32;
+  int right = ((NX + TX_MAX - 1) / TX_MAX) * TX_MAX - NX + XM;
   f.ncols = XM + NX + right;
   f.elems = (size_t)f.ncols * f.LDZ;
   f.origin = (size_t)XM * f.LDZ + ZM;
@@ -135,26 +149,28 @@ enum StepMode : int {
 
 // One time step over every tile of a batch: the first n_int tiles are
 // interior tiles (one CTA each, stream s_int), the next n_pad pad tiles
-// (one CTA each, stream s_pad; the absorbing boundary fused in).  `exact` selects the build that rounds like
-// the reference; otherwise the contracted build.
+// (one CTA each, stream s_pad; the absorbing boundary fused in), tiles of
+// shape `shape` (TileShapeId).  `exact` selects the build that rounds like the
+// reference; otherwise the contracted build.
 cudaError_t launch_step(int mode, bool exact, const ShotDev *d_shots, const Tile *d_tiles,
-                        int n_int, int n_pad, int num_sms, const StepArgs &a, int *d_err,
+                        int n_int, int n_pad, int shape, const StepArgs &a, int *d_err,
                         cudaStream_t s_int, cudaStream_t s_pad);
 namespace exact {
 cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, int n_int,
-                        int n_pad, int num_sms, const StepArgs &a, int *d_err, cudaStream_t s_int,
+                        int n_pad, int shape, const StepArgs &a, int *d_err, cudaStream_t s_int,
                         cudaStream_t s_pad);
 cudaError_t configure();
 }  // namespace exact
 namespace fast {
 cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, int n_int,
-                        int n_pad, int num_sms, const StepArgs &a, int *d_err, cudaStream_t s_int,
+                        int n_pad, int shape, const StepArgs &a, int *d_err, cudaStream_t s_int,
                         cudaStream_t s_pad);
 cudaError_t configure();
 // one reverse step of the exact Born adjoint over the adjoint tile list
 // (interior tiles on s_int, pad tiles on s_pad)
-cudaError_t launch_adjoint(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
-                           const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad);
+cudaError_t launch_adjoint(int shape, const ShotDev *d_shots, const Tile *d_tiles, int n_int,
+                           int n_pad, const StepArgs &a, int *d_err, cudaStream_t s_int,
+                           cudaStream_t s_pad);
 cudaError_t configure_adjoint();
 }  // namespace fast
 cudaError_t launch_finalize_image(const ShotDev *d_shots, int nshots, cudaStream_t s);

@@ -256,11 +256,11 @@ cudaError_t configure_kernels() {
 }
 
 cudaError_t launch_step(int mode, bool use_exact, const ShotDev *d_shots, const Tile *d_tiles,
-                        int n_int, int n_pad, int num_sms, const StepArgs &a, int *d_err,
+                        int n_int, int n_pad, int shape, const StepArgs &a, int *d_err,
                         cudaStream_t s_int, cudaStream_t s_pad) {
-  return use_exact ? exact::launch_step(mode, d_shots, d_tiles, n_int, n_pad, num_sms, a, d_err,
+  return use_exact ? exact::launch_step(mode, d_shots, d_tiles, n_int, n_pad, shape, a, d_err,
                                         s_int, s_pad)
-                   : fast::launch_step(mode, d_shots, d_tiles, n_int, n_pad, num_sms, a, d_err,
+                   : fast::launch_step(mode, d_shots, d_tiles, n_int, n_pad, shape, a, d_err,
                                        s_int, s_pad);
 }
 

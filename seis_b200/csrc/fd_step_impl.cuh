@@ -7,48 +7,78 @@ namespace seis {
 namespace SEIS_NS {
 
 namespace {
-template <int MODE>
+template <int S, int MODE>
 cudaError_t setup() {
-  cudaError_t e = cudaFuncSetAttribute(tile_kernel<MODE, TILE_INTERIOR>,
+  cudaError_t e = cudaFuncSetAttribute(tile_kernel<S, MODE>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)TCfg<MODE, TILE_INTERIOR>::bytes);
+                                       (int)TCfg<S, MODE>::bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(pad_tile_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)PCfg<MODE>::bytes);
+    e = cudaFuncSetAttribute(pad_tile_kernel<S, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)PCfg<S, MODE>::bytes);
+  return e;
+}
+
+template <int S>
+cudaError_t setup_shape() {
+  cudaError_t e = setup<S, MODE_MODEL>();
+  if (e == cudaSuccess) e = setup<S, MODE_RCV>();
+  if (e == cudaSuccess) e = setup<S, MODE_BORN>();
   return e;
 }
 
 // Interior tiles on s_int, pad tiles on s_pad (concurrently).
-template <int MODE>
+template <int S, int MODE>
 cudaError_t launch_t(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
                      const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad) {
+  constexpr int NT = Geo<S>::NT;
   if (n_int > 0)
-    tile_kernel<MODE, TILE_INTERIOR><<<n_int, NT_T, TCfg<MODE, TILE_INTERIOR>::bytes, s_int>>>(
-        d_shots, d_tiles, a, d_err);
+    tile_kernel<S, MODE><<<n_int, NT, TCfg<S, MODE>::bytes, s_int>>>(d_shots, d_tiles, a, d_err);
   if (n_pad > 0)
-    pad_tile_kernel<MODE><<<n_pad, NT_T, PCfg<MODE>::bytes, s_pad>>>(d_shots, d_tiles + n_int, a,
-                                                                     d_err);
+    pad_tile_kernel<S, MODE><<<n_pad, NT, PCfg<S, MODE>::bytes, s_pad>>>(d_shots, d_tiles + n_int,
+                                                                       a, d_err);
   return cudaGetLastError();
+}
+
+template <int S>
+cudaError_t launch_mode(int mode, const ShotDev *d_shots, const Tile *d_tiles, int n_int,
+                        int n_pad, const StepArgs &a, int *d_err, cudaStream_t s_int,
+                        cudaStream_t s_pad) {
+  switch (mode) {
+    case MODE_MODEL:
+      return launch_t<S, MODE_MODEL>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    case MODE_RCV:
+      return launch_t<S, MODE_RCV>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    case MODE_BORN:
+      return launch_t<S, MODE_BORN>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    default:
+      return cudaErrorInvalidValue;
+  }
 }
 }  // namespace
 
 cudaError_t configure() {
-  cudaError_t e = setup<MODE_MODEL>();
-  if (e == cudaSuccess) e = setup<MODE_RCV>();
-  if (e == cudaSuccess) e = setup<MODE_BORN>();
+  cudaError_t e = setup_shape<SHAPE_32x64>();
+  if (e == cudaSuccess) e = setup_shape<SHAPE_64x32>();
+  if (e == cudaSuccess) e = setup_shape<SHAPE_16x128>();
+  if (e == cudaSuccess) e = setup_shape<SHAPE_64x64>();
+  if (e == cudaSuccess) e = setup_shape<SHAPE_32x32>();
   return e;
 }
 
 cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, int n_int,
-                        int n_pad, int num_sms, const StepArgs &a, int *d_err, cudaStream_t s_int,
+                        int n_pad, int shape, const StepArgs &a, int *d_err, cudaStream_t s_int,
                         cudaStream_t s_pad) {
-  switch (mode) {
-    case MODE_MODEL:
-      return launch_t<MODE_MODEL>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
-    case MODE_RCV:
-      return launch_t<MODE_RCV>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
-    case MODE_BORN:
-      return launch_t<MODE_BORN>(d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+  switch (shape) {
+    case SHAPE_32x64:
+      return launch_mode<SHAPE_32x64>(mode, d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    case SHAPE_64x32:
+      return launch_mode<SHAPE_64x32>(mode, d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    case SHAPE_16x128:
+      return launch_mode<SHAPE_16x128>(mode, d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    case SHAPE_64x64:
+      return launch_mode<SHAPE_64x64>(mode, d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
+    case SHAPE_32x32:
+      return launch_mode<SHAPE_32x32>(mode, d_shots, d_tiles, n_int, n_pad, a, d_err, s_int, s_pad);
     default:
       return cudaErrorInvalidValue;
   }

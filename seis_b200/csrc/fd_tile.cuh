@@ -23,21 +23,47 @@
 namespace seis {
 namespace SEIS_NS {
 
-constexpr int NT_T = 256;          // threads per CTA
-constexpr int QZ = TZ / 4;         // row quads per column (16)
-constexpr int SR = TZ + 2 * ZM;    // staged rows per column (80)
-constexpr int CW_C = TX + 2 * HXC; // staged columns of the current fields (42)
-constexpr int CW_P = TX + 2;       // staged columns of the other arrays (34)
+// Geometry of tile shape S (TileShapeId).
+template <int S>
+struct Geo {
+  static constexpr int TX = shape_tx(S), TZ = shape_tz(S);
+  static constexpr int NT = TX * TZ / 8;       // threads per CTA
+  static constexpr int QZ = TZ / 4;            // row quads per column
+  static constexpr int SR = TZ + 2 * ZM;       // staged rows per column
+  static constexpr int CW_C = TX + 2 * HXC;    // staged columns of the current fields
+  static constexpr int CW_P = TX + 2;          // staged columns of the other arrays
+  static constexpr int U3C = TX + 2;           // pad tiles: two-way values of tile + halo
+  static constexpr int U3R = TZ + 8;
+  static constexpr int U3N = U3C * U3R;
+  static constexpr int NHALO = 2 * (TX + 2) + 2 * TZ;  // halo ring cells of a tile
+  static_assert(NT % 32 == 0 && NT <= 1024, "whole warps");
+  static_assert(NT * sizeof(int) >= sizeof(ShotDev), "one thread per word of the shot table");
+};
+// Local names for the geometry of shape S inside a kernel or device function.
+#define SEIS_GEO(S)                                                                   \
+  using G_ = Geo<S>;                                                                  \
+  constexpr int TX = G_::TX, TZ = G_::TZ, NT_T = G_::NT, QZ = G_::QZ, SR = G_::SR;    \
+  constexpr int CW_C = G_::CW_C, CW_P = G_::CW_P;                                     \
+  (void)TX; (void)TZ; (void)NT_T; (void)QZ; (void)SR; (void)CW_C; (void)CW_P
+
+// CTAs per SM that a kernel's shared memory allows (227 KB per SM, 1 KB
+// reserved per CTA), at most `cap`.
+constexpr int ctas_fit(size_t bytes, int cap) {
+  return (int)((227 * 1024) / (bytes + 1024)) < cap ? (int)((227 * 1024) / (bytes + 1024)) : cap;
+}
 
 // Staged arrays of one tile (one buffer, one tile per CTA: several CTAs per SM
 // hide the copy latency).
-template <int MODE, int KIND>
+template <int S, int MODE>
 struct TCfg {
+  using G = Geo<S>;
   static constexpr bool BORN = MODE == MODE_BORN;
   static constexpr int NCUR = BORN ? 2 : 1;   // arrays staged with the wide halo
   static constexpr int NOTH = BORN ? 4 : 2;   // prev, vel [, prev B, dv]
-  static constexpr int BUF = (NCUR * CW_C + NOTH * CW_P) * SR;  // floats per buffer
+  static constexpr int BUF = (NCUR * G::CW_C + NOTH * G::CW_P) * G::SR;  // floats per buffer
   static constexpr size_t bytes = sizeof(float) * (size_t)BUF + 16;
+  // at most 768 threads per SM (85 registers a thread)
+  static constexpr int MIN_CTAS = ctas_fit(bytes, 768 / G::NT) > 0 ? ctas_fit(bytes, 768 / G::NT) : 1;
 };
 
 // ---- PTX helpers: mbarrier + bulk asynchronous copy global -> shared
@@ -100,8 +126,10 @@ __device__ __forceinline__ void set_comp(float4 &v, int r, float x) {
   if (r == 0) v.x = x; else if (r == 1) v.y = x; else if (r == 2) v.z = x; else v.w = x;
 }
 
-// Accessor of one staged array by padded-grid coordinates.
-struct SA {
+// Accessor of one staged array by padded-grid coordinates (SR staged rows
+// per column).
+template <int SR>
+struct SAT {
   const float *s;  // staged column (x0 - halo) row (z0 - ZM)
   int x0h, z0m;    // x0 - halo, z0 - ZM
   __device__ __forceinline__ float operator()(int ix, int iz) const {
@@ -162,6 +190,7 @@ __device__ __forceinline__ void save_strips(const ShotDev &g, int strip_k, int i
 
 // 8th-order two-way update of two columns x 4 rows from shared memory
 // (fd.cpp:1259-1270): u3 = vvzz uzz + vvxx uxx + 2 cur - prev.
+template <class SA>
 __device__ __forceinline__ void pair_twoway(const SA &C, const SA &P, const SA &V, const ShotDev &g,
                                             int ix, int iz0, float4 out[2], float4 cen[2],
                                             float4 prv[2], float4 vel[2]) {
@@ -190,6 +219,7 @@ __device__ __forceinline__ void pair_twoway(const SA &C, const SA &P, const SA &
 }
 
 // Same for one column x 4 rows.
+template <class SA>
 __device__ __forceinline__ float4 col_twoway(const SA &C, const SA &P, const SA &V, const ShotDev &g,
                                              int ix, int iz0, float4 &cen, float4 &prv,
                                              float4 &vel) {
@@ -221,7 +251,7 @@ __device__ __forceinline__ float4 col_twoway(const SA &C, const SA &P, const SA 
 // snapshots carry one power-of-two scale per (snapshot, tile), taken from the
 // tile's largest magnitude so that the scaled values lie in [0.5, 1).  Every
 // thread of the CTA calls this (it holds block barriers).
-template <int NTH, int NV>
+template <int NTH, int NV, int TX, int TZ>
 __device__ void snap_write(const ShotDev &g, int k, int x0, int z0, const float (&v)[NV],
                            const int (&xs)[NV], const int (&zs)[NV], unsigned mask, float *red) {
   float scale = 1.0f;
@@ -277,13 +307,11 @@ struct GA {
 };
 
 // Two-way values of a pad tile and its one-cell halo in shared memory:
-// columns x0-1 .. x0+TX, rows z0-4 .. z0+TZ+3 (the tile's row quads stay
-// 16-byte aligned; only rows z0-1 .. z0+TZ are used).
-constexpr int U3C = TX + 2;
-constexpr int U3R = TZ + 8;
-constexpr int U3N = U3C * U3R;
-constexpr int NHALO = 2 * (TX + 2) + 2 * TZ;  // halo ring cells of a tile
-struct UA {
+// columns x0-1 .. x0+TX, rows z0-4 .. z0+TZ+3 (U3R = TZ + 8 rows per column;
+// the tile's row quads stay 16-byte aligned; only rows z0-1 .. z0+TZ are
+// used).
+template <int U3R>
+struct UAT {
   float *s;
   int x0, z0;
   __device__ __forceinline__ float &ref(int ix, int iz) const {
@@ -293,6 +321,7 @@ struct UA {
 };
 // Halo cell i of the tile at (x0, z0): the rows above and below the tile
 // (TX + 2 cells each, corners included), then the columns left and right.
+template <int TX, int TZ>
 __device__ __forceinline__ void halo_cell(int i, int x0, int z0, int &hx, int &hz) {
   if (i < 2 * (TX + 2)) {
     hx = x0 - 1 + i % (TX + 2);
@@ -304,12 +333,15 @@ __device__ __forceinline__ void halo_cell(int i, int x0, int z0, int &hx, int &h
   }
 }
 
-template <int MODE>
+template <int S, int MODE>
 struct PCfg {
+  using G = Geo<S>;
   static constexpr int NF = MODE == MODE_BORN ? 2 : 1;  // fields with two-way arrays
-  static constexpr int BUF = TCfg<MODE, TILE_PAD>::BUF;
-  static constexpr size_t bytes = sizeof(float) * ((size_t)BUF + (size_t)NF * U3N) + 16;
-  static constexpr int MIN_CTAS = MODE == MODE_BORN ? 2 : 3;
+  static constexpr int BUF = TCfg<S, MODE>::BUF;
+  static constexpr size_t bytes = sizeof(float) * ((size_t)BUF + (size_t)NF * G::U3N) + 16;
+  // Born: at most 512 threads per SM (128 registers a thread), else 768
+  static constexpr int CAP = (MODE == MODE_BORN ? 512 : 768) / G::NT;
+  static constexpr int MIN_CTAS = ctas_fit(bytes, CAP) > 0 ? ctas_fit(bytes, CAP) : 1;
 };
 
 // Stage the arrays of one tile with 2-D tensor copies: rows [z0 - ZM, z0 +
@@ -317,10 +349,11 @@ struct PCfg {
 // allocation start (row + ZM, column + XM), so coordinates are never negative
 // and the row coordinate is a multiple of TZ (16-byte aligned).  Thread 0
 // issues the copies; every thread then waits on the mbarrier.
-template <int MODE, int KIND>
+template <int S, int MODE>
 __device__ __forceinline__ bool stage_tile(const ShotDev &g, const StepArgs &a, int x0, int z0,
                                            float *bb, uint64_t *bar) {
-  using C = TCfg<MODE, KIND>;
+  SEIS_GEO(S);
+  using C = TCfg<S, MODE>;
   if (threadIdx.x == 0) {
     fence_proxy_async();
     mbar_expect_tx(bar, (uint32_t)(C::BUF * sizeof(float)));
@@ -346,12 +379,13 @@ __device__ __forceinline__ bool stage_tile(const ShotDev &g, const StepArgs &a, 
 
 // Interior tiles: every cell a model cell in the 8th-order region, where the
 // absorbing blend is the identity (w = 1, u31 = 0; src/util/fd.cpp:55-56).
-template <int MODE, int KIND>
-__global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict__ shots,
-                                                       const Tile *__restrict__ tiles, StepArgs a,
-                                                       int *__restrict__ err) {
-  static_assert(KIND == TILE_INTERIOR, "pad tiles run pad_tile_kernel");
-  using C = TCfg<MODE, KIND>;
+template <int S, int MODE>
+__global__ void __launch_bounds__(Geo<S>::NT, TCfg<S, MODE>::MIN_CTAS) tile_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
+    int *__restrict__ err) {
+  SEIS_GEO(S);
+  using SA = SAT<SR>;
+  using C = TCfg<S, MODE>;
   constexpr bool BORN = C::BORN;
   extern __shared__ __align__(128) unsigned char smraw[];
   float *bb = reinterpret_cast<float *>(smraw);
@@ -368,7 +402,7 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
   }
   __syncthreads();
   const ShotDev &g = sg;
-  if (!stage_tile<MODE, KIND>(g, a, t.x0, t.z0, bb, bar)) {
+  if (!stage_tile<S, MODE>(g, a, t.x0, t.z0, bb, bar)) {
     if (tid == 0) atomicExch(err, 1);
     return;
   }
@@ -449,7 +483,7 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
       *reinterpret_cast<float4 *>(nb_ + (size_t)cxj * g.LDZ + iz0) = ob[j];
     }
   }
-  if (snap) snap_write<NT_T, 8>(g, aa.snap_k, x0, z0, lv, lx, lz, mask, red);
+  if (snap) snap_write<NT_T, 8, TX, TZ>(g, aa.snap_k, x0, z0, lv, lx, lz, mask, red);
 }
 
 // Pad tiles: tiles with a pad cell, a cell within 3 of the grid edge (frame,
@@ -469,16 +503,20 @@ __global__ void __launch_bounds__(NT_T, 3) tile_kernel(const ShotDev *__restrict
 //     blend (processBoundary fd.cpp:1092-1179, :55-56), stored.
 // A halo cell's two-way value is formed by the same per-cell arithmetic as
 // in the tile that owns it.
-template <int MODE>
-__global__ void __launch_bounds__(NT_T, PCfg<MODE>::MIN_CTAS) pad_tile_kernel(
+template <int S, int MODE>
+__global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_tile_kernel(
     const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
     int *__restrict__ err) {
-  using C = TCfg<MODE, TILE_PAD>;
+  SEIS_GEO(S);
+  using SA = SAT<SR>;
+  using UA = UAT<G_::U3R>;
+  constexpr int U3N = G_::U3N, NHALO = G_::NHALO;
+  using C = TCfg<S, MODE>;
   constexpr bool BORN = C::BORN;
   extern __shared__ __align__(128) unsigned char smraw[];
   float *bb = reinterpret_cast<float *>(smraw);
   float *u3m = bb + C::BUF;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(u3m + PCfg<MODE>::NF * U3N);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(u3m + PCfg<S, MODE>::NF * U3N);
   __shared__ ShotDev sg;
   __shared__ float red[33];
   const int tid = threadIdx.x;
@@ -492,7 +530,7 @@ __global__ void __launch_bounds__(NT_T, PCfg<MODE>::MIN_CTAS) pad_tile_kernel(
   __syncthreads();
   const ShotDev &g = sg;
   const int x0 = t.x0, z0 = t.z0, NX = g.NX, NZ = g.NZ;
-  if (!stage_tile<MODE, TILE_PAD>(g, a, x0, z0, bb, bar)) {
+  if (!stage_tile<S, MODE>(g, a, x0, z0, bb, bar)) {
     if (tid == 0) atomicExch(err, 1);
     return;
   }
@@ -655,7 +693,7 @@ __global__ void __launch_bounds__(NT_T, PCfg<MODE>::MIN_CTAS) pad_tile_kernel(
   // source (zero outside the grid, where nothing reads them)
   for (int i = tid; i < NHALO; i += NT_T) {
     int hx, hz;
-    halo_cell(i, x0, z0, hx, hz);
+    halo_cell<TX, TZ>(i, x0, z0, hx, hz);
     if (hx < 0 || hz < 0 || hx >= NX || hz >= NZ) {
       UA_.ref(hx, hz) = 0.0f;
       if (BORN) UB_.ref(hx, hz) = 0.0f;
@@ -681,7 +719,7 @@ __global__ void __launch_bounds__(NT_T, PCfg<MODE>::MIN_CTAS) pad_tile_kernel(
   }
   // snapshot of the model cells' source terms (holds block barriers), then
   // every two-way value of the tile and halo is in shared memory
-  if (snap) snap_write<NT_T, 8>(g, aa.snap_k, x0, z0, lv, lx, lz, mask, red);
+  if (snap) snap_write<NT_T, 8, TX, TZ>(g, aa.snap_k, x0, z0, lv, lx, lz, mask, red);
   __syncthreads();
 
   // 4. pad cells: one-way update and blend

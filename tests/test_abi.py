@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert seis_b200.lib().seis_fd_abi_version() == 1
+    assert seis_b200.lib().seis_fd_abi_version() == 2
 
 
 def test_ricker_matches_reference_wavelet():
