@@ -70,7 +70,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OBJ_DIR, exist_ok=True)
     srcs, headers = _sources()
     nvcc = _nvcc()
-    objs = []
+    objs, cmds = [], []
     for src in srcs:
         obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
         objs.append(obj)
@@ -82,9 +82,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
             cmd = [nvcc, *ARCH, *NVCC_COMMON, *flav, "-I", CSRC, "-I", INCLUDE, "-c", "-o", obj, src]
         else:
             cmd = ["g++", *CXX_FLAGS, "-I", CSRC, "-I", INCLUDE, "-I", _cuda_include(), "-c", "-o", obj, src]
-        out = _run(cmd)
-        if verbose and out.strip():
-            sys.stderr.write(out)
+        cmds.append(cmd)
+    # translation units compile independently (the step kernels of every tile
+    # shape make the CUDA ones the slow part)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for out in ex.map(_run, cmds):
+            if verbose and out.strip():
+                sys.stderr.write(out)
     if force or _stale(LIB, objs):
         _run([nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"])
     return LIB

@@ -141,3 +141,42 @@ def test_lsrtm_in_shot_groups_is_bit_identical(ctx, group, ck):
     assert rr0 == rr1
     assert np.array_equal(h0, h1)
     assert np.array_equal(m0, m1)
+
+
+@pytest.mark.parametrize("name,kw", [
+    ("bf16_every4_fast", dict(snap_every=4, snap_dtype=SNAP_BF16)),
+    ("bf16_every4_fast_checkpoints", dict(snap_every=4, snap_dtype=SNAP_BF16, checkpoint_every=64)),
+    ("f32_every1_exact", dict(snap_every=1, snap_dtype=SNAP_F32, exact=True)),
+])
+def test_lsrtm_1200x400_subset_vs_fp64_cgls(ctx, name, kw):
+    """Two shots of the 1200 x 400 LSRTM survey (nt cut to 500), three CG
+    iterations, against the FP64 CGLS of the same shots and data
+    (tests/golden/lsrtm_fp64.npz, made by tests/golden/make_lsrtm_fp64.py):
+    the residual curve and the model (on the fixture's every-4th-cell
+    subsample) within 1e-3 relative."""
+    import hashlib
+    import os
+
+    from helpers import GOLDEN
+    from seis_b200 import synth
+    g = np.load(os.path.join(GOLDEN, "lsrtm_fp64.npz"))
+    sv = synth.lsrtm(nt=int(g["nt"])).subset([int(k) for k in g["shots"]])
+    wav = sv.wavelet()
+    dobs = [O.born(s, wav.astype(np.float64), sv.sub(sv.vel0, i), sv.sub(sv.dv, i),
+                   prec="f64").astype(np.float32) for i, s in enumerate(sv.shots)]
+    assert [hashlib.sha256(d.tobytes()).hexdigest() for d in dobs] == [str(h) for h in g["data_sha"]]
+    with Lsrtm(ctx, sv.nx, sv.nz, sv.shots, sv.x0, **kw) as ls:
+        ls.set_background(sv.vel0, wav)
+        for k, d in enumerate(dobs):
+            ls.set_data(k, d)
+        rr0 = ls.reset()
+        hist = ls.iterate(int(g["niter"]))
+        m = ls.model()
+    st = int(g["step"])
+    err_m = rel_l2(m[::st, ::st], g["m_sub"])
+    ref_h = g["hist"] / g["rr0"]
+    err_h = float(np.max(np.abs(hist / rr0 - ref_h) / ref_h))
+    print(f"{name}: rr0 rel {abs(rr0 - g['rr0']) / g['rr0']:.2e}, residual curve rel "
+          f"{err_h:.2e}, model rel L2 {err_m:.2e} vs FP64 CGLS")
+    assert abs(rr0 - float(g["rr0"])) <= 1e-6 * float(g["rr0"])
+    assert err_h <= 1e-3 and err_m <= 1e-3
