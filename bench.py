@@ -180,16 +180,19 @@ def load_synth():
     return mod
 
 
-def workload(name: str, rank: int, world: int):
-    """(whole survey, this rank's shot indices, solver options)."""
+def workload(name: str, rank: int, world: int, shots: int = None, nt: int = None):
+    """(whole survey, this rank's shot indices, solver options); `shots` (per
+    GPU) and `nt` (recorded samples) default to the workload's own."""
     synth = load_synth()
     if name == "lsrtm_large":
-        full = synth.large_sweep(vmax=3000.0)
-        mine = [k * STRIDE + rank for k in range(SAMPLE)]
+        k = min(shots or SAMPLE, SAMPLE)
+        full = synth.large_sweep(vmax=3000.0, nt=nt or 8000)
+        mine = [j * STRIDE + rank for j in range(k)]
         return full, mine, {"checkpoint_every": CK_EVERY}
     if name == "lsrtm_1200x400":
-        full = synth.lsrtm(nshots=32 * world)
-        mine = list(range(32 * rank, 32 * rank + 32))
+        k = shots or 32
+        full = synth.lsrtm(nshots=k * world, nt=nt or 5000)
+        mine = list(range(k * rank, k * rank + k))
         return full, mine, {"checkpoint_every": 0}
     raise SystemExit(f"unknown workload {name}")
 
@@ -208,8 +211,8 @@ def config_of(name: str, full, sv, world: int) -> dict:
                      if world > 1 else "none"}
     if name == "lsrtm_large":
         c.update({"velocity_cap_m_s": 3000.0, "checkpoint_every": CK_EVERY,
-                  "shot_indices_rank0": [k * STRIDE for k in range(SAMPLE)],
-                  "sample": f"{SAMPLE} of the survey's {len(full.shots)} shots per GPU "
+                  "shot_indices_rank0": [k * STRIDE for k in range(len(sv.shots))],
+                  "sample": f"{len(sv.shots)} of the survey's {len(full.shots)} shots per GPU "
                             f"(every {STRIDE}th)"})
     return c
 
@@ -274,7 +277,7 @@ def run_reference(args, rank, world):
     """The reference's CPU path on this workload (bounded sample per step)."""
     if rank != 0:
         return
-    full, mine, _ = workload(args.workload, rank, world)
+    full, mine, _ = workload(args.workload, rank, world, args.shots, args.nt)
     sv = full.subset(mine)
     cap = 24 if args.workload == "lsrtm_large" else 150
     vals, last = [], None
@@ -429,6 +432,11 @@ def main():
     ap.add_argument("--workload", default="lsrtm_large", choices=["lsrtm_large", "lsrtm_1200x400"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--shots", type=int, default=None,
+                    help="shots per GPU (default: the workload's, 8 of lsrtm_large, 32 of "
+                         "lsrtm_1200x400)")
+    ap.add_argument("--nt", type=int, default=None,
+                    help="recorded time samples (default: the workload's)")
     args = ap.parse_args()
     rank, world, local = dist_init()
     if args.impl == "reference":
@@ -442,7 +450,7 @@ def main():
 
     torch.cuda.set_device(local)
     from seis_b200.shards import DeviceEngine, ShardedCGLS, nccl_reduce
-    full, mine, opts = workload(args.workload, rank, world)
+    full, mine, opts = workload(args.workload, rank, world, args.shots, args.nt)
     sv = full.subset(mine)
     shots = sv.shots
     ck = opts["checkpoint_every"]
