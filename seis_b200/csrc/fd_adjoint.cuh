@@ -54,7 +54,8 @@ struct AGeo {
   static constexpr int NHALO = 2 * (G::TX + 2) + 2 * G::TZ;
   static constexpr int HPT = (NHALO + G::NT - 1) / G::NT;  // halo cells per thread
   static constexpr int PAD_FLOATS = 4 * WIDE + NARROW + RN;
-  static_assert(5 * RN <= 3 * WIDE + NARROW + RN, "ring arrays fit over the dead buffers");
+  static_assert(5 * RN + G::TX * G::TZ <= 3 * WIDE + NARROW + RN,
+                "ring arrays and the tile's L fit over the dead buffers");
   static constexpr size_t TILE_SMEM = sizeof(float) * (size_t)(4 * WIDE + NARROW) + 16;
   static constexpr size_t PAD_SMEM = sizeof(float) * (size_t)PAD_FLOATS + 16;
   static constexpr int MIN_I = ctas_fit(TILE_SMEM, 768 / G::NT) > 0 ? ctas_fit(TILE_SMEM, 768 / G::NT) : 1;
@@ -478,7 +479,8 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
     }
   }
   __syncthreads();  // sL1, sL2, sWZ, sWX and sCOR are dead: the ring arrays go there
-  // rho = (1 - w) L of the ring cells, times their one-way coefficients
+  float *sLt = rp0 + 5 * RN;  // L of the tile's cells, [TX][TZ]
+  // rho = (1 - w) L of a ring cell, times its one-way coefficients
   auto put_ring = [&](int cx, int cz, const PadPos &pp, bool ring, float L) {
     const int i = ridx(cx, cz);
     int mask = 0;
@@ -490,66 +492,78 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
     rp2[i] = p2;
     rp3[i] = p3;
   };
+  // the owners keep L of the tile in shared memory and clear the roles of
+  // the tile cells that are no ring cells; the halo's ring cells are formed
+  // by the threads that hold their L
 #pragma unroll
   for (int k = 0; k < 8; k++) {
     const int cx = ix + k / 4, cz = iz0 + k % 4;
-    const bool in = cx < NX && cz < NZ;
-    const PadPos pp = pad_pos(g, cx, cz);
-    put_ring(cx, cz, pp, in && pp.ring > 0, Lt[k]);
+    sLt[(cx - x0) * TZ + (cz - z0)] = Lt[k];
+    if (!(cx < NX && cz < NZ && pad_pos(g, cx, cz).ring > 0)) rmask[ridx(cx, cz)] = 0;
   }
 #pragma unroll
   for (int h = 0; h < HPT; h++)
     if (tid + h * A_NT_I < ADJ_NHALO) put_ring(hx[h], hz[h], hp[h], hring[h], Lh[h]);
   __syncthreads();
+  // the ring cells of the tile (its pad cells), shared evenly by all threads
+  const int xe_ = min(x0 + TX, NX), ze_ = min(z0 + TZ, NZ);
+  const CellList ring(x0, z0, xe_, ze_, g.pml, g.pml + g.nx, g.pml, g.pml + g.nz);
+  for (int i = tid; i < ring.n; i += A_NT_I) {
+    int cx, cz;
+    ring.cell(i, cx, cz);
+    put_ring(cx, cz, pad_pos(g, cx, cz), true, sLt[(cx - x0) * TZ + (cz - z0)]);
+  }
+  __syncthreads();
 
-  // M = w L + P_u3^T rho on the pad and model edge cells (L elsewhere), E of
-  // the next step and the kept prev terms
+  // M = w L + P_u3^T rho, E of the next step and the kept prev terms on the
+  // pad and model edge cells (the cells outside the model less its edge),
+  // shared evenly by all threads
   float *out = g.fa[(a.rot + 2) % 3];
+  const CellList aff(x0, z0, xe_, ze_, g.pml + 1, g.pml + g.nx - 1, g.pml + 1, g.pml + g.nz - 1);
+  for (int i = tid; i < aff.n; i += A_NT_I) {
+    int cx, cz;
+    aff.cell(i, cx, cz);
+    float m = 0.0f, e = 0.0f, b = 0.0f;
+#pragma unroll
+    for (int dx = -1; dx <= 1; dx++)
+#pragma unroll
+      for (int dz = -1; dz <= 1; dz++) {
+        const int q = ridx(cx + dx, cz + dz);
+        // this cell sits at offset (-dx, -dz) from the ring cell
+        switch ((rmask[q] >> role_slot(-dx, -dz)) & 7) {
+          case ROLE_SELF: e += rp2[q]; b += rp0[q]; break;
+          case ROLE_INNER: m += rp0[q]; e += rp2[q]; b -= rp3[q]; break;
+          case ROLE_TANG: b += rp1[q]; break;
+          case ROLE_DIAG: m += rp1[q]; break;
+          case ROLE_CZ: m += rp0[q]; break;
+          case ROLE_CX: m += rp1[q]; break;
+          case ROLE_CSELF: e += rp2[q]; break;
+          default: break;
+        }
+      }
+    const PadPos pt = pad_pos(g, cx, cz);
+    const float w = pt.ring == 0 ? 1.0f : pad_weight(g, pt);
+    const size_t at = (size_t)cx * g.LDZ + cz;
+    out[at] = w * sLt[(cx - x0) * TZ + (cz - z0)] + m;
+    Enext[at] = e + g.adj_b[at];
+    g.adj_b[at] = b;
+  }
+  // the other cells: M = L, from the owners' registers
+  auto inner = [&](int cx, int cz) {
+    return cx > g.pml && cx < g.pml + g.nx - 1 && cz > g.pml && cz < g.pml + g.nz - 1;
+  };
 #pragma unroll
   for (int j = 0; j < 2; j++) {
     const int cx = ix + j;
     if (cx >= NX || iz0 >= NZ) continue;
     const size_t col = (size_t)cx * g.LDZ;
-    float4 o;
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-      const int cz = iz0 + r;
-      float L = Lt[4 * j + r];
-      const PadPos pt = pad_pos(g, cx, cz);
-      const bool edge_cell = cx == g.pml || cx == g.pml + g.nx - 1 || cz == g.pml ||
-                             cz == g.pml + g.nz - 1;
-      if (cz < NZ && (pt.ring > 0 || edge_cell)) {
-        float m = 0.0f, e = 0.0f, b = 0.0f;
-#pragma unroll
-        for (int dx = -1; dx <= 1; dx++)
-#pragma unroll
-          for (int dz = -1; dz <= 1; dz++) {
-            const int i = ridx(cx + dx, cz + dz);
-            // this cell sits at offset (-dx, -dz) from the ring cell
-            switch ((rmask[i] >> role_slot(-dx, -dz)) & 7) {
-              case ROLE_SELF: e += rp2[i]; b += rp0[i]; break;
-              case ROLE_INNER: m += rp0[i]; e += rp2[i]; b -= rp3[i]; break;
-              case ROLE_TANG: b += rp1[i]; break;
-              case ROLE_DIAG: m += rp1[i]; break;
-              case ROLE_CZ: m += rp0[i]; break;
-              case ROLE_CX: m += rp1[i]; break;
-              case ROLE_CSELF: e += rp2[i]; break;
-              default: break;
-            }
-          }
-        const float w = pt.ring == 0 ? 1.0f : pad_weight(g, pt);
-        L = w * L + m;
-        Enext[col + cz] = e + g.adj_b[col + cz];
-        g.adj_b[col + cz] = b;
-      }
-      set_comp(o, r, L);
-    }
-    if (iz0 + 3 < NZ) {
-      *reinterpret_cast<float4 *>(out + col + iz0) = o;
+    if (iz0 + 3 < NZ && inner(cx, iz0) && inner(cx, iz0 + 3)) {
+      *reinterpret_cast<float4 *>(out + col + iz0) =
+          make_float4(Lt[4 * j], Lt[4 * j + 1], Lt[4 * j + 2], Lt[4 * j + 3]);
     } else {
 #pragma unroll
       for (int r = 0; r < 4; r++)
-        if (iz0 + r < NZ) out[col + iz0 + r] = comp(o, r);
+        if (iz0 + r < NZ && inner(cx, iz0 + r)) out[col + iz0 + r] = Lt[4 * j + r];
     }
   }
 }

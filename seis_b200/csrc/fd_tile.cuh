@@ -306,6 +306,48 @@ struct GA {
   }
 };
 
+// The grid cells of a tile [x0, x0 + TX) x [z0, z0 + TZ) that lie outside a
+// rectangle [rx0, rx1) x [rz0, rz1) (the model, or the model less its edge
+// cells), enumerated column by column, z fastest, so that the threads of a
+// CTA can share them evenly and consecutive threads touch consecutive rows.
+struct CellList {
+  int x0, z0, xe, ze;  // tile cells inside the grid: [x0, xe) x [z0, ze)
+  int ma, mb;          // tile columns crossing the rectangle: [ma, mb)
+  int top, bot;        // cells of such a column above / below the rectangle
+  int cp, cm, n;       // cells per other column, per crossing column, in all
+  __device__ __forceinline__ CellList(int x0_, int z0_, int xe_, int ze_, int rx0, int rx1,
+                                      int rz0, int rz1)
+      : x0(x0_), z0(z0_), xe(xe_), ze(ze_) {
+    ma = min(max(rx0, x0), xe);
+    mb = min(max(rx1, ma), xe);
+    top = max(0, min(ze, rz0) - z0);
+    bot = max(0, ze - max(z0, rz1));
+    if (rz1 <= rz0) top = ze - z0, bot = 0;  // empty rectangle: whole columns
+    cp = ze - z0;
+    cm = top + bot;
+    n = (xe - x0 - (mb - ma)) * cp + (mb - ma) * cm;
+  }
+  __device__ __forceinline__ void cell(int i, int &cx, int &cz) const {
+    const int na = (ma - x0) * cp;
+    if (i < na) {
+      cx = x0 + i / cp;
+      cz = z0 + i % cp;
+      return;
+    }
+    i -= na;
+    const int nm = (mb - ma) * cm;
+    if (i < nm) {
+      cx = ma + i / cm;
+      const int r = i % cm;
+      cz = r < top ? z0 + r : ze - bot + (r - top);
+      return;
+    }
+    i -= nm;
+    cx = mb + i / cp;
+    cz = z0 + i % cp;
+  }
+};
+
 // Two-way values of a pad tile and its one-cell halo in shared memory:
 // columns x0-1 .. x0+TX, rows z0-4 .. z0+TZ+3 (U3R = TZ + 8 rows per column;
 // the tile's row quads stay 16-byte aligned; only rows z0-1 .. z0+TZ are
@@ -722,21 +764,16 @@ __global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_tile_
   if (snap) snap_write<NT_T, 8, TX, TZ>(g, aa.snap_k, x0, z0, lv, lx, lz, mask, red);
   __syncthreads();
 
-  // 4. pad cells: one-way update and blend
-  if (ix < NX && iz0 < NZ) {
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-      const int cxj = ix + j;
-      if (cxj >= NX) continue;
-#pragma unroll
-      for (int r = 0; r < 4; r++) {
-        const int iz = iz0 + r;
-        if (iz >= NZ || model(cxj, iz)) continue;
-        const size_t at = (size_t)cxj * g.LDZ + iz;
-        out_a[at] = absorb_cell(UA_(cxj, iz), UA_, CA, PA, VV, g, cxj, iz);
-        if (BORN) nb_[at] = absorb_cell(UB_(cxj, iz), UB_, CB, PB, VV, g, cxj, iz);
-      }
-    }
+  // 4. pad cells: one-way update and blend, the tile's pad cells shared
+  // evenly by all threads
+  const CellList pads(x0, z0, min(x0 + TX, NX), min(z0 + TZ, NZ), g.pml, g.pml + g.nx, g.pml,
+                      g.pml + g.nz);
+  for (int i = tid; i < pads.n; i += NT_T) {
+    int cxj, iz;
+    pads.cell(i, cxj, iz);
+    const size_t at = (size_t)cxj * g.LDZ + iz;
+    out_a[at] = absorb_cell(UA_(cxj, iz), UA_, CA, PA, VV, g, cxj, iz);
+    if (BORN) nb_[at] = absorb_cell(UB_(cxj, iz), UB_, CB, PB, VV, g, cxj, iz);
   }
 }
 
