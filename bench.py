@@ -324,9 +324,9 @@ def kernel_roofline(ctx, sv, iter_ms, launches_per_iter):
     (separate plans over the same shots, the two kernels of a step concurrent
     as in a run), their share of one iteration, and the roofline of the
     kernel with the largest share."""
-    from seis_b200._lib import IN_VEL, IN_WAVELET, OP_BORN, OP_BORN_ADJOINT, Plan
+    from seis_b200._lib import IN_VEL, IN_WAVELET, OP_BORN, OP_BORN_ADJOINT, TILE_SHAPES, Plan
     wav = sv.wavelet()
-    rows = []
+    rows, tuning = [], {}
     for op, name in ((OP_BORN, "born"), (OP_BORN_ADJOINT, "adjoint")):
         with Plan(ctx, op, sv.shots) as p:
             if op == OP_BORN:
@@ -334,6 +334,12 @@ def kernel_roofline(ctx, sv, iter_ms, launches_per_iter):
             for i in range(len(sv.shots)):
                 p.set(i, IN_VEL, sv.sub(sv.vel0, i))
                 p.set(i, IN_WAVELET, wav)
+            # the autotuner's step time of every tile shape on these shots (the
+            # solver's plans of the same signature use the same choice)
+            best, per_shape = p.autotune(steps=10, force=True)
+            tuning[name] = {"chosen": "%dx%d" % TILE_SHAPES[best],
+                            "step_ms": {"%dx%d" % TILE_SHAPES[k]: v
+                                        for k, v in enumerate(per_shape)}}
             p.time_kernels(10)
             ms, by = p.time_kernels(100)
         n = launches_per_iter[name]
@@ -349,7 +355,7 @@ def kernel_roofline(ctx, sv, iter_ms, launches_per_iter):
                      "GB_s": (by[0] + by[1]) / (ms[2] * 1e6)})
     kern = [r for r in rows if not r["kernel"].endswith("_step")]
     top = max(kern, key=lambda r: r["ms"] * r["launches_per_iter"])
-    return top, rows
+    return top, rows, tuning
 
 
 def adjoint_images(ctx, sv, dobs, every, dtype, ck):
@@ -557,7 +563,7 @@ def main():
 
     # ---- roofline of the kernel with the largest share
     per_iter_launches = {"born": shots[0].NT, "adjoint": shots[0].NT + 1}
-    top, rows = kernel_roofline(ctx, sv, ms_per_step, per_iter_launches)
+    top, rows, tuning = kernel_roofline(ctx, sv, ms_per_step, per_iter_launches)
     hbm, src = peaks()
     ach = top["bytes"] / (top["ms"] * 1e-3) / 1e9
     line = {
@@ -574,6 +580,7 @@ def main():
                      "traffic_unit": "bytes per launch (ncu dram read + write, scaled by cells)",
                      "kernel": top["kernel"], "peak_source": src, "kernel_ms": top["ms"],
                      "share": top["share"], "kernels": rows},
+        "tile_shapes": tuning,
         "gpu_launches": launches,
         "clocks": clocks,
     }
