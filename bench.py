@@ -12,7 +12,7 @@ scheme -- its absorbing boundary, which this library reproduces bit for bit --
 grows without bound over 8120 steps from a Courant number of about 0.33 up.
 One GPU runs a sample of 8 of the 256 shots (shots 0, 32, ..., 224; under
 torchrun rank r takes shots r, 32 + r, ...: weak scaling, no collective on
-the data path), with the solver as the full survey needs it on a GPU: BF16
+the data path), with the solver as the full survey needs it on a GPU: FP16
 source-term snapshots every 4 steps with one power-of-two scale per tile,
 source-field checkpoints every 256 steps, FP64 CG scalars.  One step = one CG
 iteration over the sample: Born modeling of its 8 shots (two fields per step),
@@ -49,7 +49,7 @@ iteration time.
   second of the same work.
 
 Workload ``lsrtm_1200x400``: one CG iteration of the 32-shot 1200 x 400 survey
-(10 m, nt 5000 + 94, dt 0.8 ms, 20 Hz, BF16 snapshots every 4 steps kept
+(10 m, nt 5000 + 94, dt 0.8 ms, 20 Hz, FP16 snapshots every 4 steps kept
 whole, no checkpoints).
 """
 from __future__ import annotations
@@ -204,7 +204,7 @@ def config_of(name: str, full, sv, world: int) -> dict:
          "shots_timed_total": len(sv.shots) * world, "apertures_rank0": [s.nx for s in sv.shots],
          "grid": f"{full.nx}x{full.nz} at {full.dx:g} m, pml {s0.pml}",
          "nt": s0.nt, "ndel": s0.ndel, "dt_s": s0.dt, "ricker_hz": full.fr,
-         "snapshots": f"BF16 every {SNAP_EVERY} steps, per-tile power-of-two scale",
+         "snapshots": f"FP16 every {SNAP_EVERY} steps, per-tile power-of-two scale",
          "step": "one CG iteration over the GPU's shots: Born of every shot, its exact "
                  "adjoint, FP64 CG algebra",
          "exchange": "per CG iteration: NCCL all-reduce of the image and 2 FP64 sums"
@@ -452,7 +452,7 @@ def main():
 
     import torch
     from seis_b200 import Context
-    from seis_b200._lib import SNAP_BF16, Lsrtm
+    from seis_b200._lib import SNAP_F16, Lsrtm
 
     torch.cuda.set_device(local)
     from seis_b200.shards import DeviceEngine, ShardedCGLS, nccl_reduce
@@ -463,7 +463,7 @@ def main():
     ctx = Context(local)
     wav = sv.wavelet()
     dobs = observed_data(ctx, sv)
-    ls = Lsrtm(ctx, sv.nx, sv.nz, shots, sv.x0, snap_every=SNAP_EVERY, snap_dtype=SNAP_BF16,
+    ls = Lsrtm(ctx, sv.nx, sv.nz, shots, sv.x0, snap_every=SNAP_EVERY, snap_dtype=SNAP_F16,
                checkpoint_every=ck)
     ls.set_background(sv.vel0, wav)
     for i, d in enumerate(dobs):
@@ -535,7 +535,7 @@ def main():
     # ---- the same iteration with the plans rebuilt in every application
     regroup = None
     if world == 1 and not args.no_plain and args.workload == "lsrtm_large":
-        with Lsrtm(ctx, sv.nx, sv.nz, shots, sv.x0, snap_every=SNAP_EVERY, snap_dtype=SNAP_BF16,
+        with Lsrtm(ctx, sv.nx, sv.nz, shots, sv.x0, snap_every=SNAP_EVERY, snap_dtype=SNAP_F16,
                    checkpoint_every=ck, group_shots=len(shots)) as lg:
             lg.set_background(sv.vel0, wav)
             for i, d in enumerate(dobs):
@@ -554,7 +554,7 @@ def main():
     plain = errors = None
     if world == 1 and not args.no_plain:
         t_plain, img_plain = plain_fp32(ctx, sv, dobs, ck)
-        img_mixed = adjoint_images(ctx, sv, dobs, SNAP_EVERY, SNAP_BF16, ck)
+        img_mixed = adjoint_images(ctx, sv, dobs, SNAP_EVERY, SNAP_F16, ck)
         plain = {"iter_ms": t_plain * 1e3, "shots": len(shots),
                  "how": "one shot per plan and graph; Born run, then the exact adjoint with FP32 "
                         "snapshots at every step" + (f" (checkpoints every {ck} steps)" if ck else "")

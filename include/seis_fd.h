@@ -194,7 +194,7 @@ int seis_fd_rtm_plane(seis_fd_ctx *ctx, const seis_shot_desc *shot, const float 
 /* Storage of the source-term snapshots (background second time derivative)
  * that SEIS_OP_BORN_ADJOINT images with. */
 #define SEIS_SNAP_F32 1
-#define SEIS_SNAP_BF16 2   /* one power-of-two scale per snapshot and 32x64 tile */
+#define SEIS_SNAP_BF16 2   /* one power-of-two scale per snapshot and kernel tile */
 #define SEIS_SNAP_F16 3    /* same */
 
 int seis_fd_plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *shots,
@@ -341,7 +341,8 @@ int seis_fd_vec_axpby(seis_fd_ctx *ctx, float *d_y, const float *d_x, double a, 
 typedef struct seis_fd_lsrtm seis_fd_lsrtm;
 typedef struct {
   int snap_every;  /* source-term snapshot interval (default 1)            */
-  int snap_dtype;  /* SEIS_SNAP_* (default SEIS_SNAP_BF16)                 */
+  int snap_dtype;  /* SEIS_SNAP_* (default SEIS_SNAP_F16: with the per-tile
+                      scale, 3 more mantissa bits than BF16 at the same size) */
   int exact;       /* Born kernels round like the reference (default 0)    */
   int checkpoint_every; /* source-field checkpoint interval (default 0 = keep
                            every snapshot; see seis_fd_plan_set_checkpoints) */

@@ -391,7 +391,7 @@ class Lsrtm:
         lets the autotuner pick each plan's tile shape; else a TILE_* shape."""
         self.ctx, self.nx, self.nz, self.shots = ctx, nx, nz, list(shots)
         self._descs = shot_array(self.shots)
-        o = LsrtmOptsC(snap_every, SNAP_BF16 if snap_dtype is None else snap_dtype,
+        o = LsrtmOptsC(snap_every, SNAP_F16 if snap_dtype is None else snap_dtype,
                        1 if exact else 0, checkpoint_every, group_shots,
                        0 if tile_shape is None else tile_shape + 1)
         h = ctypes.c_void_p()

@@ -1902,7 +1902,7 @@ int seis_fd_lsrtm_create_mapped(seis_fd_ctx *ctx, int nx, int nz, int nshot,
     }
     off += shots[k].nx;
   }
-  seis_lsrtm_opts o{1, SEIS_SNAP_BF16, 0, 0, 0, 0};
+  seis_lsrtm_opts o{1, SEIS_SNAP_F16, 0, 0, 0, 0};
   if (opts) o = *opts;
   seis_fd_lsrtm *L = new (std::nothrow) seis_fd_lsrtm();
   if (!L) return fail(ctx, SEIS_ERR_NOMEM, "host allocation failed");

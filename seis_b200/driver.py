@@ -19,7 +19,7 @@ import sys
 
 import numpy as np
 
-from ._lib import Context, LsrtmOptsC, SNAP_BF16, SeisError, lib
+from ._lib import Context, LsrtmOptsC, SNAP_F16, SeisError, lib
 
 _P, _I = ctypes.c_void_p, ctypes.c_int
 
@@ -165,7 +165,7 @@ class Driver:
         return ss
 
     def lsrtm(self, niter: int, born_data: bool = False, snap_every: int = 1,
-              snap_dtype: int = SNAP_BF16, exact: bool = False, checkpoint_every: int = 0,
+              snap_dtype: int = SNAP_F16, exact: bool = False, checkpoint_every: int = 0,
               group_shots: int = 0):
         """(model [nx][nz], [|d|^2, |r|^2 per iteration]) of CGLS over all shots;
         checkpoint_every > 0 keeps source-field checkpoints instead of every snapshot,
