@@ -352,6 +352,39 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
     tma_load_2d(sV, g.maps + MAP_VEL_WIDE, z0, x0 + XM - HXC, bar);
     tma_load_2d(sL2, g.maps + MAP_FA_NARROW + a.rot % 3, z0, x0 + XM - 1, bar);
   }
+  // this step's ring terms E of the thread's tile columns and halo cells,
+  // loaded while the tensor copies are in flight
+  const float *Ecur = g.adj_e[a.rot & 1];
+  float *Enext = g.adj_e[(a.rot + 1) & 1];
+  const int qz = tid % QZ, cxp = tid / QZ;
+  const int ix = x0 + 2 * cxp, iz0 = z0 + 4 * qz;
+  float4 e4[2];
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    e4[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ix + j < NX && iz0 < NZ)
+      e4[j] = *reinterpret_cast<const float4 *>(Ecur + (size_t)(ix + j) * g.LDZ + iz0);
+  }
+  int hx[HPT], hz[HPT];
+  float eh[HPT];
+  PadPos hp[HPT];
+  bool hring[HPT];
+#pragma unroll
+  for (int h = 0; h < HPT; h++) {
+    const int i = tid + h * A_NT_I;
+    hx[h] = hz[h] = -1;
+    eh[h] = 0.0f;
+    hp[h] = PadPos{};
+    hring[h] = false;
+    if (i >= ADJ_NHALO) continue;
+    adj_halo_cell<TX, TZ>(i, x0, z0, hx[h], hz[h]);
+    const int cx = hx[h], cz = hz[h];
+    if (cx >= 0 && cz >= 0 && cx < NX && cz < NZ) {
+      hp[h] = pad_pos(g, cx, cz);
+      hring[h] = hp[h].ring > 0;
+    }
+    if (hring[h]) eh[h] = Ecur[(size_t)cx * g.LDZ + cz];
+  }
   if (!mbar_wait(bar, 0)) {
     if (tid == 0) atomicExch(err, 2);
     return;
@@ -396,12 +429,8 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
     }
   }
   __syncthreads();
-  const float *Ecur = g.adj_e[a.rot & 1];
-  float *Enext = g.adj_e[(a.rot + 1) & 1];
 
   // L of the tile's cells (kept in registers), imaging on its model cells
-  const int qz = tid % QZ, cxp = tid / QZ;
-  const int ix = x0 + 2 * cxp, iz0 = z0 + 4 * qz;
   const bool img = a.snap_k >= 0 && g.snap != nullptr;
   float Lt[8];
   {
@@ -416,9 +445,6 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
       const float zz[12] = {za4.x, za4.y, za4.z, za4.w, zb4.x, zb4.y,
                             zb4.z, zb4.w, zc4.x, zc4.y, zc4.z, zc4.w};
       const float4 l1 = L1.quad(cx, iz0), l2 = L2.quad(cx, iz0);
-      float4 e4 = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (cx < NX && iz0 < NZ)
-        e4 = *reinterpret_cast<const float4 *>(Ecur + (size_t)cx * g.LDZ + iz0);
       const int x = cx - g.pml;
       const int gzr = (x >= 0 && x < g.nx && cx < NX) ? g.gz[x] + g.pml : -1;
 #pragma unroll
@@ -431,7 +457,7 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
                                comp(xm[j + 6], r), comp(xm[j + 7], r), comp(xm[j + 8], r));
         float v = sz_ + sx_ + 2.0f * comp(l1, r);
         if (edge && cx < NX && cz < NZ && near4(cx, cz)) v = v + sCOR[ridx(cx, cz)];
-        v = v - comp(l2, r) + comp(e4, r);
+        v = v - comp(l2, r) + comp(e4[j], r);
         if (a.rec_k >= 0 && cz == gzr) v += g.rec[(size_t)a.rec_k * g.nx + x];
         Lt[4 * j + r] = v;
         const int z = cz - g.pml;
@@ -444,24 +470,11 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
   }
   // L of the halo's pad cells (the only halo cells whose rho is read); halo
   // cell tid + h * A_NT_I of thread tid
-  int hx[HPT], hz[HPT];
   float Lh[HPT];
-  PadPos hp[HPT];
-  bool hring[HPT];
 #pragma unroll
   for (int h = 0; h < HPT; h++) {
-    const int i = tid + h * A_NT_I;
-    hx[h] = hz[h] = -1;
     Lh[h] = 0.0f;
-    hp[h] = PadPos{};
-    hring[h] = false;
-    if (i >= ADJ_NHALO) continue;
-    adj_halo_cell<TX, TZ>(i, x0, z0, hx[h], hz[h]);
     const int cx = hx[h], cz = hz[h];
-    if (cx >= 0 && cz >= 0 && cx < NX && cz < NZ) {
-      hp[h] = pad_pos(g, cx, cz);
-      hring[h] = hp[h].ring > 0;
-    }
     if (hring[h]) {
       const float sz_ = lap8(WZ(cx, cz - 4), WZ(cx, cz - 3), WZ(cx, cz - 2), WZ(cx, cz - 1),
                              WZ(cx, cz), WZ(cx, cz + 1), WZ(cx, cz + 2), WZ(cx, cz + 3),
@@ -471,7 +484,7 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
                              WX(cx + 4, cz));
       float v = sz_ + sx_ + 2.0f * L1(cx, cz);
       if (edge && near4(cx, cz)) v = v + sCOR[ridx(cx, cz)];
-      v = v - L2(cx, cz) + Ecur[(size_t)cx * g.LDZ + cz];
+      v = v - L2(cx, cz) + eh[h];
       const int x = cx - g.pml;
       if (a.rec_k >= 0 && x >= 0 && x < g.nx && cz == g.gz[x] + g.pml)
         v += g.rec[(size_t)a.rec_k * g.nx + x];
@@ -520,7 +533,23 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
   // shared evenly by all threads
   float *out = g.fa[(a.rot + 2) % 3];
   const CellList aff(x0, z0, xe_, ze_, g.pml + 1, g.pml + g.nx - 1, g.pml + 1, g.pml + g.nz - 1);
-  for (int i = tid; i < aff.n; i += A_NT_I) {
+  // the kept prev terms of the thread's cells, loaded before any store
+  constexpr int KMAX = (TX * TZ + A_NT_I - 1) / A_NT_I;
+  float bold[KMAX];
+#pragma unroll
+  for (int k = 0; k < KMAX; k++) {
+    const int i = tid + k * A_NT_I;
+    bold[k] = 0.0f;
+    if (i < aff.n) {
+      int cx, cz;
+      aff.cell(i, cx, cz);
+      bold[k] = g.adj_b[(size_t)cx * g.LDZ + cz];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < KMAX; k++) {
+    const int i = tid + k * A_NT_I;
+    if (i >= aff.n) continue;
     int cx, cz;
     aff.cell(i, cx, cz);
     float m = 0.0f, e = 0.0f, b = 0.0f;
@@ -545,7 +574,7 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
     const float w = pt.ring == 0 ? 1.0f : pad_weight(g, pt);
     const size_t at = (size_t)cx * g.LDZ + cz;
     out[at] = w * sLt[(cx - x0) * TZ + (cz - z0)] + m;
-    Enext[at] = e + g.adj_b[at];
+    Enext[at] = e + bold[k];
     g.adj_b[at] = b;
   }
   // the other cells: M = L, from the owners' registers

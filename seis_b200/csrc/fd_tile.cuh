@@ -62,8 +62,10 @@ struct TCfg {
   static constexpr int NOTH = BORN ? 4 : 2;   // prev, vel [, prev B, dv]
   static constexpr int BUF = (NCUR * G::CW_C + NOTH * G::CW_P) * G::SR;  // floats per buffer
   static constexpr size_t bytes = sizeof(float) * (size_t)BUF + 16;
-  // at most 768 threads per SM (85 registers a thread)
-  static constexpr int MIN_CTAS = ctas_fit(bytes, 768 / G::NT) > 0 ? ctas_fit(bytes, 768 / G::NT) : 1;
+  // interior tiles: at most 1024 threads per SM for one field (64 registers
+  // a thread), 768 for Born's two (85 registers)
+  static constexpr int CAP = (BORN ? 768 : 1024) / G::NT;
+  static constexpr int MIN_CTAS = ctas_fit(bytes, CAP) > 0 ? ctas_fit(bytes, CAP) : 1;
 };
 
 // ---- PTX helpers: mbarrier + bulk asynchronous copy global -> shared
@@ -612,22 +614,34 @@ __global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_tile_
   const int za = max(z0 - 1, 0), zb = min(z0 + TZ + 1, NZ);
   const bool edge = xa <= 3 || za <= 3 || xb - 1 >= NX - 4 || zb - 1 >= NZ - 4;
   if (edge) {
-    const int ra = a.rot % 3, rb = a.rot_b % 3;
-    float *const *FA = MODE == MODE_RCV ? g.fb : g.fa;
-    const int rr = MODE == MODE_RCV ? rb : ra;
-    const GA GCa{FA[(rr + 1) % 3], g.LDZ}, GPa{FA[rr], g.LDZ}, GV{g.vel, g.LDZ};
-    const GA GCb{g.fb[(rb + 1) % 3], g.LDZ}, GPb{g.fb[rb], g.LDZ};
+    // every read of the band's formulas lies in the staged window, except the
+    // frame's normal extrapolation in a tile of at most two grid columns (it
+    // reaches the velocity two columns inside, past the one-column halo):
+    // such a tile reads global memory
+    auto bands = [&](const auto &Ca, const auto &Pa, const auto &Vv, const auto &Cb,
+                     const auto &Pb) {
 #pragma unroll 1
-    for (int b = 0; b < 4; b++) {  // top, bottom, left, right band
-      const int bxa = b == 3 ? max(xa, NX - 4) : xa, bxb = b == 2 ? min(xb, 4) : xb;
-      const int bza = b == 1 ? max(za, NZ - 4) : za, bzb = b == 0 ? min(zb, 4) : zb;
-      const int nr = bzb - bza, nc = bxb - bxa;
-      if (nr <= 0 || nc <= 0) continue;
-      for (int i = tid; i < nr * nc; i += NT_T) {
-        const int cx = bxa + i / nr, cz = bza + i % nr;
-        UA_.ref(cx, cz) = twoway_cell(GCa, GPa, GV, g, cx, cz);
-        if (BORN) UB_.ref(cx, cz) = twoway_cell(GCb, GPb, GV, g, cx, cz);
+      for (int b = 0; b < 4; b++) {  // top, bottom, left, right band
+        const int bxa = b == 3 ? max(xa, NX - 4) : xa, bxb = b == 2 ? min(xb, 4) : xb;
+        const int bza = b == 1 ? max(za, NZ - 4) : za, bzb = b == 0 ? min(zb, 4) : zb;
+        const int nr = bzb - bza, nc = bxb - bxa;
+        if (nr <= 0 || nc <= 0) continue;
+        for (int i = tid; i < nr * nc; i += NT_T) {
+          const int cx = bxa + i / nr, cz = bza + i % nr;
+          UA_.ref(cx, cz) = twoway_cell(Ca, Pa, Vv, g, cx, cz);
+          if (BORN) UB_.ref(cx, cz) = twoway_cell(Cb, Pb, Vv, g, cx, cz);
+        }
       }
+    };
+    if (x0 <= NX - 2) {
+      bands(CA, PA, VV, CB, PB);
+    } else {
+      const int ra = a.rot % 3, rb = a.rot_b % 3;
+      float *const *FA = MODE == MODE_RCV ? g.fb : g.fa;
+      const int rr = MODE == MODE_RCV ? rb : ra;
+      const GA GCa{FA[(rr + 1) % 3], g.LDZ}, GPa{FA[rr], g.LDZ}, GV{g.vel, g.LDZ};
+      const GA GCb{g.fb[(rb + 1) % 3], g.LDZ}, GPb{g.fb[rb], g.LDZ};
+      bands(GCa, GPa, GV, GCb, GPb);
     }
     __syncthreads();
   }
