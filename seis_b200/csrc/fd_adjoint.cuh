@@ -84,6 +84,39 @@ __device__ __forceinline__ float snap_inv_scale(const ShotDev &g, int k, int x0,
   return 1.0f / g.snap_scale[(size_t)k * ntx * g.ntz + (x0 / TX) * g.ntz + z0 / TZ];
 }
 
+// Imaging loads of one column quad (model column x, model rows z .. z+3, the
+// rows with bit r of `ok` set): the snapshot values and the accumulator, all
+// issued before the quad's arithmetic so that their latencies overlap; the
+// matching stores follow in image_store.
+struct ImageQuad {
+  float lap[4];
+  double acc[4];
+};
+__device__ __forceinline__ void image_load(const ShotDev &g, int k, int x, int z, unsigned ok,
+                                           ImageQuad &q) {
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    q.lap[r] = 0.0f;
+    q.acc[r] = 0.0;
+    if ((ok >> r) & 1u) {
+      q.lap[r] = snap_load(g, k, x, z + r);
+      q.acc[r] = g.grad[(size_t)x * g.nz + z + r];
+    }
+  }
+}
+// grad += w lap M1 on the quad's cells (the product rounded to float, then
+// accumulated in double)
+__device__ __forceinline__ void image_store(const ShotDev &g, int x, int z, unsigned ok,
+                                            const ImageQuad &q, float inv_scale, float w,
+                                            const float4 &m1) {
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+    if ((ok >> r) & 1u) {
+      const float lap = q.lap[r] * inv_scale;
+      g.grad[(size_t)x * g.nz + z + r] = q.acc[r] + (double)(w * lap * comp(m1, r));
+    }
+}
+
 // ---------------------------------------------------------------- interior
 // L_k = Lz(vz M1) + Lx(vx M1) + 2 M1 - M2 + R^T d ; grad += w lap M1.  On these
 // tiles M = L (no ring cell within one cell), so the staged arrays (named L1,
@@ -150,6 +183,8 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_I) adj_interior_kerne
     const float4 l1 = L1.quad(ix + j, iz0), l2 = L2.quad(ix + j, iz0);
     const int x = ix + j - g.pml;
     const int gzr = g.gz[x] + g.pml;
+    ImageQuad iq;
+    if (img) image_load(g, a.snap_k, x, iz0 - g.pml, 0xFu, iq);
     float4 o;
 #pragma unroll
     for (int r = 0; r < 4; r++) {
@@ -161,12 +196,8 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_I) adj_interior_kerne
       float v = sz_ + sx_ + 2.0f * comp(l1, r) - comp(l2, r);
       if (a.rec_k >= 0 && iz0 + r == gzr) v += g.rec[(size_t)a.rec_k * g.nx + x];
       set_comp(o, r, v);
-      if (img) {
-        const int z = iz0 + r - g.pml;
-        float lap = snap_load(g, a.snap_k, x, z) * inv_scale;
-        g.grad[(size_t)x * g.nz + z] += (double)(a.img_w * lap * comp(l1, r));
-      }
     }
+    if (img) image_store(g, x, iz0 - g.pml, 0xFu, iq, inv_scale, a.img_w, l1);
     *reinterpret_cast<float4 *>(out + (size_t)(ix + j) * g.LDZ + iz0) = o;
   }
 }
@@ -447,6 +478,14 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
       const float4 l1 = L1.quad(cx, iz0), l2 = L2.quad(cx, iz0);
       const int x = cx - g.pml;
       const int gzr = (x >= 0 && x < g.nx && cx < NX) ? g.gz[x] + g.pml : -1;
+      unsigned ok = 0;  // the quad's model cells
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const int z = iz0 + r - g.pml;
+        if (cx < NX && x >= 0 && x < g.nx && z >= 0 && z < g.nz) ok |= 1u << r;
+      }
+      ImageQuad iq;
+      if (img) image_load(g, a.snap_k, x, iz0 - g.pml, ok, iq);
 #pragma unroll
       for (int r = 0; r < 4; r++) {
         const int cz = iz0 + r;
@@ -460,12 +499,8 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
         v = v - comp(l2, r) + comp(e4[j], r);
         if (a.rec_k >= 0 && cz == gzr) v += g.rec[(size_t)a.rec_k * g.nx + x];
         Lt[4 * j + r] = v;
-        const int z = cz - g.pml;
-        if (img && cx < NX && x >= 0 && x < g.nx && z >= 0 && z < g.nz) {
-          const float lap = snap_load(g, a.snap_k, x, z) * inv_scale;
-          g.grad[(size_t)x * g.nz + z] += (double)(a.img_w * lap * comp(l1, r));
-        }
       }
+      if (img) image_store(g, x, iz0 - g.pml, ok, iq, inv_scale, a.img_w, l1);
     }
   }
   // L of the halo's pad cells (the only halo cells whose rho is read); halo
