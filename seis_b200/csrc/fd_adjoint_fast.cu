@@ -3,6 +3,7 @@
 // operator that the LSRTM solver applies, so it carries the same coefficient
 // rounding; it has no reference rounding to reproduce.
 #define SEIS_NS fast
+#define SEIS_FAST_MATH 1
 #include "fd_adjoint.cuh"
 
 namespace seis {

@@ -127,10 +127,15 @@ __device__ __forceinline__ PadPos pad_pos(const ShotDev &g, int ix, int iz) {
 }
 
 // Blend weight of a pad cell: the x ramp wins in the corners
-// (InitInversion.cpp:20-37).
+// (InitInversion.cpp:20-37).  The contracted build (SEIS_FAST_MATH)
+// multiplies by precomputed reciprocals where the reference divides.
 __device__ __forceinline__ float pad_weight(const ShotDev &g, const PadPos &p) {
   int d = p.distx > 0 ? p.distx : p.distz;
+#ifdef SEIS_FAST_MATH
+  return 1.0f - (float)d * g.inv_pml;
+#else
   return 1.0f - (float)d * 1.0f / (float)g.pml;
+#endif
 }
 
 // Absorbing blend of one cell with two-way value u3 (fd.cpp:1092-1179, blend
@@ -154,14 +159,24 @@ __device__ float absorb_cell(float u3, const U3A &U3, const A &cur, const A &P, 
     u31 = -tmp / (g.ax1 + g.ax2 + ax3);
   } else if (pp.distz == pp.ring) {  // top / bottom strip, inner along z
     int I = pp.du > 0 ? iz + 1 : iz - 1;
+#ifdef SEIS_FAST_MATH
+    float a2 = g.hdt2 * (1.0f / v);
+    float a3 = v * g.q4dx2;
+#else
     float a2 = g.hdt2 / v;
     float a3 = v / 4.0f / g.dx / g.dx;
+#endif
     u31 = oneway(g.a1z, a2, a3, U3(ix, I), U3(ix + 1, I), U3(ix - 1, I), cur(ix, iz),
                  cur(ix, I), P(ix, iz), P(ix, I), P(ix + 1, iz), P(ix - 1, iz));
   } else {  // left / right strip, inner along x
     int I = pp.dl > 0 ? ix + 1 : ix - 1;
+#ifdef SEIS_FAST_MATH
+    float a2 = g.hdt2 * (1.0f / v);
+    float a3 = v * g.q4dz2;
+#else
     float a2 = g.hdt2 / v;
     float a3 = v / 4.0f / g.dz / g.dz;
+#endif
     u31 = oneway(g.a1x, a2, a3, U3(I, iz), U3(I, iz + 1), U3(I, iz - 1), cur(ix, iz),
                  cur(I, iz), P(ix, iz), P(I, iz), P(ix, iz + 1), P(ix, iz - 1));
   }

@@ -224,6 +224,9 @@ void fill_scalars(ShotDev &g, const seis_shot_desc &s) {
   g.sqrt2f = std::sqrt(2.0f);
   g.sqrt2d = std::sqrt(2.0);
   g.idt2 = 1.0f / dt / dt;
+  g.q4dx2 = 1.0f / 4.0f / dx / dx;
+  g.q4dz2 = 1.0f / 4.0f / dz / dz;
+  g.inv_pml = s.pml > 0 ? 1.0f / (float)s.pml : 0.0f;
 }
 
 // Tiles of every shot's padded grid; interior tiles (every cell a model cell

@@ -103,6 +103,10 @@ struct ShotDev {
   // of a step, in two buffers used by alternate steps (this step's read, the
   // next step's written); the prev-ring terms kept for the step after next
   float *adj_e[2], *adj_b;
+  // reciprocals for the contracted build's absorbing formulas: 1/4/dx/dx,
+  // 1/4/dz/dz, 1/pml
+  float q4dx2, q4dz2, inv_pml;
+  int pad3_;
 };
 enum SnapType : int { SNAP_NONE = 0, SNAP_F32 = 1, SNAP_BF16 = 2, SNAP_F16 = 3 };
 static_assert(sizeof(ShotDev) % sizeof(int) == 0 && sizeof(ShotDev) <= 256 * sizeof(int),

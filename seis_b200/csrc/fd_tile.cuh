@@ -312,11 +312,16 @@ struct GA {
 // rectangle [rx0, rx1) x [rz0, rz1) (the model, or the model less its edge
 // cells), enumerated column by column, z fastest, so that the threads of a
 // CTA can share them evenly and consecutive threads touch consecutive rows.
+// Column indices come from a float reciprocal: for i < 2^13 and column
+// lengths of at most 128, (i + 0.5) / len lies at least 0.5 / len = 2^-8 from
+// an integer and the rounded product within 2^-10 of it, so its floor is the
+// integer quotient.
 struct CellList {
   int x0, z0, xe, ze;  // tile cells inside the grid: [x0, xe) x [z0, ze)
   int ma, mb;          // tile columns crossing the rectangle: [ma, mb)
   int top, bot;        // cells of such a column above / below the rectangle
   int cp, cm, n;       // cells per other column, per crossing column, in all
+  float rcp, rcm;      // 1 / cp, 1 / cm
   __device__ __forceinline__ CellList(int x0_, int z0_, int xe_, int ze_, int rx0, int rx1,
                                       int rz0, int rz1)
       : x0(x0_), z0(z0_), xe(xe_), ze(ze_) {
@@ -328,25 +333,33 @@ struct CellList {
     cp = ze - z0;
     cm = top + bot;
     n = (xe - x0 - (mb - ma)) * cp + (mb - ma) * cm;
+    rcp = cp > 0 ? 1.0f / (float)cp : 0.0f;
+    rcm = cm > 0 ? 1.0f / (float)cm : 0.0f;
+  }
+  static __device__ __forceinline__ int quot(int i, float r) {
+    return (int)(((float)i + 0.5f) * r);
   }
   __device__ __forceinline__ void cell(int i, int &cx, int &cz) const {
     const int na = (ma - x0) * cp;
     if (i < na) {
-      cx = x0 + i / cp;
-      cz = z0 + i % cp;
+      const int q = quot(i, rcp);
+      cx = x0 + q;
+      cz = z0 + (i - q * cp);
       return;
     }
     i -= na;
     const int nm = (mb - ma) * cm;
     if (i < nm) {
-      cx = ma + i / cm;
-      const int r = i % cm;
+      const int q = quot(i, rcm);
+      cx = ma + q;
+      const int r = i - q * cm;
       cz = r < top ? z0 + r : ze - bot + (r - top);
       return;
     }
     i -= nm;
-    cx = mb + i / cp;
-    cz = z0 + i % cp;
+    const int q = quot(i, rcp);
+    cx = mb + q;
+    cz = z0 + (i - q * cp);
   }
 };
 
