@@ -350,6 +350,16 @@ int encode_maps(Plan &p, std::vector<ShotDev> &sds, CUtensorMap **d_out) {
     if (!rc) rc = encode_map(p.ctx, g, g.vel, rows, narrow, &m[MAP_VEL]);
     if (!rc) rc = encode_map(p.ctx, g, g.vel, rows, wide, &m[MAP_VEL_WIDE]);
     if (!rc && g.dv) rc = encode_map(p.ctx, g, g.dv, rows, narrow, &m[MAP_DV]);
+    // interior tiles
+    const int TX = shape_tx(p.shape), TZ = shape_tz(p.shape);
+    for (int k = 0; k < 3 && !rc; k++) {
+      rc = encode_map(p.ctx, g, g.fa[k], TZ + 2 * HI, TX + 2 * HI, &m[MAP_FA_HALO + k]);
+      if (!rc) rc = encode_map(p.ctx, g, g.fa[k], TZ, TX, &m[MAP_FA_TILE + k]);
+      if (!rc && g.fb[k]) rc = encode_map(p.ctx, g, g.fb[k], TZ + 2 * HI, TX + 2 * HI, &m[MAP_FB_HALO + k]);
+      if (!rc && g.fb[k]) rc = encode_map(p.ctx, g, g.fb[k], TZ, TX, &m[MAP_FB_TILE + k]);
+    }
+    if (!rc) rc = encode_map(p.ctx, g, g.vel, TZ, TX, &m[MAP_VEL_TILE]);
+    if (!rc && g.dv) rc = encode_map(p.ctx, g, g.dv, TZ, TX, &m[MAP_DV_TILE]);
     if (rc) return rc;
   }
   int rc = p.alloc(d_out, maps.size());

@@ -30,6 +30,7 @@ constexpr int TX_MAX = 64;
 constexpr int TZ_MAX = 128;
 constexpr int HXC = 5;      // column halo of the current field (stencil radius 4 + 1)
 constexpr int ZM = 8;
+constexpr int HI = 4;       // interior tiles: column and row halo of the current field
 constexpr int XM = 16;
 constexpr int LAYERS = 4;   // boundary layers kept for reconstruction
 
@@ -45,8 +46,10 @@ struct Tile {
 
 // 2-D TMA tensor maps of one shot (each describes one margin-padded field
 // allocation, LDZ rows x ncols columns; box = staged rows x staged columns).
-// Wide boxes (TX + 2*HXC columns) stage a field read as "current"; narrow boxes
-// (TX + 2 columns) a field read as "previous", the velocity or dv.
+// Pad tiles: wide boxes (TX + 2*HXC columns, TZ + 2*ZM rows) stage a field read
+// as "current"; narrow boxes (TX + 2 columns) a field read as "previous", the
+// velocity or dv.  Interior tiles: the current field with an HI-cell halo on
+// every side, the other arrays as the tile alone.
 enum MapIndex : int {
   MAP_FA_WIDE = 0,    // + rotating buffer index 0..2
   MAP_FA_NARROW = 3,
@@ -55,7 +58,13 @@ enum MapIndex : int {
   MAP_VEL = 12,
   MAP_DV = 13,
   MAP_VEL_WIDE = 14,  // velocity with the wide halo (adjoint kernels)
-  NMAPS = 15,
+  MAP_FA_HALO = 15,   // interior tiles: (TX + 2 HI) x (TZ + 2 HI), + buffer index
+  MAP_FB_HALO = 18,
+  MAP_FA_TILE = 21,   // interior tiles: TX x TZ, + buffer index
+  MAP_FB_TILE = 24,
+  MAP_VEL_TILE = 27,
+  MAP_DV_TILE = 28,
+  NMAPS = 29,
 };
 
 // Device descriptor of one shot in a batch.  Scalars derived from dt/dx/dz are

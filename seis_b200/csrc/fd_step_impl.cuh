@@ -7,6 +7,14 @@ namespace seis {
 namespace SEIS_NS {
 
 namespace {
+// CTAs of the persistent interior kernel: as many as are resident at once
+template <int S, int MODE>
+struct LoopGrid {
+  static int ctas;
+};
+template <int S, int MODE>
+int LoopGrid<S, MODE>::ctas = 0;
+
 template <int S, int MODE>
 cudaError_t setup() {
   cudaError_t e = cudaFuncSetAttribute(tile_kernel<S, MODE>,
@@ -15,6 +23,17 @@ cudaError_t setup() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(pad_tile_kernel<S, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)PCfg<S, MODE>::bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(interior_loop_kernel<S, MODE>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)LCfg<S, MODE>::bytes);
+  int dev = 0, nsm = 0, per = 0;
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, interior_loop_kernel<S, MODE>,
+                                                      Geo<S>::NT, LCfg<S, MODE>::bytes);
+  if (e == cudaSuccess) LoopGrid<S, MODE>::ctas = (per > 0 ? per : 1) * nsm;
   return e;
 }
 
@@ -26,13 +45,17 @@ cudaError_t setup_shape() {
   return e;
 }
 
-// Interior tiles on s_int, pad tiles on s_pad (concurrently).
+// Interior tiles on s_int (persistent CTAs), pad tiles on s_pad (one CTA
+// each), concurrently.
 template <int S, int MODE>
 cudaError_t launch_t(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
                      const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad) {
   constexpr int NT = Geo<S>::NT;
-  if (n_int > 0)
-    tile_kernel<S, MODE><<<n_int, NT, TCfg<S, MODE>::bytes, s_int>>>(d_shots, d_tiles, a, d_err);
+  if (n_int > 0) {
+    const int g = LoopGrid<S, MODE>::ctas < n_int ? LoopGrid<S, MODE>::ctas : n_int;
+    interior_loop_kernel<S, MODE><<<g, NT, LCfg<S, MODE>::bytes, s_int>>>(d_shots, d_tiles, n_int,
+                                                                         a, d_err);
+  }
   if (n_pad > 0)
     pad_tile_kernel<S, MODE><<<n_pad, NT, PCfg<S, MODE>::bytes, s_pad>>>(d_shots, d_tiles + n_int,
                                                                        a, d_err);

@@ -132,8 +132,8 @@ __device__ __forceinline__ void set_comp(float4 &v, int r, float x) {
 // per column).
 template <int SR>
 struct SAT {
-  const float *s;  // staged column (x0 - halo) row (z0 - ZM)
-  int x0h, z0m;    // x0 - halo, z0 - ZM
+  const float *s;  // staged column x0h, row z0m
+  int x0h, z0m;    // first staged column and row (the tile's origin less the halo)
   __device__ __forceinline__ float operator()(int ix, int iz) const {
     return s[(ix - x0h) * SR + (iz - z0m)];
   }
@@ -192,8 +192,8 @@ __device__ __forceinline__ void save_strips(const ShotDev &g, int strip_k, int i
 
 // 8th-order two-way update of two columns x 4 rows from shared memory
 // (fd.cpp:1259-1270): u3 = vvzz uzz + vvxx uxx + 2 cur - prev.
-template <class SA>
-__device__ __forceinline__ void pair_twoway(const SA &C, const SA &P, const SA &V, const ShotDev &g,
+template <class SC, class SO>
+__device__ __forceinline__ void pair_twoway(const SC &C, const SO &P, const SO &V, const ShotDev &g,
                                             int ix, int iz0, float4 out[2], float4 cen[2],
                                             float4 prv[2], float4 vel[2]) {
   float4 xm[10];
@@ -434,51 +434,25 @@ __device__ __forceinline__ bool stage_tile(const ShotDev &g, const StepArgs &a, 
   return mbar_wait(bar, 0);
 }
 
-// Interior tiles: every cell a model cell in the 8th-order region, where the
-// absorbing blend is the identity (w = 1, u31 = 0; src/util/fd.cpp:55-56).
-template <int S, int MODE>
-__global__ void __launch_bounds__(Geo<S>::NT, TCfg<S, MODE>::MIN_CTAS) tile_kernel(
-    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
-    int *__restrict__ err) {
+// The cells of one interior tile (every cell a model cell in the 8th-order
+// region, where the absorbing blend is the identity: w = 1, u31 = 0;
+// src/util/fd.cpp:55-56) from its staged arrays: the current fields CA, CB
+// (with the stencil's halo), previous fields PA, PB, velocity VV and
+// perturbation DV; one 4-row x 2-column micro-tile per thread.  Every thread
+// of the CTA calls this (the snapshot holds block barriers).
+template <int S, int MODE, class SC, class SO>
+__device__ __forceinline__ void interior_cells(const ShotDev &g, const StepArgs &a, int x0, int z0,
+                                               const SC &CA, const SC &CB, const SO &PA,
+                                               const SO &VV, const SO &PB, const SO &DV,
+                                               float *red) {
   SEIS_GEO(S);
-  using SA = SAT<SR>;
-  using C = TCfg<S, MODE>;
-  constexpr bool BORN = C::BORN;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  float *bb = reinterpret_cast<float *>(smraw);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(bb + C::BUF);
-  __shared__ ShotDev sg;
-  __shared__ float red[33];
-  const int tid = threadIdx.x;
-  const Tile t = tiles[blockIdx.x];
-  if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
-    reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    fence_barrier_init();
-  }
-  __syncthreads();
-  const ShotDev &g = sg;
-  if (!stage_tile<S, MODE>(g, a, t.x0, t.z0, bb, bar)) {
-    if (tid == 0) atomicExch(err, 1);
-    return;
-  }
-  auto arr_off = [](int arr) -> int {
-    return arr < C::NCUR ? arr * CW_C * SR : C::NCUR * CW_C * SR + (arr - C::NCUR) * CW_P * SR;
-  };
+  constexpr bool BORN = MODE == MODE_BORN;
   StepArgs aa = a;
   if (MODE != MODE_RCV && aa.rec_k >= g.nt) aa.rec_k = -1;
   float *na = g.fa[(a.rot + 2) % 3];
   float *nb_ = g.fb[(a.rot_b + 2) % 3];
   float *out_a = MODE == MODE_RCV ? nb_ : na;
-  const int x0 = t.x0, z0 = t.z0;
-  const int zm = z0 - ZM;
-  const SA CA{bb + arr_off(0), x0 - HXC, zm};
-  const SA CB{bb + arr_off(BORN ? 1 : 0), x0 - HXC, zm};
-  const SA PA{bb + arr_off(C::NCUR), x0 - 1, zm};
-  const SA VV{bb + arr_off(C::NCUR + 1), x0 - 1, zm};
-  const SA PB{bb + arr_off(BORN ? C::NCUR + 2 : C::NCUR), x0 - 1, zm};
-  const SA DV{bb + arr_off(BORN ? C::NCUR + 3 : C::NCUR + 1), x0 - 1, zm};
+  const int tid = threadIdx.x;
   const int qz = tid % QZ, cx = tid / QZ;  // micro-tile: rows 4qz.., columns 2cx, 2cx+1
   const int ix = x0 + 2 * cx, iz0 = z0 + 4 * qz;
   const bool record = MODE != MODE_RCV && aa.rec_k >= 0;
@@ -541,6 +515,167 @@ __global__ void __launch_bounds__(Geo<S>::NT, TCfg<S, MODE>::MIN_CTAS) tile_kern
     }
   }
   if (snap) snap_write<NT_T, 8, TX, TZ>(g, aa.snap_k, x0, z0, lv, lx, lz, mask, red);
+}
+
+// Interior tiles, one per CTA (the tile list's first n_int tiles).
+template <int S, int MODE>
+__global__ void __launch_bounds__(Geo<S>::NT, TCfg<S, MODE>::MIN_CTAS) tile_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
+    int *__restrict__ err) {
+  SEIS_GEO(S);
+  using SA = SAT<SR>;
+  using C = TCfg<S, MODE>;
+  constexpr bool BORN = C::BORN;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float *bb = reinterpret_cast<float *>(smraw);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(bb + C::BUF);
+  __shared__ ShotDev sg;
+  __shared__ float red[33];
+  const int tid = threadIdx.x;
+  const Tile t = tiles[blockIdx.x];
+  if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+    reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const ShotDev &g = sg;
+  if (!stage_tile<S, MODE>(g, a, t.x0, t.z0, bb, bar)) {
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  auto arr_off = [](int arr) -> int {
+    return arr < C::NCUR ? arr * CW_C * SR : C::NCUR * CW_C * SR + (arr - C::NCUR) * CW_P * SR;
+  };
+  const int x0 = t.x0, z0 = t.z0, zm = z0 - ZM;
+  const SA CA{bb + arr_off(0), x0 - HXC, zm};
+  const SA CB{bb + arr_off(BORN ? 1 : 0), x0 - HXC, zm};
+  const SA PA{bb + arr_off(C::NCUR), x0 - 1, zm};
+  const SA VV{bb + arr_off(C::NCUR + 1), x0 - 1, zm};
+  const SA PB{bb + arr_off(BORN ? C::NCUR + 2 : C::NCUR), x0 - 1, zm};
+  const SA DV{bb + arr_off(BORN ? C::NCUR + 3 : C::NCUR + 1), x0 - 1, zm};
+  interior_cells<S, MODE>(g, a, x0, z0, CA, CB, PA, VV, PB, DV, red);
+}
+
+// Persistent interior kernel: CTA b of G takes the interior tiles b, b + G,
+// b + 2G, ... through two shared-memory stages, so that the tensor copies of
+// its next tile are in flight while the current one is computed.  The
+// current fields are staged with an HI-cell halo on every side, the other
+// arrays as the tile alone (interior cells read them at the cell only).
+template <int S, int MODE>
+struct LCfg {
+  using G = Geo<S>;
+  static constexpr bool BORN = MODE == MODE_BORN;
+  static constexpr int NCUR = BORN ? 2 : 1;  // current fields
+  static constexpr int NOTH = BORN ? 4 : 2;  // prev, vel [, prev B, dv]
+  static constexpr int CW = G::TX + 2 * HI, RW = G::TZ + 2 * HI;
+  static constexpr int TILE = G::TX * G::TZ;
+  static constexpr int STAGE = NCUR * CW * RW + NOTH * TILE;  // floats
+  static constexpr size_t bytes = 2 * sizeof(float) * (size_t)STAGE + 2 * sizeof(uint64_t);
+  // static shared memory: two shot tables and the snapshot reduction
+  static constexpr size_t static_bytes = 2 * sizeof(ShotDev) + 33 * sizeof(float);
+  // at most 512 threads per SM for Born's two fields (128 registers a
+  // thread), 1024 for one
+  static constexpr int CAP = (BORN ? 512 : 1024) / G::NT;
+  static constexpr int MIN_CTAS =
+      ctas_fit(bytes + static_bytes, CAP) > 0 ? ctas_fit(bytes + static_bytes, CAP) : 1;
+  static_assert((NCUR * CW * RW * sizeof(float)) % 128 == 0 && (TILE * sizeof(float)) % 128 == 0 &&
+                    (STAGE * sizeof(float)) % 128 == 0,
+                "tensor-copy destinations stay 128-byte aligned");
+};
+
+template <int S, int MODE>
+__global__ void __launch_bounds__(Geo<S>::NT, LCfg<S, MODE>::MIN_CTAS) interior_loop_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, int n, StepArgs a,
+    int *__restrict__ err) {
+  SEIS_GEO(S);
+  using L = LCfg<S, MODE>;
+  constexpr bool BORN = L::BORN;
+  constexpr int CW = L::CW, RW = L::RW, TILE = L::TILE;
+  using SW = SAT<RW>;  // current fields, HI-cell halo
+  using ST = SAT<TZ>;  // the other arrays, the tile alone
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float *stage0 = reinterpret_cast<float *>(smraw);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(stage0 + 2 * L::STAGE);
+  __shared__ ShotDev sg[2];
+  __shared__ float red[33];
+  const int tid = threadIdx.x;
+  int i = blockIdx.x;
+  if (i >= n) return;
+  auto load_shot = [&](int st, int ti) {
+    const int shot = tiles[ti].shot;
+    if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+      reinterpret_cast<int *>(&sg[st])[tid] = reinterpret_cast<const int *>(shots + shot)[tid];
+  };
+  // thread 0: the tensor copies of tile ti into stage st (row coordinates
+  // count from the allocation start, ZM rows above row 0; columns XM to the
+  // left of column 0)
+  auto issue = [&](int st, int ti) {
+    const Tile t = tiles[ti];
+    const CUtensorMap *maps = shots[t.shot].maps;
+    float *bb = stage0 + st * L::STAGE;
+    fence_proxy_async();
+    mbar_expect_tx(bar + st, (uint32_t)(L::STAGE * sizeof(float)));
+    const int ra = a.rot % 3, rca = (a.rot + 1) % 3, rb = a.rot_b % 3, rcb = (a.rot_b + 1) % 3;
+    int cur[2], oth[4];
+    if (MODE == MODE_RCV) {
+      cur[0] = MAP_FB_HALO + rcb; oth[0] = MAP_FB_TILE + rb; oth[1] = MAP_VEL_TILE;
+    } else if (!BORN) {
+      cur[0] = MAP_FA_HALO + rca; oth[0] = MAP_FA_TILE + ra; oth[1] = MAP_VEL_TILE;
+    } else {
+      cur[0] = MAP_FA_HALO + rca; cur[1] = MAP_FB_HALO + rcb;
+      oth[0] = MAP_FA_TILE + ra; oth[1] = MAP_VEL_TILE; oth[2] = MAP_FB_TILE + rb; oth[3] = MAP_DV_TILE;
+    }
+#pragma unroll
+    for (int c = 0; c < L::NCUR; c++)
+      tma_load_2d(bb + c * CW * RW, maps + cur[c], t.z0 + ZM - HI, t.x0 + XM - HI, bar + st);
+#pragma unroll
+    for (int o = 0; o < L::NOTH; o++)
+      tma_load_2d(bb + L::NCUR * CW * RW + o * TILE, maps + oth[o], t.z0 + ZM, t.x0 + XM, bar + st);
+  };
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+    fence_barrier_init();
+  }
+  load_shot(0, i);
+  __syncthreads();
+  if (tid == 0) issue(0, i);
+  uint32_t par = 0;  // bit st: parity of the next completion of stage st
+  int st = 0;
+  for (;;) {
+    const int next = i + (int)gridDim.x;
+    const bool more = next < n;
+    if (more) {  // the other stage was released at the end of the last tile
+      load_shot(st ^ 1, next);
+      if (tid == 0) issue(st ^ 1, next);
+    }
+    bool ok = mbar_wait(bar + st, (par >> st) & 1u);
+    par ^= 1u << st;
+    if (!__syncthreads_and(ok)) {
+      // the copies in flight into the other stage land before the CTA ends
+      if (tid == 0) {
+        atomicExch(err, 1);
+        if (more) mbar_wait(bar + (st ^ 1), (par >> (st ^ 1)) & 1u);
+      }
+      return;
+    }
+    const Tile t = tiles[i];
+    const float *bb = stage0 + st * L::STAGE;
+    const float *ob = bb + L::NCUR * CW * RW;
+    const SW CA{bb, t.x0 - HI, t.z0 - HI};
+    const SW CB{bb + (BORN ? CW * RW : 0), t.x0 - HI, t.z0 - HI};
+    const ST PA{ob, t.x0, t.z0};
+    const ST VV{ob + TILE, t.x0, t.z0};
+    const ST PB{ob + (BORN ? 2 : 0) * TILE, t.x0, t.z0};
+    const ST DV{ob + (BORN ? 3 : 1) * TILE, t.x0, t.z0};
+    interior_cells<S, MODE>(sg[st], a, t.x0, t.z0, CA, CB, PA, VV, PB, DV, red);
+    __syncthreads();  // stage st and its shot table are free for the tile after next
+    if (!more) break;
+    i = next;
+    st ^= 1;
+  }
 }
 
 // Pad tiles: tiles with a pad cell, a cell within 3 of the grid edge (frame,
@@ -759,11 +894,25 @@ __global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_tile_
   }
 
   // 3. the halo ring: the same two-way values, injection and scattering
-  // source (zero outside the grid, where nothing reads them)
+  // source, for the halo cells next to a pad cell of the tile (the one-way
+  // update reads its neighbours within one cell; zero elsewhere, where
+  // nothing reads them)
+  const int xe = min(x0 + TX, NX), ze = min(z0 + TZ, NZ);
+  auto tile_pad = [&](int cx, int cz) {
+    return cx >= x0 && cx < xe && cz >= z0 && cz < ze && !model(cx, cz);
+  };
   for (int i = tid; i < NHALO; i += NT_T) {
     int hx, hz;
     halo_cell<TX, TZ>(i, x0, z0, hx, hz);
-    if (hx < 0 || hz < 0 || hx >= NX || hz >= NZ) {
+    bool read = false;
+    if (i < 2 * (TX + 2)) {  // row above / below: the tile row next to it
+      const int zz = hz < z0 ? z0 : ze - 1;
+      read = tile_pad(hx - 1, zz) || tile_pad(hx, zz) || tile_pad(hx + 1, zz);
+    } else {  // column left / right
+      const int xx = hx < x0 ? x0 : xe - 1;
+      read = tile_pad(xx, hz - 1) || tile_pad(xx, hz) || tile_pad(xx, hz + 1);
+    }
+    if (!read || hx < 0 || hz < 0 || hx >= NX || hz >= NZ) {
       UA_.ref(hx, hz) = 0.0f;
       if (BORN) UB_.ref(hx, hz) = 0.0f;
       continue;

@@ -9,6 +9,8 @@ tests (tests/test_gpu_configs.py).
   Gaussian-smoothed background (sigma 10 cells), nt 4000 + 75, 20 Hz, source
   (368, 1), receivers at row 1 (fd.cpp:81-177), and the reference RTM of that
   Born gather (fd.cpp:592-719);
+* the same modeling and Born gathers from the restatement's double build
+  (FP64), to state every FP32 result's error against an FP64 run;
 * the dot-product test of the FP64 Born operator and its exact transpose
   (the C restatement's double build) on the same 737 x 240 shot with seeded
   N(0, 1) vectors m (737 x 240, rng seed 22) and d (737 x 4000, drawn next).
@@ -44,6 +46,11 @@ def sha(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()
 
 
+def rel(a, b) -> float:
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
 def dot_vectors(nx: int, nz: int, nt: int):
     rng = np.random.default_rng(22)
     m = rng.standard_normal((nx, nz)).astype(np.float32)
@@ -65,6 +72,11 @@ def main():
                c1_rec_norm=np.linalg.norm(rec1.astype(np.float64)),
                c1_rec_sub=rec1[::STEP_C1].copy())
     print(f"config 1 modeling {time.time() - t:.1f} s, max|rec| {np.abs(rec1).max():.4g}")
+    t = time.time()
+    rec1_64 = O.modeling(s1, wav1.astype(np.float64), c1.vel, prec="f64")
+    out.update(c1_rec_f64_sub=rec1_64[::STEP_C1].copy())
+    print(f"config 1 modeling FP64 {time.time() - t:.1f} s, reference vs FP64 "
+          f"{rel(rec1[::STEP_C1], rec1_64[::STEP_C1]):.3e}")
 
     t = time.time()
     c2 = synth.born_rtm_pair()
@@ -72,6 +84,11 @@ def main():
     wav2 = O.ricker(s2.dt, c2.fr, s2.ndel, s2.NT, impl="ref")
     born2 = O.born(s2, wav2, c2.vel0, c2.dv, impl="ref")
     print(f"config 2 Born {time.time() - t:.1f} s, max|born| {np.abs(born2).max():.4g}")
+    t = time.time()
+    born2_64 = O.born(s2, wav2.astype(np.float64), c2.vel0, c2.dv, prec="f64")
+    out.update(c2_born_f64_sub=born2_64[::STEP_BORN].copy())
+    print(f"config 2 Born FP64 {time.time() - t:.1f} s, reference vs FP64 "
+          f"{rel(born2[::STEP_BORN], born2_64[::STEP_BORN]):.3e}")
     t = time.time()
     img2 = O.rtm(s2, wav2, c2.vel0, born2, impl="ref")
     print(f"config 2 RTM {time.time() - t:.1f} s, max|img| {np.abs(img2).max():.4g}")

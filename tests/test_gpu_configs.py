@@ -10,13 +10,12 @@ made by tests/golden/make_config_golden.py from the compiled reference).
 
 Bar: the exact build (the one the single-shot calls run) equals the reference
 bit for bit (SHA-256 of the float32 output, and the stored subsample element
-by element).  The fast build (multiply-add contraction, approximate division;
-the LSRTM solver's Born operator) drifts from it as the run gets longer:
-within 1e-5 relative L2 up to about 1000 steps, 1.0e-4 for the 2100-step
-modeling and 2.4e-4 for the 4075-step Born run, with IEEE division instead of
-the approximate one just as large (3.6e-4 and 1.6e-4), so the drift is the
-rounding of the contracted multiply-adds accumulated over the run; it is
-gated at 2.5 times those figures."""
+by element).  The fast build (multiply-add contraction, approximate division
+and reciprocals; the LSRTM solver's Born operator) rounds differently, and
+every FP32 result is stated against the FP64 run of the same algorithm (the
+restatement's double build, stored with the fixture): the reference's own
+FP32 arithmetic is 1.2e-4 (modeling, 2100 steps) and 2.4e-4 (Born, 4075
+steps) from FP64, and the fast build must stay within three times that."""
 import hashlib
 import os
 
@@ -28,7 +27,7 @@ from seis_b200 import fd, synth
 from seis_b200._lib import IN_DV, IN_VEL, IN_WAVELET, OP_BORN, OP_MODELING, OUT_GATHER, Plan
 
 pytestmark = pytest.mark.gpu
-FAST_TOL = {1: 2.5e-4, 2: 6e-4}  # fast build vs reference, by configuration
+FAST_VS_REF_FP64 = 3.0  # fast build's FP64 error over the reference's
 STEP_C1, STEP_BORN, STEP_IMG = 16, 48, 8  # subsamples of the fixture
 
 
@@ -63,9 +62,11 @@ def test_config1_modeling_201x201(ctx, gold):
     assert np.array_equal(rec[::STEP_C1], gold["c1_rec_sub"])
     assert sha(rec) == str(gold["c1_rec_sha"])
     fast = run_fast(ctx, OP_MODELING, s, wav, c.vel)
-    err = rel_l2(fast, rec)
-    print(f"config 1 fast vs reference: rel L2 {err:.2e}")
-    assert err <= FAST_TOL[1]
+    f64 = gold["c1_rec_f64_sub"]
+    e_ref, e_fast = rel_l2(rec[::STEP_C1], f64), rel_l2(fast[::STEP_C1], f64)
+    print(f"config 1 vs FP64: reference {e_ref:.2e}, fast {e_fast:.2e}; "
+          f"fast vs reference {rel_l2(fast, rec):.2e}")
+    assert e_fast <= FAST_VS_REF_FP64 * e_ref
 
 
 @pytest.fixture(scope="module")
@@ -85,9 +86,11 @@ def test_config2_born_737x240(ctx, gold, config2):
     assert np.array_equal(born[::STEP_BORN], gold["c2_born_sub"])
     assert sha(born) == str(gold["c2_born_sha"])
     fast = run_fast(ctx, OP_BORN, c.shots[0], wav, c.vel0, c.dv)
-    err = rel_l2(fast, born)
-    print(f"config 2 Born fast vs reference: rel L2 {err:.2e}")
-    assert err <= FAST_TOL[2]
+    f64 = gold["c2_born_f64_sub"]
+    e_ref, e_fast = rel_l2(born[::STEP_BORN], f64), rel_l2(fast[::STEP_BORN], f64)
+    print(f"config 2 Born vs FP64: reference {e_ref:.2e}, fast {e_fast:.2e}; "
+          f"fast vs reference {rel_l2(fast, born):.2e}")
+    assert e_fast <= FAST_VS_REF_FP64 * e_ref
 
 
 def test_config2_rtm_737x240(ctx, gold, config2):

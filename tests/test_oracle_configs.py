@@ -25,6 +25,9 @@ def test_restatement_reproduces_config1_gather():
     assert sha(wav) == str(gold["c1_wav_sha"])
     rec = O.modeling(s, wav, c.vel)
     assert sha(rec) == str(gold["c1_rec_sha"])
+    # the FP64 gather the GPU tests state the FP32 errors against
+    rec64 = O.modeling(s, wav.astype(np.float64), c.vel, prec="f64")
+    assert np.array_equal(rec64[::16], gold["c1_rec_f64_sub"])
 
 
 def test_fp64_pair_is_a_transpose_on_the_737x240_grid():
