@@ -320,39 +320,48 @@ NCU_TRAFFIC_PER_CELL = {}
 
 
 def kernel_roofline(ctx, sv, iter_ms, launches_per_iter):
-    """Per-kernel CUDA-event durations of the Born and adjoint step kernels
-    (separate plans over the same shots, the two kernels of a step concurrent
-    as in a run), their share of one iteration, and the roofline of the
-    kernel with the largest share."""
-    from seis_b200._lib import IN_VEL, IN_WAVELET, OP_BORN, OP_BORN_ADJOINT, TILE_SHAPES, Plan
+    """Per-kernel CUDA-event durations of the step kernels of one iteration --
+    the Born step, the adjoint's reverse step and the source-field step it
+    recomputes per checkpoint segment -- on separate plans over the same
+    shots: every kernel timed alone (interior tiles, then pad tiles), and the
+    step as a run launches it (both kernels, concurrently).  Returns the row
+    of the kernel with the largest share of the iteration (alone-time x
+    launches), every row, and the autotuner's step times per tile shape."""
+    from seis_b200._lib import (IN_DV, IN_VEL, IN_WAVELET, OP_BORN, OP_BORN_ADJOINT, OP_MODELING,
+                                TILE_SHAPES, Plan)
     wav = sv.wavelet()
     rows, tuning = [], {}
-    for op, name in ((OP_BORN, "born"), (OP_BORN_ADJOINT, "adjoint")):
+    for op, name in ((OP_BORN, "born"), (OP_BORN_ADJOINT, "adjoint"), (OP_MODELING, "source")):
+        n = launches_per_iter.get(name, 0)
+        if not n:
+            continue
         with Plan(ctx, op, sv.shots) as p:
-            if op == OP_BORN:
-                p.set_exact(False)  # the solver's Born operator runs the fast build
+            if op != OP_BORN_ADJOINT:
+                p.set_exact(False)  # the solver's forward operators run the fast build
             for i in range(len(sv.shots)):
                 p.set(i, IN_VEL, sv.sub(sv.vel0, i))
                 p.set(i, IN_WAVELET, wav)
-            # the autotuner's step time of every tile shape on these shots (the
-            # solver's plans of the same signature use the same choice)
-            best, per_shape = p.autotune(steps=10, force=True)
-            tuning[name] = {"chosen": "%dx%d" % TILE_SHAPES[best],
-                            "step_ms": {"%dx%d" % TILE_SHAPES[k]: v
-                                        for k, v in enumerate(per_shape)}}
+                if op == OP_BORN:
+                    p.set(i, IN_DV, sv.sub(sv.dv, i))
+            if op != OP_MODELING:
+                # the autotuner's step time of every tile shape on these shots
+                # (the solver's plans of the same signature use the same choice)
+                best, per_shape = p.autotune(steps=10, force=True)
+                tuning[name] = {"chosen": "%dx%d" % TILE_SHAPES[best],
+                                "step_ms": {"%dx%d" % TILE_SHAPES[k]: v
+                                            for k, v in enumerate(per_shape)}}
             p.time_kernels(10)
             ms, by = p.time_kernels(100)
-        n = launches_per_iter[name]
         per_cell = 32.0 if op == OP_BORN else 16.0
         for k, kname in ((0, "interior"), (1, "pad")):
             kern = f"{name}_{kname}"
             tr = NCU_TRAFFIC_PER_CELL.get(kern)
             rows.append({"kernel": kern, "ms": ms[k], "bytes": by[k], "launches_per_iter": n,
                          "share": ms[k] * n / iter_ms, "GB_s": by[k] / (ms[k] * 1e6),
-                         "traffic": tr * by[k] / per_cell if tr else None})
+                         "traffic": tr * by[k] / per_cell if tr else None, "timed": "alone"})
         rows.append({"kernel": f"{name}_step", "ms": ms[2], "bytes": by[0] + by[1],
                      "launches_per_iter": n, "share": ms[2] * n / iter_ms,
-                     "GB_s": (by[0] + by[1]) / (ms[2] * 1e6)})
+                     "GB_s": (by[0] + by[1]) / (ms[2] * 1e6), "timed": "as run"})
     kern = [r for r in rows if not r["kernel"].endswith("_step")]
     top = max(kern, key=lambda r: r["ms"] * r["launches_per_iter"])
     return top, rows, tuning
@@ -562,7 +571,10 @@ def main():
         errors = image_errors(mine, img_mixed, img_plain)
 
     # ---- roofline of the kernel with the largest share
-    per_iter_launches = {"born": shots[0].NT, "adjoint": shots[0].NT + 1}
+    # per iteration: the Born steps, the reverse steps, and with checkpoints
+    # the source-field steps recomputed segment by segment
+    per_iter_launches = {"born": shots[0].NT, "adjoint": shots[0].NT + 1,
+                         "source": shots[0].NT if ck else 0}
     top, rows, tuning = kernel_roofline(ctx, sv, ms_per_step, per_iter_launches)
     hbm, src = peaks()
     ach = top["bytes"] / (top["ms"] * 1e-3) / 1e9

@@ -244,14 +244,16 @@ int64_t seis_fd_plan_device_bytes(const seis_fd_plan *plan);
  * level (relative L2 well below 1e-5) and the kernels issue fewer
  * instructions. */
 int seis_fd_plan_set_exact(seis_fd_plan *plan, int exact);
-/* Kernel timing: run `steps` time steps of the plan's propagation kernels
- * eagerly (outside the graph) with CUDA events around each launch on its own
- * stream, on the plan's current fields.  The interior-tile kernel and the
- * pad-tile kernel of a step run concurrently.  ms[0] = mean interior-kernel
- * duration, ms[1] = mean pad-kernel duration, ms[2] = mean step.  bytes[0] =
- * algorithmic bytes one interior launch moves (16 per field-update: read prev,
- * cur, velocity; write next), bytes[1] = same for the pad launch.  The plan's
- * fields are clobbered; the next run starts from its cleared state. */
+/* Kernel timing: run 2 x `steps` time steps of the plan's propagation kernels
+ * eagerly (outside the graph) on the plan's current fields: `steps` with the
+ * interior-tile kernel and the pad-tile kernel one after the other, each
+ * bracketed by CUDA events on its own stream, then `steps` as a run launches
+ * them (concurrently, on two streams).  ms[0] = mean interior-kernel
+ * duration, ms[1] = mean pad-kernel duration (each alone), ms[2] = mean step
+ * as run.  bytes[0] = algorithmic bytes one interior launch moves (16 per
+ * field-update: read prev, cur, velocity; write next), bytes[1] = same for the
+ * pad launch.  The plan's fields are clobbered; the next run starts from its
+ * cleared state. */
 int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double *bytes);
 
 /* Tile shapes of the step kernels (columns x rows of one CTA's tile; no

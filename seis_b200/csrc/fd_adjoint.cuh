@@ -202,6 +202,138 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_I) adj_interior_kerne
   }
 }
 
+// Persistent form of the interior kernel: CTA b of G takes the interior tiles
+// b, b + G, ... through two shared-memory stages (M1 and the velocity with an
+// HI-cell halo, M2 as the tile alone), the tensor copies of the next tile in
+// flight while the current one is computed.  vx M1 replaces the staged
+// velocity in place; vz M1 has its own array.
+template <int S>
+struct ALCfg {
+  using G = Geo<S>;
+  static constexpr int CW = G::TX + 2 * HI, RW = G::TZ + 2 * HI;
+  static constexpr int HALO = CW * RW, TILE = G::TX * G::TZ;
+  static constexpr int STAGE = 2 * HALO + TILE;  // M1, velocity, M2
+  static constexpr size_t bytes = sizeof(float) * (2 * (size_t)STAGE + HALO) + 2 * sizeof(uint64_t);
+  static constexpr size_t static_bytes = 2 * sizeof(ShotDev);
+  static constexpr int MIN_CTAS = ctas_fit(bytes + static_bytes, 768 / G::NT) > 0
+                                      ? ctas_fit(bytes + static_bytes, 768 / G::NT)
+                                      : 1;
+  static_assert((HALO * sizeof(float)) % 128 == 0 && (TILE * sizeof(float)) % 128 == 0,
+                "tensor-copy destinations stay 128-byte aligned");
+};
+
+template <int S>
+__global__ void __launch_bounds__(Geo<S>::NT, ALCfg<S>::MIN_CTAS) adj_interior_loop_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, int n, StepArgs a,
+    int *__restrict__ err) {
+  SEIS_AGEO(S);
+  using L = ALCfg<S>;
+  constexpr int CW = L::CW, RW = L::RW, HALO = L::HALO;
+  using SW = SAT<RW>;
+  using ST = SAT<TZ>;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float *stage0 = reinterpret_cast<float *>(smraw);
+  float *sWZ = stage0 + 2 * L::STAGE;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sWZ + HALO);
+  __shared__ ShotDev sg[2];
+  const int tid = threadIdx.x;
+  int i = blockIdx.x;
+  if (i >= n) return;
+  auto load_shot = [&](int st, int ti) {
+    const int shot = tiles[ti].shot;
+    if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+      reinterpret_cast<int *>(&sg[st])[tid] = reinterpret_cast<const int *>(shots + shot)[tid];
+  };
+  auto issue = [&](int st, int ti) {  // thread 0
+    const Tile t = tiles[ti];
+    const CUtensorMap *maps = shots[t.shot].maps;
+    float *bb = stage0 + st * L::STAGE;
+    fence_proxy_async();
+    mbar_expect_tx(bar + st, (uint32_t)(L::STAGE * sizeof(float)));
+    tma_load_2d(bb, maps + MAP_FA_HALO + (a.rot + 1) % 3, t.z0 + ZM - HI, t.x0 + XM - HI, bar + st);
+    tma_load_2d(bb + HALO, maps + MAP_VEL_HALO, t.z0 + ZM - HI, t.x0 + XM - HI, bar + st);
+    tma_load_2d(bb + 2 * HALO, maps + MAP_FA_TILE + a.rot % 3, t.z0 + ZM, t.x0 + XM, bar + st);
+  };
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+    fence_barrier_init();
+  }
+  load_shot(0, i);
+  __syncthreads();
+  if (tid == 0) issue(0, i);
+  uint32_t par = 0;
+  int st = 0;
+  const int qz = tid % QZ, cx = tid / QZ;
+  for (;;) {
+    const int next = i + (int)gridDim.x;
+    const bool more = next < n;
+    if (more) {
+      load_shot(st ^ 1, next);
+      if (tid == 0) issue(st ^ 1, next);
+    }
+    bool ok = mbar_wait(bar + st, (par >> st) & 1u);
+    par ^= 1u << st;
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) {
+        atomicExch(err, 2);
+        if (more) mbar_wait(bar + (st ^ 1), (par >> (st ^ 1)) & 1u);
+      }
+      return;
+    }
+    const ShotDev &g = sg[st];
+    const Tile t = tiles[i];
+    const int x0 = t.x0, z0 = t.z0;
+    float *sL1 = stage0 + st * L::STAGE, *sWX = sL1 + HALO;
+    const float *sL2 = sL1 + 2 * HALO;
+    for (int k = tid; k < HALO; k += A_NT_I) {  // vx M1 over the velocity, vz M1
+      const Coef c = coef(sWX[k], g);
+      const float l = sL1[k];
+      sWZ[k] = c.vz * l;
+      sWX[k] = c.vx * l;
+    }
+    __syncthreads();
+    const SW L1{sL1, x0 - HI, z0 - HI}, WZ{sWZ, x0 - HI, z0 - HI}, WX{sWX, x0 - HI, z0 - HI};
+    const ST L2{sL2, x0, z0};
+    const int ix = x0 + 2 * cx, iz0 = z0 + 4 * qz;
+    float *out = g.fa[(a.rot + 2) % 3];
+    float4 xm[10];
+#pragma unroll
+    for (int m = 0; m < 10; m++) xm[m] = WX.quad(ix - 4 + m, iz0);
+    const bool img = a.snap_k >= 0 && g.snap != nullptr;
+    const float inv_scale = img ? snap_inv_scale<TX, TZ>(g, a.snap_k, x0, z0) : 0.0f;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const float4 za = WZ.quad(ix + j, iz0 - 4), zb = WZ.quad(ix + j, iz0),
+                   zc = WZ.quad(ix + j, iz0 + 4);
+      const float zz[12] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w, zc.x, zc.y, zc.z, zc.w};
+      const float4 l1 = L1.quad(ix + j, iz0), l2 = L2.quad(ix + j, iz0);
+      const int x = ix + j - g.pml;
+      const int gzr = g.gz[x] + g.pml;
+      ImageQuad iq;
+      if (img) image_load(g, a.snap_k, x, iz0 - g.pml, 0xFu, iq);
+      float4 o;
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        float sz_ = lap8(zz[r], zz[r + 1], zz[r + 2], zz[r + 3], zz[r + 4], zz[r + 5], zz[r + 6],
+                         zz[r + 7], zz[r + 8]);
+        float sx_ = lap8(comp(xm[j], r), comp(xm[j + 1], r), comp(xm[j + 2], r),
+                         comp(xm[j + 3], r), comp(xm[j + 4], r), comp(xm[j + 5], r),
+                         comp(xm[j + 6], r), comp(xm[j + 7], r), comp(xm[j + 8], r));
+        float v = sz_ + sx_ + 2.0f * comp(l1, r) - comp(l2, r);
+        if (a.rec_k >= 0 && iz0 + r == gzr) v += g.rec[(size_t)a.rec_k * g.nx + x];
+        set_comp(o, r, v);
+      }
+      if (img) image_store(g, x, iz0 - g.pml, 0xFu, iq, inv_scale, a.img_w, l1);
+      *reinterpret_cast<float4 *>(out + (size_t)(ix + j) * g.LDZ + iz0) = o;
+    }
+    __syncthreads();  // stage st, vz M1 and the shot table are free
+    if (!more) break;
+    i = next;
+    st ^= 1;
+  }
+}
+
 // 8th-order weight of offset m (|m| <= 4), fd.cpp:1245-1253
 __device__ __forceinline__ float tap8(int m) {
   m = m < 0 ? -m : m;

@@ -10,6 +10,14 @@ namespace seis {
 namespace fast {
 
 namespace {
+// CTAs of the persistent interior kernel: as many as are resident at once
+template <int S>
+struct AdjLoopGrid {
+  static int ctas;
+};
+template <int S>
+int AdjLoopGrid<S>::ctas = 0;
+
 template <int S>
 cudaError_t setup_adjoint() {
   cudaError_t e = cudaFuncSetAttribute(adj_interior_kernel<S>,
@@ -18,6 +26,16 @@ cudaError_t setup_adjoint() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(adj_pad_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)AGeo<S>::PAD_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(adj_interior_loop_kernel<S>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ALCfg<S>::bytes);
+  int dev = 0, nsm = 0, per = 0;
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, adj_interior_loop_kernel<S>,
+                                                      Geo<S>::NT, ALCfg<S>::bytes);
+  if (e == cudaSuccess) AdjLoopGrid<S>::ctas = (per > 0 ? per : 1) * nsm;
   return e;
 }
 
@@ -25,8 +43,11 @@ template <int S>
 cudaError_t launch_adj(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
                        const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad) {
   constexpr int NT = Geo<S>::NT;
-  if (n_int > 0)
-    adj_interior_kernel<S><<<n_int, NT, AGeo<S>::TILE_SMEM, s_int>>>(d_shots, d_tiles, a, d_err);
+  if (n_int > 0) {
+    const int g = AdjLoopGrid<S>::ctas < n_int ? AdjLoopGrid<S>::ctas : n_int;
+    adj_interior_loop_kernel<S><<<g, NT, ALCfg<S>::bytes, s_int>>>(d_shots, d_tiles, n_int, a,
+                                                                   d_err);
+  }
   if (n_pad > 0)
     adj_pad_kernel<S><<<n_pad, NT, AGeo<S>::PAD_SMEM, s_pad>>>(d_shots, d_tiles + n_int, a,
                                                                 d_err);

@@ -359,6 +359,7 @@ int encode_maps(Plan &p, std::vector<ShotDev> &sds, CUtensorMap **d_out) {
       if (!rc && g.fb[k]) rc = encode_map(p.ctx, g, g.fb[k], TZ, TX, &m[MAP_FB_TILE + k]);
     }
     if (!rc) rc = encode_map(p.ctx, g, g.vel, TZ, TX, &m[MAP_VEL_TILE]);
+    if (!rc) rc = encode_map(p.ctx, g, g.vel, TZ + 2 * HI, TX + 2 * HI, &m[MAP_VEL_HALO]);
     if (!rc && g.dv) rc = encode_map(p.ctx, g, g.dv, TZ, TX, &m[MAP_DV_TILE]);
     if (rc) return rc;
   }
@@ -1270,12 +1271,14 @@ int64_t seis_fd_plan_launches_per_run(const seis_fd_plan *plan) {
 }
 
 namespace {
-// `steps` time steps of the plan's step kernels (forward plans: the operator's
-// step; adjoint plans: the reverse step without imaging), the interior kernel
-// on the main stream and the pad kernel on the auxiliary one, concurrently,
-// each bracketed by CUDA events on its own stream.  ms = mean interior, pad
-// and whole-step milliseconds; bytes = algorithmic bytes of the interior and
-// pad tiles (16 per field cell-update).  The fields are cleared afterwards.
+// 2 x `steps` time steps of the plan's step kernels (forward plans: the
+// operator's step; adjoint plans: the reverse step without imaging): first
+// the interior and the pad kernel one after the other, each bracketed by CUDA
+// events on its own stream, then `steps` steps as a run launches them (the
+// two concurrently).  ms = mean interior and pad kernel milliseconds (each
+// alone) and mean step milliseconds (as run); bytes = algorithmic bytes of
+// the interior and pad tiles (16 per field cell-update).  The fields are
+// cleared afterwards.
 int time_steps(Plan &p, int steps, double *ms, double *bytes) {
   seis_fd_ctx *ctx = p.ctx;
   const int TX = shape_tx(p.shape), TZ = shape_tz(p.shape);
@@ -1297,36 +1300,47 @@ int time_steps(Plan &p, int steps, double *ms, double *bytes) {
   StepArgs a{};
   a.nshots = p.nshot;
   a.strip_k = -1;
+  // the interior and the pad kernel of a step on the main / auxiliary stream
+  auto launch = [&](int ni, int np) -> cudaError_t {
+    return adj ? fast::launch_adjoint(p.shape, p.d_sd, d_tl, ni, np, a, ctx->d_err, ctx->stream,
+                                      ctx->aux)
+               : launch_step(mode, p.exact, p.d_sd, d_tl, ni, np, p.shape, a, ctx->d_err,
+                             ctx->stream, ctx->aux);
+  };
   double t_int = 0, t_pad = 0, t_step = 0;
-  for (int k = 0; k < steps; k++) {
+  for (int k = 0; k < 2 * steps; k++) {
+    const bool alone = k < steps;  // first each kernel alone, then the step as it runs
     a.rot = k; a.rot_b = k;
     int it = k % p.NT;
     a.src_k = it >= 1 ? it - 1 : -1;
     a.rec_k = it - p.ndel >= 0 && p.op != OP_RTM && !adj ? it - p.ndel : -1;
     CK(cudaEventRecord(ev[0], ctx->stream));
-    CK(cudaStreamWaitEvent(ctx->aux, ev[0], 0));
-    CK(cudaEventRecord(ev[2], ctx->aux));
-    if (adj) {
-      CK(fast::launch_adjoint(p.shape, p.d_sd, d_tl, n_int, 0, a, ctx->d_err, ctx->stream,
-                              ctx->aux));
-      CK(fast::launch_adjoint(p.shape, p.d_sd, d_tl + n_int, 0, n_pad, a, ctx->d_err,
-                              ctx->stream, ctx->aux));
+    if (alone) {
+      CK(launch(n_int, 0));
+      CK(cudaEventRecord(ev[1], ctx->stream));
+      CK(cudaEventRecord(ev[2], ctx->stream));
+      CK(cudaStreamWaitEvent(ctx->aux, ev[2], 0));
+      CK(launch(0, n_pad));
+      CK(cudaEventRecord(ev[3], ctx->aux));
+      CK(cudaStreamWaitEvent(ctx->stream, ev[3], 0));
     } else {
-      CK(launch_step(mode, p.exact, p.d_sd, d_tl, n_int, 0, p.shape, a, ctx->d_err, ctx->stream,
-                     ctx->aux));
-      CK(launch_step(mode, p.exact, p.d_sd, d_tl + n_int, 0, n_pad, p.shape, a, ctx->d_err,
-                     ctx->stream, ctx->aux));
+      CK(cudaStreamWaitEvent(ctx->aux, ev[0], 0));
+      CK(launch(n_int, n_pad));
+      CK(cudaEventRecord(ev[3], ctx->aux));
+      CK(cudaStreamWaitEvent(ctx->stream, ev[3], 0));
     }
-    CK(cudaEventRecord(ev[1], ctx->stream));
-    CK(cudaEventRecord(ev[3], ctx->aux));
-    CK(cudaStreamWaitEvent(ctx->stream, ev[3], 0));
     CK(cudaEventRecord(ev[4], ctx->stream));
     CK(cudaEventSynchronize(ev[4]));
-    float a1 = 0, a2 = 0, a3 = 0;
-    CK(cudaEventElapsedTime(&a1, ev[0], ev[1]));
-    CK(cudaEventElapsedTime(&a2, ev[2], ev[3]));
-    CK(cudaEventElapsedTime(&a3, ev[0], ev[4]));
-    t_int += a1; t_pad += a2; t_step += a3;
+    if (alone) {
+      float a1 = 0, a2 = 0;
+      CK(cudaEventElapsedTime(&a1, ev[0], ev[1]));
+      CK(cudaEventElapsedTime(&a2, ev[2], ev[3]));
+      t_int += a1; t_pad += a2;
+    } else {
+      float a3 = 0;
+      CK(cudaEventElapsedTime(&a3, ev[0], ev[4]));
+      t_step += a3;
+    }
     ctx->launches += 2;
   }
   for (auto &e : ev) cudaEventDestroy(e);

@@ -64,7 +64,8 @@ enum MapIndex : int {
   MAP_FB_TILE = 24,
   MAP_VEL_TILE = 27,
   MAP_DV_TILE = 28,
-  NMAPS = 29,
+  MAP_VEL_HALO = 29,  // interior tiles of the adjoint: velocity with the HI-cell halo
+  NMAPS = 30,
 };
 
 // Device descriptor of one shot in a batch.  Scalars derived from dt/dx/dz are
