@@ -271,13 +271,29 @@ int seis_fd_plan_time_kernels(seis_fd_plan *plan, int steps, double *ms, double 
 int seis_fd_plan_set_tile_shape(seis_fd_plan *plan, int shape);
 /* The plan's tile shape, or SEIS_ERR_ARG. */
 int seis_fd_plan_tile_shape(const seis_fd_plan *plan);
+/* Launch form of a step (flags; results are identical in every form):
+ * SEIS_LAUNCH_OVERLAP: the interior-tile and the pad-tile kernel concurrently
+ * on two streams (else one after the other on the context's stream);
+ * SEIS_LAUNCH_PERSISTENT: interior tiles by the persistent kernel (as many
+ * CTAs as are resident at once, each taking every G-th tile through two
+ * shared-memory stages); SEIS_LAUNCH_PER_TILE: one interior tile per CTA;
+ * neither: the persistent kernel when each of its CTAs gets at least 4 tiles
+ * (the default, flags 0). */
+#define SEIS_LAUNCH_OVERLAP 1
+#define SEIS_LAUNCH_PERSISTENT 2
+#define SEIS_LAUNCH_PER_TILE 4
+int seis_fd_plan_set_launch(seis_fd_plan *plan, int flags);
+/* The plan's launch flags, or SEIS_ERR_ARG. */
+int seis_fd_plan_launch(const seis_fd_plan *plan);
 /* Autotuner: time `steps` steps of the plan's own kernels (as
  * seis_fd_plan_time_kernels, on its current inputs) in every tile shape and
- * keep the fastest.  The choice is cached in the process per plan signature
- * (operator, build flavour, every shot's padded grid) and reused by later
- * plans of the same signature unless `force` is set.  h_ms[SEIS_TILE_SHAPES]
- * (may be null) receives each shape's mean step time (0 where not timed),
- * *h_best (may be null) the shape kept.  The plan's fields are clobbered. */
+ * launch form (one tile per CTA or persistent, one after the other or
+ * overlapped), and keep the fastest.  The choice is cached in the
+ * process per plan signature (operator, build flavour, every shot's padded
+ * grid) and reused by later plans of the same signature unless `force` is
+ * set.  h_ms[SEIS_TILE_SHAPES] (may be null) receives each shape's shortest
+ * mean step time (0 where not timed), *h_best (may be null) the shape kept.
+ * The plan's fields are clobbered. */
 int seis_fd_plan_autotune(seis_fd_plan *plan, int steps, int force, double *h_ms, int *h_best);
 
 /* Batched forms of the single-shot calls: h_*[i] are the arrays of shot i. */

@@ -123,6 +123,8 @@ def lib():
                                                 ctypes.POINTER(ctypes.c_double)]
         L.seis_fd_plan_set_tile_shape.argtypes = [P, I]
         L.seis_fd_plan_tile_shape.argtypes = [P]
+        L.seis_fd_plan_set_launch.argtypes = [P, I]
+        L.seis_fd_plan_launch.argtypes = [P]
         L.seis_fd_plan_autotune.argtypes = [P, I, I, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_int)]
         PP = ctypes.POINTER(P)
@@ -232,6 +234,7 @@ def validate_shot(shot: "Shot") -> str:
  OP_RTM_TRUE, OP_RTM_UPDOWN, OP_ILLUM_PLANE) = range(10)
 SNAP_F32, SNAP_BF16, SNAP_F16 = 1, 2, 3
 # tile shapes of the step kernels (include/seis_fd.h SEIS_TILE_*)
+LAUNCH_OVERLAP, LAUNCH_PERSISTENT, LAUNCH_PER_TILE = 1, 2, 4  # include/seis_fd.h SEIS_LAUNCH_*
 TILE_32x64, TILE_64x32, TILE_16x128, TILE_64x64, TILE_32x32 = range(5)
 TILE_SHAPES = {TILE_32x64: (32, 64), TILE_64x32: (64, 32), TILE_16x128: (16, 128),
                TILE_64x64: (64, 64), TILE_32x32: (32, 32)}
@@ -304,8 +307,18 @@ class Plan:
     def tile_shape(self) -> int:
         return int(self.ctx.L.seis_fd_plan_tile_shape(self.h))
 
+    def set_launch(self, flags: int):
+        """LAUNCH_* flags (include/seis_fd.h): overlap the interior and pad
+        kernels of a step; persistent or one-tile-per-CTA interior kernel."""
+        self.ctx.check(self.ctx.L.seis_fd_plan_set_launch(self.h, flags))
+
+    @property
+    def launch(self) -> int:
+        return int(self.ctx.L.seis_fd_plan_launch(self.h))
+
     def autotune(self, steps: int = 10, force: bool = False):
-        """(chosen shape, mean step ms of every shape; 0 where not timed)."""
+        """(chosen shape, shortest mean step ms of every shape over the launch
+        forms; 0 where not timed).  The launch form kept is `launch`."""
         ms = (ctypes.c_double * len(TILE_SHAPES))()
         best = ctypes.c_int()
         self.ctx.check(self.ctx.L.seis_fd_plan_autotune(self.h, steps, 1 if force else 0, ms,

@@ -236,6 +236,8 @@ __global__ void __launch_bounds__(Geo<S>::NT, ALCfg<S>::MIN_CTAS) adj_interior_l
   float *sWZ = stage0 + 2 * L::STAGE;
   uint64_t *bar = reinterpret_cast<uint64_t *>(sWZ + HALO);
   __shared__ ShotDev sg[2];
+  __shared__ int2 sxz[2];  // tile origin of each stage
+  __shared__ int s_fail;
   const int tid = threadIdx.x;
   int i = blockIdx.x;
   if (i >= n) return;
@@ -246,6 +248,7 @@ __global__ void __launch_bounds__(Geo<S>::NT, ALCfg<S>::MIN_CTAS) adj_interior_l
   };
   auto issue = [&](int st, int ti) {  // thread 0
     const Tile t = tiles[ti];
+    sxz[st] = make_int2(t.x0, t.z0);
     const CUtensorMap *maps = shots[t.shot].maps;
     float *bb = stage0 + st * L::STAGE;
     fence_proxy_async();
@@ -258,10 +261,12 @@ __global__ void __launch_bounds__(Geo<S>::NT, ALCfg<S>::MIN_CTAS) adj_interior_l
     mbar_init(bar, 1);
     mbar_init(bar + 1, 1);
     fence_barrier_init();
+    s_fail = 0;
   }
   load_shot(0, i);
   __syncthreads();
   if (tid == 0) issue(0, i);
+  __syncthreads();  // the first tile's origin
   uint32_t par = 0;
   int st = 0;
   const int qz = tid % QZ, cx = tid / QZ;
@@ -272,18 +277,18 @@ __global__ void __launch_bounds__(Geo<S>::NT, ALCfg<S>::MIN_CTAS) adj_interior_l
       load_shot(st ^ 1, next);
       if (tid == 0) issue(st ^ 1, next);
     }
-    bool ok = mbar_wait(bar + st, (par >> st) & 1u);
-    par ^= 1u << st;
-    if (!__syncthreads_and(ok)) {
-      if (tid == 0) {
-        atomicExch(err, 2);
-        if (more) mbar_wait(bar + (st ^ 1), (par >> (st ^ 1)) & 1u);
-      }
-      return;
-    }
+    // this tile's receiver rows and snapshot scale, loaded while its copies
+    // land
     const ShotDev &g = sg[st];
-    const Tile t = tiles[i];
-    const int x0 = t.x0, z0 = t.z0;
+    const int x0 = sxz[st].x, z0 = sxz[st].y;
+    const int ix = x0 + 2 * cx, iz0 = z0 + 4 * qz;
+    const int gzr[2] = {g.gz[ix - g.pml] + g.pml, g.gz[ix + 1 - g.pml] + g.pml};
+    const bool img = a.snap_k >= 0 && g.snap != nullptr;
+    const float inv_scale = img ? snap_inv_scale<TX, TZ>(g, a.snap_k, x0, z0) : 0.0f;
+    // a wait that gives up leaves garbage in the stage (indices stay in
+    // range); the CTA then ends after this tile
+    if (!mbar_wait(bar + st, (par >> st) & 1u)) s_fail = 1;
+    par ^= 1u << st;
     float *sL1 = stage0 + st * L::STAGE, *sWX = sL1 + HALO;
     const float *sL2 = sL1 + 2 * HALO;
     for (int k = tid; k < HALO; k += A_NT_I) {  // vx M1 over the velocity, vz M1
@@ -295,13 +300,10 @@ __global__ void __launch_bounds__(Geo<S>::NT, ALCfg<S>::MIN_CTAS) adj_interior_l
     __syncthreads();
     const SW L1{sL1, x0 - HI, z0 - HI}, WZ{sWZ, x0 - HI, z0 - HI}, WX{sWX, x0 - HI, z0 - HI};
     const ST L2{sL2, x0, z0};
-    const int ix = x0 + 2 * cx, iz0 = z0 + 4 * qz;
     float *out = g.fa[(a.rot + 2) % 3];
     float4 xm[10];
 #pragma unroll
     for (int m = 0; m < 10; m++) xm[m] = WX.quad(ix - 4 + m, iz0);
-    const bool img = a.snap_k >= 0 && g.snap != nullptr;
-    const float inv_scale = img ? snap_inv_scale<TX, TZ>(g, a.snap_k, x0, z0) : 0.0f;
 #pragma unroll
     for (int j = 0; j < 2; j++) {
       const float4 za = WZ.quad(ix + j, iz0 - 4), zb = WZ.quad(ix + j, iz0),
@@ -309,7 +311,6 @@ __global__ void __launch_bounds__(Geo<S>::NT, ALCfg<S>::MIN_CTAS) adj_interior_l
       const float zz[12] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w, zc.x, zc.y, zc.z, zc.w};
       const float4 l1 = L1.quad(ix + j, iz0), l2 = L2.quad(ix + j, iz0);
       const int x = ix + j - g.pml;
-      const int gzr = g.gz[x] + g.pml;
       ImageQuad iq;
       if (img) image_load(g, a.snap_k, x, iz0 - g.pml, 0xFu, iq);
       float4 o;
@@ -321,13 +322,20 @@ __global__ void __launch_bounds__(Geo<S>::NT, ALCfg<S>::MIN_CTAS) adj_interior_l
                          comp(xm[j + 3], r), comp(xm[j + 4], r), comp(xm[j + 5], r),
                          comp(xm[j + 6], r), comp(xm[j + 7], r), comp(xm[j + 8], r));
         float v = sz_ + sx_ + 2.0f * comp(l1, r) - comp(l2, r);
-        if (a.rec_k >= 0 && iz0 + r == gzr) v += g.rec[(size_t)a.rec_k * g.nx + x];
+        if (a.rec_k >= 0 && iz0 + r == gzr[j]) v += g.rec[(size_t)a.rec_k * g.nx + x];
         set_comp(o, r, v);
       }
       if (img) image_store(g, x, iz0 - g.pml, 0xFu, iq, inv_scale, a.img_w, l1);
       *reinterpret_cast<float4 *>(out + (size_t)(ix + j) * g.LDZ + iz0) = o;
     }
-    __syncthreads();  // stage st, vz M1 and the shot table are free
+    __syncthreads();  // stage st, vz M1, its origin and shot table are free
+    if (s_fail) {
+      if (tid == 0) {
+        atomicExch(err, 2);
+        if (more) mbar_wait(bar + (st ^ 1), (par >> (st ^ 1)) & 1u);
+      }
+      return;
+    }
     if (!more) break;
     i = next;
     st ^= 1;

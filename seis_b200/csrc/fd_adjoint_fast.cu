@@ -43,10 +43,14 @@ template <int S>
 cudaError_t launch_adj(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
                        const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad) {
   constexpr int NT = Geo<S>::NT;
-  if (n_int > 0) {
-    const int g = AdjLoopGrid<S>::ctas < n_int ? AdjLoopGrid<S>::ctas : n_int;
-    adj_interior_loop_kernel<S><<<g, NT, ALCfg<S>::bytes, s_int>>>(d_shots, d_tiles, n_int, a,
-                                                                   d_err);
+  // the persistent interior kernel as a.loop says; by default when every CTA
+  // gets at least 4 tiles (as the forward step)
+  const int G = AdjLoopGrid<S>::ctas;
+  if (n_int > 0 && (a.loop > 0 || (a.loop < 0 && n_int >= 4 * G))) {
+    adj_interior_loop_kernel<S><<<G < n_int ? G : n_int, NT, ALCfg<S>::bytes, s_int>>>(
+        d_shots, d_tiles, n_int, a, d_err);
+  } else if (n_int > 0) {
+    adj_interior_kernel<S><<<n_int, NT, AGeo<S>::TILE_SMEM, s_int>>>(d_shots, d_tiles, a, d_err);
   }
   if (n_pad > 0)
     adj_pad_kernel<S><<<n_pad, NT, AGeo<S>::PAD_SMEM, s_pad>>>(d_shots, d_tiles + n_int, a,

@@ -142,6 +142,10 @@ struct Plan {
   CUtensorMap *d_maps_h = nullptr;
   bool exact = true;
   int shape = SHAPE_32x64;   // tile shape of every kernel of the plan (TileShapeId)
+  // the interior and pad kernels of a step on two streams, concurrently
+  // (else one after the other on the main stream)
+  bool overlap = false;
+  int loop = -1;  // interior kernel form (StepArgs::loop)
   std::vector<void *> allocs;
   std::vector<size_t> alloc_bytes;
   ShotDev *d_sd = nullptr;
@@ -537,14 +541,22 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
 
 // One time step of every shot: the interior-tile kernel on the main stream and
 // the pad-tile kernel on the auxiliary stream, joined before the next step.
-int step(Plan &p, int mode, const StepArgs &a, const ShotDev *shots = nullptr) {
+int step(Plan &p, int mode, const StepArgs &a0, const ShotDev *shots = nullptr) {
   seis_fd_ctx *ctx = p.ctx;
-  CK(cudaEventRecord(ctx->fork, ctx->stream));
-  CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
+  StepArgs a = a0;
+  a.loop = p.loop;
+  cudaStream_t s_pad = ctx->stream;
+  if (p.overlap) {
+    CK(cudaEventRecord(ctx->fork, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
+    s_pad = ctx->aux;
+  }
   CK(launch_step(mode, p.exact, shots ? shots : p.d_sd, p.d_tiles, p.n_int, p.n_pad, p.shape, a,
-                 ctx->d_err, ctx->stream, ctx->aux));
-  CK(cudaEventRecord(ctx->join, ctx->aux));
-  CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
+                 ctx->d_err, ctx->stream, s_pad));
+  if (p.overlap) {
+    CK(cudaEventRecord(ctx->join, ctx->aux));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
+  }
   ctx->launches += (p.n_int > 0) + (p.n_pad > 0);
   return SEIS_OK;
 }
@@ -640,14 +652,22 @@ int ensure_snapshots(Plan &p) {
 }
 
 // One reverse step of the exact adjoint over the adjoint tile list.
-int adj_step(Plan &p, const StepArgs &a) {
+int adj_step(Plan &p, const StepArgs &a0) {
   seis_fd_ctx *ctx = p.ctx;
-  CK(cudaEventRecord(ctx->fork, ctx->stream));
-  CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
+  StepArgs a = a0;
+  a.loop = p.loop;
+  cudaStream_t s_pad = ctx->stream;
+  if (p.overlap) {
+    CK(cudaEventRecord(ctx->fork, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->aux, ctx->fork, 0));
+    s_pad = ctx->aux;
+  }
   CK(fast::launch_adjoint(p.shape, p.d_sd, p.d_adj_tiles, p.n_int_adj, p.n_pad_adj, a,
-                          ctx->d_err, ctx->stream, ctx->aux));
-  CK(cudaEventRecord(ctx->join, ctx->aux));
-  CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
+                          ctx->d_err, ctx->stream, s_pad));
+  if (p.overlap) {
+    CK(cudaEventRecord(ctx->join, ctx->aux));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
+  }
   ctx->launches += (p.n_int_adj > 0) + (p.n_pad_adj > 0);
   return SEIS_OK;
 }
@@ -982,7 +1002,7 @@ int plan_run(Plan &p) {
     int64_t before = ctx->launches;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     int rc = enqueue_operator(p);
-    if (rc) {
+    if (rc && p.overlap) {
       // rejoin the auxiliary stream so that it leaves the capture with the
       // main stream (an unjoined fork would keep it capturing)
       cudaEventRecord(ctx->join, ctx->aux);
@@ -1274,8 +1294,9 @@ namespace {
 // 2 x `steps` time steps of the plan's step kernels (forward plans: the
 // operator's step; adjoint plans: the reverse step without imaging): first
 // the interior and the pad kernel one after the other, each bracketed by CUDA
-// events on its own stream, then `steps` steps as a run launches them (the
-// two concurrently).  ms = mean interior and pad kernel milliseconds (each
+// events on its own stream, then `steps` steps as a run launches them (one
+// after the other, or concurrently on two streams when the plan overlaps
+// them).  ms = mean interior and pad kernel milliseconds (each
 // alone) and mean step milliseconds (as run); bytes = algorithmic bytes of
 // the interior and pad tiles (16 per field cell-update).  The fields are
 // cleared afterwards.
@@ -1300,6 +1321,7 @@ int time_steps(Plan &p, int steps, double *ms, double *bytes) {
   StepArgs a{};
   a.nshots = p.nshot;
   a.strip_k = -1;
+  a.loop = p.loop;
   // the interior and the pad kernel of a step on the main / auxiliary stream
   auto launch = [&](int ni, int np) -> cudaError_t {
     return adj ? fast::launch_adjoint(p.shape, p.d_sd, d_tl, ni, np, a, ctx->d_err, ctx->stream,
@@ -1323,11 +1345,16 @@ int time_steps(Plan &p, int steps, double *ms, double *bytes) {
       CK(launch(0, n_pad));
       CK(cudaEventRecord(ev[3], ctx->aux));
       CK(cudaStreamWaitEvent(ctx->stream, ev[3], 0));
-    } else {
+    } else if (p.overlap) {
       CK(cudaStreamWaitEvent(ctx->aux, ev[0], 0));
       CK(launch(n_int, n_pad));
       CK(cudaEventRecord(ev[3], ctx->aux));
       CK(cudaStreamWaitEvent(ctx->stream, ev[3], 0));
+    } else {
+      CK(adj ? fast::launch_adjoint(p.shape, p.d_sd, d_tl, n_int, n_pad, a, ctx->d_err,
+                                    ctx->stream, ctx->stream)
+             : launch_step(mode, p.exact, p.d_sd, d_tl, n_int, n_pad, p.shape, a, ctx->d_err,
+                           ctx->stream, ctx->stream));
     }
     CK(cudaEventRecord(ev[4], ctx->stream));
     CK(cudaEventSynchronize(ev[4]));
@@ -1410,41 +1437,60 @@ std::string tune_key(const Plan &p) {
   return k;
 }
 
-// Time `steps` steps of the plan in every tile shape and keep the fastest
-// (the cached choice for this plan's signature unless `force`).  ms: the
+// The launch form of a plan's steps (the captured graph follows it).
+void set_launch(Plan &p, bool overlap, int loop) {
+  if (p.overlap == overlap && p.loop == loop) return;
+  p.overlap = overlap;
+  p.loop = loop;
+  if (p.exec) cudaGraphExecDestroy(p.exec);
+  if (p.graph) cudaGraphDestroy(p.graph);
+  p.exec = nullptr;
+  p.graph = nullptr;
+}
+
+// Time `steps` steps of the plan in every tile shape and launch form (the
+// interior kernel one tile per CTA or persistent, the interior and pad
+// kernels one after the other or concurrently) and keep the fastest (the
+// cached choice for this plan's signature unless `force`).  ms: the shortest
 // mean step time of every shape (0 where not timed), may be null.
 int autotune(Plan &p, int steps, bool force, double *ms, int *best) {
   const std::string key = tune_key(p);
   if (ms)
     for (int s = 0; s < NSHAPES; s++) ms[s] = 0.0;
+  // choice = 4 shape + 2 persistent + overlap
+  auto apply = [&](int c) {
+    set_launch(p, (c & 1) != 0, (c >> 1) & 1);
+    return apply_shape(p, c >> 2);
+  };
   if (!force) {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      if (best) *best = it->second;
-      return apply_shape(p, it->second);
+      if (best) *best = it->second >> 2;
+      return apply(it->second);
     }
   }
-  int pick = p.shape;
+  int pick = 0;
   double t_best = 0.0;
-  for (int s = 0; s < NSHAPES; s++) {
-    int rc = apply_shape(p, s);
+  for (int c = 0; c < 4 * NSHAPES; c++) {
+    int rc = apply(c);
     double t[3];
     if (!rc) rc = time_steps(p, 3, t, nullptr);  // warm-up
     if (!rc) rc = time_steps(p, steps, t, nullptr);
     if (rc) return rc;
-    if (ms) ms[s] = t[2];
-    if (s == 0 || t[2] < t_best) {
+    const int s = c >> 2;
+    if (ms && (ms[s] == 0.0 || t[2] < ms[s])) ms[s] = t[2];
+    if (c == 0 || t[2] < t_best) {
       t_best = t[2];
-      pick = s;
+      pick = c;
     }
   }
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune_cache[key] = pick;
   }
-  if (best) *best = pick;
-  return apply_shape(p, pick);
+  if (best) *best = pick >> 2;
+  return apply(pick);
 }
 }  // namespace
 
@@ -1462,6 +1508,23 @@ int seis_fd_plan_set_tile_shape(seis_fd_plan *plan, int shape) {
 
 int seis_fd_plan_tile_shape(const seis_fd_plan *plan) {
   return plan && plan->p ? plan->p->shape : SEIS_ERR_ARG;
+}
+
+int seis_fd_plan_set_launch(seis_fd_plan *plan, int flags) {
+  if (!plan || !plan->p) return SEIS_ERR_ARG;
+  if (flags & ~(SEIS_LAUNCH_OVERLAP | SEIS_LAUNCH_PERSISTENT | SEIS_LAUNCH_PER_TILE) ||
+      ((flags & SEIS_LAUNCH_PERSISTENT) && (flags & SEIS_LAUNCH_PER_TILE)))
+    return fail(plan->p->ctx, SEIS_ERR_ARG, "launch flags %d", flags);
+  const int loop = (flags & SEIS_LAUNCH_PERSISTENT) ? 1 : (flags & SEIS_LAUNCH_PER_TILE) ? 0 : -1;
+  set_launch(*plan->p, (flags & SEIS_LAUNCH_OVERLAP) != 0, loop);
+  return SEIS_OK;
+}
+
+int seis_fd_plan_launch(const seis_fd_plan *plan) {
+  if (!plan || !plan->p) return SEIS_ERR_ARG;
+  const Plan &p = *plan->p;
+  return (p.overlap ? SEIS_LAUNCH_OVERLAP : 0) | (p.loop > 0 ? SEIS_LAUNCH_PERSISTENT : 0) |
+         (p.loop == 0 ? SEIS_LAUNCH_PER_TILE : 0);
 }
 
 int seis_fd_plan_autotune(seis_fd_plan *plan, int steps, int force, double *h_ms, int *h_best) {

@@ -133,6 +133,9 @@ struct StepArgs {
   int snap_k = -1;   // snapshot index written (forward) or imaged (adjoint)
   float img_w = 0.f; // adjoint: weight of the imaging term (snapshot interval)
   int illum_on = 0;  // add the square of every model cell's new value to g.illum
+  // interior kernel: -1 the persistent one when each of its CTAs gets at
+  // least 4 tiles, else one tile per CTA; 0 one tile per CTA; 1 persistent
+  int loop = -1;
 };
 
 // Allocation geometry of one field of a shot: LDZ floats per column, and the

@@ -45,16 +45,21 @@ cudaError_t setup_shape() {
   return e;
 }
 
-// Interior tiles on s_int (persistent CTAs), pad tiles on s_pad (one CTA
-// each), concurrently.
+// Interior tiles on s_int, pad tiles (one CTA each) on s_pad.  The interior
+// kernel is the persistent one as a.loop says; by default when each of its
+// CTAs gets at least LOOP_MIN_TILES tiles (its double buffering pays, and the
+// last round of tiles is a small part of the launch).
+constexpr int LOOP_MIN_TILES = 4;
 template <int S, int MODE>
 cudaError_t launch_t(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
                      const StepArgs &a, int *d_err, cudaStream_t s_int, cudaStream_t s_pad) {
   constexpr int NT = Geo<S>::NT;
-  if (n_int > 0) {
-    const int g = LoopGrid<S, MODE>::ctas < n_int ? LoopGrid<S, MODE>::ctas : n_int;
-    interior_loop_kernel<S, MODE><<<g, NT, LCfg<S, MODE>::bytes, s_int>>>(d_shots, d_tiles, n_int,
-                                                                         a, d_err);
+  const int G = LoopGrid<S, MODE>::ctas;
+  if (n_int > 0 && (a.loop > 0 || (a.loop < 0 && n_int >= LOOP_MIN_TILES * G))) {
+    interior_loop_kernel<S, MODE><<<G < n_int ? G : n_int, NT, LCfg<S, MODE>::bytes, s_int>>>(
+        d_shots, d_tiles, n_int, a, d_err);
+  } else if (n_int > 0) {
+    tile_kernel<S, MODE><<<n_int, NT, TCfg<S, MODE>::bytes, s_int>>>(d_shots, d_tiles, a, d_err);
   }
   if (n_pad > 0)
     pad_tile_kernel<S, MODE><<<n_pad, NT, PCfg<S, MODE>::bytes, s_pad>>>(d_shots, d_tiles + n_int,

@@ -1,18 +1,19 @@
 // Time-step kernels of the 2-D acoustic FD engine (sm_100a).
 //
 // One step of a batch is two launches over the tile list, on two streams:
-//  * tile_kernel<MODE, TILE_INTERIOR>: tiles whose every cell is a model cell
-//    in the 8th-order region; the absorbing blend is the identity there
-//    (w = 1, u31 = 0; src/util/fd.cpp:55-56);
-//  * pad_tile_kernel<MODE>: every other tile, in one pass: the two-way update
-//    (frame and low-order cells by the per-cell formula), injection, the
-//    two-way values of the tile and a one-cell halo kept in shared memory,
-//    then the one-way update and blend of the pad cells (processBoundary,
-//    fd.cpp:1092-1179).
-// Both: one 32 x 64 tile per CTA, 2-D TMA tensor copies of the current field
-// (5-column / 8-row halo), the previous field, the velocity and, for Born, the
-// perturbation (1-column / 8-row halo) into shared memory (one mbarrier, no
-// multicast); each thread owns a 4-row x 2-column micro-tile.
+//  * interior_loop_kernel<S, MODE>: tiles whose every cell is a model cell in
+//    the 8th-order region, where the absorbing blend is the identity
+//    (w = 1, u31 = 0; src/util/fd.cpp:55-56); persistent CTAs, each taking
+//    every G-th tile through two shared-memory stages (the tensor copies of
+//    the next tile in flight while the current one is computed);
+//  * pad_tile_kernel<S, MODE>: every other tile, one per CTA, in one pass:
+//    the two-way update (frame and low-order cells by the per-cell formula),
+//    injection, the two-way values of the tile and a one-cell halo kept in
+//    shared memory, then the one-way update and blend of the pad cells
+//    (processBoundary, fd.cpp:1092-1179).
+// Tiles are TX x TZ cells (shape S); arrays are staged by 2-D TMA tensor
+// copies into shared memory (mbarriers, bounded waits, no multicast); each
+// thread owns a 4-row x 2-column micro-tile.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -438,13 +439,14 @@ __device__ __forceinline__ bool stage_tile(const ShotDev &g, const StepArgs &a, 
 // region, where the absorbing blend is the identity: w = 1, u31 = 0;
 // src/util/fd.cpp:55-56) from its staged arrays: the current fields CA, CB
 // (with the stencil's halo), previous fields PA, PB, velocity VV and
-// perturbation DV; one 4-row x 2-column micro-tile per thread.  Every thread
-// of the CTA calls this (the snapshot holds block barriers).
+// perturbation DV; one 4-row x 2-column micro-tile per thread, gzq the padded
+// receiver rows of its two columns.  Every thread of the CTA calls this (the
+// snapshot holds block barriers).
 template <int S, int MODE, class SC, class SO>
 __device__ __forceinline__ void interior_cells(const ShotDev &g, const StepArgs &a, int x0, int z0,
                                                const SC &CA, const SC &CB, const SO &PA,
                                                const SO &VV, const SO &PB, const SO &DV,
-                                               float *red) {
+                                               const int (&gzq)[2], float *red) {
   SEIS_GEO(S);
   constexpr bool BORN = MODE == MODE_BORN;
   StepArgs aa = a;
@@ -458,9 +460,6 @@ __device__ __forceinline__ void interior_cells(const ShotDev &g, const StepArgs 
   const bool record = MODE != MODE_RCV && aa.rec_k >= 0;
   const bool snap = MODE != MODE_RCV && aa.snap_k >= 0 && g.snap != nullptr;
 
-  int gzq[2];
-#pragma unroll
-  for (int j = 0; j < 2; j++) gzq[j] = g.gz[ix + j - g.pml] + g.pml;
   float lv[8];
   int lx[8], lz[8];
   unsigned mask = 0;
@@ -555,7 +554,9 @@ __global__ void __launch_bounds__(Geo<S>::NT, TCfg<S, MODE>::MIN_CTAS) tile_kern
   const SA VV{bb + arr_off(C::NCUR + 1), x0 - 1, zm};
   const SA PB{bb + arr_off(BORN ? C::NCUR + 2 : C::NCUR), x0 - 1, zm};
   const SA DV{bb + arr_off(BORN ? C::NCUR + 3 : C::NCUR + 1), x0 - 1, zm};
-  interior_cells<S, MODE>(g, a, x0, z0, CA, CB, PA, VV, PB, DV, red);
+  const int ix = x0 + 2 * (tid / QZ);
+  const int gzq[2] = {g.gz[ix - g.pml] + g.pml, g.gz[ix + 1 - g.pml] + g.pml};
+  interior_cells<S, MODE>(g, a, x0, z0, CA, CB, PA, VV, PB, DV, gzq, red);
 }
 
 // Persistent interior kernel: CTA b of G takes the interior tiles b, b + G,
@@ -599,7 +600,9 @@ __global__ void __launch_bounds__(Geo<S>::NT, LCfg<S, MODE>::MIN_CTAS) interior_
   float *stage0 = reinterpret_cast<float *>(smraw);
   uint64_t *bar = reinterpret_cast<uint64_t *>(stage0 + 2 * L::STAGE);
   __shared__ ShotDev sg[2];
+  __shared__ int2 sxz[2];  // tile origin of each stage
   __shared__ float red[33];
+  __shared__ int s_fail;
   const int tid = threadIdx.x;
   int i = blockIdx.x;
   if (i >= n) return;
@@ -613,6 +616,7 @@ __global__ void __launch_bounds__(Geo<S>::NT, LCfg<S, MODE>::MIN_CTAS) interior_
   // left of column 0)
   auto issue = [&](int st, int ti) {
     const Tile t = tiles[ti];
+    sxz[st] = make_int2(t.x0, t.z0);
     const CUtensorMap *maps = shots[t.shot].maps;
     float *bb = stage0 + st * L::STAGE;
     fence_proxy_async();
@@ -638,12 +642,15 @@ __global__ void __launch_bounds__(Geo<S>::NT, LCfg<S, MODE>::MIN_CTAS) interior_
     mbar_init(bar, 1);
     mbar_init(bar + 1, 1);
     fence_barrier_init();
+    s_fail = 0;
   }
   load_shot(0, i);
   __syncthreads();
   if (tid == 0) issue(0, i);
+  __syncthreads();  // the first tile's origin
   uint32_t par = 0;  // bit st: parity of the next completion of stage st
   int st = 0;
+  const int cxq = 2 * (tid / QZ);
   for (;;) {
     const int next = i + (int)gridDim.x;
     const bool more = next < n;
@@ -651,9 +658,25 @@ __global__ void __launch_bounds__(Geo<S>::NT, LCfg<S, MODE>::MIN_CTAS) interior_
       load_shot(st ^ 1, next);
       if (tid == 0) issue(st ^ 1, next);
     }
-    bool ok = mbar_wait(bar + st, (par >> st) & 1u);
+    // this tile's receiver rows, loaded while its copies land
+    const ShotDev &g = sg[st];
+    const int x0 = sxz[st].x, z0 = sxz[st].y;
+    const int gzq[2] = {g.gz[x0 + cxq - g.pml] + g.pml, g.gz[x0 + cxq + 1 - g.pml] + g.pml};
+    // a wait that gives up leaves garbage in the stage (indices stay in
+    // range); the CTA then ends after this tile
+    if (!mbar_wait(bar + st, (par >> st) & 1u)) s_fail = 1;
     par ^= 1u << st;
-    if (!__syncthreads_and(ok)) {
+    const float *bb = stage0 + st * L::STAGE;
+    const float *ob = bb + L::NCUR * CW * RW;
+    const SW CA{bb, x0 - HI, z0 - HI};
+    const SW CB{bb + (BORN ? CW * RW : 0), x0 - HI, z0 - HI};
+    const ST PA{ob, x0, z0};
+    const ST VV{ob + TILE, x0, z0};
+    const ST PB{ob + (BORN ? 2 : 0) * TILE, x0, z0};
+    const ST DV{ob + (BORN ? 3 : 1) * TILE, x0, z0};
+    interior_cells<S, MODE>(g, a, x0, z0, CA, CB, PA, VV, PB, DV, gzq, red);
+    __syncthreads();  // stage st, its origin and shot table are free for the tile after next
+    if (s_fail) {
       // the copies in flight into the other stage land before the CTA ends
       if (tid == 0) {
         atomicExch(err, 1);
@@ -661,17 +684,6 @@ __global__ void __launch_bounds__(Geo<S>::NT, LCfg<S, MODE>::MIN_CTAS) interior_
       }
       return;
     }
-    const Tile t = tiles[i];
-    const float *bb = stage0 + st * L::STAGE;
-    const float *ob = bb + L::NCUR * CW * RW;
-    const SW CA{bb, t.x0 - HI, t.z0 - HI};
-    const SW CB{bb + (BORN ? CW * RW : 0), t.x0 - HI, t.z0 - HI};
-    const ST PA{ob, t.x0, t.z0};
-    const ST VV{ob + TILE, t.x0, t.z0};
-    const ST PB{ob + (BORN ? 2 : 0) * TILE, t.x0, t.z0};
-    const ST DV{ob + (BORN ? 3 : 1) * TILE, t.x0, t.z0};
-    interior_cells<S, MODE>(sg[st], a, t.x0, t.z0, CA, CB, PA, VV, PB, DV, red);
-    __syncthreads();  // stage st and its shot table are free for the tile after next
     if (!more) break;
     i = next;
     st ^= 1;
