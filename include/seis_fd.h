@@ -277,8 +277,8 @@ int seis_fd_plan_tile_shape(const seis_fd_plan *plan);
  * SEIS_LAUNCH_PERSISTENT: interior tiles by the persistent kernel (as many
  * CTAs as are resident at once, each taking every G-th tile through two
  * shared-memory stages); SEIS_LAUNCH_PER_TILE: one interior tile per CTA;
- * neither: the persistent kernel when each of its CTAs gets at least 4 tiles
- * (the default, flags 0). */
+ * neither: the persistent kernel when each of its CTAs gets at least 4 tiles.
+ * A new plan has SEIS_LAUNCH_OVERLAP. */
 #define SEIS_LAUNCH_OVERLAP 1
 #define SEIS_LAUNCH_PERSISTENT 2
 #define SEIS_LAUNCH_PER_TILE 4

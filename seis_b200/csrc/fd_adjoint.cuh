@@ -397,8 +397,11 @@ __device__ float dcur(const ShotDev &g, const VA &V, int cx, int cz, int tx, int
 }
 
 // The part of S_cur^T M at cell (tx, tz) that comes from frame and low-order
-// consumers (cells within 3 of the grid edge) on its radius-4 cross; nonzero
-// only within 4 of the edge.
+// consumers (cells within 3 of the grid edge) on its cross; nonzero only
+// within 4 of the edge.  A 2nd-order consumer reads its neighbours within one
+// cell, a frame consumer (edge row or column) those within one cell along
+// the edge and three cells along its normal extrapolation: the other
+// offsets' coefficients are zero and are skipped.
 template <class A>
 __device__ float edge_terms(const ShotDev &g, const A &M, const A &V, int tx, int tz) {
   const int NX = g.NX, NZ = g.NZ;
@@ -408,11 +411,17 @@ __device__ float edge_terms(const ShotDev &g, const A &M, const A &V, int tx, in
   };
   float s = 0.0f;
 #pragma unroll 1
-  for (int m = -4; m <= 4; m++)
-    if (low(tx, tz + m)) s = s + dcur(g, V, tx, tz + m, tx, tz) * M(tx, tz + m);
+  for (int m = -3; m <= 3; m++) {
+    const int cz = tz + m;
+    if ((m >= -1 && m <= 1) || cz == 0 || cz == NZ - 1)
+      if (low(tx, cz)) s = s + dcur(g, V, tx, cz, tx, tz) * M(tx, cz);
+  }
 #pragma unroll 1
-  for (int m = -4; m <= 4; m++)
-    if (m != 0 && low(tx + m, tz)) s = s + dcur(g, V, tx + m, tz, tx, tz) * M(tx + m, tz);
+  for (int m = -3; m <= 3; m++) {
+    const int cx = tx + m;
+    if (m != 0 && ((m >= -1 && m <= 1) || cx == 0 || cx == NX - 1))
+      if (low(cx, tz)) s = s + dcur(g, V, cx, tz, tx, tz) * M(cx, tz);
+  }
   return s;
 }
 
@@ -680,14 +689,18 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
     rp2[i] = p2;
     rp3[i] = p3;
   };
-  // the owners keep L of the tile in shared memory and clear the roles of
-  // the tile cells that are no ring cells; the halo's ring cells are formed
-  // by the threads that hold their L
+  // the owners keep L of the tile in shared memory and clear the roles and
+  // terms of the tile cells that are no ring cells; the halo's ring cells are
+  // formed by the threads that hold their L
 #pragma unroll
   for (int k = 0; k < 8; k++) {
     const int cx = ix + k / 4, cz = iz0 + k % 4;
     sLt[(cx - x0) * TZ + (cz - z0)] = Lt[k];
-    if (!(cx < NX && cz < NZ && pad_pos(g, cx, cz).ring > 0)) rmask[ridx(cx, cz)] = 0;
+    if (!(cx < NX && cz < NZ && pad_pos(g, cx, cz).ring > 0)) {
+      const int q = ridx(cx, cz);
+      rmask[q] = 0;
+      rp0[q] = rp1[q] = rp2[q] = rp3[q] = 0.0f;
+    }
   }
 #pragma unroll
   for (int h = 0; h < HPT; h++)
@@ -728,23 +741,68 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
     int cx, cz;
     aff.cell(i, cx, cz);
     float m = 0.0f, e = 0.0f, b = 0.0f;
+    // Away from the corners every ring cell within one cell of this one lies
+    // in the same strip: its roles follow from the strip's inner direction
+    // (top / bottom: +-z, left / right: +-x) and the terms are summed in the
+    // order of the general gather below (non-ring cells hold zero terms).
+    const int fz = (cx - 1 >= g.pml && cx + 1 <= g.pml + g.nx - 1 && g.nz >= 3)
+                       ? (cz <= g.pml ? 1 : (cz >= g.pml + g.nz - 1 ? -1 : 0))
+                       : 0;
+    const int fx = (fz == 0 && cz - 1 >= g.pml && cz + 1 <= g.pml + g.nz - 1 && g.nx >= 3)
+                       ? (cx <= g.pml ? 1 : (cx >= g.pml + g.nx - 1 ? -1 : 0))
+                       : 0;
+    const int c0 = ridx(cx, cz);
+    if (fz > 0) {  // top strip: this cell is the inner neighbour of the one above
+      const int qi = ridx(cx, cz - 1);
+      m += rp1[ridx(cx - 1, cz - 1)];
+      b += rp1[ridx(cx - 1, cz)];
+      m += rp0[qi]; e += rp2[qi]; b -= rp3[qi];
+      e += rp2[c0]; b += rp0[c0];
+      m += rp1[ridx(cx + 1, cz - 1)];
+      b += rp1[ridx(cx + 1, cz)];
+    } else if (fz < 0) {  // bottom strip
+      const int qi = ridx(cx, cz + 1);
+      b += rp1[ridx(cx - 1, cz)];
+      m += rp1[ridx(cx - 1, cz + 1)];
+      e += rp2[c0]; b += rp0[c0];
+      m += rp0[qi]; e += rp2[qi]; b -= rp3[qi];
+      b += rp1[ridx(cx + 1, cz)];
+      m += rp1[ridx(cx + 1, cz + 1)];
+    } else if (fx > 0) {  // left strip
+      const int qi = ridx(cx - 1, cz);
+      m += rp1[ridx(cx - 1, cz - 1)];
+      m += rp0[qi]; e += rp2[qi]; b -= rp3[qi];
+      m += rp1[ridx(cx - 1, cz + 1)];
+      b += rp1[ridx(cx, cz - 1)];
+      e += rp2[c0]; b += rp0[c0];
+      b += rp1[ridx(cx, cz + 1)];
+    } else if (fx < 0) {  // right strip
+      const int qi = ridx(cx + 1, cz);
+      b += rp1[ridx(cx, cz - 1)];
+      e += rp2[c0]; b += rp0[c0];
+      b += rp1[ridx(cx, cz + 1)];
+      m += rp1[ridx(cx + 1, cz - 1)];
+      m += rp0[qi]; e += rp2[qi]; b -= rp3[qi];
+      m += rp1[ridx(cx + 1, cz + 1)];
+    } else {
 #pragma unroll
-    for (int dx = -1; dx <= 1; dx++)
+      for (int dx = -1; dx <= 1; dx++)
 #pragma unroll
-      for (int dz = -1; dz <= 1; dz++) {
-        const int q = ridx(cx + dx, cz + dz);
-        // this cell sits at offset (-dx, -dz) from the ring cell
-        switch ((rmask[q] >> role_slot(-dx, -dz)) & 7) {
-          case ROLE_SELF: e += rp2[q]; b += rp0[q]; break;
-          case ROLE_INNER: m += rp0[q]; e += rp2[q]; b -= rp3[q]; break;
-          case ROLE_TANG: b += rp1[q]; break;
-          case ROLE_DIAG: m += rp1[q]; break;
-          case ROLE_CZ: m += rp0[q]; break;
-          case ROLE_CX: m += rp1[q]; break;
-          case ROLE_CSELF: e += rp2[q]; break;
-          default: break;
+        for (int dz = -1; dz <= 1; dz++) {
+          const int q = ridx(cx + dx, cz + dz);
+          // this cell sits at offset (-dx, -dz) from the ring cell
+          switch ((rmask[q] >> role_slot(-dx, -dz)) & 7) {
+            case ROLE_SELF: e += rp2[q]; b += rp0[q]; break;
+            case ROLE_INNER: m += rp0[q]; e += rp2[q]; b -= rp3[q]; break;
+            case ROLE_TANG: b += rp1[q]; break;
+            case ROLE_DIAG: m += rp1[q]; break;
+            case ROLE_CZ: m += rp0[q]; break;
+            case ROLE_CX: m += rp1[q]; break;
+            case ROLE_CSELF: e += rp2[q]; break;
+            default: break;
+          }
         }
-      }
+    }
     const PadPos pt = pad_pos(g, cx, cz);
     const float w = pt.ring == 0 ? 1.0f : pad_weight(g, pt);
     const size_t at = (size_t)cx * g.LDZ + cz;

@@ -138,50 +138,84 @@ __device__ __forceinline__ float pad_weight(const ShotDev &g, const PadPos &p) {
 #endif
 }
 
-// Absorbing blend of one cell with two-way value u3 (fd.cpp:1092-1179, blend
-// :55-56).  U3 = two-way field (tile + 1 halo); cur/P/V = current, previous,
-// velocity.
-template <class U3A, class A>
-__device__ float absorb_cell(float u3, const U3A &U3, const A &cur, const A &P, const A &V,
-                             const ShotDev &g, int ix, int iz) {
+// What the absorbing update of one pad cell needs besides the fields
+// (fd.cpp:1092-1179, blend :55-56): its kind, inner neighbour and the
+// velocity-dependent coefficients, formed once per cell and applied to every
+// field of the cell (Born's two fields share them).
+struct Absorb {
+  int kind;        // 0 model cell, 1 diagonal corner, 2 top / bottom strip, 3 left / right strip
+  int I;           // strips: the inner neighbour's row (kind 2) or column (kind 3)
+  int sxn, szn;    // corners: one cell toward the interior
+  float a1, a2, a3;  // strips: one-way coefficients; corners: a3 = ax3
+  float w;           // blend weight
+};
+template <class A>
+__device__ __forceinline__ Absorb absorb_geom(const A &V, const ShotDev &g, int ix, int iz) {
+  Absorb q;
   PadPos pp = pad_pos(g, ix, iz);
-  if (pp.ring == 0) return u3 + 0.0f;  // interior: w = 1, u31 = 0
+  q.kind = 0;
+  q.I = 0;
+  q.sxn = q.szn = 0;
+  q.a1 = q.a2 = q.a3 = 0.0f;
+  q.w = 1.0f;
+  if (pp.ring == 0) return q;  // interior: w = 1, u31 = 0
   float v = V(ix, iz);
-  float u31;
   if (pp.distx == pp.ring && pp.distz == pp.ring) {  // diagonal corner, fd.cpp:1146-1178
-    int sxn = pp.dl > 0 ? 1 : -1, szn = pp.du > 0 ? 1 : -1;  // toward the interior
-    float ax3;
+    q.kind = 1;
+    q.sxn = pp.dl > 0 ? 1 : -1;  // toward the interior
+    q.szn = pp.du > 0 ? 1 : -1;
     if (pp.dl > 0 && pp.du > 0)  // upper-left: sqrt(2)/v/dt formed in double, fd.cpp:1176
-      ax3 = __double2float_rn(g.sqrt2d / (double)v / (double)g.dt);
+      q.a3 = __double2float_rn(g.sqrt2d / (double)v / (double)g.dt);
     else
-      ax3 = g.sqrt2f / v / g.dt;
-    float tmp = -g.ax1 * U3(ix, iz + szn) - g.ax2 * U3(ix + sxn, iz) + ax3 * (-cur(ix, iz));
-    u31 = -tmp / (g.ax1 + g.ax2 + ax3);
+      q.a3 = g.sqrt2f / v / g.dt;
   } else if (pp.distz == pp.ring) {  // top / bottom strip, inner along z
-    int I = pp.du > 0 ? iz + 1 : iz - 1;
+    q.kind = 2;
+    q.I = pp.du > 0 ? iz + 1 : iz - 1;
+    q.a1 = g.a1z;
 #ifdef SEIS_FAST_MATH
-    float a2 = g.hdt2 * (1.0f / v);
-    float a3 = v * g.q4dx2;
+    q.a2 = g.hdt2 * (1.0f / v);
+    q.a3 = v * g.q4dx2;
 #else
-    float a2 = g.hdt2 / v;
-    float a3 = v / 4.0f / g.dx / g.dx;
+    q.a2 = g.hdt2 / v;
+    q.a3 = v / 4.0f / g.dx / g.dx;
 #endif
-    u31 = oneway(g.a1z, a2, a3, U3(ix, I), U3(ix + 1, I), U3(ix - 1, I), cur(ix, iz),
-                 cur(ix, I), P(ix, iz), P(ix, I), P(ix + 1, iz), P(ix - 1, iz));
   } else {  // left / right strip, inner along x
-    int I = pp.dl > 0 ? ix + 1 : ix - 1;
+    q.kind = 3;
+    q.I = pp.dl > 0 ? ix + 1 : ix - 1;
+    q.a1 = g.a1x;
 #ifdef SEIS_FAST_MATH
-    float a2 = g.hdt2 * (1.0f / v);
-    float a3 = v * g.q4dz2;
+    q.a2 = g.hdt2 * (1.0f / v);
+    q.a3 = v * g.q4dz2;
 #else
-    float a2 = g.hdt2 / v;
-    float a3 = v / 4.0f / g.dz / g.dz;
+    q.a2 = g.hdt2 / v;
+    q.a3 = v / 4.0f / g.dz / g.dz;
 #endif
-    u31 = oneway(g.a1x, a2, a3, U3(I, iz), U3(I, iz + 1), U3(I, iz - 1), cur(ix, iz),
+  }
+  q.w = pad_weight(g, pp);
+  return q;
+}
+
+// Absorbing blend of one field at one cell with two-way value u3.  U3 =
+// two-way field (tile + 1 halo); cur/P = current and previous field.
+template <class U3A, class A>
+__device__ __forceinline__ float absorb_apply(const Absorb &q, float u3, const U3A &U3,
+                                              const A &cur, const A &P, const ShotDev &g, int ix,
+                                              int iz) {
+  if (q.kind == 0) return u3 + 0.0f;
+  float u31;
+  if (q.kind == 1) {
+    float tmp = -g.ax1 * U3(ix, iz + q.szn) - g.ax2 * U3(ix + q.sxn, iz) + q.a3 * (-cur(ix, iz));
+    u31 = -tmp / (g.ax1 + g.ax2 + q.a3);
+  } else if (q.kind == 2) {
+    const int I = q.I;
+    u31 = oneway(q.a1, q.a2, q.a3, U3(ix, I), U3(ix + 1, I), U3(ix - 1, I), cur(ix, iz),
+                 cur(ix, I), P(ix, iz), P(ix, I), P(ix + 1, iz), P(ix - 1, iz));
+  } else {
+    const int I = q.I;
+    u31 = oneway(q.a1, q.a2, q.a3, U3(I, iz), U3(I, iz + 1), U3(I, iz - 1), cur(ix, iz),
                  cur(I, iz), P(ix, iz), P(I, iz), P(ix, iz + 1), P(ix, iz - 1));
   }
-  float w = pad_weight(g, pp);
-  return u3 * w + u31 * (1.0f - w);
+  return u3 * q.w + u31 * (1.0f - q.w);
 }
 
 }  // namespace SEIS_NS

@@ -144,7 +144,7 @@ struct Plan {
   int shape = SHAPE_32x64;   // tile shape of every kernel of the plan (TileShapeId)
   // the interior and pad kernels of a step on two streams, concurrently
   // (else one after the other on the main stream)
-  bool overlap = false;
+  bool overlap = true;
   int loop = -1;  // interior kernel form (StepArgs::loop)
   std::vector<void *> allocs;
   std::vector<size_t> alloc_bytes;
@@ -1322,11 +1322,14 @@ int time_steps(Plan &p, int steps, double *ms, double *bytes) {
   a.nshots = p.nshot;
   a.strip_k = -1;
   a.loop = p.loop;
-  // the interior and the pad kernel of a step on the main / auxiliary stream
-  auto launch = [&](int ni, int np) -> cudaError_t {
-    return adj ? fast::launch_adjoint(p.shape, p.d_sd, d_tl, ni, np, a, ctx->d_err, ctx->stream,
+  // the interior tiles (the list's first n_int) or the pad tiles alone, on
+  // the main / auxiliary stream
+  auto launch = [&](bool interior) -> cudaError_t {
+    const int ni = interior ? n_int : 0, np = interior ? 0 : n_pad;
+    const Tile *t0 = interior ? d_tl : d_tl + n_int;
+    return adj ? fast::launch_adjoint(p.shape, p.d_sd, t0, ni, np, a, ctx->d_err, ctx->stream,
                                       ctx->aux)
-               : launch_step(mode, p.exact, p.d_sd, d_tl, ni, np, p.shape, a, ctx->d_err,
+               : launch_step(mode, p.exact, p.d_sd, t0, ni, np, p.shape, a, ctx->d_err,
                              ctx->stream, ctx->aux);
   };
   double t_int = 0, t_pad = 0, t_step = 0;
@@ -1338,16 +1341,19 @@ int time_steps(Plan &p, int steps, double *ms, double *bytes) {
     a.rec_k = it - p.ndel >= 0 && p.op != OP_RTM && !adj ? it - p.ndel : -1;
     CK(cudaEventRecord(ev[0], ctx->stream));
     if (alone) {
-      CK(launch(n_int, 0));
+      CK(launch(true));
       CK(cudaEventRecord(ev[1], ctx->stream));
       CK(cudaEventRecord(ev[2], ctx->stream));
       CK(cudaStreamWaitEvent(ctx->aux, ev[2], 0));
-      CK(launch(0, n_pad));
+      CK(launch(false));
       CK(cudaEventRecord(ev[3], ctx->aux));
       CK(cudaStreamWaitEvent(ctx->stream, ev[3], 0));
     } else if (p.overlap) {
       CK(cudaStreamWaitEvent(ctx->aux, ev[0], 0));
-      CK(launch(n_int, n_pad));
+      CK(adj ? fast::launch_adjoint(p.shape, p.d_sd, d_tl, n_int, n_pad, a, ctx->d_err,
+                                    ctx->stream, ctx->aux)
+             : launch_step(mode, p.exact, p.d_sd, d_tl, n_int, n_pad, p.shape, a, ctx->d_err,
+                           ctx->stream, ctx->aux));
       CK(cudaEventRecord(ev[3], ctx->aux));
       CK(cudaStreamWaitEvent(ctx->stream, ev[3], 0));
     } else {

@@ -960,8 +960,9 @@ __global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_tile_
     int cxj, iz;
     pads.cell(i, cxj, iz);
     const size_t at = (size_t)cxj * g.LDZ + iz;
-    out_a[at] = absorb_cell(UA_(cxj, iz), UA_, CA, PA, VV, g, cxj, iz);
-    if (BORN) nb_[at] = absorb_cell(UB_(cxj, iz), UB_, CB, PB, VV, g, cxj, iz);
+    const Absorb q = absorb_geom(VV, g, cxj, iz);
+    out_a[at] = absorb_apply(q, UA_(cxj, iz), UA_, CA, PA, g, cxj, iz);
+    if (BORN) nb_[at] = absorb_apply(q, UB_(cxj, iz), UB_, CB, PB, g, cxj, iz);
   }
 }
 
