@@ -495,36 +495,29 @@ __device__ __forceinline__ void adj_halo_cell(int i, int x0, int z0, int &hx, in
 // neighbours or consumers outside the 8th-order region; grad += w lap M1 on
 // its model cells; then M, E (next step) and B of its pad and model edge
 // cells, L = M elsewhere.
+// One pad tile at (x0, z0): thread 0 issues its tensor copies on `bar`
+// (phase parity `parity`); the result is whether they landed in time (when
+// not, the buffers hold garbage, every index stays in range and the caller
+// reports the error).  Every thread of the CTA calls this (it holds block
+// barriers).
 template <int S>
-__global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
-    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
-    int *__restrict__ err) {
+__device__ __forceinline__ bool adj_pad_cells(const ShotDev &g, const StepArgs &a, int x0, int z0,
+                                              unsigned char *smraw, uint64_t *bar,
+                                              uint32_t parity) {
   SEIS_AGEO(S);
   using SA = SAT<SR>;
   constexpr int RW = AG_::RW, RN = AG_::RN, ADJ_NHALO = AG_::NHALO, HPT = AG_::HPT;
-  extern __shared__ __align__(128) unsigned char smraw[];
   float *sV = reinterpret_cast<float *>(smraw);   // wide
   float *sL1 = sV + WIDE;                          // wide
   float *sL2 = sL1 + WIDE;                         // narrow
   float *sWZ = sL2 + NARROW;                       // wide
   float *sWX = sWZ + WIDE;                         // wide
   float *sCOR = sWX + WIDE;                        // tile + halo: frame / low-order terms
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sCOR + RN);
   // ring arrays of tile + halo, over sL1 .. sCOR once L is formed
   float *rp0 = sL1, *rp1 = rp0 + RN, *rp2 = rp1 + RN, *rp3 = rp2 + RN;
   int *rmask = reinterpret_cast<int *>(rp3 + RN);
   const int tid = threadIdx.x;
-  const Tile t = tiles[blockIdx.x];
-  __shared__ ShotDev sg;
-  if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
-    reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    fence_barrier_init();
-  }
-  __syncthreads();
-  const ShotDev &g = sg;
-  const int x0 = t.x0, z0 = t.z0, NX = g.NX, NZ = g.NZ;
+  const int NX = g.NX, NZ = g.NZ;
   if (tid == 0) {
     fence_proxy_async();
     mbar_expect_tx(bar, (uint32_t)((2 * WIDE + NARROW) * sizeof(float)));
@@ -565,10 +558,7 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
     }
     if (hring[h]) eh[h] = Ecur[(size_t)cx * g.LDZ + cz];
   }
-  if (!mbar_wait(bar, 0)) {
-    if (tid == 0) atomicExch(err, 2);
-    return;
-  }
+  const bool ok = mbar_wait(bar, parity);
   // vz M1, vx M1 of the 8th-order consumers (zero elsewhere)
   for (int i = tid; i < WIDE; i += A_NT_I) {
     const int cx = x0 - HXC + i / SR, cz = z0 - ZM + i % SR;
@@ -827,6 +817,81 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
       for (int r = 0; r < 4; r++)
         if (iz0 + r < NZ && inner(cx, iz0 + r)) out[col + iz0 + r] = Lt[4 * j + r];
     }
+  }
+  return ok;
+}
+
+template <int S>
+__global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
+    int *__restrict__ err) {
+  SEIS_AGEO(S);
+  extern __shared__ __align__(128) unsigned char smraw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + sizeof(float) * AG_::PAD_FLOATS);
+  const int tid = threadIdx.x;
+  const Tile t = tiles[blockIdx.x];
+  __shared__ ShotDev sg;
+  if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+    reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (!adj_pad_cells<S>(sg, a, t.x0, t.z0, smraw, bar, 0) && tid == 0) atomicExch(err, 2);
+}
+
+// Persistent form: CTA b of G takes the pad tiles b, b + G, ...; the next
+// tile's shot-table entry is fetched while the current tile is computed.
+template <int S>
+__global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_loop_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, int n, StepArgs a,
+    int *__restrict__ err) {
+  SEIS_AGEO(S);
+  extern __shared__ __align__(128) unsigned char smraw[];
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + sizeof(float) * AG_::PAD_FLOATS);
+  __shared__ ShotDev sg[2];
+  __shared__ int2 sxz[2];
+  __shared__ int s_fail;
+  const int tid = threadIdx.x;
+  int i = blockIdx.x;
+  if (i >= n) return;
+  auto load_shot = [&](int st, int ti) {
+    const int shot = tiles[ti].shot;
+    if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+      reinterpret_cast<int *>(&sg[st])[tid] = reinterpret_cast<const int *>(shots + shot)[tid];
+  };
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+    s_fail = 0;
+    const Tile t = tiles[i];
+    sxz[0] = make_int2(t.x0, t.z0);
+  }
+  load_shot(0, i);
+  __syncthreads();
+  uint32_t par = 0;
+  int st = 0;
+  for (;;) {
+    const int next = i + (int)gridDim.x;
+    const bool more = next < n;
+    if (more) {  // the next tile's shot table, fetched while this one runs
+      load_shot(st ^ 1, next);
+      if (tid == 0) {
+        const Tile t = tiles[next];
+        sxz[st ^ 1] = make_int2(t.x0, t.z0);
+      }
+    }
+    if (!adj_pad_cells<S>(sg[st], a, sxz[st].x, sxz[st].y, smraw, bar, par)) s_fail = 1;
+    par ^= 1u;
+    __syncthreads();  // the buffers, this slot's table and origin are free
+    if (s_fail) {
+      if (tid == 0) atomicExch(err, 2);
+      return;
+    }
+    if (!more) break;
+    i = next;
+    st ^= 1;
   }
 }
 

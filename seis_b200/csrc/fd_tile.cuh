@@ -408,13 +408,11 @@ struct PCfg {
 // and the row coordinate is a multiple of TZ (16-byte aligned).  Thread 0
 // issues the copies; every thread then waits on the mbarrier.
 template <int S, int MODE>
-__device__ __forceinline__ bool stage_tile(const ShotDev &g, const StepArgs &a, int x0, int z0,
+__device__ __forceinline__ void issue_tile(const ShotDev &g, const StepArgs &a, int x0, int z0,
                                            float *bb, uint64_t *bar) {
   SEIS_GEO(S);
   using C = TCfg<S, MODE>;
-  if (threadIdx.x == 0) {
-    fence_proxy_async();
-    mbar_expect_tx(bar, (uint32_t)(C::BUF * sizeof(float)));
+  {
     const int ra = a.rot % 3, rca = (a.rot + 1) % 3, rb = a.rot_b % 3, rcb = (a.rot_b + 1) % 3;
     int maps[6];
     if (MODE == MODE_RCV) {
@@ -431,6 +429,16 @@ __device__ __forceinline__ bool stage_tile(const ShotDev &g, const StepArgs &a, 
       const int off = arr < C::NCUR ? arr * CW_C * SR : C::NCUR * CW_C * SR + (arr - C::NCUR) * CW_P * SR;
       tma_load_2d(bb + off, g.maps + maps[arr], z0, col, bar);
     }
+  }
+}
+template <int S, int MODE>
+__device__ __forceinline__ bool stage_tile(const ShotDev &g, const StepArgs &a, int x0, int z0,
+                                           float *bb, uint64_t *bar) {
+  using C = TCfg<S, MODE>;
+  if (threadIdx.x == 0) {
+    fence_proxy_async();
+    mbar_expect_tx(bar, (uint32_t)(C::BUF * sizeof(float)));
+    issue_tile<S, MODE>(g, a, x0, z0, bb, bar);
   }
   return mbar_wait(bar, 0);
 }
@@ -707,37 +715,21 @@ __global__ void __launch_bounds__(Geo<S>::NT, LCfg<S, MODE>::MIN_CTAS) interior_
 //     blend (processBoundary fd.cpp:1092-1179, :55-56), stored.
 // A halo cell's two-way value is formed by the same per-cell arithmetic as
 // in the tile that owns it.
+// The cells of one pad tile at (x0, z0) from its staged arrays bb (wide
+// current fields, narrow previous fields, velocity, perturbation) and the
+// two-way scratch u3m; the phases are listed above.  Every thread of the CTA
+// calls this (it holds block barriers).
 template <int S, int MODE>
-__global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_tile_kernel(
-    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
-    int *__restrict__ err) {
+__device__ __forceinline__ void pad_cells(const ShotDev &g, const StepArgs &a, int x0, int z0,
+                                          const float *bb, float *u3m, float *red) {
   SEIS_GEO(S);
   using SA = SAT<SR>;
   using UA = UAT<G_::U3R>;
   constexpr int U3N = G_::U3N, NHALO = G_::NHALO;
   using C = TCfg<S, MODE>;
   constexpr bool BORN = C::BORN;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  float *bb = reinterpret_cast<float *>(smraw);
-  float *u3m = bb + C::BUF;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(u3m + PCfg<S, MODE>::NF * U3N);
-  __shared__ ShotDev sg;
-  __shared__ float red[33];
   const int tid = threadIdx.x;
-  const Tile t = tiles[blockIdx.x];
-  if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
-    reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    fence_barrier_init();
-  }
-  __syncthreads();
-  const ShotDev &g = sg;
-  const int x0 = t.x0, z0 = t.z0, NX = g.NX, NZ = g.NZ;
-  if (!stage_tile<S, MODE>(g, a, x0, z0, bb, bar)) {
-    if (tid == 0) atomicExch(err, 1);
-    return;
-  }
+  const int NX = g.NX, NZ = g.NZ;
   auto arr_off = [](int arr) -> int {
     return arr < C::NCUR ? arr * CW_C * SR : C::NCUR * CW_C * SR + (arr - C::NCUR) * CW_P * SR;
   };
@@ -963,6 +955,105 @@ __global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_tile_
     const Absorb q = absorb_geom(VV, g, cxj, iz);
     out_a[at] = absorb_apply(q, UA_(cxj, iz), UA_, CA, PA, g, cxj, iz);
     if (BORN) nb_[at] = absorb_apply(q, UB_(cxj, iz), UB_, CB, PB, g, cxj, iz);
+  }
+}
+
+template <int S, int MODE>
+__global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_tile_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, StepArgs a,
+    int *__restrict__ err) {
+  SEIS_GEO(S);
+  using C = TCfg<S, MODE>;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float *bb = reinterpret_cast<float *>(smraw);
+  float *u3m = bb + C::BUF;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(u3m + PCfg<S, MODE>::NF * G_::U3N);
+  __shared__ ShotDev sg;
+  __shared__ float red[33];
+  const int tid = threadIdx.x;
+  const Tile t = tiles[blockIdx.x];
+  if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+    reinterpret_cast<int *>(&sg)[tid] = reinterpret_cast<const int *>(shots + t.shot)[tid];
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (!stage_tile<S, MODE>(sg, a, t.x0, t.z0, bb, bar)) {
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  pad_cells<S, MODE>(sg, a, t.x0, t.z0, bb, u3m, red);
+}
+
+// Persistent form: CTA b of G takes the pad tiles b, b + G, ... through one
+// staging buffer; the next tile's shot-table entry is fetched while the
+// current tile is computed, and its tensor copies are issued as soon as the
+// buffer is free.
+template <int S, int MODE>
+__global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_loop_kernel(
+    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, int n, StepArgs a,
+    int *__restrict__ err) {
+  SEIS_GEO(S);
+  using C = TCfg<S, MODE>;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float *bb = reinterpret_cast<float *>(smraw);
+  float *u3m = bb + C::BUF;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(u3m + PCfg<S, MODE>::NF * G_::U3N);
+  __shared__ ShotDev sg[2];
+  __shared__ int2 sxz[2];
+  __shared__ float red[33];
+  __shared__ int s_fail;
+  const int tid = threadIdx.x;
+  int i = blockIdx.x;
+  if (i >= n) return;
+  auto load_shot = [&](int st, int ti) {
+    const int shot = tiles[ti].shot;
+    if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
+      reinterpret_cast<int *>(&sg[st])[tid] = reinterpret_cast<const int *>(shots + shot)[tid];
+  };
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+    s_fail = 0;
+    const Tile t = tiles[i];
+    sxz[0] = make_int2(t.x0, t.z0);
+  }
+  load_shot(0, i);
+  __syncthreads();
+  uint32_t par = 0;
+  int st = 0;
+  // thread 0 issues the copies of the slot's tile; every thread waits
+  auto stage = [&](int slot) -> bool {
+    if (tid == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(bar, (uint32_t)(C::BUF * sizeof(float)));
+      issue_tile<S, MODE>(sg[slot], a, sxz[slot].x, sxz[slot].y, bb, bar);
+    }
+    const bool ok = mbar_wait(bar, par);
+    par ^= 1u;
+    return ok;
+  };
+  for (;;) {
+    const int next = i + (int)gridDim.x;
+    const bool more = next < n;
+    if (more) {  // the next tile's shot table, fetched while this one runs
+      load_shot(st ^ 1, next);
+      if (tid == 0) {
+        const Tile t = tiles[next];
+        sxz[st ^ 1] = make_int2(t.x0, t.z0);
+      }
+    }
+    if (!stage(st)) s_fail = 1;  // garbage in the buffer, indices in range
+    pad_cells<S, MODE>(sg[st], a, sxz[st].x, sxz[st].y, bb, u3m, red);
+    __syncthreads();  // the buffer, this slot's table and origin are free
+    if (s_fail) {
+      if (tid == 0) atomicExch(err, 1);
+      return;
+    }
+    if (!more) break;
+    i = next;
+    st ^= 1;
   }
 }
 
