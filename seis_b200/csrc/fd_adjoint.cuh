@@ -841,59 +841,5 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_kernel(
   if (!adj_pad_cells<S>(sg, a, t.x0, t.z0, smraw, bar, 0) && tid == 0) atomicExch(err, 2);
 }
 
-// Persistent form: CTA b of G takes the pad tiles b, b + G, ...; the next
-// tile's shot-table entry is fetched while the current tile is computed.
-template <int S>
-__global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_P) adj_pad_loop_kernel(
-    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, int n, StepArgs a,
-    int *__restrict__ err) {
-  SEIS_AGEO(S);
-  extern __shared__ __align__(128) unsigned char smraw[];
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + sizeof(float) * AG_::PAD_FLOATS);
-  __shared__ ShotDev sg[2];
-  __shared__ int2 sxz[2];
-  __shared__ int s_fail;
-  const int tid = threadIdx.x;
-  int i = blockIdx.x;
-  if (i >= n) return;
-  auto load_shot = [&](int st, int ti) {
-    const int shot = tiles[ti].shot;
-    if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
-      reinterpret_cast<int *>(&sg[st])[tid] = reinterpret_cast<const int *>(shots + shot)[tid];
-  };
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    fence_barrier_init();
-    s_fail = 0;
-    const Tile t = tiles[i];
-    sxz[0] = make_int2(t.x0, t.z0);
-  }
-  load_shot(0, i);
-  __syncthreads();
-  uint32_t par = 0;
-  int st = 0;
-  for (;;) {
-    const int next = i + (int)gridDim.x;
-    const bool more = next < n;
-    if (more) {  // the next tile's shot table, fetched while this one runs
-      load_shot(st ^ 1, next);
-      if (tid == 0) {
-        const Tile t = tiles[next];
-        sxz[st ^ 1] = make_int2(t.x0, t.z0);
-      }
-    }
-    if (!adj_pad_cells<S>(sg[st], a, sxz[st].x, sxz[st].y, smraw, bar, par)) s_fail = 1;
-    par ^= 1u;
-    __syncthreads();  // the buffers, this slot's table and origin are free
-    if (s_fail) {
-      if (tid == 0) atomicExch(err, 2);
-      return;
-    }
-    if (!more) break;
-    i = next;
-    st ^= 1;
-  }
-}
-
 }  // namespace SEIS_NS
 }  // namespace seis

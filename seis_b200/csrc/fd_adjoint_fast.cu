@@ -17,12 +17,6 @@ struct AdjLoopGrid {
 };
 template <int S>
 int AdjLoopGrid<S>::ctas = 0;
-template <int S>
-struct AdjPadLoopGrid {
-  static int ctas;
-};
-template <int S>
-int AdjPadLoopGrid<S>::ctas = 0;
 
 template <int S>
 cudaError_t setup_adjoint() {
@@ -42,13 +36,6 @@ cudaError_t setup_adjoint() {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, adj_interior_loop_kernel<S>,
                                                       Geo<S>::NT, ALCfg<S>::bytes);
   if (e == cudaSuccess) AdjLoopGrid<S>::ctas = (per > 0 ? per : 1) * nsm;
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(adj_pad_loop_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)AGeo<S>::PAD_SMEM);
-  if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, adj_pad_loop_kernel<S>, Geo<S>::NT,
-                                                      AGeo<S>::PAD_SMEM);
-  if (e == cudaSuccess) AdjPadLoopGrid<S>::ctas = (per > 0 ? per : 1) * nsm;
   return e;
 }
 
@@ -65,14 +52,9 @@ cudaError_t launch_adj(const ShotDev *d_shots, const Tile *d_tiles, int n_int, i
   } else if (n_int > 0) {
     adj_interior_kernel<S><<<n_int, NT, AGeo<S>::TILE_SMEM, s_int>>>(d_shots, d_tiles, a, d_err);
   }
-  const int GP = AdjPadLoopGrid<S>::ctas;
-  if (n_pad > 0 && (a.loop > 0 || (a.loop < 0 && n_pad >= 4 * GP))) {
-    adj_pad_loop_kernel<S><<<GP < n_pad ? GP : n_pad, NT, AGeo<S>::PAD_SMEM, s_pad>>>(
-        d_shots, d_tiles + n_int, n_pad, a, d_err);
-  } else if (n_pad > 0) {
+  if (n_pad > 0)
     adj_pad_kernel<S><<<n_pad, NT, AGeo<S>::PAD_SMEM, s_pad>>>(d_shots, d_tiles + n_int, a,
                                                                 d_err);
-  }
   return cudaGetLastError();
 }
 }  // namespace

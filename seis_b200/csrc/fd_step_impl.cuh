@@ -14,12 +14,6 @@ struct LoopGrid {
 };
 template <int S, int MODE>
 int LoopGrid<S, MODE>::ctas = 0;
-template <int S, int MODE>
-struct PadLoopGrid {
-  static int ctas;
-};
-template <int S, int MODE>
-int PadLoopGrid<S, MODE>::ctas = 0;
 
 template <int S, int MODE>
 cudaError_t setup() {
@@ -40,13 +34,6 @@ cudaError_t setup() {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, interior_loop_kernel<S, MODE>,
                                                       Geo<S>::NT, LCfg<S, MODE>::bytes);
   if (e == cudaSuccess) LoopGrid<S, MODE>::ctas = (per > 0 ? per : 1) * nsm;
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(pad_loop_kernel<S, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)PCfg<S, MODE>::bytes);
-  if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pad_loop_kernel<S, MODE>, Geo<S>::NT,
-                                                      PCfg<S, MODE>::bytes);
-  if (e == cudaSuccess) PadLoopGrid<S, MODE>::ctas = (per > 0 ? per : 1) * nsm;
   return e;
 }
 
@@ -58,10 +45,10 @@ cudaError_t setup_shape() {
   return e;
 }
 
-// Interior tiles on s_int, pad tiles on s_pad.  Each kernel is the
-// persistent one as a.loop says; by default when each of its CTAs gets at
-// least LOOP_MIN_TILES tiles (the prefetching pays, and the last round of
-// tiles is a small part of the launch); else one tile per CTA.
+// Interior tiles on s_int, pad tiles (one CTA each) on s_pad.  The interior
+// kernel is the persistent one as a.loop says; by default when each of its
+// CTAs gets at least LOOP_MIN_TILES tiles (its double buffering pays, and the
+// last round of tiles is a small part of the launch).
 constexpr int LOOP_MIN_TILES = 4;
 template <int S, int MODE>
 cudaError_t launch_t(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int n_pad,
@@ -74,14 +61,9 @@ cudaError_t launch_t(const ShotDev *d_shots, const Tile *d_tiles, int n_int, int
   } else if (n_int > 0) {
     tile_kernel<S, MODE><<<n_int, NT, TCfg<S, MODE>::bytes, s_int>>>(d_shots, d_tiles, a, d_err);
   }
-  const int GP = PadLoopGrid<S, MODE>::ctas;
-  if (n_pad > 0 && (a.loop > 0 || (a.loop < 0 && n_pad >= LOOP_MIN_TILES * GP))) {
-    pad_loop_kernel<S, MODE><<<GP < n_pad ? GP : n_pad, NT, PCfg<S, MODE>::bytes, s_pad>>>(
-        d_shots, d_tiles + n_int, n_pad, a, d_err);
-  } else if (n_pad > 0) {
+  if (n_pad > 0)
     pad_tile_kernel<S, MODE><<<n_pad, NT, PCfg<S, MODE>::bytes, s_pad>>>(d_shots, d_tiles + n_int,
                                                                        a, d_err);
-  }
   return cudaGetLastError();
 }
 

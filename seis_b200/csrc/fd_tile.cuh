@@ -986,76 +986,5 @@ __global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_tile_
   pad_cells<S, MODE>(sg, a, t.x0, t.z0, bb, u3m, red);
 }
 
-// Persistent form: CTA b of G takes the pad tiles b, b + G, ... through one
-// staging buffer; the next tile's shot-table entry is fetched while the
-// current tile is computed, and its tensor copies are issued as soon as the
-// buffer is free.
-template <int S, int MODE>
-__global__ void __launch_bounds__(Geo<S>::NT, PCfg<S, MODE>::MIN_CTAS) pad_loop_kernel(
-    const ShotDev *__restrict__ shots, const Tile *__restrict__ tiles, int n, StepArgs a,
-    int *__restrict__ err) {
-  SEIS_GEO(S);
-  using C = TCfg<S, MODE>;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  float *bb = reinterpret_cast<float *>(smraw);
-  float *u3m = bb + C::BUF;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(u3m + PCfg<S, MODE>::NF * G_::U3N);
-  __shared__ ShotDev sg[2];
-  __shared__ int2 sxz[2];
-  __shared__ float red[33];
-  __shared__ int s_fail;
-  const int tid = threadIdx.x;
-  int i = blockIdx.x;
-  if (i >= n) return;
-  auto load_shot = [&](int st, int ti) {
-    const int shot = tiles[ti].shot;
-    if (tid < (int)(sizeof(ShotDev) / sizeof(int)))
-      reinterpret_cast<int *>(&sg[st])[tid] = reinterpret_cast<const int *>(shots + shot)[tid];
-  };
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    fence_barrier_init();
-    s_fail = 0;
-    const Tile t = tiles[i];
-    sxz[0] = make_int2(t.x0, t.z0);
-  }
-  load_shot(0, i);
-  __syncthreads();
-  uint32_t par = 0;
-  int st = 0;
-  // thread 0 issues the copies of the slot's tile; every thread waits
-  auto stage = [&](int slot) -> bool {
-    if (tid == 0) {
-      fence_proxy_async();
-      mbar_expect_tx(bar, (uint32_t)(C::BUF * sizeof(float)));
-      issue_tile<S, MODE>(sg[slot], a, sxz[slot].x, sxz[slot].y, bb, bar);
-    }
-    const bool ok = mbar_wait(bar, par);
-    par ^= 1u;
-    return ok;
-  };
-  for (;;) {
-    const int next = i + (int)gridDim.x;
-    const bool more = next < n;
-    if (more) {  // the next tile's shot table, fetched while this one runs
-      load_shot(st ^ 1, next);
-      if (tid == 0) {
-        const Tile t = tiles[next];
-        sxz[st ^ 1] = make_int2(t.x0, t.z0);
-      }
-    }
-    if (!stage(st)) s_fail = 1;  // garbage in the buffer, indices in range
-    pad_cells<S, MODE>(sg[st], a, sxz[st].x, sxz[st].y, bb, u3m, red);
-    __syncthreads();  // the buffer, this slot's table and origin are free
-    if (s_fail) {
-      if (tid == 0) atomicExch(err, 1);
-      return;
-    }
-    if (!more) break;
-    i = next;
-    st ^= 1;
-  }
-}
-
 }  // namespace SEIS_NS
 }  // namespace seis
