@@ -397,30 +397,71 @@ __device__ float dcur(const ShotDev &g, const VA &V, int cx, int cz, int tx, int
 }
 
 // The part of S_cur^T M at cell (tx, tz) that comes from frame and low-order
-// consumers (cells within 3 of the grid edge) on its cross; nonzero only
+// consumers (cells within 3 of the grid edge) on its cross is nonzero only
 // within 4 of the edge.  A 2nd-order consumer reads its neighbours within one
-// cell, a frame consumer (edge row or column) those within one cell along
-// the edge and three cells along its normal extrapolation: the other
-// offsets' coefficients are zero and are skipped.
-template <class A>
-__device__ float edge_terms(const ShotDev &g, const A &M, const A &V, int tx, int tz) {
-  const int NX = g.NX, NZ = g.NZ;
-  auto low = [&](int cx, int cz) {  // a grid cell outside the 8th-order region
-    return cx >= 0 && cx < NX && cz >= 0 && cz < NZ &&
-           !(cx >= 4 && cx <= NX - 5 && cz >= 4 && cz <= NZ - 5);
-  };
-  float s = 0.0f;
-#pragma unroll 1
-  for (int m = -3; m <= 3; m++) {
-    const int cz = tz + m;
-    if ((m >= -1 && m <= 1) || cz == 0 || cz == NZ - 1)
-      if (low(tx, cz)) s = s + dcur(g, V, tx, cz, tx, tz) * M(tx, cz);
+// cell, a frame consumer (edge row or column) those within one cell along the
+// edge and three cells along its normal extrapolation, so the part is
+//   sum over m = -3..3 of c_z[m] M(tx, tz + m) + sum over m != 0 of c_x[m] M(tx + m, tz)
+// with c = dcur of the consumer (zero for the other offsets and for
+// consumers in the 8th-order region).  The coefficients depend on the
+// velocity only: this kernel forms them for every cell of the four edge
+// bands of every shot (band cell i of band b, see edge_index).
+__global__ void edge_coef_kernel(const ShotDev *__restrict__ shots, int nshots) {
+  const ShotDev &g = shots[blockIdx.y];
+  const int NX = g.NX, NZ = g.NZ, n = edge_cells(NX, NZ);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int b, cx, cz;
+  if (i < 5 * NX) {
+    b = 0; cx = i / 5; cz = i % 5;
+  } else if (i < 10 * NX) {
+    b = 1; cx = (i - 5 * NX) / 5; cz = NZ - 5 + (i - 5 * NX) % 5;
+  } else if (i < 10 * NX + 5 * NZ) {
+    b = 2; cx = (i - 10 * NX) / NZ; cz = (i - 10 * NX) % NZ;
+  } else {
+    b = 3; cx = NX - 5 + (i - 10 * NX - 5 * NZ) / NZ; cz = (i - 10 * NX - 5 * NZ) % NZ;
   }
-#pragma unroll 1
+  (void)b;
+  const GA V{g.vel, g.LDZ};
+  auto low = [&](int x, int z) {
+    return x >= 0 && x < NX && z >= 0 && z < NZ && !(x >= 4 && x <= NX - 5 && z >= 4 && z <= NZ - 5);
+  };
+  float *c = g.edge_coef + i;
+  const bool in = cx >= 0 && cx < NX && cz >= 0 && cz < NZ;
+  int k = 0;
+  for (int m = -3; m <= 3; m++, k++) {
+    const int z = cz + m;
+    float v = 0.0f;
+    if (in && ((m >= -1 && m <= 1) || z == 0 || z == NZ - 1) && low(cx, z))
+      v = dcur(g, V, cx, z, cx, cz);
+    c[(size_t)k * n] = v;
+  }
   for (int m = -3; m <= 3; m++) {
-    const int cx = tx + m;
-    if (m != 0 && ((m >= -1 && m <= 1) || cx == 0 || cx == NX - 1))
-      if (low(cx, tz)) s = s + dcur(g, V, cx, tz, tx, tz) * M(cx, tz);
+    if (m == 0) continue;
+    const int x = cx + m;
+    float v = 0.0f;
+    if (in && ((m >= -1 && m <= 1) || x == 0 || x == NX - 1) && low(x, cz))
+      v = dcur(g, V, x, cz, cx, cz);
+    c[(size_t)k * n] = v;
+    k++;
+  }
+}
+
+// The frame and low-order part at band cell (tx, tz) of band b from the
+// precomputed coefficients (z taps, then x taps, each by increasing offset)
+template <class A>
+__device__ __forceinline__ float edge_terms_pre(const ShotDev &g, const A &M, int b, int tx,
+                                                int tz) {
+  const int n = edge_cells(g.NX, g.NZ);
+  const float *c = g.edge_coef + edge_index(b, g.NX, g.NZ, tx, tz);
+  float s = 0.0f;
+#pragma unroll
+  for (int m = -3; m <= 3; m++) s = s + __ldg(c + (size_t)(m + 3) * n) * M(tx, tz + m);
+#pragma unroll
+  for (int m = -3, k = 7; m <= 3; m++) {
+    if (m == 0) continue;
+    s = s + __ldg(c + (size_t)k * n) * M(tx + m, tz);
+    k++;
   }
   return s;
 }
@@ -594,7 +635,7 @@ __device__ __forceinline__ bool adj_pad_cells(const ShotDev &g, const StepArgs &
       if (nr <= 0 || nc <= 0) continue;
       for (int i = tid; i < nr * nc; i += A_NT_I) {
         const int cx = bxa + i / nr, cz = bza + i % nr;
-        sCOR[ridx(cx, cz)] = edge_terms(g, L1, V, cx, cz);
+        sCOR[ridx(cx, cz)] = edge_terms_pre(g, L1, b, cx, cz);
       }
     }
   }

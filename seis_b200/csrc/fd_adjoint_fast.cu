@@ -68,6 +68,12 @@ cudaError_t configure_adjoint() {
   return e;
 }
 
+cudaError_t launch_edge_coef(const ShotDev *d_shots, int nshots, int max_cells, cudaStream_t s) {
+  if (nshots <= 0 || max_cells <= 0) return cudaSuccess;
+  edge_coef_kernel<<<dim3((max_cells + 255) / 256, nshots), 256, 0, s>>>(d_shots, nshots);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_adjoint(int shape, const ShotDev *d_shots, const Tile *d_tiles, int n_int,
                            int n_pad, const StepArgs &a, int *d_err, cudaStream_t s_int,
                            cudaStream_t s_pad) {

@@ -474,6 +474,7 @@ int plan_create(seis_fd_ctx *ctx, int op, int nshot, const seis_shot_desc *descs
       if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_e[0]);
       if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_e[1]);
       if (rc == SEIS_OK) rc = alloc_field(*p, g, &g.adj_b);
+      if (rc == SEIS_OK) rc = p->alloc(&g.edge_coef, (size_t)EDGE_TAPS * edge_cells(g.NX, g.NZ));
     }
     g.ntz = (g.NZ + shape_tz(p->shape) - 1) / shape_tz(p->shape);
     if (rc == SEIS_OK) {
@@ -913,8 +914,19 @@ int recompute_segment(Plan &p, int s0, int s1) {
 
 // Reverse pass of the exact adjoint: L_k for k = NT .. 0 from L_{k+1}, L_{k+2};
 // the step producing L_k images the source term of step k with mu(L_{k+1}).
+// The exact adjoint's edge-band coefficients of every shot of the plan.
+int edge_coefs(Plan &p) {
+  int most = 0;
+  for (const ShotDev &g : p.sd) most = std::max(most, edge_cells(g.NX, g.NZ));
+  CK(fast::launch_edge_coef(p.d_sd, p.nshot, most, p.ctx->stream));
+  p.ctx->launches++;
+  return SEIS_OK;
+}
+
 int run_adjoint(Plan &p) {
   seis_fd_ctx *ctx = p.ctx;
+  int rc0 = edge_coefs(p);
+  if (rc0) return rc0;
   for (const ShotDev &g : p.sd) {
     FieldGeom fg = field_geom(g.NX, g.NZ);
     for (int k = 0; k < 3; k++)
@@ -1317,6 +1329,10 @@ int time_steps(Plan &p, int steps, double *ms, double *bytes) {
     const ShotDev &g = p.sd[t.shot];
     int64_t c = (int64_t)std::min(TX, g.NX - t.x0) * std::min(TZ, g.NZ - t.z0);
     ((int)i < n_int ? cells_int : cells_pad) += c;
+  }
+  if (adj) {
+    int rc0 = edge_coefs(p);
+    if (rc0) return rc0;
   }
   StepArgs a{};
   a.nshots = p.nshot;

@@ -117,7 +117,23 @@ struct ShotDev {
   // 1/4/dz/dz, 1/pml
   float q4dx2, q4dz2, inv_pml;
   int pad3_;
+  // exact adjoint: coefficients of the transposed frame and low-order terms
+  // of the cells within 4 of the grid edge (EDGE_TAPS per cell, tap-major:
+  // tap k of band cell i at edge_coef[k * edge_cells(NX, NZ) + i]; band
+  // cells indexed by edge_index)
+  float *edge_coef;
 };
+// Cells of the four edge bands of a padded grid: the 5 top and 5 bottom rows
+// (column-major, 5 rows per column) and the 5 left and 5 right columns.
+constexpr int EDGE_TAPS = 13;  // 7 along z (offsets -3..3), 6 along x (-3..3 but 0)
+__host__ __device__ inline int edge_cells(int NX, int NZ) { return 10 * (NX + NZ); }
+// Band b (0 top, 1 bottom, 2 left, 3 right) cell (cx, cz) -> its index.
+__host__ __device__ inline int edge_index(int b, int NX, int NZ, int cx, int cz) {
+  return b == 0 ? cx * 5 + cz
+       : b == 1 ? 5 * NX + cx * 5 + (cz - (NZ - 5))
+       : b == 2 ? 10 * NX + cx * NZ + cz
+                : 10 * NX + 5 * NZ + (cx - (NX - 5)) * NZ + cz;
+}
 enum SnapType : int { SNAP_NONE = 0, SNAP_F32 = 1, SNAP_BF16 = 2, SNAP_F16 = 3 };
 static_assert(sizeof(ShotDev) % sizeof(int) == 0 && sizeof(ShotDev) <= 256 * sizeof(int),
               "ShotDev is copied word by word into shared memory");
@@ -185,6 +201,9 @@ cudaError_t launch_step(int mode, const ShotDev *d_shots, const Tile *d_tiles, i
 cudaError_t configure();
 // one reverse step of the exact Born adjoint over the adjoint tile list
 // (interior tiles on s_int, pad tiles on s_pad)
+// the exact adjoint's edge-band coefficients of every shot (after its
+// velocity is in place); max_cells = the largest edge_cells of the batch
+cudaError_t launch_edge_coef(const ShotDev *d_shots, int nshots, int max_cells, cudaStream_t s);
 cudaError_t launch_adjoint(int shape, const ShotDev *d_shots, const Tile *d_tiles, int n_int,
                            int n_pad, const StepArgs &a, int *d_err, cudaStream_t s_int,
                            cudaStream_t s_pad);
