@@ -117,6 +117,14 @@ __device__ __forceinline__ void image_store(const ShotDev &g, int x, int z, unsi
     }
 }
 
+// vz M, vx M of four consecutive cells (coef per cell, as the scalar form)
+__device__ __forceinline__ void weigh_quad(const ShotDev &g, const float4 &v, const float4 &l,
+                                           float4 &wz, float4 &wx) {
+  const Coef c0 = coef(v.x, g), c1 = coef(v.y, g), c2 = coef(v.z, g), c3 = coef(v.w, g);
+  wz = make_float4(c0.vz * l.x, c1.vz * l.y, c2.vz * l.z, c3.vz * l.w);
+  wx = make_float4(c0.vx * l.x, c1.vx * l.y, c2.vx * l.z, c3.vx * l.w);
+}
+
 // ---------------------------------------------------------------- interior
 // L_k = Lz(vz M1) + Lx(vx M1) + 2 M1 - M2 + R^T d ; grad += w lap M1.  On these
 // tiles M = L (no ring cell within one cell), so the staged arrays (named L1,
@@ -157,12 +165,14 @@ __global__ void __launch_bounds__(Geo<S>::NT, AGeo<S>::MIN_I) adj_interior_kerne
     if (tid == 0) atomicExch(err, 2);
     return;
   }
-  // weighted fields vz L1, vx L1 on the staged window
-  for (int i = tid; i < WIDE; i += A_NT_I) {
-    Coef k = coef(sV[i], g);
-    float l = sL1[i];
-    sWZ[i] = k.vz * l;
-    sWX[i] = k.vx * l;
+  // weighted fields vz L1, vx L1 on the staged window, a quad at a time
+  static_assert(WIDE % 4 == 0, "whole quads");
+  for (int i = 4 * tid; i < WIDE; i += 4 * A_NT_I) {
+    float4 wz, wx;
+    weigh_quad(g, *reinterpret_cast<const float4 *>(sV + i),
+               *reinterpret_cast<const float4 *>(sL1 + i), wz, wx);
+    *reinterpret_cast<float4 *>(sWZ + i) = wz;
+    *reinterpret_cast<float4 *>(sWX + i) = wx;
   }
   __syncthreads();
   const int zm = z0 - ZM;
@@ -291,11 +301,13 @@ __global__ void __launch_bounds__(Geo<S>::NT, ALCfg<S>::MIN_CTAS) adj_interior_l
     par ^= 1u << st;
     float *sL1 = stage0 + st * L::STAGE, *sWX = sL1 + HALO;
     const float *sL2 = sL1 + 2 * HALO;
-    for (int k = tid; k < HALO; k += A_NT_I) {  // vx M1 over the velocity, vz M1
-      const Coef c = coef(sWX[k], g);
-      const float l = sL1[k];
-      sWZ[k] = c.vz * l;
-      sWX[k] = c.vx * l;
+    static_assert(HALO % 4 == 0, "whole quads");
+    for (int k = 4 * tid; k < HALO; k += 4 * A_NT_I) {  // vx M1 over the velocity, vz M1
+      float4 wz, wx;
+      weigh_quad(g, *reinterpret_cast<const float4 *>(sWX + k),
+                 *reinterpret_cast<const float4 *>(sL1 + k), wz, wx);
+      *reinterpret_cast<float4 *>(sWZ + k) = wz;
+      *reinterpret_cast<float4 *>(sWX + k) = wx;
     }
     __syncthreads();
     const SW L1{sL1, x0 - HI, z0 - HI}, WZ{sWZ, x0 - HI, z0 - HI}, WX{sWX, x0 - HI, z0 - HI};
@@ -600,17 +612,28 @@ __device__ __forceinline__ bool adj_pad_cells(const ShotDev &g, const StepArgs &
     if (hring[h]) eh[h] = Ecur[(size_t)cx * g.LDZ + cz];
   }
   const bool ok = mbar_wait(bar, parity);
-  // vz M1, vx M1 of the 8th-order consumers (zero elsewhere)
-  for (int i = tid; i < WIDE; i += A_NT_I) {
+  // vz M1, vx M1 of the 8th-order consumers (zero elsewhere), a quad of rows
+  // at a time (SR and the window's first row are multiples of 4)
+  static_assert(SR % 4 == 0 && WIDE % 4 == 0, "whole quads");
+  for (int i = 4 * tid; i < WIDE; i += 4 * A_NT_I) {
     const int cx = x0 - HXC + i / SR, cz = z0 - ZM + i % SR;
-    float wz = 0.0f, wx = 0.0f;
-    if (cx >= 4 && cx <= NX - 5 && cz >= 4 && cz <= NZ - 5) {
-      const Coef k = coef(sV[i], g);
-      wz = k.vz * sL1[i];
-      wx = k.vx * sL1[i];
+    float4 wz = make_float4(0.f, 0.f, 0.f, 0.f), wx = wz;
+    if (cx >= 4 && cx <= NX - 5) {
+      if (cz >= 4 && cz + 3 <= NZ - 5) {
+        weigh_quad(g, *reinterpret_cast<const float4 *>(sV + i),
+                   *reinterpret_cast<const float4 *>(sL1 + i), wz, wx);
+      } else {
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+          if (cz + r >= 4 && cz + r <= NZ - 5) {
+            const Coef k = coef(sV[i + r], g);
+            set_comp(wz, r, k.vz * sL1[i + r]);
+            set_comp(wx, r, k.vx * sL1[i + r]);
+          }
+      }
     }
-    sWZ[i] = wz;
-    sWX[i] = wx;
+    *reinterpret_cast<float4 *>(sWZ + i) = wz;
+    *reinterpret_cast<float4 *>(sWX + i) = wx;
   }
   const int zm = z0 - ZM;
   const SA L1{sL1, x0 - HXC, zm}, V{sV, x0 - HXC, zm}, WZ{sWZ, x0 - HXC, zm},

@@ -916,10 +916,11 @@ int recompute_segment(Plan &p, int s0, int s1) {
 // the step producing L_k images the source term of step k with mu(L_{k+1}).
 // The exact adjoint's edge-band coefficients of every shot of the plan.
 int edge_coefs(Plan &p) {
+  seis_fd_ctx *ctx = p.ctx;
   int most = 0;
   for (const ShotDev &g : p.sd) most = std::max(most, edge_cells(g.NX, g.NZ));
-  CK(fast::launch_edge_coef(p.d_sd, p.nshot, most, p.ctx->stream));
-  p.ctx->launches++;
+  CK(fast::launch_edge_coef(p.d_sd, p.nshot, most, ctx->stream));
+  ctx->launches++;
   return SEIS_OK;
 }
 
