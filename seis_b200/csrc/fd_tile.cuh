@@ -811,26 +811,7 @@ __device__ __forceinline__ void pad_cells(const ShotDev &g, const StepArgs &a, i
     lz[k] = iz0 + k % 4;
   }
   const bool vecq = !edge || (ix >= 4 && ix + 1 <= NX - 5 && iz0 >= 4 && iz0 + 3 <= NZ - 5);
-  // a micro-tile in the 8th-order region whose every cell is a pad cell: no
-  // injection, recording or scattering source reaches it (they act on model
-  // cells), so its two-way values go to shared memory as they are (field B
-  // plus the zero source term, as below)
-  const bool pad_q = vecq && ix + 1 < NX && iz0 + 3 < NZ &&
-                     (ix + 1 < g.pml || ix >= g.pml + g.nx || iz0 + 3 < g.pml ||
-                      iz0 >= g.pml + g.nz);
-  if (pad_q) {
-    float4 o[2], cen[2], prv[2], vel[2];
-    pair_twoway(CA, PA, VV, g, ix, iz0, o, cen, prv, vel);
-#pragma unroll
-    for (int j = 0; j < 2; j++) *reinterpret_cast<float4 *>(&UA_.ref(ix + j, iz0)) = o[j];
-    if (BORN) {
-      pair_twoway(CB, PB, VV, g, ix, iz0, o, cen, prv, vel);
-#pragma unroll
-      for (int j = 0; j < 2; j++)
-        *reinterpret_cast<float4 *>(&UB_.ref(ix + j, iz0)) =
-            make_float4(o[j].x + 0.0f, o[j].y + 0.0f, o[j].z + 0.0f, o[j].w + 0.0f);
-    }
-  } else if (ix < NX && iz0 < NZ) {
+  if (ix < NX && iz0 < NZ) {
     auto quad_in = [&](int cx) { return cx < NX && iz0 + 3 < NZ; };
     auto quad_model = [&](int cx) {
       return cx >= g.pml && cx < g.pml + g.nx && iz0 >= g.pml && iz0 + 3 < g.pml + g.nz;
