@@ -319,9 +319,16 @@ def observed_data(ctx, sv):
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of one
-# launch of each step kernel, from ncu captures (profiles/); a launch's
-# traffic is this times the cells it updates.
-NCU_TRAFFIC_PER_CELL = {}
+# launch of each step kernel, from the ncu captures summarised in profiles/
+# (16 shots of the 1200 x 400 survey; Born kernels at 32 x 32 tiles, adjoint
+# kernels at 64 x 32); a launch's traffic is this times the cells it
+# updates (the captures' halo overhead is that of their tile shapes).
+NCU_TRAFFIC_PER_CELL = {
+    "born_interior": 215.0e6 / (6336 * 1024),
+    "born_pad": 141.0e6 / (3264 * 1024),
+    "adjoint_interior": 97.4e6 / (103809024 / 16),
+    "adjoint_pad": 127.2e6 / (1632 * 2048),
+}
 
 
 def kernel_roofline(ctx, sv, iter_ms, launches_per_iter):
