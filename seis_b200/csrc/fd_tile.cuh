@@ -812,10 +812,6 @@ __device__ __forceinline__ void pad_cells(const ShotDev &g, const StepArgs &a, i
   }
   const bool vecq = !edge || (ix >= 4 && ix + 1 <= NX - 5 && iz0 >= 4 && iz0 + 3 <= NZ - 5);
   if (ix < NX && iz0 < NZ) {
-    auto quad_in = [&](int cx) { return cx < NX && iz0 + 3 < NZ; };
-    auto quad_model = [&](int cx) {
-      return cx >= g.pml && cx < g.pml + g.nx && iz0 >= g.pml && iz0 + 3 < g.pml + g.nz;
-    };
     int gzq[2] = {rcv_row(ix), rcv_row(ix + 1)};
     float4 o[2], cen[2], prv[2], vel[2];
     pair_twoway(CA, PA, VV, g, ix, iz0, o, cen, prv, vel);
@@ -827,22 +823,47 @@ __device__ __forceinline__ void pad_cells(const ShotDev &g, const StepArgs &a, i
           if (ix + j < NX && iz0 + r < NZ && near_edge(ix + j, iz0 + r))
             set_comp(o[j], r, UA_(ix + j, iz0 + r));
     float4 qs[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+    // the quad's rows inside the grid and inside the model's rows (bit r =
+    // row iz0 + r), and per column the cells inside the grid (cin), the model
+    // cells (cm) and whether a source or receiver row falls in the quad
+    unsigned rin = 0u, rmod = 0u;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int iz = iz0 + r;
+      if (iz < NZ) rin |= 1u << r;
+      if (iz < NZ && iz >= g.pml && iz < g.pml + g.nz) rmod |= 1u << r;
+    }
+    unsigned cin[2], cm[2];
+    bool inj[2];
 #pragma unroll
     for (int j = 0; j < 2; j++) {
       const int cxj = ix + j;
+      const bool colm = cxj < NX && cxj >= g.pml && cxj < g.pml + g.nx;
+      cin[j] = cxj < NX ? rin : 0u;
+      cm[j] = colm ? rmod : 0u;
+      if (MODE != MODE_RCV)
+        inj[j] = aa.src_k >= 0 && g.szp >= iz0 && g.szp <= iz0 + 3 &&
+                 (g.sou ? colm : cxj == g.sxp);
+      else
+        inj[j] = aa.rec_k >= 0 && gzq[j] >= iz0 - 1 && gzq[j] <= iz0 + 3;
+    }
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const int cxj = ix + j;
+      const bool qin = cin[j] == 0xFu, qmod = cm[j] == 0xFu;
       float4 u4 = o[j];
 #pragma unroll
       for (int r = 0; r < 4; r++) {
         const int iz = iz0 + r;
-        if (cxj >= NX || iz >= NZ) continue;
-        Coef kk = coef(comp(vel[j], r), g);
-        const float u = inject<MODE>(g, aa, cxj, iz, gzq[j], comp(o[j], r), kk.vt2);
+        if (!((cin[j] >> r) & 1u)) continue;
+        float u = comp(o[j], r);
+        if (inj[j]) u = inject<MODE>(g, aa, cxj, iz, gzq[j], u, coef(comp(vel[j], r), g).vt2);
         set_comp(u4, r, u);
-        if (!quad_in(cxj)) UA_.ref(cxj, iz) = u;
-        if (!model(cxj, iz)) continue;  // pad cell: finished in part 4
+        if (!qin) UA_.ref(cxj, iz) = u;
+        if (!((cm[j] >> r) & 1u)) continue;  // pad cell: finished in part 4
         const float out = u + 0.0f;
         set_comp(o[j], r, out);
-        if (!quad_model(cxj)) out_a[(size_t)cxj * g.LDZ + iz] = out;
+        if (!qmod) out_a[(size_t)cxj * g.LDZ + iz] = out;
         if (!BORN && record && iz == gzq[j])
           g.rec[(size_t)aa.rec_k * g.nx + (cxj - g.pml)] = out;
         if (MODE != MODE_BORN && aa.strip_k >= 0) save_strips(g, aa.strip_k, cxj, iz, out);
@@ -857,12 +878,13 @@ __device__ __forceinline__ void pad_cells(const ShotDev &g, const StepArgs &a, i
           if (BORN) {
             float vv = comp(vel[j], r);
             float vel3 = 2.0f / (vv * vv * vv);
-            set_comp(qs[j], r, kk.vt2 * lap * vel3 * DV(cxj, iz));
+            const float vt2 = coef(vv, g).vt2;
+            set_comp(qs[j], r, vt2 * lap * vel3 * DV(cxj, iz));
           }
         }
       }
-      if (quad_in(cxj)) *reinterpret_cast<float4 *>(&UA_.ref(cxj, iz0)) = u4;
-      if (quad_model(cxj)) *reinterpret_cast<float4 *>(out_a + (size_t)cxj * g.LDZ + iz0) = o[j];
+      if (qin) *reinterpret_cast<float4 *>(&UA_.ref(cxj, iz0)) = u4;
+      if (qmod) *reinterpret_cast<float4 *>(out_a + (size_t)cxj * g.LDZ + iz0) = o[j];
     }
     if (BORN) {
       float4 ob[2], cb4[2], pb4[2], vb4[2];
@@ -877,22 +899,23 @@ __device__ __forceinline__ void pad_cells(const ShotDev &g, const StepArgs &a, i
 #pragma unroll
       for (int j = 0; j < 2; j++) {
         const int cxj = ix + j;
+        const bool qin = cin[j] == 0xFu, qmod = cm[j] == 0xFu;
         float4 u4 = ob[j];
 #pragma unroll
         for (int r = 0; r < 4; r++) {
           const int iz = iz0 + r;
-          if (cxj >= NX || iz >= NZ) continue;
+          if (!((cin[j] >> r) & 1u)) continue;
           const float u = comp(ob[j], r) + comp(qs[j], r);
           set_comp(u4, r, u);
-          if (!quad_in(cxj)) UB_.ref(cxj, iz) = u;
-          if (!model(cxj, iz)) continue;
+          if (!qin) UB_.ref(cxj, iz) = u;
+          if (!((cm[j] >> r) & 1u)) continue;
           const float out = u + 0.0f;
           set_comp(ob[j], r, out);
-          if (!quad_model(cxj)) nb_[(size_t)cxj * g.LDZ + iz] = out;
+          if (!qmod) nb_[(size_t)cxj * g.LDZ + iz] = out;
           if (record && iz == gzq[j]) g.rec[(size_t)aa.rec_k * g.nx + (cxj - g.pml)] = out;
         }
-        if (quad_in(cxj)) *reinterpret_cast<float4 *>(&UB_.ref(cxj, iz0)) = u4;
-        if (quad_model(cxj)) *reinterpret_cast<float4 *>(nb_ + (size_t)cxj * g.LDZ + iz0) = ob[j];
+        if (qin) *reinterpret_cast<float4 *>(&UB_.ref(cxj, iz0)) = u4;
+        if (qmod) *reinterpret_cast<float4 *>(nb_ + (size_t)cxj * g.LDZ + iz0) = ob[j];
       }
     }
   }
