@@ -750,7 +750,9 @@ __device__ __forceinline__ bool adj_pad_cells(const ShotDev &g, const StepArgs &
   for (int k = 0; k < 8; k++) {
     const int cx = ix + k / 4, cz = iz0 + k % 4;
     sLt[(cx - x0) * TZ + (cz - z0)] = Lt[k];
-    if (!(cx < NX && cz < NZ && pad_pos(g, cx, cz).ring > 0)) {
+    // a ring cell is a pad cell (outside the model), pad_pos(...).ring > 0
+    const bool pad = cx < g.pml || cx >= g.pml + g.nx || cz < g.pml || cz >= g.pml + g.nz;
+    if (!(cx < NX && cz < NZ && pad)) {
       const int q = ridx(cx, cz);
       rmask[q] = 0;
       rp0[q] = rp1[q] = rp2[q] = rp3[q] = 0.0f;
