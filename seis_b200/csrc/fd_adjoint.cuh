@@ -59,7 +59,9 @@ struct AGeo {
   static constexpr size_t TILE_SMEM = sizeof(float) * (size_t)(4 * WIDE + NARROW) + 16;
   static constexpr size_t PAD_SMEM = sizeof(float) * (size_t)PAD_FLOATS + 16;
   static constexpr int MIN_I = ctas_fit(TILE_SMEM, 768 / G::NT) > 0 ? ctas_fit(TILE_SMEM, 768 / G::NT) : 1;
-  static constexpr int MIN_P = ctas_fit(PAD_SMEM, 512 / G::NT) > 0 ? ctas_fit(PAD_SMEM, 512 / G::NT) : 1;
+  // pad tiles: up to 768 threads per SM (85 registers a thread, some spilled:
+  // the extra warps hide more of the kernel's latency than the spills cost)
+  static constexpr int MIN_P = ctas_fit(PAD_SMEM, 768 / G::NT) > 0 ? ctas_fit(PAD_SMEM, 768 / G::NT) : 1;
 };
 #define SEIS_AGEO(S)                                                        \
   SEIS_GEO(S);                                                              \
@@ -225,8 +227,9 @@ struct ALCfg {
   static constexpr int STAGE = 2 * HALO + TILE;  // M1, velocity, M2
   static constexpr size_t bytes = sizeof(float) * (2 * (size_t)STAGE + HALO) + 2 * sizeof(uint64_t);
   static constexpr size_t static_bytes = 2 * sizeof(ShotDev);
-  static constexpr int MIN_CTAS = ctas_fit(bytes + static_bytes, 768 / G::NT) > 0
-                                      ? ctas_fit(bytes + static_bytes, 768 / G::NT)
+  // at most 512 threads per SM: 128 registers a thread, no spills
+  static constexpr int MIN_CTAS = ctas_fit(bytes + static_bytes, 512 / G::NT) > 0
+                                      ? ctas_fit(bytes + static_bytes, 512 / G::NT)
                                       : 1;
   static_assert((HALO * sizeof(float)) % 128 == 0 && (TILE * sizeof(float)) % 128 == 0,
                 "tensor-copy destinations stay 128-byte aligned");
