@@ -397,8 +397,9 @@ struct PCfg {
   static constexpr int NF = MODE == MODE_BORN ? 2 : 1;  // fields with two-way arrays
   static constexpr int BUF = TCfg<S, MODE>::BUF;
   static constexpr size_t bytes = sizeof(float) * ((size_t)BUF + (size_t)NF * G::U3N) + 16;
-  // Born: at most 512 threads per SM (128 registers a thread), else 768
-  static constexpr int CAP = (MODE == MODE_BORN ? 512 : 768) / G::NT;
+  // Born: at most 512 threads per SM (128 registers a thread), else 1024
+  // (64 registers, some spilled: the extra warps pay for them)
+  static constexpr int CAP = (MODE == MODE_BORN ? 512 : 1024) / G::NT;
   static constexpr int MIN_CTAS = ctas_fit(bytes, CAP) > 0 ? ctas_fit(bytes, CAP) : 1;
 };
 
